@@ -1,0 +1,428 @@
+"""B200-native matrix-free P1 geometric multigrid with HyTeG's operator API.
+
+The classes mirror the reference's host interface (names, argument meaning and error
+behaviour) and forward to the C-ABI of libhyteg_b200.so (include/hyteg_b200.h):
+
+  PrimitiveStorage.cuboid(...)      MeshInfo::meshCuboid + SetupPrimitiveStorage
+  P1Function(name, storage, lmin, lmax)                 VertexDoFFunction.hpp:66-77
+    .interpolate / .assign / .add / .dotGlobal / .communicate
+  P1ConstantLaplaceOperator(storage, lmin, lmax)       P1ConstantOperator.hpp:165-166
+    .apply(src, dst, level, flag, updateType)           Operator.hpp:73-80
+    .smooth_sor / .smooth_gs / *_backwards              Smoothables.hpp:30-102
+  P1toP1LinearRestriction().restrict(f, srcLevel, flag)
+  P1toP1LinearProlongation().prolongate / prolongateAndAdd
+  SORSmoother(relax), CGSolver(...), GeometricMultigridSolver(...)
+
+Every computation runs on the GPU; importing the package without the built library raises.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _capi
+from ._capi import HygError, call, dptr, iptr, i64ptr
+
+# DoFType (src/hyteg/types/types.hpp:35-44)
+Inner = 1
+DirichletBoundary = 2
+NeumannBoundary = 4
+FreeslipBoundary = 8
+All = 15
+# UpdateType
+Replace = 0
+Add = 1
+# primitive kinds
+VERTEX, EDGE, FACE, CELL = 0, 1, 2, 3
+VCYCLE, WCYCLE = 0, 1
+
+
+def device_count():
+    return _capi.lib.hg_device_count()
+
+
+class HostMesh:
+    """Host-only view of a discretization: topology, reference layout, halo and stencil tables."""
+
+    def __init__(self, handle, max_level):
+        self._h = handle
+        self.max_level = max_level
+
+    @classmethod
+    def cuboid(cls, lo, hi, nx, ny, nz, max_level):
+        h = ctypes.c_void_p()
+        lo_ = np.asarray(lo, dtype=np.float64)
+        hi_ = np.asarray(hi, dtype=np.float64)
+        call("hg_mesh_create_cuboid", dptr(lo_), dptr(hi_), nx, ny, nz, max_level, ctypes.byref(h))
+        return cls(h, max_level)
+
+    @classmethod
+    def from_tets(cls, coords, tets, max_level):
+        h = ctypes.c_void_p()
+        c = np.ascontiguousarray(coords, dtype=np.float64)
+        t = np.ascontiguousarray(tets, dtype=np.int32)
+        call("hg_mesh_create_tets", len(c), dptr(c), len(t), iptr(t), max_level, ctypes.byref(h))
+        return cls(h, max_level)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _capi.lib.hg_mesh_destroy(self._h)
+            self._h = None
+
+    def counts(self):
+        c = np.zeros(4, dtype=np.int32)
+        call("hg_mesh_counts", self._h, iptr(c))
+        return tuple(int(v) for v in c)
+
+    def set_cell_coefficients(self, k):
+        k = np.ascontiguousarray(k, dtype=np.float64)
+        call("hg_mesh_set_cell_coefficients", self._h, dptr(k), len(k))
+
+    def primitive(self, kind, prim):
+        ids = np.zeros(4, dtype=np.int32)
+        xyz = np.zeros(3)
+        flag = ctypes.c_int()
+        call("hg_mesh_primitive_vertices", self._h, kind, prim, iptr(ids), dptr(xyz), ctypes.byref(flag))
+        return [int(i) for i in ids if i >= 0], xyz, flag.value
+
+    def neighbours(self, kind, prim, which):
+        ids = np.zeros(64, dtype=np.int32)
+        n = ctypes.c_int()
+        call("hg_mesh_primitive_neighbours", self._h, kind, prim, which, iptr(ids), 64, ctypes.byref(n))
+        return [int(i) for i in ids[: n.value]]
+
+    def layout(self, level, kind, prim):
+        off = ctypes.c_int64()
+        size = ctypes.c_int64()
+        call("hg_mesh_primitive_layout", self._h, level, kind, prim, ctypes.byref(off), ctypes.byref(size))
+        return off.value, size.value
+
+    def level_size(self, level):
+        n = ctypes.c_int64()
+        call("hg_mesh_level_size", self._h, level, ctypes.byref(n))
+        return n.value
+
+    def slot_info(self, level):
+        n = self.level_size(level)
+        xyz = np.zeros((n, 3))
+        owned = np.zeros(n, dtype=np.int8)
+        call("hg_mesh_slot_info", self._h, level, dptr(xyz), owned.ctypes.data_as(ctypes.POINTER(ctypes.c_byte)), n)
+        return xyz, owned
+
+    def halo_table(self, level, group):
+        n = ctypes.c_int64()
+        call("hg_mesh_halo_table", self._h, level, group, None, None, ctypes.byref(n))
+        dst = np.zeros(n.value, dtype=np.int64)
+        src = np.zeros(n.value, dtype=np.int64)
+        call("hg_mesh_halo_table", self._h, level, group, i64ptr(dst), i64ptr(src), ctypes.byref(n))
+        return dst, src
+
+    def cell_stencil(self, level, form, cell):
+        w = np.zeros(15)
+        call("hg_mesh_cell_stencil", self._h, level, form, cell, dptr(w))
+        return w
+
+    def face_stencil(self, level, form, face):
+        layer = np.zeros(32, dtype=np.int32)
+        dx = np.zeros(32, dtype=np.int32)
+        dy = np.zeros(32, dtype=np.int32)
+        w = np.zeros(32)
+        n = ctypes.c_int()
+        call("hg_mesh_face_stencil", self._h, level, form, face, iptr(layer), iptr(dx), iptr(dy), dptr(w), 32,
+             ctypes.byref(n))
+        k = n.value
+        return layer[:k].copy(), dx[:k].copy(), dy[:k].copy(), w[:k].copy()
+
+    def low_stencil(self, level, form, kind, prim):
+        rel = np.zeros(128, dtype=np.int64)
+        w = np.zeros(128)
+        n = ctypes.c_int()
+        call("hg_mesh_low_stencil", self._h, level, form, kind, prim, i64ptr(rel), dptr(w), 128, ctypes.byref(n))
+        return rel[: n.value].copy(), w[: n.value].copy()
+
+
+class PrimitiveStorage:
+    """Macro-mesh, device arena and stream of one problem (PrimitiveStorage.hpp:111-521)."""
+
+    def __init__(self, handle, max_level, mesh_args):
+        self._h = handle
+        self.max_level = max_level
+        self._mesh_args = mesh_args
+        self._host = None
+
+    @classmethod
+    def cuboid(cls, lo, hi, nx, ny, nz, max_level):
+        h = ctypes.c_void_p()
+        lo_ = np.asarray(lo, dtype=np.float64)
+        hi_ = np.asarray(hi, dtype=np.float64)
+        call("hg_storage_create_cuboid", dptr(lo_), dptr(hi_), nx, ny, nz, max_level, ctypes.byref(h))
+        return cls(h, max_level, ("cuboid", (tuple(lo), tuple(hi), nx, ny, nz)))
+
+    @classmethod
+    def from_tets(cls, coords, tets, max_level):
+        h = ctypes.c_void_p()
+        c = np.ascontiguousarray(coords, dtype=np.float64)
+        t = np.ascontiguousarray(tets, dtype=np.int32)
+        call("hg_storage_create_tets", len(c), dptr(c), len(t), iptr(t), max_level, ctypes.byref(h))
+        return cls(h, max_level, ("tets", (c, t)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _capi.lib.hg_storage_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def host(self):
+        """HostMesh of the same topology (built lazily; used for coordinates of interpolation)."""
+        if self._host is None:
+            kind, a = self._mesh_args
+            if kind == "cuboid":
+                self._host = HostMesh.cuboid(a[0], a[1], a[2], a[3], a[4], self.max_level)
+            else:
+                self._host = HostMesh.from_tets(a[0], a[1], self.max_level)
+            if getattr(self, "_k", None) is not None:
+                self._host.set_cell_coefficients(self._k)
+        return self._host
+
+    def counts(self):
+        c = np.zeros(4, dtype=np.int32)
+        call("hg_storage_counts", self._h, iptr(c))
+        return tuple(int(v) for v in c)
+
+    def set_cell_coefficients(self, k):
+        k = np.ascontiguousarray(k, dtype=np.float64)
+        call("hg_storage_set_cell_coefficients", self._h, dptr(k), len(k))
+        self._k = k
+        if self._host is not None:
+            self._host.set_cell_coefficients(k)
+
+    def set_stream(self, stream_ptr):
+        call("hg_storage_set_stream", self._h, ctypes.c_void_p(stream_ptr))
+
+    def synchronize(self):
+        call("hg_storage_synchronize", self._h)
+
+    def level_size(self, level):
+        n = ctypes.c_int64()
+        call("hg_level_size", self._h, level, ctypes.byref(n))
+        return n.value
+
+    def layout(self, level, kind, prim):
+        off = ctypes.c_int64()
+        size = ctypes.c_int64()
+        call("hg_primitive_layout", self._h, level, kind, prim, ctypes.byref(off), ctypes.byref(size))
+        return off.value, size.value
+
+
+class P1Function:
+    """P1 (vertex-DoF) function on levels [minLevel, maxLevel], FP64 or FP32 on the device."""
+
+    def __init__(self, name, storage, minLevel, maxLevel, dtype=np.float64):
+        self.name = name
+        self.storage = storage
+        self.minLevel = minLevel
+        self.maxLevel = maxLevel
+        self.dtype = np.dtype(dtype)
+        prec = {np.dtype(np.float64): 8, np.dtype(np.float32): 4}[self.dtype]
+        h = ctypes.c_int()
+        call("hg_function_create", storage.handle, minLevel, maxLevel, prec, ctypes.byref(h))
+        self.id = h.value
+
+    def __del__(self):
+        st = getattr(self, "storage", None)
+        if st is not None and st.handle:
+            _capi.lib.hg_function_destroy(st.handle, self.id)
+
+    def device_ptr(self, level):
+        p = ctypes.c_void_p()
+        call("hg_function_device_ptr", self.storage.handle, self.id, level, ctypes.byref(p))
+        return p.value
+
+    def to_numpy(self, level):
+        n = self.storage.level_size(level)
+        a = np.empty(n, dtype=self.dtype)
+        call("hg_function_download", self.storage.handle, self.id, level, a.ctypes.data_as(ctypes.c_void_p), n)
+        return a
+
+    def from_numpy(self, level, a):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        call("hg_function_upload", self.storage.handle, self.id, level, a.ctypes.data_as(ctypes.c_void_p), a.size)
+
+    def communicate(self, level):
+        call("hg_communicate", self.storage.handle, self.id, level)
+
+    def interpolate(self, value, level, flag=All):
+        """Constant (on the device) or callable f(x, y, z) evaluated at every slot's coordinates."""
+        if callable(value):
+            xyz, owned = self.storage.host().slot_info(level)
+            cur = self.to_numpy(level)
+            vals = np.asarray(value(xyz[:, 0], xyz[:, 1], xyz[:, 2]), dtype=np.float64)
+            mask = _flag_mask(self.storage, level, flag)
+            cur[mask] = vals[mask]
+            self.from_numpy(level, cur)
+        else:
+            call("hg_interpolate_const", self.storage.handle, self.id, float(value), level, flag)
+
+    def assign(self, scalars, functions, level, flag=All):
+        s = np.ascontiguousarray(scalars, dtype=np.float64)
+        f = np.ascontiguousarray([g.id for g in functions], dtype=np.int32)
+        call("hg_assign", self.storage.handle, self.id, level, flag, len(f), dptr(s), iptr(f))
+
+    def add(self, scalars, functions, level, flag=All):
+        s = np.ascontiguousarray(scalars, dtype=np.float64)
+        f = np.ascontiguousarray([g.id for g in functions], dtype=np.int32)
+        call("hg_add", self.storage.handle, self.id, level, flag, len(f), dptr(s), iptr(f))
+
+    def copy_from(self, other, level, flag=All, add=False):
+        """Copy (with precision conversion) from another function: the FP64 <-> FP32 bridge."""
+        call("hg_copy_cast", self.storage.handle, self.id, other.id, level, flag, 1 if add else 0)
+
+    def dotGlobal(self, other, level, flag=All):
+        out = ctypes.c_double()
+        call("hg_dot", self.storage.handle, self.id, other.id, level, flag, ctypes.byref(out))
+        return out.value
+
+
+def _flag_mask(storage, level, flag):
+    """Boolean mask over a level buffer: slots of primitives whose DoFType matches flag."""
+    host = storage.host()
+    n = host.level_size(level)
+    mask = np.zeros(n, dtype=bool)
+    counts = host.counts()
+    bc = {0: Inner, 1: DirichletBoundary, 2: NeumannBoundary, 3: FreeslipBoundary}
+    for kind in range(4):
+        for p in range(counts[kind]):
+            _, _, mflag = host.primitive(kind, p)
+            t = Inner if kind == CELL else bc.get(mflag, Inner)
+            if t & flag:
+                off, size = host.layout(level, kind, p)
+                mask[off:off + size] = True
+    return mask
+
+
+class _P1ConstantOperator:
+    FORM = 0
+
+    def __init__(self, storage, minLevel, maxLevel):
+        self.storage = storage
+        self.minLevel = minLevel
+        self.maxLevel = maxLevel
+        h = ctypes.c_int()
+        call("hg_operator_create", storage.handle, self.FORM, minLevel, maxLevel, ctypes.byref(h))
+        self.id = h.value
+
+    def __del__(self):
+        st = getattr(self, "storage", None)
+        if st is not None and st.handle:
+            _capi.lib.hg_operator_destroy(st.handle, self.id)
+
+    def apply(self, src, dst, level, flag, updateType=Replace):
+        if src is dst:
+            raise ValueError("apply: src and dst must be different functions")
+        call("hg_apply", self.storage.handle, self.id, src.id, dst.id, level, flag, updateType)
+
+    def residual(self, x, b, r, level, flag):
+        """r = b - A x (fused apply + assign of GeometricMultigridSolver.hpp:185-186)."""
+        call("hg_residual", self.storage.handle, self.id, x.id, b.id, r.id, level, flag)
+
+    def smooth_sor(self, dst, rhs, relax, level, flag):
+        call("hg_smooth_sor", self.storage.handle, self.id, dst.id, rhs.id, float(relax), level, flag, 0)
+
+    def smooth_sor_backwards(self, dst, rhs, relax, level, flag):
+        call("hg_smooth_sor", self.storage.handle, self.id, dst.id, rhs.id, float(relax), level, flag, 1)
+
+    def smooth_gs(self, dst, rhs, level, flag):
+        self.smooth_sor(dst, rhs, 1.0, level, flag)
+
+    def smooth_gs_backwards(self, dst, rhs, level, flag):
+        self.smooth_sor_backwards(dst, rhs, 1.0, level, flag)
+
+
+class P1ConstantLaplaceOperator(_P1ConstantOperator):
+    """-div(k grad u) with k piecewise constant per macro-cell (k = 1 unless set on the storage)."""
+    FORM = 0
+
+
+class P1ConstantMassOperator(_P1ConstantOperator):
+    FORM = 1
+
+
+class P1toP1LinearRestriction:
+    def restrict(self, function, sourceLevel, flag):
+        call("hg_restrict", function.storage.handle, function.id, sourceLevel, flag)
+
+
+class P1toP1LinearProlongation:
+    def prolongate(self, function, sourceLevel, flag):
+        call("hg_prolongate", function.storage.handle, function.id, sourceLevel, flag, 0)
+
+    def prolongateAndAdd(self, function, sourceLevel, flag):
+        call("hg_prolongate", function.storage.handle, function.id, sourceLevel, flag, 1)
+
+
+class SORSmoother:
+    def __init__(self, relax):
+        self.relax = relax
+
+    def solve(self, A, x, b, level):
+        A.smooth_sor(x, b, self.relax, level, Inner | NeumannBoundary)
+
+
+class CGSolver:
+    def __init__(self, storage, minLevel, maxLevel, maxIter=2 ** 31 - 1, tolerance=1e-16):
+        self.storage = storage
+        self.maxIter = maxIter
+        self.tolerance = tolerance
+        self.iterations = 0
+        self.residual = 0.0
+
+    def solve(self, A, x, b, level):
+        it = ctypes.c_int()
+        res = ctypes.c_double()
+        call("hg_cg_solve", self.storage.handle, A.id, x.id, b.id, level, int(min(self.maxIter, 2 ** 31 - 1)),
+             float(self.tolerance), ctypes.byref(it), ctypes.byref(res))
+        self.iterations = it.value
+        self.residual = res.value
+
+
+class GeometricMultigridSolver:
+    """GeometricMultigridSolver.hpp:42-116. The smoother must be an SORSmoother and the coarse
+    solver a CGSolver; transfers are the linear P1 restriction/prolongation."""
+
+    def __init__(self, storage, smoother, coarseSolver, restrictionOperator, prolongationOperator, minLevel, maxLevel,
+                 preSmoothSteps=3, postSmoothSteps=3, smoothIncrementOnCoarserGrids=0, cycleType=VCYCLE,
+                 A=None, dtype=np.float64):
+        if not isinstance(smoother, SORSmoother):
+            raise TypeError("The SOR-Smoother requires the SORSmoothable interface.")
+        if not isinstance(coarseSolver, CGSolver):
+            raise TypeError("coarse solver must be a CGSolver")
+        if smoothIncrementOnCoarserGrids != 0:
+            raise ValueError("smoothIncrementOnCoarserGrids != 0 is not supported")
+        self.storage = storage
+        self.args = (minLevel, maxLevel, preSmoothSteps, postSmoothSteps, float(smoother.relax), cycleType,
+                     int(min(coarseSolver.maxIter, 2 ** 31 - 1)), float(coarseSolver.tolerance),
+                     {np.dtype(np.float64): 8, np.dtype(np.float32): 4}[np.dtype(dtype)])
+        self._cache = {}
+
+    def _handle(self, A):
+        if A.id not in self._cache:
+            h = ctypes.c_int()
+            a = self.args
+            call("hg_gmg_create", self.storage.handle, A.id, a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7], a[8],
+                 ctypes.byref(h))
+            self._cache[A.id] = h.value
+        return self._cache[A.id]
+
+    def solve(self, A, x, b, level):
+        call("hg_gmg_solve", self.storage.handle, self._handle(A), x.id, b.id, level)
+
+    def __del__(self):
+        st = getattr(self, "storage", None)
+        if st is not None and st.handle:
+            for h in self._cache.values():
+                _capi.lib.hg_gmg_destroy(st.handle, h)

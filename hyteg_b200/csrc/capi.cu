@@ -1,0 +1,643 @@
+// extern "C" entry points (declared in include/hyteg_b200.h). Each call converts C++
+// exceptions into an int status and records the message for hg_last_error().
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <map>
+#include <string>
+
+#include "../../include/hyteg_b200.h"
+#include "solvers.hpp"
+#include "storage.hpp"
+
+struct hg_storage {
+  hg::Storage* s;
+};
+
+struct hg_mesh {
+  hg::Discretization* d;
+  std::map<std::pair<int, int>, hg::LevelStencils> stencils;  // (level, form)
+};
+
+#define HG_TRY try {
+#define HG_CATCH                                    \
+  }                                                 \
+  catch (const hg::Error& e) {                      \
+    hg::g_lastError = e.what();                     \
+    return e.code;                                  \
+  }                                                 \
+  catch (const std::exception& e) {                 \
+    hg::g_lastError = e.what();                     \
+    return HG_ERR_INTERNAL;                         \
+  }                                                 \
+  return HG_OK;
+
+static hg::Storage& S(hg_storage* h) {
+  hg::argCheck(h != nullptr && h->s != nullptr, "null storage handle");
+  return *h->s;
+}
+static const hg::Storage& S(const hg_storage* h) {
+  hg::argCheck(h != nullptr && h->s != nullptr, "null storage handle");
+  return *h->s;
+}
+static void levelCheck(const hg::Storage& s, int L) { hg::argCheck(L >= 0 && L <= s.maxLevel(), "level out of range"); }
+
+extern "C" {
+
+const char* hg_last_error(void) { return hg::g_lastError.c_str(); }
+
+int hg_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+static int createFrom(const hg::Topology& topo, int maxLevel, hg_storage** out) {
+  hg::argCheck(out != nullptr, "null output pointer");
+  if (hg_device_count() == 0) throw hg::Error(HG_ERR_CUDA, "no CUDA device visible");
+  hg::Topology t = topo;
+  t.setBoundaryFlags(1, 0);
+  hg_storage* h = new hg_storage();
+  try {
+    h->s = new hg::Storage(t, maxLevel);
+  } catch (...) {
+    delete h;
+    throw;
+  }
+  *out = h;
+  return HG_OK;
+}
+
+int hg_storage_create_cuboid(const double lo[3], const double hi[3], int nx, int ny, int nz, int max_level,
+                             hg_storage** out) {
+  HG_TRY
+  hg::argCheck(lo && hi, "null corner");
+  hg::argCheck(nx > 0 && ny > 0 && nz > 0, "subdivisions must be positive");
+  hg::argCheck(max_level >= 0 && max_level <= 10, "max_level out of range [0,10]");
+  for (int d = 0; d < 3; ++d) hg::argCheck(lo[d] < hi[d], "lower corner must be below upper corner");
+  return createFrom(hg::meshCuboid(lo, hi, nx, ny, nz), max_level, out);
+  HG_CATCH
+}
+
+int hg_storage_create_tets(int nverts, const double* coords, int ncells, const int* tets, int max_level,
+                           hg_storage** out) {
+  HG_TRY
+  hg::argCheck(nverts > 0 && ncells > 0 && coords && tets, "empty mesh");
+  hg::argCheck(max_level >= 0 && max_level <= 10, "max_level out of range [0,10]");
+  std::vector<std::array<double, 3>> c(nverts);
+  for (int i = 0; i < nverts; ++i) c[i] = {coords[3 * i], coords[3 * i + 1], coords[3 * i + 2]};
+  std::vector<std::array<int, 4>> t(ncells);
+  for (int i = 0; i < ncells; ++i) {
+    for (int k = 0; k < 4; ++k) {
+      hg::argCheck(tets[4 * i + k] >= 0 && tets[4 * i + k] < nverts, "tet vertex index out of range");
+      t[i][k] = tets[4 * i + k];
+    }
+  }
+  return createFrom(hg::Topology::fromTets(c, t), max_level, out);
+  HG_CATCH
+}
+
+int hg_storage_destroy(hg_storage* h) {
+  HG_TRY
+  if (!h) return HG_OK;
+  delete h->s;
+  delete h;
+  HG_CATCH
+}
+
+int hg_storage_counts(const hg_storage* h, int counts[4]) {
+  HG_TRY
+  const auto& t = S(h).disc.topo();
+  counts[0] = (int)t.verts.size();
+  counts[1] = (int)t.edges.size();
+  counts[2] = (int)t.faces.size();
+  counts[3] = (int)t.cells.size();
+  HG_CATCH
+}
+
+int hg_storage_set_stream(hg_storage* h, void* stream) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  s.stream = stream ? (cudaStream_t)stream : s.ownStream;
+  HG_CATCH
+}
+
+int hg_storage_synchronize(hg_storage* h) {
+  HG_TRY
+  hg::cudaCheck(cudaStreamSynchronize(S(h).stream), "synchronize");
+  HG_CATCH
+}
+
+int hg_storage_set_cell_coefficients(hg_storage* h, const double* k, int ncells) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  auto& cells = const_cast<hg::Topology&>(s.disc.topo()).cells;
+  hg::argCheck(k != nullptr && ncells == (int)cells.size(), "one coefficient per macro-cell required");
+  for (int i = 0; i < ncells; ++i) {
+    hg::argCheck(k[i] > 0.0, "coefficients must be positive");
+    cells[i].k = k[i];
+  }
+  HG_CATCH
+}
+
+int hg_primitive_vertices(const hg_storage* h, int kind, int prim, int ids[4], double coords[3], int* flag) {
+  HG_TRY
+  const auto& t = S(h).disc.topo();
+  for (int i = 0; i < 4; ++i) ids[i] = -1;
+  switch (kind) {
+    case HG_VERTEX:
+      hg::argCheck(prim >= 0 && prim < (int)t.verts.size(), "bad vertex");
+      ids[0] = prim;
+      for (int d = 0; d < 3; ++d) coords[d] = t.verts[prim].x[d];
+      *flag = t.verts[prim].flag;
+      break;
+    case HG_EDGE:
+      hg::argCheck(prim >= 0 && prim < (int)t.edges.size(), "bad edge");
+      for (int i = 0; i < 2; ++i) ids[i] = t.edges[prim].v[i];
+      *flag = t.edges[prim].flag;
+      break;
+    case HG_FACE:
+      hg::argCheck(prim >= 0 && prim < (int)t.faces.size(), "bad face");
+      for (int i = 0; i < 3; ++i) ids[i] = t.faces[prim].v[i];
+      *flag = t.faces[prim].flag;
+      break;
+    case HG_CELL:
+      hg::argCheck(prim >= 0 && prim < (int)t.cells.size(), "bad cell");
+      for (int i = 0; i < 4; ++i) ids[i] = t.cells[prim].v[i];
+      *flag = t.cells[prim].flag;
+      break;
+    default:
+      hg::argCheck(false, "bad kind");
+  }
+  HG_CATCH
+}
+
+int hg_primitive_neighbours(const hg_storage* h, int kind, int prim, int which, int* ids, int cap, int* count) {
+  HG_TRY
+  const auto& t = S(h).disc.topo();
+  const std::vector<int>* v = nullptr;
+  if (kind == HG_VERTEX) {
+    hg::argCheck(prim >= 0 && prim < (int)t.verts.size(), "bad vertex");
+    v = which == HG_EDGE ? &t.verts[prim].edges : which == HG_FACE ? &t.verts[prim].faces : &t.verts[prim].cells;
+  } else if (kind == HG_EDGE) {
+    hg::argCheck(prim >= 0 && prim < (int)t.edges.size(), "bad edge");
+    v = which == HG_FACE ? &t.edges[prim].faces : &t.edges[prim].cells;
+  } else if (kind == HG_FACE) {
+    hg::argCheck(prim >= 0 && prim < (int)t.faces.size(), "bad face");
+    v = &t.faces[prim].cells;
+  } else {
+    hg::argCheck(false, "cells have no higher-dimensional neighbours");
+  }
+  *count = (int)v->size();
+  for (int i = 0; i < (int)v->size() && i < cap; ++i) ids[i] = (*v)[i];
+  HG_CATCH
+}
+
+int hg_primitive_layout(const hg_storage* h, int level, int kind, int prim, int64_t* offset, int64_t* size) {
+  HG_TRY
+  const hg::Storage& s = S(h);
+  levelCheck(s, level);
+  hg::argCheck(kind >= 0 && kind <= 3, "bad kind");
+  const auto& lay = s.disc.level(level);
+  hg::argCheck(prim >= 0 && prim < (int)lay.off[kind].size(), "bad primitive index");
+  *offset = lay.off[kind][prim];
+  *size = lay.size[kind][prim];
+  HG_CATCH
+}
+
+int hg_level_size(const hg_storage* h, int level, int64_t* n) {
+  HG_TRY
+  const hg::Storage& s = S(h);
+  levelCheck(s, level);
+  *n = s.disc.level(level).total;
+  HG_CATCH
+}
+
+int hg_function_create(hg_storage* h, int min_level, int max_level, int precision, int* fn) {
+  HG_TRY
+  hg::argCheck(fn != nullptr, "null output");
+  *fn = S(h).createFunction(min_level, max_level, precision);
+  HG_CATCH
+}
+
+int hg_function_destroy(hg_storage* h, int fn) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  s.fn(fn);
+  s.fns.erase(fn);
+  HG_CATCH
+}
+
+int hg_function_device_ptr(hg_storage* h, int fn, int level, void** ptr) {
+  HG_TRY
+  *ptr = S(h).data(fn, level);
+  HG_CATCH
+}
+
+int hg_function_upload(hg_storage* h, int fn, int level, const void* host, int64_t n) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  hg::Function& f = s.fn(fn);
+  hg::argCheck(n == s.disc.level(level).total, "upload size must equal the level buffer size");
+  hg::cudaCheck(cudaMemcpyAsync(s.data(fn, level), host, (size_t)n * f.prec, cudaMemcpyHostToDevice, s.stream), "upload");
+  hg::cudaCheck(cudaStreamSynchronize(s.stream), "upload sync");
+  HG_CATCH
+}
+
+int hg_function_download(hg_storage* h, int fn, int level, void* host, int64_t n) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  hg::Function& f = s.fn(fn);
+  hg::argCheck(n == s.disc.level(level).total, "download size must equal the level buffer size");
+  hg::cudaCheck(cudaMemcpyAsync(host, s.data(fn, level), (size_t)n * f.prec, cudaMemcpyDeviceToHost, s.stream), "download");
+  hg::cudaCheck(cudaStreamSynchronize(s.stream), "download sync");
+  HG_CATCH
+}
+
+int hg_communicate(hg_storage* h, int fn, int level) {
+  HG_TRY
+  S(h).communicate(fn, level, (1 << hg::G_COUNT) - 1);
+  HG_CATCH
+}
+
+int hg_interpolate_const(hg_storage* h, int fn, double value, int level, unsigned flag) {
+  HG_TRY
+  S(h).lincomb(fn, level, flag, 0, nullptr, nullptr, false, value);
+  HG_CATCH
+}
+
+int hg_assign(hg_storage* h, int dst, int level, unsigned flag, int n, const double* scalars, const int* srcs) {
+  HG_TRY
+  S(h).lincomb(dst, level, flag, n, scalars, srcs, false, 0.0);
+  HG_CATCH
+}
+
+int hg_add(hg_storage* h, int dst, int level, unsigned flag, int n, const double* scalars, const int* srcs) {
+  HG_TRY
+  S(h).lincomb(dst, level, flag, n, scalars, srcs, true, 0.0);
+  HG_CATCH
+}
+
+int hg_copy_cast(hg_storage* h, int dst, int src, int level, unsigned flag, int add) {
+  HG_TRY
+  S(h).copyCast(dst, src, level, flag, add != 0);
+  HG_CATCH
+}
+
+int hg_dot(hg_storage* h, int a, int b, int level, unsigned flag, double* out) {
+  HG_TRY
+  *out = S(h).dot(a, b, level, flag);
+  HG_CATCH
+}
+
+int hg_operator_create(hg_storage* h, int form, int min_level, int max_level, int* op) {
+  HG_TRY
+  *op = S(h).createOperator(form, min_level, max_level);
+  HG_CATCH
+}
+
+int hg_operator_destroy(hg_storage* h, int op) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  s.op(op);
+  hg::argCheck(op != s.structureOp, "internal operator");
+  s.ops.erase(op);
+  HG_CATCH
+}
+
+int hg_apply(hg_storage* h, int op, int src, int dst, int level, unsigned flag, int update) {
+  HG_TRY
+  hg::argCheck(update == 0 || update == 1, "update must be 0 (Replace) or 1 (Add)");
+  S(h).apply(op, src, dst, level, flag, update);
+  HG_CATCH
+}
+
+int hg_residual(hg_storage* h, int op, int x, int b, int r, int level, unsigned flag) {
+  HG_TRY
+  S(h).residual(op, x, b, r, level, flag);
+  HG_CATCH
+}
+
+int hg_smooth_sor(hg_storage* h, int op, int dst, int rhs, double omega, int level, unsigned flag, int backwards) {
+  HG_TRY
+  hg::argCheck(omega > 0.0 && omega < 2.0, "relaxation must lie in (0, 2)");
+  S(h).smoothSor(op, dst, rhs, omega, level, flag, backwards != 0);
+  HG_CATCH
+}
+
+int hg_restrict(hg_storage* h, int fn, int src_level, unsigned flag) {
+  HG_TRY
+  S(h).restrictFn(fn, src_level, flag);
+  HG_CATCH
+}
+
+int hg_prolongate(hg_storage* h, int fn, int src_level, unsigned flag, int add) {
+  HG_TRY
+  S(h).prolongate(fn, src_level, flag, add != 0);
+  HG_CATCH
+}
+
+int hg_cg_solve(hg_storage* h, int op, int x, int b, int level, int max_iter, double tol, int* iterations,
+                double* final_residual) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  const int prec = s.fn(x).prec;
+  const int p = s.createFunction(level, level, prec), z = s.createFunction(level, level, prec),
+            ap = s.createFunction(level, level, prec), r = s.createFunction(level, level, prec);
+  int it = 0;
+  double res = 0;
+  try {
+    it = hg::cgSolve(s, op, x, b, level, max_iter, tol, p, z, ap, r, &res);
+  } catch (...) {
+    for (int id : {p, z, ap, r}) s.fns.erase(id);
+    throw;
+  }
+  for (int id : {p, z, ap, r}) s.fns.erase(id);
+  if (iterations) *iterations = it;
+  if (final_residual) *final_residual = res;
+  HG_CATCH
+}
+
+int hg_gmg_create(hg_storage* h, int op, int min_level, int max_level, int pre_smooth, int post_smooth, double omega,
+                  int cycle_type, int coarse_max_iter, double coarse_tol, int precision, int* gmg) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  s.op(op);
+  hg::argCheck(min_level >= 0 && max_level <= s.maxLevel() && min_level <= max_level, "invalid level range");
+  hg::argCheck(pre_smooth >= 0 && post_smooth >= 0, "negative smoothing steps");
+  hg::argCheck(cycle_type == 0 || cycle_type == 1, "cycle type must be 0 (V) or 1 (W)");
+  hg::argCheck(omega > 0.0 && omega < 2.0, "relaxation must lie in (0, 2)");
+  std::unique_ptr<hg::Gmg> g(new hg::Gmg(s, op, min_level, max_level, pre_smooth, post_smooth, omega, cycle_type,
+                                         coarse_max_iter, coarse_tol, precision));
+  const int id = s.nextId++;
+  s.gmgs[id] = std::move(g);
+  *gmg = id;
+  HG_CATCH
+}
+
+int hg_gmg_destroy(hg_storage* h, int gmg) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  hg::argCheck(s.gmgs.count(gmg) == 1, "unknown multigrid handle");
+  s.gmgs.erase(gmg);
+  HG_CATCH
+}
+
+int hg_gmg_solve(hg_storage* h, int gmg, int x, int b, int level) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  auto it = s.gmgs.find(gmg);
+  hg::argCheck(it != s.gmgs.end(), "unknown multigrid handle");
+  it->second->solve(x, b, level);
+  HG_CATCH
+}
+
+// ---------------------------------------------------------------------------------------
+// host-only mesh view
+// ---------------------------------------------------------------------------------------
+static hg_mesh* M(const hg_mesh* m) {
+  hg::argCheck(m != nullptr && m->d != nullptr, "null mesh handle");
+  return const_cast<hg_mesh*>(m);
+}
+static const hg::LevelStencils& meshStencil(const hg_mesh* mc, int level, int form) {
+  hg_mesh* m = const_cast<hg_mesh*>(mc);
+  hg::argCheck(level >= 0 && level <= m->d->maxLevel(), "level out of range");
+  hg::argCheck(form == 0 || form == 1, "unknown form");
+  auto key = std::make_pair(level, form);
+  auto it = m->stencils.find(key);
+  if (it == m->stencils.end()) it = m->stencils.emplace(key, hg::assembleStencils(*m->d, level, (hg::FormKind)form)).first;
+  return it->second;
+}
+
+static int meshFrom(const hg::Topology& topo, int maxLevel, hg_mesh** out) {
+  hg::argCheck(out != nullptr, "null output pointer");
+  hg::Topology t = topo;
+  t.setBoundaryFlags(1, 0);
+  hg_mesh* m = new hg_mesh();
+  try {
+    m->d = new hg::Discretization(t, maxLevel);
+  } catch (...) {
+    delete m;
+    throw;
+  }
+  *out = m;
+  return HG_OK;
+}
+
+int hg_mesh_create_cuboid(const double lo[3], const double hi[3], int nx, int ny, int nz, int max_level, hg_mesh** out) {
+  HG_TRY
+  hg::argCheck(lo && hi, "null corner");
+  hg::argCheck(nx > 0 && ny > 0 && nz > 0, "subdivisions must be positive");
+  hg::argCheck(max_level >= 0 && max_level <= 10, "max_level out of range [0,10]");
+  for (int d = 0; d < 3; ++d) hg::argCheck(lo[d] < hi[d], "lower corner must be below upper corner");
+  return meshFrom(hg::meshCuboid(lo, hi, nx, ny, nz), max_level, out);
+  HG_CATCH
+}
+
+int hg_mesh_create_tets(int nverts, const double* coords, int ncells, const int* tets, int max_level, hg_mesh** out) {
+  HG_TRY
+  hg::argCheck(nverts > 0 && ncells > 0 && coords && tets, "empty mesh");
+  hg::argCheck(max_level >= 0 && max_level <= 10, "max_level out of range [0,10]");
+  std::vector<std::array<double, 3>> c(nverts);
+  for (int i = 0; i < nverts; ++i) c[i] = {coords[3 * i], coords[3 * i + 1], coords[3 * i + 2]};
+  std::vector<std::array<int, 4>> t(ncells);
+  for (int i = 0; i < ncells; ++i)
+    for (int k = 0; k < 4; ++k) {
+      hg::argCheck(tets[4 * i + k] >= 0 && tets[4 * i + k] < nverts, "tet vertex index out of range");
+      t[i][k] = tets[4 * i + k];
+    }
+  return meshFrom(hg::Topology::fromTets(c, t), max_level, out);
+  HG_CATCH
+}
+
+int hg_mesh_destroy(hg_mesh* m) {
+  HG_TRY
+  if (!m) return HG_OK;
+  delete m->d;
+  delete m;
+  HG_CATCH
+}
+
+int hg_mesh_counts(const hg_mesh* m, int counts[4]) {
+  HG_TRY
+  const auto& t = M(m)->d->topo();
+  counts[0] = (int)t.verts.size();
+  counts[1] = (int)t.edges.size();
+  counts[2] = (int)t.faces.size();
+  counts[3] = (int)t.cells.size();
+  HG_CATCH
+}
+
+int hg_mesh_set_cell_coefficients(hg_mesh* m, const double* k, int ncells) {
+  HG_TRY
+  auto& cells = const_cast<hg::Topology&>(M(m)->d->topo()).cells;
+  hg::argCheck(k != nullptr && ncells == (int)cells.size(), "one coefficient per macro-cell required");
+  for (int i = 0; i < ncells; ++i) {
+    hg::argCheck(k[i] > 0.0, "coefficients must be positive");
+    cells[i].k = k[i];
+  }
+  m->stencils.clear();
+  HG_CATCH
+}
+
+int hg_mesh_primitive_vertices(const hg_mesh* m, int kind, int prim, int ids[4], double coords[3], int* flag) {
+  HG_TRY
+  const auto& t = M(m)->d->topo();
+  for (int i = 0; i < 4; ++i) ids[i] = -1;
+  switch (kind) {
+    case HG_VERTEX:
+      hg::argCheck(prim >= 0 && prim < (int)t.verts.size(), "bad vertex");
+      ids[0] = prim;
+      for (int d = 0; d < 3; ++d) coords[d] = t.verts[prim].x[d];
+      *flag = t.verts[prim].flag;
+      break;
+    case HG_EDGE:
+      hg::argCheck(prim >= 0 && prim < (int)t.edges.size(), "bad edge");
+      for (int i = 0; i < 2; ++i) ids[i] = t.edges[prim].v[i];
+      *flag = t.edges[prim].flag;
+      break;
+    case HG_FACE:
+      hg::argCheck(prim >= 0 && prim < (int)t.faces.size(), "bad face");
+      for (int i = 0; i < 3; ++i) ids[i] = t.faces[prim].v[i];
+      *flag = t.faces[prim].flag;
+      break;
+    case HG_CELL:
+      hg::argCheck(prim >= 0 && prim < (int)t.cells.size(), "bad cell");
+      for (int i = 0; i < 4; ++i) ids[i] = t.cells[prim].v[i];
+      *flag = t.cells[prim].flag;
+      break;
+    default:
+      hg::argCheck(false, "bad kind");
+  }
+  HG_CATCH
+}
+
+int hg_mesh_primitive_neighbours(const hg_mesh* m, int kind, int prim, int which, int* ids, int cap, int* count) {
+  HG_TRY
+  const auto& t = M(m)->d->topo();
+  const std::vector<int>* v = nullptr;
+  if (kind == HG_VERTEX) {
+    hg::argCheck(prim >= 0 && prim < (int)t.verts.size(), "bad vertex");
+    v = which == HG_EDGE ? &t.verts[prim].edges : which == HG_FACE ? &t.verts[prim].faces : &t.verts[prim].cells;
+  } else if (kind == HG_EDGE) {
+    hg::argCheck(prim >= 0 && prim < (int)t.edges.size(), "bad edge");
+    v = which == HG_FACE ? &t.edges[prim].faces : &t.edges[prim].cells;
+  } else if (kind == HG_FACE) {
+    hg::argCheck(prim >= 0 && prim < (int)t.faces.size(), "bad face");
+    v = &t.faces[prim].cells;
+  } else {
+    hg::argCheck(false, "cells have no higher-dimensional neighbours");
+  }
+  *count = (int)v->size();
+  for (int i = 0; i < (int)v->size() && i < cap; ++i) ids[i] = (*v)[i];
+  HG_CATCH
+}
+
+int hg_mesh_primitive_layout(const hg_mesh* m, int level, int kind, int prim, int64_t* offset, int64_t* size) {
+  HG_TRY
+  const hg::Discretization& d = *M(m)->d;
+  hg::argCheck(level >= 0 && level <= d.maxLevel(), "level out of range");
+  hg::argCheck(kind >= 0 && kind <= 3, "bad kind");
+  const auto& lay = d.level(level);
+  hg::argCheck(prim >= 0 && prim < (int)lay.off[kind].size(), "bad primitive index");
+  *offset = lay.off[kind][prim];
+  *size = lay.size[kind][prim];
+  HG_CATCH
+}
+
+int hg_mesh_level_size(const hg_mesh* m, int level, int64_t* n) {
+  HG_TRY
+  const hg::Discretization& d = *M(m)->d;
+  hg::argCheck(level >= 0 && level <= d.maxLevel(), "level out of range");
+  *n = d.level(level).total;
+  HG_CATCH
+}
+
+int hg_mesh_slot_info(const hg_mesh* m, int level, double* xyz, signed char* owned, int64_t n) {
+  HG_TRY
+  const hg::Discretization& d = *M(m)->d;
+  hg::argCheck(level >= 0 && level <= d.maxLevel(), "level out of range");
+  const auto& lay = d.level(level);
+  hg::argCheck(n == lay.total, "buffer size must equal the level size");
+  const auto& topo = d.topo();
+  const double N = (double)lay.N;
+  for (int64_t i = 0; i < n; ++i) owned[i] = -1;
+  for (int64_t i = 0; i < 3 * n; ++i) xyz[i] = 0.0;
+  for (int kind = 0; kind < 4; ++kind)
+    for (size_t p = 0; p < lay.off[kind].size(); ++p)
+      for (int64_t s = 0; s < lay.size[kind][p]; ++s) {
+        const hg::Bary b = d.slotBary(level, kind, (int)p, s);
+        const int64_t g = lay.off[kind][p] + s;
+        for (int k = 0; k < 3; ++k) {
+          double v = 0.0;
+          for (int i = 0; i < b.n; ++i) v += (double)b.b[i] * topo.verts[b.v[i]].x[k];
+          xyz[3 * g + k] = v / N;
+        }
+        const hg::Slot o = d.owner(level, b);
+        owned[g] = (o.kind == kind && o.prim == (int)p && o.local == s) ? 1 : 0;
+      }
+  HG_CATCH
+}
+
+int hg_mesh_halo_table(const hg_mesh* m, int level, int group, int64_t* dst, int64_t* src, int64_t* n) {
+  HG_TRY
+  const hg::Discretization& d = *M(m)->d;
+  hg::argCheck(level >= 0 && level <= d.maxLevel(), "level out of range");
+  hg::argCheck(group >= 0 && group < hg::G_COUNT, "bad halo group");
+  const auto& lay = d.level(level);
+  const int64_t cnt = (int64_t)lay.commDst[group].size();
+  if (dst && src) {
+    hg::argCheck(*n >= cnt, "output too small");
+    std::memcpy(dst, lay.commDst[group].data(), cnt * sizeof(int64_t));
+    std::memcpy(src, lay.commSrc[group].data(), cnt * sizeof(int64_t));
+  }
+  *n = cnt;
+  HG_CATCH
+}
+
+int hg_mesh_cell_stencil(const hg_mesh* m, int level, int form, int cell, double w[15]) {
+  HG_TRY
+  const auto& st = meshStencil(M(m), level, form);
+  hg::argCheck(cell >= 0 && cell < (int)st.cell.size(), "bad cell");
+  for (int k = 0; k < 15; ++k) w[k] = st.cell[cell][k];
+  HG_CATCH
+}
+
+int hg_mesh_face_stencil(const hg_mesh* m, int level, int form, int face, int* layer, int* dx, int* dy, double* w,
+                         int cap, int* n) {
+  HG_TRY
+  const auto& st = meshStencil(M(m), level, form);
+  hg::argCheck(face >= 0 && face < (int)st.face.size(), "bad face");
+  const auto& e = st.face[face];
+  *n = (int)e.size();
+  hg::argCheck(cap >= (int)e.size(), "output too small");
+  for (size_t k = 0; k < e.size(); ++k) {
+    layer[k] = e[k].layer;
+    dx[k] = e[k].dx;
+    dy[k] = e[k].dy;
+    w[k] = e[k].w;
+  }
+  HG_CATCH
+}
+
+int hg_mesh_low_stencil(const hg_mesh* m, int level, int form, int kind, int prim, int64_t* rel, double* w, int cap,
+                        int* n) {
+  HG_TRY
+  const auto& st = meshStencil(M(m), level, form);
+  hg::argCheck(kind == HG_EDGE || kind == HG_VERTEX, "kind must be edge or vertex");
+  const auto& v = kind == HG_EDGE ? st.edge : st.vert;
+  hg::argCheck(prim >= 0 && prim < (int)v.size(), "bad primitive");
+  const auto& e = v[prim];
+  *n = (int)e.size();
+  hg::argCheck(cap >= (int)e.size(), "output too small");
+  for (size_t k = 0; k < e.size(); ++k) {
+    rel[k] = e[k].rel;
+    w[k] = e[k].w;
+  }
+  HG_CATCH
+}
+
+}  // extern "C"

@@ -1,0 +1,98 @@
+// CG and geometric multigrid drivers on top of the device kernels (host orchestration; all
+// vector work stays on the device, only convergence scalars are read back).
+#include <cmath>
+
+#include "../../include/hyteg_b200.h"
+#include "solvers.hpp"
+#include "storage.hpp"
+
+namespace hg {
+
+// CGSolver::solve (src/hyteg/solvers/CGSolver.hpp:69-150) with the identity preconditioner
+// (solvers/preconditioners/IdentityPreconditioner.hpp:39-45): z = r.
+int cgSolve(Storage& s, int op, int x, int b, int L, int maxIter, double tol, int p, int z, int ap, int r,
+            double* finalRes) {
+  const unsigned flag = HG_INNER | HG_NEUMANN | HG_FREESLIP;
+  const double one = 1.0;
+  if (finalRes) *finalRes = 0.0;
+  if (maxIter == 0) return 0;
+  s.apply(op, x, p, L, flag, 0);
+  {
+    const double sc[2] = {1.0, -1.0};
+    const int src[2] = {b, p};
+    s.lincomb(r, L, flag, 2, sc, src, false, 0.0);
+  }
+  s.lincomb(z, L, flag, 1, &one, &r, false, 0.0);
+  s.lincomb(p, L, flag, 1, &one, &z, false, 0.0);
+  double prsold = s.dot(r, z, L, flag);
+  const double resStart = std::sqrt(s.dot(r, r, L, flag));
+  if (finalRes) *finalRes = resStart;
+  if (resStart < tol) return 0;
+  int it = 0;
+  for (int i = 0; i < maxIter; ++i) {
+    it = i + 1;
+    s.apply(op, p, ap, L, flag, 0);
+    const double pAp = s.dot(p, ap, L, flag);
+    const double alpha = prsold / pAp;
+    s.lincomb(x, L, flag, 1, &alpha, &p, true, 0.0);
+    const double malpha = -alpha;
+    s.lincomb(r, L, flag, 1, &malpha, &ap, true, 0.0);
+    const double rsnew = s.dot(r, r, L, flag);
+    const double sq = std::sqrt(rsnew);
+    if (finalRes) *finalRes = sq;
+    if (sq < tol) break;
+    s.lincomb(z, L, flag, 1, &one, &r, false, 0.0);
+    const double prsnew = s.dot(r, z, L, flag);
+    const double beta = prsnew / prsold;
+    const double sc[2] = {1.0, beta};
+    const int src[2] = {z, p};
+    s.lincomb(p, L, flag, 2, sc, src, false, 0.0);
+    prsold = prsnew;
+  }
+  return it;
+}
+
+Gmg::Gmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int post_, double omega_, int cycle_, int cmax,
+         double ctol, int prec_)
+    : s(st), op(op_), minL(minL_), maxL(maxL_), pre(pre_), post(post_), omega(omega_), cycle(cycle_),
+      coarseMaxIter(cmax), coarseTol(ctol), prec(prec_) {
+  tmp = s.createFunction(minL, maxL, prec);
+  cp = s.createFunction(minL, minL, prec);
+  cz = s.createFunction(minL, minL, prec);
+  cap = s.createFunction(minL, minL, prec);
+  cr = s.createFunction(minL, minL, prec);
+}
+
+Gmg::~Gmg() {
+  for (int id : {tmp, cp, cz, cap, cr}) s.fns.erase(id);
+}
+
+// GeometricMultigridSolver::solveRecursively (src/hyteg/solvers/GeometricMultigridSolver.hpp:136-235)
+void Gmg::solveRecursively(int x, int b, int L) {
+  const unsigned flag = HG_INNER | HG_NEUMANN;
+  if (L == minL) {
+    cgSolve(s, op, x, b, L, coarseMaxIter, coarseTol, cp, cz, cap, cr, nullptr);
+    return;
+  }
+  for (int i = 0; i < pre; ++i) s.smoothSor(op, x, b, omega, L, flag, false);
+  s.residual(op, x, b, tmp, L, flag);
+  s.restrictFn(tmp, L, flag);
+  const double one = 1.0;
+  s.lincomb(b, L - 1, flag, 1, &one, &tmp, false, 0.0);
+  s.lincomb(x, L - 1, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+  solveRecursively(x, b, L - 1);
+  if (cycle == 1) solveRecursively(x, b, L - 1);
+  s.prolongate(x, L - 1, flag, true);
+  for (int i = 0; i < post; ++i) s.smoothSor(op, x, b, omega, L, flag, false);
+}
+
+void Gmg::solve(int x, int b, int L) {
+  argCheck(L >= minL && L <= maxL, "gmg: level outside the solver's range");
+  Function& fx = s.fn(x);
+  Function& fb = s.fn(b);
+  argCheck(fx.prec == prec && fb.prec == prec, "gmg: function precision differs from the solver's");
+  argCheck(fx.minL <= minL && fb.minL <= minL && fx.maxL >= L && fb.maxL >= L, "gmg: functions must span the level range");
+  solveRecursively(x, b, L);
+}
+
+}  // namespace hg

@@ -1,0 +1,577 @@
+// hg_storage: device arena, per-level work tables, operators, solvers and the C-ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/hyteg_b200.h"
+#include "discretization.hpp"
+#include "kernels.cuh"
+#include "solvers.hpp"
+#include "storage.hpp"
+
+namespace hg {
+
+thread_local std::string g_lastError;
+static const int kAllGroups = (1 << G_COUNT) - 1;
+
+void cudaCheck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    if (e == cudaErrorMemoryAllocation) {
+      (void)cudaGetLastError();
+      throw Error(HG_ERR_OOM, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    throw Error(HG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+void argCheck(bool ok, const std::string& msg) {
+  if (!ok) throw Error(HG_ERR_ARG, msg);
+}
+
+DevBuf::~DevBuf() {
+  if (p) cudaFree(p);
+}
+void* DevBuf::alloc(size_t n) {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = n;
+  if (n) cudaCheck(cudaMalloc(&p, n), "cudaMalloc");
+  return p;
+}
+
+template <class V>
+static void* upload(std::vector<std::unique_ptr<DevBuf>>& keep, const std::vector<V>& h, cudaStream_t st) {
+  keep.emplace_back(new DevBuf());
+  void* d = keep.back()->alloc(std::max<size_t>(h.size(), 1) * sizeof(V));
+  if (!h.empty()) cudaCheck(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, st), "upload");
+  return d;
+}
+
+static unsigned char dofType(int meshFlag) {
+  // BoundaryCondition::create0123BC (src/hyteg/boundary/BoundaryConditions.cpp:26-33)
+  switch (meshFlag) {
+    case 1: return HG_DIRICHLET;
+    case 2: return HG_NEUMANN;
+    case 3: return HG_FREESLIP;
+    default: return HG_INNER;
+  }
+}
+
+Storage::Storage(const Topology& topo, int maxLevel) : disc(topo, maxLevel) {
+  cudaCheck(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "cudaStreamCreate");
+  stream = ownStream;
+  levels.resize(maxLevel + 1);
+  for (int L = 0; L <= maxLevel; ++L) buildLevel(L);
+  scalars.alloc(64 * sizeof(double));
+  cudaCheck(cudaMemsetAsync(scalars.p, 0, 64 * sizeof(double), stream), "memset");
+  cudaCheck(cudaStreamSynchronize(stream), "sync");
+}
+
+Storage::~Storage() {
+  gmgs.clear();
+  ops.clear();
+  fns.clear();
+  levels.clear();
+  if (ownStream) cudaStreamDestroy(ownStream);
+}
+
+void Storage::buildLevel(int L) {
+  const Topology& topo = disc.topo();
+  const LevelLayout& lay = disc.level(L);
+  LevelData& ld = levels[L];
+  ld.lay = &lay;
+  dev::LevelDev& lv = ld.lv;
+  lv.L = L;
+  lv.N = (int)lay.N;
+  lv.w = (int)lay.w;
+  lv.nCells = (int)topo.cells.size();
+  lv.nFaces = (int)topo.faces.size();
+  lv.nEdges = (int)topo.edges.size();
+  lv.nLow = (int)(topo.edges.size() + topo.verts.size());
+  const int64_t N = lay.N, w = lay.w;
+  argCheck(lay.total < (int64_t(1) << 32), "level buffer exceeds 32-bit halo indices");
+
+  std::vector<int64_t> lowOff;
+  std::vector<int> lowFirst, lowCount;
+  std::vector<unsigned char> cellType, faceType, lowType;
+  for (auto& c : topo.cells) cellType.push_back(dofType(c.flag));
+  for (auto& f : topo.faces) faceType.push_back(dofType(f.flag));
+  for (size_t e = 0; e < topo.edges.size(); ++e) {
+    lowOff.push_back(lay.off[KE][e]);
+    lowFirst.push_back(1);
+    lowCount.push_back((int)std::max<int64_t>(N - 1, 0));
+    lowType.push_back(dofType(topo.edges[e].flag));
+  }
+  for (size_t v = 0; v < topo.verts.size(); ++v) {
+    lowOff.push_back(lay.off[KV][v]);
+    lowFirst.push_back(0);
+    lowCount.push_back(1);
+    lowType.push_back(dofType(topo.verts[v].flag));
+  }
+  ld.hostCellType = cellType;
+  ld.hostFaceType = faceType;
+  ld.hostLowType = lowType;
+
+  std::vector<dev::CellBlock> cb;
+  if (N >= 4)
+    for (int c = 0; c < lv.nCells; ++c)
+      for (int z = 1; z <= N - 3; ++z) {
+        const int W = (int)(w - z);
+        const int a = W + 1 - 1;                                   // rowStart(W, 1)
+        const int e = (W - 2) * (W + 1) - ((W - 2) * (W - 1)) / 2;  // rowStart(W, W-2)
+        for (int s = a; s < e; s += dev::kBlock) cb.push_back({c, z, s, 0});
+      }
+  std::vector<dev::FaceBlock> fb;
+  if (N >= 3)
+    for (int f = 0; f < lv.nFaces; ++f) {
+      const int W = (int)w;
+      const int a = W, e = (W - 2) * (W + 1) - ((W - 2) * (W - 1)) / 2;
+      for (int s = a; s < e; s += dev::kBlock) fb.push_back({f, s});
+    }
+  std::vector<dev::LowBlock> lb;
+  for (int p = 0; p < lv.nLow; ++p) {
+    if (p == lv.nEdges) lv.nLowEdgeBlocks = (int)lb.size();
+    for (int s = lowFirst[p]; s < lowFirst[p] + lowCount[p]; s += dev::kBlock) lb.push_back({p, s});
+  }
+  if (lv.nEdges == lv.nLow) lv.nLowEdgeBlocks = (int)lb.size();
+
+  std::vector<dev::Chunk> chunks;
+  auto addChunks = [&](int64_t off, int64_t size, int type) {
+    for (int64_t s = 0; s < size; s += 8192) chunks.push_back({off + s, (int)std::min<int64_t>(8192, size - s), type});
+  };
+  for (int c = 0; c < lv.nCells; ++c) addChunks(lay.off[KC][c], lay.size[KC][c], cellType[c]);
+  for (int f = 0; f < lv.nFaces; ++f) addChunks(lay.off[KF][f], lay.size[KF][f], faceType[f]);
+  for (int e = 0; e < lv.nEdges; ++e) addChunks(lay.off[KE][e], lay.size[KE][e], lowType[e]);
+  for (size_t v = 0; v < topo.verts.size(); ++v) addChunks(lay.off[KV][v], lay.size[KV][v], lowType[lv.nEdges + v]);
+
+  // halo table in the five destination groups
+  std::vector<uint2> comm;
+  for (int k = 0; k < G_COUNT; ++k) {
+    ld.commBegin[k] = (int64_t)comm.size();
+    for (size_t i = 0; i < lay.commDst[k].size(); ++i)
+      comm.push_back(make_uint2((unsigned)lay.commDst[k][i], (unsigned)lay.commSrc[k][i]));
+    ld.commCount[k] = (int64_t)comm.size() - ld.commBegin[k];
+  }
+
+  auto& keep = ld.keep;
+  lv.cellOff = (const int64_t*)upload(keep, lay.off[KC], stream);
+  lv.faceOff = (const int64_t*)upload(keep, lay.off[KF], stream);
+  lv.lowOff = (const int64_t*)upload(keep, lowOff, stream);
+  lv.lowFirst = (const int*)upload(keep, lowFirst, stream);
+  lv.lowCount = (const int*)upload(keep, lowCount, stream);
+  lv.cellType = (const unsigned char*)upload(keep, cellType, stream);
+  lv.faceType = (const unsigned char*)upload(keep, faceType, stream);
+  lv.lowType = (const unsigned char*)upload(keep, lowType, stream);
+  lv.cellBlocks = (const dev::CellBlock*)upload(keep, cb, stream);
+  lv.nCellBlocks = (int)cb.size();
+  lv.faceBlocks = (const dev::FaceBlock*)upload(keep, fb, stream);
+  lv.nFaceBlocks = (int)fb.size();
+  lv.lowBlocks = (const dev::LowBlock*)upload(keep, lb, stream);
+  lv.nLowBlocks = (int)lb.size();
+  ld.comm = (uint2*)upload(keep, comm, stream);
+  ld.chunks = (dev::Chunk*)upload(keep, chunks, stream);
+  ld.nChunks = (int)chunks.size();
+  ld.partial.alloc(sizeof(double) * std::max(1, lv.nCellBlocks + lv.nFaceBlocks + lv.nLowBlocks));
+  cudaCheck(cudaStreamSynchronize(stream), "level upload");
+}
+
+// ------------------------------------------------------------------------------------------
+// functions
+// ------------------------------------------------------------------------------------------
+Function& Storage::fn(int id) {
+  auto it = fns.find(id);
+  argCheck(it != fns.end(), "unknown function handle");
+  return *it->second;
+}
+void* Storage::data(int id, int L) {
+  Function& f = fn(id);
+  argCheck(L >= f.minL && L <= f.maxL, "level outside the function's level range");
+  return f.levels[L - f.minL]->p;
+}
+int Storage::createFunction(int minL, int maxL, int prec) {
+  argCheck(minL >= 0 && maxL <= maxLevel() && minL <= maxL, "invalid level range");
+  argCheck(prec == 8 || prec == 4, "precision must be 8 or 4");
+  std::unique_ptr<Function> f(new Function());
+  f->minL = minL;
+  f->maxL = maxL;
+  f->prec = prec;
+  for (int L = minL; L <= maxL; ++L) {
+    f->levels.emplace_back(new DevBuf());
+    const size_t bytes = (size_t)levels[L].lay->total * prec;
+    f->levels.back()->alloc(bytes);
+    cudaCheck(cudaMemsetAsync(f->levels.back()->p, 0, bytes, stream), "memset");
+  }
+  const int id = nextId++;
+  fns[id] = std::move(f);
+  return id;
+}
+
+static unsigned grid1d(int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 32); }
+
+void Storage::communicate(int id, int L, int groupMask) {
+  Function& f = fn(id);
+  void* d = data(id, L);
+  const LevelData& ld = levels[L];
+  // one gather per contiguous run of selected groups
+  int k = 0;
+  while (k < G_COUNT) {
+    if (!(groupMask & (1 << k))) {
+      ++k;
+      continue;
+    }
+    const int64_t begin = ld.commBegin[k];
+    int64_t n = 0;
+    while (k < G_COUNT && (groupMask & (1 << k))) n += ld.commCount[k++];
+    if (n == 0) continue;
+    if (f.prec == 8)
+      dev::commGatherKernel<double><<<grid1d(n), 256, 0, stream>>>((double*)d, ld.comm + begin, n);
+    else
+      dev::commGatherKernel<float><<<grid1d(n), 256, 0, stream>>>((float*)d, ld.comm + begin, n);
+    ++launches;
+  }
+  cudaCheck(cudaGetLastError(), "communicate");
+}
+
+void Storage::lincomb(int dst, int L, unsigned mask, int n, const double* a, const int* srcs, bool add,
+                      double constant) {
+  argCheck(n >= 0 && n <= 3, "at most three source functions");
+  Function& fd = fn(dst);
+  void* pd = data(dst, L);
+  const void* ps[3] = {nullptr, nullptr, nullptr};
+  double sc[3] = {0, 0, 0};
+  for (int i = 0; i < n; ++i) {
+    argCheck(fn(srcs[i]).prec == fd.prec, "assign/add require functions of equal precision");
+    ps[i] = data(srcs[i], L);
+    sc[i] = a[i];
+  }
+  const LevelData& ld = levels[L];
+  if (ld.nChunks == 0) return;
+  if (fd.prec == 8)
+    dev::lincombKernel<double><<<ld.nChunks, dev::kBlock, 0, stream>>>(
+        ld.chunks, mask, (double*)pd, n, (const double*)ps[0], (const double*)ps[1], (const double*)ps[2], sc[0], sc[1],
+        sc[2], add ? 1 : 0, constant);
+  else
+    dev::lincombKernel<float><<<ld.nChunks, dev::kBlock, 0, stream>>>(
+        ld.chunks, mask, (float*)pd, n, (const float*)ps[0], (const float*)ps[1], (const float*)ps[2], sc[0], sc[1],
+        sc[2], add ? 1 : 0, constant);
+  ++launches;
+  cudaCheck(cudaGetLastError(), "lincomb");
+}
+
+void Storage::copyCast(int dst, int src, int L, unsigned mask, bool add) {
+  Function& fd = fn(dst);
+  Function& fs = fn(src);
+  void* pd = data(dst, L);
+  void* ps = data(src, L);
+  const LevelData& ld = levels[L];
+  if (ld.nChunks == 0) return;
+  const int a = add ? 1 : 0;
+  if (fd.prec == 8 && fs.prec == 8)
+    dev::castKernel<double, double><<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (double*)pd, (const double*)ps, a);
+  else if (fd.prec == 8)
+    dev::castKernel<double, float><<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (double*)pd, (const float*)ps, a);
+  else if (fs.prec == 8)
+    dev::castKernel<float, double><<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (float*)pd, (const double*)ps, a);
+  else
+    dev::castKernel<float, float><<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (float*)pd, (const float*)ps, a);
+  ++launches;
+  cudaCheck(cudaGetLastError(), "copyCast");
+}
+
+void Storage::dotAsync(int a, int b, int L, unsigned mask, double* dOut) {
+  Function& fa = fn(a);
+  argCheck(fa.prec == fn(b).prec, "dot requires functions of equal precision");
+  const LevelData& ld = levels[L];
+  const int nb = ld.lv.nCellBlocks + ld.lv.nFaceBlocks + ld.lv.nLowBlocks;
+  if (fa.prec == 8)
+    dev::dotKernel<double><<<nb, dev::kBlock, 0, stream>>>(ld.lv, (const double*)data(a, L), (const double*)data(b, L), mask,
+                                                           (double*)ld.partial.p);
+  else
+    dev::dotKernel<float><<<nb, dev::kBlock, 0, stream>>>(ld.lv, (const float*)data(a, L), (const float*)data(b, L), mask,
+                                                          (double*)ld.partial.p);
+  dev::reduceKernel<<<1, dev::kBlock, 0, stream>>>((const double*)ld.partial.p, nb, dOut);
+  launches += 2;
+  cudaCheck(cudaGetLastError(), "dot");
+}
+
+double Storage::dot(int a, int b, int L, unsigned mask) {
+  double* d = (double*)scalars.p;
+  dotAsync(a, b, L, mask, d);
+  double h = 0;
+  cudaCheck(cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, stream), "dot readback");
+  cudaCheck(cudaStreamSynchronize(stream), "dot sync");
+  return h;
+}
+
+// ------------------------------------------------------------------------------------------
+// operators
+// ------------------------------------------------------------------------------------------
+template <class T>
+static dev::StencilDev<T> packStencil(std::vector<std::unique_ptr<DevBuf>>& keep, const LevelStencils& st, int nEdges,
+                                      cudaStream_t stream) {
+  std::vector<T> cellW;
+  for (auto& c : st.cell)
+    for (int k = 0; k < 16; ++k) cellW.push_back(T(c[k]));
+  std::vector<dev::FaceEnt<T>> fe(st.face.size() * 16);
+  std::vector<int> fc(st.face.size());
+  for (size_t f = 0; f < st.face.size(); ++f) {
+    argCheck(st.face[f].size() <= 16, "face stencil exceeds 16 entries");
+    fc[f] = (int)st.face[f].size();
+    for (size_t k = 0; k < st.face[f].size(); ++k)
+      fe[16 * f + k] = {T(st.face[f][k].w), st.face[f][k].layer, st.face[f][k].dx, st.face[f][k].dy};
+  }
+  std::vector<int> off{0};
+  std::vector<int64_t> rel;
+  std::vector<T> wv;
+  auto addLow = [&](const std::vector<LowEntry>& ent) {
+    for (auto& e : ent) {
+      rel.push_back(e.rel);
+      wv.push_back(T(e.w));
+    }
+    off.push_back((int)rel.size());
+  };
+  for (auto& e : st.edge) addLow(e);
+  for (auto& v : st.vert) addLow(v);
+  (void)nEdges;
+  dev::StencilDev<T> d;
+  d.cellW = (const T*)upload(keep, cellW, stream);
+  d.faceEnt = (const dev::FaceEnt<T>*)upload(keep, fe, stream);
+  d.faceEntCount = (const int*)upload(keep, fc, stream);
+  d.lowEntOff = (const int*)upload(keep, off, stream);
+  d.lowEntRel = (const int64_t*)upload(keep, rel, stream);
+  d.lowEntW = (const T*)upload(keep, wv, stream);
+  return d;
+}
+
+int Storage::createOperator(int form, int minL, int maxL) {
+  argCheck(form == FORM_LAPLACE || form == FORM_MASS, "unknown form");
+  argCheck(minL >= 0 && maxL <= maxLevel() && minL <= maxL, "invalid level range");
+  std::unique_ptr<Operator> op(new Operator());
+  op->form = form;
+  op->minL = minL;
+  op->maxL = maxL;
+  for (int L = minL; L <= maxL; ++L) {
+    op->host.push_back(assembleStencils(disc, L, (FormKind)form));
+    op->d.push_back(packStencil<double>(op->keep, op->host.back(), (int)disc.topo().edges.size(), stream));
+    op->f.push_back(packStencil<float>(op->keep, op->host.back(), (int)disc.topo().edges.size(), stream));
+  }
+  cudaCheck(cudaStreamSynchronize(stream), "operator upload");
+  const int id = nextId++;
+  ops[id] = std::move(op);
+  return id;
+}
+
+Operator& Storage::op(int id) {
+  auto it = ops.find(id);
+  argCheck(it != ops.end(), "unknown operator handle");
+  return *it->second;
+}
+
+template <class T>
+const dev::StencilDev<T>& stencilOf(Operator& o, int L);
+template <>
+const dev::StencilDev<double>& stencilOf<double>(Operator& o, int L) {
+  return o.d[L - o.minL];
+}
+template <>
+const dev::StencilDev<float>& stencilOf<float>(Operator& o, int L) {
+  return o.f[L - o.minL];
+}
+
+template <class T, int MODE>
+void Storage::stencilOp(Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask) {
+  const LevelData& ld = levels[L];
+  const dev::StencilDev<T>& st = stencilOf<T>(o, L);
+  if (ld.lv.nCellBlocks) {
+    dev::cellStencilKernel<T, MODE><<<ld.lv.nCellBlocks, dev::kBlock, 0, stream>>>(ld.lv, st.cellW, dst, src, rhs, mask);
+    ++launches;
+  }
+  if (ld.lv.nFaceBlocks) {
+    dev::faceStencilKernel<T, MODE><<<ld.lv.nFaceBlocks, dev::kBlock, 0, stream>>>(ld.lv, st, dst, src, rhs, mask);
+    ++launches;
+  }
+  if (ld.lv.nLowBlocks) {
+    dev::lowStencilKernel<T, MODE><<<ld.lv.nLowBlocks, dev::kBlock, 0, stream>>>(ld.lv, st, dst, src, rhs, mask, 0);
+    ++launches;
+  }
+  cudaCheck(cudaGetLastError(), "stencil kernel");
+}
+
+void Storage::apply(int opId, int src, int dst, int L, unsigned mask, int update) {
+  Operator& o = op(opId);
+  argCheck(L >= o.minL && L <= o.maxL, "level outside the operator's level range");
+  argCheck(src != dst, "apply: src and dst must differ");
+  Function& fs = fn(src);
+  argCheck(fs.prec == fn(dst).prec, "apply: precision mismatch");
+  communicate(src, L, kAllGroups);
+  if (fs.prec == 8) {
+    if (update == 0) stencilOp<double, dev::MODE_REPLACE>(o, L, (double*)data(dst, L), (const double*)data(src, L), nullptr, mask);
+    else stencilOp<double, dev::MODE_ADD>(o, L, (double*)data(dst, L), (const double*)data(src, L), nullptr, mask);
+  } else {
+    if (update == 0) stencilOp<float, dev::MODE_REPLACE>(o, L, (float*)data(dst, L), (const float*)data(src, L), nullptr, mask);
+    else stencilOp<float, dev::MODE_ADD>(o, L, (float*)data(dst, L), (const float*)data(src, L), nullptr, mask);
+  }
+}
+
+void Storage::residual(int opId, int x, int b, int r, int L, unsigned mask) {
+  Operator& o = op(opId);
+  argCheck(L >= o.minL && L <= o.maxL, "level outside the operator's level range");
+  argCheck(x != r && b != r, "residual: r must differ from x and b");
+  Function& fx = fn(x);
+  argCheck(fx.prec == fn(b).prec && fx.prec == fn(r).prec, "residual: precision mismatch");
+  communicate(x, L, kAllGroups);
+  if (fx.prec == 8)
+    stencilOp<double, dev::MODE_RESIDUAL>(o, L, (double*)data(r, L), (const double*)data(x, L), (const double*)data(b, L), mask);
+  else
+    stencilOp<float, dev::MODE_RESIDUAL>(o, L, (float*)data(r, L), (const float*)data(x, L), (const float*)data(b, L), mask);
+}
+
+template <class T>
+void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned mask, T omega, bool backwards) {
+  const LevelData& ld = levels[L];
+  const dev::StencilDev<T>& st = stencilOf<T>(o, L);
+  const dev::LevelDev& lv = ld.lv;
+  const int nVertBlocks = lv.nLowBlocks - lv.nLowEdgeBlocks;
+  auto verts = [&]() {
+    if (nVertBlocks) {
+      dev::lowSorKernel<T><<<nVertBlocks, dev::kBlock, 0, stream>>>(lv, st, u, rhs, mask, -1, omega, lv.nLowEdgeBlocks);
+      ++launches;
+    }
+  };
+  auto edges = [&](int c) {
+    if (lv.nLowEdgeBlocks) {
+      dev::lowSorKernel<T><<<lv.nLowEdgeBlocks, dev::kBlock, 0, stream>>>(lv, st, u, rhs, mask, c, omega, 0);
+      ++launches;
+    }
+  };
+  auto faces = [&](int c) {
+    if (lv.nFaceBlocks) {
+      dev::faceSorKernel<T><<<lv.nFaceBlocks, dev::kBlock, 0, stream>>>(lv, st, u, rhs, mask, c, omega);
+      ++launches;
+    }
+  };
+  auto cells = [&](int c) {
+    if (lv.nCellBlocks) {
+      dev::cellSorKernel<T><<<lv.nCellBlocks, dev::kBlock, 0, stream>>>(lv, st.cellW, u, rhs, mask, c, omega);
+      ++launches;
+    }
+  };
+  // P1Operator::smooth_sor (P1Operator.hpp:350-420): full halo refresh, then the phases
+  // V -> E -> F -> C (backwards C -> F -> E -> V) with a refresh of the next phase's copies.
+  // Only the copies the reference refreshes between phases are refreshed here, so ghost
+  // values that reach a primitive from outside its closure keep their start-of-sweep value.
+  communicate(dstId, L, kAllGroups);
+  if (!backwards) {
+    verts();
+    communicate(dstId, L, 1 << G_EDGE);           // Vertex -> Edge
+    edges(0);
+    edges(1);
+    communicate(dstId, L, 1 << G_FACE_BOUNDARY);  // Edge -> Face
+    for (int c = 0; c < 3; ++c) faces(c);
+    communicate(dstId, L, 1 << G_CELL);           // Face -> Cell
+    for (int c = 0; c < 4; ++c) cells(c);
+  } else {
+    for (int c = 3; c >= 0; --c) cells(c);
+    communicate(dstId, L, 1 << G_FACE_GHOST);     // Cell -> Face
+    for (int c = 2; c >= 0; --c) faces(c);
+    communicate(dstId, L, 1 << G_EDGE);           // Face -> Edge
+    edges(1);
+    edges(0);
+    communicate(dstId, L, 1 << G_VERT);           // Edge -> Vertex
+    verts();
+  }
+  cudaCheck(cudaGetLastError(), "sor");
+}
+
+void Storage::smoothSor(int opId, int dst, int rhs, double omega, int L, unsigned mask, bool backwards) {
+  Operator& o = op(opId);
+  argCheck(L >= o.minL && L <= o.maxL, "level outside the operator's level range");
+  argCheck(dst != rhs, "smooth_sor: dst and rhs must differ");
+  Function& fd = fn(dst);
+  argCheck(fd.prec == fn(rhs).prec, "smooth_sor: precision mismatch");
+  for (auto& c : o.host[L - o.minL].cell)
+    if (levels[L].lv.nCellBlocks && c[0] == 0.0) throw Error(HG_ERR_NUMERIC, "zero diagonal in cell stencil");
+  if (fd.prec == 8) sorT<double>(o, dst, L, (double*)data(dst, L), (const double*)data(rhs, L), mask, omega, backwards);
+  else sorT<float>(o, dst, L, (float*)data(dst, L), (const float*)data(rhs, L), mask, (float)omega, backwards);
+}
+
+// The fine-level face/edge/vertex stencil structure drives the restriction; it is taken from
+// a structure-only Laplace stencil owned by the storage (weights unused).
+const Operator& Storage::structure() {
+  if (structureOp < 0) structureOp = createOperator(FORM_LAPLACE, 0, maxLevel());
+  return op(structureOp);
+}
+
+template <class T>
+void Storage::restrictT(int id, int Lf, unsigned mask) {
+  const int Lc = Lf - 1;
+  const LevelData& lc = levels[Lc];
+  const LevelData& lf = levels[Lf];
+  T* coarse = (T*)data(id, Lc);
+  const T* fine = (const T*)data(id, Lf);
+  Operator& so = const_cast<Operator&>(structure());
+  const dev::StencilDev<T>& stf = stencilOf<T>(so, Lf);
+  communicate(id, Lf, kAllGroups);
+  if (lc.lv.nCellBlocks) {
+    dev::cellRestrictKernel<T><<<lc.lv.nCellBlocks, dev::kBlock, 0, stream>>>(lc.lv, lf.lv, coarse, fine, mask);
+    ++launches;
+  }
+  if (lc.lv.nFaceBlocks) {
+    dev::faceRestrictKernel<T><<<lc.lv.nFaceBlocks, dev::kBlock, 0, stream>>>(lc.lv, lf.lv, stf, coarse, fine, mask);
+    ++launches;
+  }
+  if (lc.lv.nLowBlocks) {
+    dev::lowRestrictKernel<T><<<lc.lv.nLowBlocks, dev::kBlock, 0, stream>>>(lc.lv, lf.lv, stf, coarse, fine, mask);
+    ++launches;
+  }
+  cudaCheck(cudaGetLastError(), "restrict");
+}
+
+void Storage::restrictFn(int id, int Lf, unsigned mask) {
+  Function& f = fn(id);
+  argCheck(Lf - 1 >= f.minL && Lf <= f.maxL, "restrict: levels outside the function's range");
+  if (f.prec == 8) restrictT<double>(id, Lf, mask);
+  else restrictT<float>(id, Lf, mask);
+}
+
+template <class T>
+void Storage::prolongT(int id, int Lc, unsigned mask, bool add) {
+  const int Lf = Lc + 1;
+  const LevelData& lc = levels[Lc];
+  const LevelData& lf = levels[Lf];
+  T* fine = (T*)data(id, Lf);
+  const T* coarse = (const T*)data(id, Lc);
+  communicate(id, Lc, kAllGroups);
+  if (lf.lv.nCellBlocks) {
+    if (add) dev::cellProlongKernel<T, true><<<lf.lv.nCellBlocks, dev::kBlock, 0, stream>>>(lf.lv, lc.lv, fine, coarse, mask);
+    else dev::cellProlongKernel<T, false><<<lf.lv.nCellBlocks, dev::kBlock, 0, stream>>>(lf.lv, lc.lv, fine, coarse, mask);
+    ++launches;
+  }
+  if (lf.lv.nFaceBlocks) {
+    if (add) dev::faceProlongKernel<T, true><<<lf.lv.nFaceBlocks, dev::kBlock, 0, stream>>>(lf.lv, lc.lv, fine, coarse, mask);
+    else dev::faceProlongKernel<T, false><<<lf.lv.nFaceBlocks, dev::kBlock, 0, stream>>>(lf.lv, lc.lv, fine, coarse, mask);
+    ++launches;
+  }
+  if (lf.lv.nLowBlocks) {
+    if (add) dev::lowProlongKernel<T, true><<<lf.lv.nLowBlocks, dev::kBlock, 0, stream>>>(lf.lv, lc.lv, fine, coarse, mask);
+    else dev::lowProlongKernel<T, false><<<lf.lv.nLowBlocks, dev::kBlock, 0, stream>>>(lf.lv, lc.lv, fine, coarse, mask);
+    ++launches;
+  }
+  cudaCheck(cudaGetLastError(), "prolongate");
+}
+
+void Storage::prolongate(int id, int Lc, unsigned mask, bool add) {
+  Function& f = fn(id);
+  argCheck(Lc >= f.minL && Lc + 1 <= f.maxL, "prolongate: levels outside the function's range");
+  if (f.prec == 8) prolongT<double>(id, Lc, mask, add);
+  else prolongT<float>(id, Lc, mask, add);
+}
+
+}  // namespace hg

@@ -1,0 +1,112 @@
+// Host-side state behind an hg_storage handle (C++; not part of the C-ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <deque>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "discretization.hpp"
+#include "kernels.cuh"
+
+namespace hg {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf();
+  void* alloc(size_t n);
+};
+
+struct LevelData {
+  const LevelLayout* lay = nullptr;
+  dev::LevelDev lv{};
+  uint2* comm = nullptr;
+  int64_t commBegin[G_COUNT] = {0, 0, 0, 0, 0}, commCount[G_COUNT] = {0, 0, 0, 0, 0};
+  dev::Chunk* chunks = nullptr;
+  int nChunks = 0;
+  DevBuf partial;
+  std::vector<unsigned char> hostCellType, hostFaceType, hostLowType;
+  std::vector<std::unique_ptr<DevBuf>> keep;
+};
+
+struct Function {
+  int minL = 0, maxL = 0, prec = 8;
+  std::vector<std::unique_ptr<DevBuf>> levels;
+};
+
+struct Operator {
+  int form = 0, minL = 0, maxL = 0;
+  std::vector<LevelStencils> host;
+  std::vector<dev::StencilDev<double>> d;
+  std::vector<dev::StencilDev<float>> f;
+  std::vector<std::unique_ptr<DevBuf>> keep;
+};
+
+struct Gmg;
+
+struct Storage {
+  Storage(const Topology& topo, int maxLevel);
+  ~Storage();
+  int maxLevel() const { return disc.maxLevel(); }
+
+  Discretization disc;
+  cudaStream_t ownStream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::deque<LevelData> levels;
+  std::map<int, std::unique_ptr<Function>> fns;
+  std::map<int, std::unique_ptr<Operator>> ops;
+  std::map<int, std::unique_ptr<Gmg>> gmgs;
+  int nextId = 1;
+  int structureOp = -1;
+  DevBuf scalars;            // device scratch for reductions
+  unsigned long long launches = 0;  // kernels launched by this storage
+
+  Function& fn(int id);
+  void* data(int id, int L);
+  int createFunction(int minL, int maxL, int prec);
+  // Refresh the copy slots of the selected groups (bit (1 << CommGroup)) from their owners.
+  void communicate(int id, int L, int groupMask);
+  void lincomb(int dst, int L, unsigned mask, int n, const double* a, const int* srcs, bool add, double constant);
+  void copyCast(int dst, int src, int L, unsigned mask, bool add);
+  void dotAsync(int a, int b, int L, unsigned mask, double* dOut);
+  double dot(int a, int b, int L, unsigned mask);
+
+  int createOperator(int form, int minL, int maxL);
+  Operator& op(int id);
+  void apply(int op, int src, int dst, int L, unsigned mask, int update);
+  void residual(int op, int x, int b, int r, int L, unsigned mask);
+  void smoothSor(int op, int dst, int rhs, double omega, int L, unsigned mask, bool backwards);
+  void restrictFn(int id, int Lf, unsigned mask);
+  void prolongate(int id, int Lc, unsigned mask, bool add);
+  const Operator& structure();
+
+  template <class T, int MODE>
+  void stencilOp(Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask);
+  template <class T>
+  void sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned mask, T omega, bool backwards);
+  template <class T>
+  void restrictT(int id, int Lf, unsigned mask);
+  template <class T>
+  void prolongT(int id, int Lc, unsigned mask, bool add);
+
+ private:
+  void buildLevel(int L);
+};
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+void cudaCheck(cudaError_t e, const char* what);
+void argCheck(bool ok, const std::string& msg);
+extern thread_local std::string g_lastError;
+
+}  // namespace hg

@@ -1,0 +1,176 @@
+/* C-ABI of the B200 matrix-free P1 geometric-multigrid hot path.
+ *
+ * Every entry point returns an int status (HG_OK = 0). Plain pointers and sizes only: no
+ * C++ or PyTorch types cross this boundary. One hg_storage owns the macro-mesh topology,
+ * all device memory of its functions and operators, and one CUDA stream; it is not
+ * thread-safe, distinct storages are independent.
+ *
+ * Function data are kept on the device in the reference's per-primitive layout
+ * (vertex / edge / face / cell arrays incl. ghost layers), see hg_primitive_layout.
+ * The entry points replace these reference interfaces (paths within wagnandr/hyteg):
+ *   hg_storage_create_cuboid   MeshInfo::meshCuboid + SetupPrimitiveStorage +
+ *                              setMeshBoundaryFlagsOnBoundary(1,0,true)
+ *                              (src/hyteg/mesh/MeshGenCuboid.cpp:32,
+ *                               src/hyteg/primitivestorage/SetupPrimitiveStorage.cpp:37,735)
+ *   hg_function_create         P1Function<real_t>(name, storage, minLevel, maxLevel)
+ *                              (src/hyteg/p1functionspace/VertexDoFFunction.hpp:66-77)
+ *   hg_communicate             VertexDoFFunction::communicate<S,R> in the six directions
+ *                              (src/hyteg/p1functionspace/VertexDoFFunction.hpp:259-284)
+ *   hg_interpolate_const       VertexDoFFunction::interpolate(constant, level, flag)
+ *   hg_assign / hg_add         VertexDoFFunction::assign / add
+ *                              (src/hyteg/p1functionspace/VertexDoFFunction.cpp:980,1077)
+ *   hg_dot                     VertexDoFFunction::dotGlobal (VertexDoFFunction.cpp:1411)
+ *   hg_operator_create         P1ConstantLaplaceOperator / P1ConstantMassOperator ctor
+ *                              (src/hyteg/p1functionspace/P1ConstantOperator.hpp:165-166)
+ *   hg_apply                   Operator::apply(src, dst, level, flag, updateType)
+ *                              (src/hyteg/operators/Operator.hpp:73-80,
+ *                               src/hyteg/p1functionspace/P1Operator.hpp:197-325)
+ *   hg_residual                GeometricMultigridSolver residual: apply + assign{1,-1}
+ *                              (src/hyteg/solvers/GeometricMultigridSolver.hpp:185-186)
+ *   hg_smooth_sor              SORSmoothable::smooth_sor / smooth_sor_backwards
+ *                              (src/hyteg/solvers/Smoothables.hpp:81-91), multicolour on the GPU
+ *   hg_restrict                P1toP1LinearRestriction::restrict
+ *                              (src/hyteg/gridtransferoperators/P1toP1LinearRestriction.cpp:163)
+ *   hg_prolongate              P1toP1LinearProlongation::prolongate / prolongateAndAdd
+ *                              (src/hyteg/gridtransferoperators/P1toP1LinearProlongation.cpp:189)
+ *   hg_cg_solve                CGSolver::solve (src/hyteg/solvers/CGSolver.hpp:69-150)
+ *   hg_gmg_*                   GeometricMultigridSolver (src/hyteg/solvers/GeometricMultigridSolver.hpp:36-259)
+ */
+#ifndef HYTEG_B200_H
+#define HYTEG_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  HG_OK = 0,
+  HG_ERR_ARG = 1,      /* invalid argument (handle, level, flag, size) */
+  HG_ERR_CUDA = 2,     /* CUDA runtime error or no device */
+  HG_ERR_OOM = 3,      /* device allocation failed */
+  HG_ERR_STATE = 4,    /* operation not valid in the current state */
+  HG_ERR_NUMERIC = 5,  /* zero diagonal, breakdown */
+  HG_ERR_INTERNAL = 6
+};
+
+/* DoFType bits (src/hyteg/types/types.hpp:35-44) */
+#define HG_INNER 1u
+#define HG_DIRICHLET 2u
+#define HG_NEUMANN 4u
+#define HG_FREESLIP 8u
+#define HG_ALL 15u
+
+/* primitive kinds */
+#define HG_VERTEX 0
+#define HG_EDGE 1
+#define HG_FACE 2
+#define HG_CELL 3
+
+typedef struct hg_storage hg_storage;
+typedef struct hg_mesh hg_mesh;
+
+/* Text of the last error of the calling thread ("" if none). */
+const char* hg_last_error(void);
+/* Number of CUDA devices visible (0 on a machine without GPU); never fails. */
+int hg_device_count(void);
+
+int hg_storage_create_cuboid(const double lo[3], const double hi[3], int nx, int ny, int nz, int max_level,
+                             hg_storage** out);
+/* Explicit tetrahedral mesh: coords[3*nverts], tets[4*ncells] (vertex IDs in cell-frame order). */
+int hg_storage_create_tets(int nverts, const double* coords, int ncells, const int* tets, int max_level,
+                           hg_storage** out);
+int hg_storage_destroy(hg_storage* s);
+/* counts[4] = {#vertices, #edges, #faces, #cells} */
+int hg_storage_counts(const hg_storage* s, int counts[4]);
+/* Use this CUDA stream (cudaStream_t) for all subsequent work; NULL = the storage's own stream. */
+int hg_storage_set_stream(hg_storage* s, void* stream);
+int hg_storage_synchronize(hg_storage* s);
+/* Piecewise-constant diffusion coefficient per macro-cell (ncells values) for operators
+ * created afterwards. */
+int hg_storage_set_cell_coefficients(hg_storage* s, const double* k, int ncells);
+/* Topology export: for kind HG_VERTEX ids[0..2]=unused, coords[3]; HG_EDGE ids[2]; HG_FACE ids[3];
+ * HG_CELL ids[4]; flag = mesh boundary flag. */
+int hg_primitive_vertices(const hg_storage* s, int kind, int prim, int ids[4], double coords[3], int* flag);
+/* Neighbour list of a primitive: which = kind of neighbours (higher dimension), returns up to cap ids. */
+int hg_primitive_neighbours(const hg_storage* s, int kind, int prim, int which, int* ids, int cap, int* count);
+/* Offset and length of a primitive's array inside one function level buffer. */
+int hg_primitive_layout(const hg_storage* s, int level, int kind, int prim, int64_t* offset, int64_t* size);
+int hg_level_size(const hg_storage* s, int level, int64_t* n);
+
+/* ---- Host-only view of the same discretization (no GPU needed): topology, per-level
+ * layout, halo tables and stencil tables, for inspection and CPU-side verification. ---- */
+int hg_mesh_create_cuboid(const double lo[3], const double hi[3], int nx, int ny, int nz, int max_level, hg_mesh** out);
+int hg_mesh_create_tets(int nverts, const double* coords, int ncells, const int* tets, int max_level, hg_mesh** out);
+int hg_mesh_destroy(hg_mesh* m);
+int hg_mesh_counts(const hg_mesh* m, int counts[4]);
+int hg_mesh_set_cell_coefficients(hg_mesh* m, const double* k, int ncells);
+int hg_mesh_primitive_vertices(const hg_mesh* m, int kind, int prim, int ids[4], double coords[3], int* flag);
+int hg_mesh_primitive_neighbours(const hg_mesh* m, int kind, int prim, int which, int* ids, int cap, int* count);
+int hg_mesh_primitive_layout(const hg_mesh* m, int level, int kind, int prim, int64_t* offset, int64_t* size);
+int hg_mesh_level_size(const hg_mesh* m, int level, int64_t* n);
+/* Coordinates (3 per slot) of the micro-vertex each slot of a level buffer holds, and per slot
+ * 1 = owned DoF, 0 = copy of a DoF owned elsewhere, -1 = alignment padding. */
+int hg_mesh_slot_info(const hg_mesh* m, int level, double* xyz, signed char* owned, int64_t n);
+/* Halo table of one group (0 vertex ghosts, 1 edge copies, 2 face boundary rows, 3 face ghost
+ * layers, 4 cell closures): pass dst = src = NULL to query *n. */
+int hg_mesh_halo_table(const hg_mesh* m, int level, int group, int64_t* dst, int64_t* src, int64_t* n);
+/* Stencil of the owned points of one primitive (form 0 diffusion, 1 mass). Cells: 15 weights in
+ * the order C E W N S NW SE TC TW TS TSE BC BE BN BNW. Faces: entries (layer, dx, dy, weight),
+ * layer 0 = face, 1 + n = ghost layer of neighbour cell n. Edges / vertices: entries
+ * (relative slot, weight). Entry 0 is the diagonal. cap = capacity of the output arrays. */
+int hg_mesh_cell_stencil(const hg_mesh* m, int level, int form, int cell, double w[15]);
+int hg_mesh_face_stencil(const hg_mesh* m, int level, int form, int face, int* layer, int* dx, int* dy, double* w,
+                         int cap, int* n);
+int hg_mesh_low_stencil(const hg_mesh* m, int level, int form, int kind, int prim, int64_t* rel, double* w, int cap,
+                        int* n);
+
+/* precision: 8 = double, 4 = float */
+int hg_function_create(hg_storage* s, int min_level, int max_level, int precision, int* fn);
+int hg_function_destroy(hg_storage* s, int fn);
+int hg_function_device_ptr(hg_storage* s, int fn, int level, void** ptr);
+/* Host <-> device copies of one level buffer (n elements of the function's precision). */
+int hg_function_upload(hg_storage* s, int fn, int level, const void* host, int64_t n);
+int hg_function_download(hg_storage* s, int fn, int level, void* host, int64_t n);
+int hg_communicate(hg_storage* s, int fn, int level);
+int hg_interpolate_const(hg_storage* s, int fn, double value, int level, unsigned flag);
+/* dst = sum_i scalars[i] * srcs[i]   (n <= 3) */
+int hg_assign(hg_storage* s, int dst, int level, unsigned flag, int n, const double* scalars, const int* srcs);
+/* dst += sum_i scalars[i] * srcs[i]  (n <= 3) */
+int hg_add(hg_storage* s, int dst, int level, unsigned flag, int n, const double* scalars, const int* srcs);
+/* dst = (precision of dst) src, or dst += src when add != 0; src and dst may differ in precision */
+int hg_copy_cast(hg_storage* s, int dst, int src, int level, unsigned flag, int add);
+int hg_dot(hg_storage* s, int a, int b, int level, unsigned flag, double* out);
+
+/* form: 0 = diffusion (Laplace, scaled by the per-cell coefficient), 1 = mass */
+int hg_operator_create(hg_storage* s, int form, int min_level, int max_level, int* op);
+int hg_operator_destroy(hg_storage* s, int op);
+/* update: 0 = Replace, 1 = Add */
+int hg_apply(hg_storage* s, int op, int src, int dst, int level, unsigned flag, int update);
+/* r = b - A x on the flagged primitives */
+int hg_residual(hg_storage* s, int op, int x, int b, int r, int level, unsigned flag);
+int hg_smooth_sor(hg_storage* s, int op, int dst, int rhs, double omega, int level, unsigned flag, int backwards);
+/* fn(src_level - 1) = R fn(src_level) */
+int hg_restrict(hg_storage* s, int fn, int src_level, unsigned flag);
+/* fn(src_level + 1) = P fn(src_level)   (add != 0: +=) */
+int hg_prolongate(hg_storage* s, int fn, int src_level, unsigned flag, int add);
+
+/* Conjugate gradients on one level (flag Inner|Neumann|Freeslip as in the reference).
+ * Stops when sqrt(r.r) < tol or after max_iter iterations. */
+int hg_cg_solve(hg_storage* s, int op, int x, int b, int level, int max_iter, double tol, int* iterations,
+                double* final_residual);
+
+/* Geometric multigrid V/W-cycles: SOR smoother (multicolour, omega), CG coarse solver. */
+int hg_gmg_create(hg_storage* s, int op, int min_level, int max_level, int pre_smooth, int post_smooth,
+                  double omega, int cycle_type /*0 V, 1 W*/, int coarse_max_iter, double coarse_tol,
+                  int precision, int* gmg);
+int hg_gmg_destroy(hg_storage* s, int gmg);
+/* One cycle: x <- MG(x, b) on max_level (x, b of the solver's precision). */
+int hg_gmg_solve(hg_storage* s, int gmg, int x, int b, int level);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HYTEG_B200_H */

@@ -1,0 +1,209 @@
+"""ctypes loader of the CPU oracle (oracle/liboracle.so) and of the reference's own kernels
+(oracle/_ref/libhyteg_ref.so). TEST INFRASTRUCTURE ONLY: imported by tests/, by
+__graft_entry__.smoke() as the checker and by bench.py's CPU-baseline leg; never by the product.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libhyteg_ref.so")
+
+P = ctypes.POINTER
+c_double, c_int, c_int64, c_void_p = ctypes.c_double, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p
+
+
+def build():
+    """make -C oracle (builds _ref only where the reference tree is present)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _load_oracle():
+    if not os.path.exists(ORACLE_LIB):
+        build()
+    lib = ctypes.CDLL(ORACLE_LIB)
+    sig = {
+        "orc_create": (c_void_p, [c_int, P(c_double), c_int, P(c_int), P(c_double), c_int]),
+        "orc_destroy": (None, [c_void_p]),
+        "orc_num_nodes": (c_int64, [c_void_p, c_int]),
+        "orc_nodes": (None, [c_void_p, c_int, P(c_double), P(c_int)]),
+        "orc_apply": (None, [c_void_p, c_int, c_int, P(c_double), P(c_double)]),
+        "orc_sor": (None, [c_void_p, c_int, P(c_double), P(c_double), c_double, c_int, c_int, c_int]),
+        "orc_sor_phases": (None, [c_void_p, c_int, P(c_double), P(c_double), c_double, c_int, c_int, c_int]),
+        "orc_restrict": (None, [c_void_p, c_int, P(c_double), P(c_double)]),
+        "orc_prolongate": (None, [c_void_p, c_int, P(c_double), P(c_double), c_int]),
+        "orc_dot": (c_double, [c_void_p, c_int, P(c_double), P(c_double)]),
+        "orc_cg": (c_int, [c_void_p, c_int, P(c_double), P(c_double), c_int, c_double, P(c_double)]),
+        "orc_gmg": (None, [c_void_p, c_int, c_int, P(c_double), P(c_double), c_int, c_int, c_int, c_double, c_int,
+                           c_int, c_double, P(c_double)]),
+        "orc_element_laplace": (None, [P(c_double), P(c_double)]),
+        "orc_element_mass": (None, [P(c_double), P(c_double)]),
+        "orc_cell_local_stencil": (None, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, P(c_double)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = _load_oracle()
+    return _lib
+
+
+def ref_lib():
+    """The reference's own kernels, or None when oracle/_ref was not built."""
+    if not os.path.exists(REF_LIB):
+        return None
+    r = ctypes.CDLL(REF_LIB)
+    d = P(c_double)
+    r.ref_apply_cell.argtypes = [d, d, c_int, d, c_int]
+    r.ref_sor_cell.argtypes = [d, d, c_int, d, c_double]
+    r.ref_apply_face.argtypes = [d, d, d, c_int, c_int64, c_int64, c_int64, d, c_int]
+    r.ref_restrict_cell.argtypes = [d, d, c_int, d, d, d]
+    r.ref_prolongate_cell.argtypes = [d, d, c_int, d, d, d]
+    r.ref_p1_tet_diffusion.argtypes = [d, d]
+    r.ref_p1_tet_mass.argtypes = [d, d]
+    for f in (r.ref_apply_cell, r.ref_sor_cell, r.ref_apply_face, r.ref_restrict_cell, r.ref_prolongate_cell,
+              r.ref_p1_tet_diffusion, r.ref_p1_tet_mass):
+        f.restype = None
+    return r
+
+
+def dp(a):
+    return a.ctypes.data_as(P(c_double))
+
+
+class Oracle:
+    """Global-vector CPU restatement on one tetrahedral macro-mesh, levels 0..max_level."""
+
+    def __init__(self, coords, tets, max_level, k=None):
+        self.coords = np.ascontiguousarray(coords, dtype=np.float64)
+        self.tets = np.ascontiguousarray(tets, dtype=np.int32)
+        kk = None if k is None else np.ascontiguousarray(k, dtype=np.float64)
+        self._k = kk
+        self.max_level = max_level
+        self.h = lib().orc_create(len(self.coords), dp(self.coords), len(self.tets),
+                                  self.tets.ctypes.data_as(P(c_int)), None if kk is None else dp(kk), max_level)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def n(self, L):
+        return int(lib().orc_num_nodes(self.h, L))
+
+    def nodes(self, L):
+        n = self.n(L)
+        xyz = np.zeros((n, 3))
+        info = np.zeros((n, 4), dtype=np.int32)
+        lib().orc_nodes(self.h, L, dp(xyz), info.ctypes.data_as(P(c_int)))
+        return xyz, info
+
+    def dirichlet(self, L):
+        return self.nodes(L)[1][:, 2].astype(bool)
+
+    def apply(self, L, u, y=None, form=0):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        y = np.zeros_like(u) if y is None else np.ascontiguousarray(y, dtype=np.float64).copy()
+        lib().orc_apply(self.h, L, form, dp(u), dp(y))
+        return y
+
+    def sor(self, L, u, f, omega, sweeps=1, multicolour=False, backwards=False):
+        u = np.ascontiguousarray(u, dtype=np.float64).copy()
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        lib().orc_sor(self.h, L, dp(u), dp(f), omega, sweeps, 1 if multicolour else 0, 1 if backwards else 0)
+        return u
+
+    def sor_phases(self, L, u, f, omega, kind_mask, multicolour=False, backwards=False):
+        u = np.ascontiguousarray(u, dtype=np.float64).copy()
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        lib().orc_sor_phases(self.h, L, dp(u), dp(f), omega, 1 if multicolour else 0, 1 if backwards else 0, kind_mask)
+        return u
+
+    def restrict(self, Lf, fine, coarse=None):
+        fine = np.ascontiguousarray(fine, dtype=np.float64)
+        coarse = np.zeros(self.n(Lf - 1)) if coarse is None else np.ascontiguousarray(coarse, dtype=np.float64).copy()
+        lib().orc_restrict(self.h, Lf, dp(fine), dp(coarse))
+        return coarse
+
+    def prolongate(self, Lc, coarse, fine=None, add=False):
+        coarse = np.ascontiguousarray(coarse, dtype=np.float64)
+        fine = np.zeros(self.n(Lc + 1)) if fine is None else np.ascontiguousarray(fine, dtype=np.float64).copy()
+        lib().orc_prolongate(self.h, Lc, dp(coarse), dp(fine), 1 if add else 0)
+        return fine
+
+    def dot(self, L, a, b):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        return lib().orc_dot(self.h, L, dp(a), dp(b))
+
+    def cg(self, L, x, b, max_iter, tol):
+        x = np.ascontiguousarray(x, dtype=np.float64).copy()
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        res = c_double()
+        it = lib().orc_cg(self.h, L, dp(x), dp(b), max_iter, tol, ctypes.byref(res))
+        return x, it, res.value
+
+    def gmg(self, L, minL, x, b, cycles, pre=3, post=3, omega=1.0, multicolour=False, cg_iter=10000, cg_tol=1e-16):
+        x = np.ascontiguousarray(x, dtype=np.float64).copy()
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        res = np.zeros(cycles)
+        lib().orc_gmg(self.h, L, minL, dp(x), dp(b), cycles, pre, post, omega, 1 if multicolour else 0, cg_iter, cg_tol,
+                      dp(res))
+        return x, res
+
+    def cell_local_stencil(self, L, cell, x, y, z, form=0):
+        out = np.zeros(15)
+        lib().orc_cell_local_stencil(self.h, L, cell, x, y, z, form, dp(out))
+        return out
+
+
+def element_laplace(coords4x3):
+    c = np.ascontiguousarray(coords4x3, dtype=np.float64).reshape(12)
+    K = np.zeros(16)
+    lib().orc_element_laplace(dp(c), dp(K))
+    return K.reshape(4, 4)
+
+
+def element_mass(coords4x3):
+    c = np.ascontiguousarray(coords4x3, dtype=np.float64).reshape(12)
+    K = np.zeros(16)
+    lib().orc_element_mass(dp(c), dp(K))
+    return K.reshape(4, 4)
+
+
+def cuboid_mesh(lo, hi, nx, ny, nz):
+    """Restatement of MeshInfo::meshCuboid (src/hyteg/mesh/MeshGenCuboid.cpp:32-171): vertex
+    coordinates and the six tetrahedra per sub-cube in their frame order."""
+    lo = np.asarray(lo, dtype=np.float64)
+    hi = np.asarray(hi, dtype=np.float64)
+    h = (hi - lo) / np.array([nx, ny, nz])
+    coords = []
+    for iz in range(nz + 1):
+        for iy in range(ny + 1):
+            for ix in range(nx + 1):
+                coords.append(lo + h * np.array([ix, iy, iz]))
+    tnode = [[4, 5, 7, 3], [0, 3, 1, 4], [4, 1, 5, 3], [5, 6, 7, 2], [1, 3, 2, 5], [7, 2, 3, 5]]
+    off = [[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]]
+
+    def vid(i, j, k):
+        return k * (nx + 1) * (ny + 1) + j * (nx + 1) + i
+
+    tets = []
+    for iz in range(nz):
+        for iy in range(ny):
+            for ix in range(nx):
+                for t in range(6):
+                    tets.append([vid(ix + off[m][0], iy + off[m][1], iz + off[m][2]) for m in tnode[t]])
+    return np.array(coords), np.array(tets, dtype=np.int32)
