@@ -1,0 +1,430 @@
+"""Benchmark of the B200 matrix-free P1 geometric-multigrid hot path.
+
+Workload (one GPU): P1 Poisson on the unit cube split into 2x2x2 sub-cubes of 6 tetrahedra
+(48 macro-cells, meshCuboid), uniformly refined to level 8 (133,432,831 inner DoFs), FP64.
+One step = one V(3,3) multigrid cycle (multicolour SOR, omega = 1, linear transfers, CG on
+level 0) on a seeded uniform[-1,1] right-hand side; value = finest inner DoFs per second.
+Also reported: standalone kernels (apply, residual, SOR sweep, restriction, prolongation),
+the roofline of the dominant kernel (cell SOR), the time to a 1e-8 relative residual, an
+end-to-end figure through host buffers, and the reference's own CPU kernels as baseline.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--level L]
+
+With N > 1 (launched through torch.distributed.run) every rank solves an independent copy of
+the problem on its GPU (the path has no inter-GPU exchange in this build: replicas only).
+"""
+import argparse
+import concurrent.futures
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic bytes per inner DoF of the level the op writes (FP64)
+BYTES = {"apply": 16, "residual": 24, "sor_sweep": 24, "restrict_per_fine": 9, "prolongate_add_per_fine": 17}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--level", type=int, default=8)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def inner_dofs(L, n=2):
+    # interior lattice points of the (n 2^L + 1)^3 grid of the cube
+    m = n * 2 ** L - 1
+    return m ** 3
+
+
+def cell_inner_dofs(L, ncells=48):
+    N = 2 ** L
+    return ncells * (N - 1) * (N - 2) * (N - 3) // 6
+
+
+# ----------------------------------------------------------------------------------------
+# clocks during the timed region
+# ----------------------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                mx = max(mx, float(c[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------
+# reference CPU kernels (oracle/_ref, compiled from the reference's own generated kernels)
+# ----------------------------------------------------------------------------------------
+def reference_cpu_pass(L, steps, warmup, threads):
+    """Finest-level cell-interior work of one V(3,3) cycle on the 48 macro-cells of the cube
+    with the reference's generated kernels (sor_3D_macrocell_P1 x 6, apply (residual),
+    restrict_3D_macrocell_P1_pull_additive, prolongate_3D_macrocell_P1_push_additive),
+    parallel over macro-cells on `threads` host threads. Returns seconds per pass."""
+    from oracle import oracle
+    import hyteg_b200 as hg
+    ref = oracle.ref_lib()
+    if ref is None:
+        return None
+    mesh = hg.HostMesh.cuboid((0, 0, 0), (1, 1, 1), 2, 2, 2, L)
+    nv, ne, nf, nc = mesh.counts()
+    w = 2 ** L + 1
+    wc = 2 ** (L - 1) + 1
+    size = w * (w + 1) * (w + 2) // 6
+    csize = wc * (wc + 1) * (wc + 2) // 6
+    rng = np.random.default_rng(1)
+    cells = []
+    for c in range(nc):
+        st = np.ascontiguousarray(mesh.cell_stencil(L, 0, c))
+        verts = mesh.primitive(hg.CELL, c)[0]
+        ncount = lambda kind, prim: float(len(mesh.neighbours(kind, prim, hg.CELL)))  # noqa: E731
+        # neighbour counts of the cell's edges, faces and vertices (P1toP1LinearRestriction.cpp:186-233)
+        edges = [mesh.neighbours(hg.VERTEX, verts[a], hg.EDGE) for a in range(4)]
+        epairs = [(0, 1), (0, 2), (1, 2), (0, 3), (1, 3), (2, 3)]
+        eid = []
+        for a, b in epairs:
+            common = set(edges[a]) & set(edges[b])
+            eid.append(common.pop())
+        fverts = [(0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3)]
+        fid = []
+        for t in fverts:
+            s = set(mesh.neighbours(hg.VERTEX, verts[t[0]], hg.FACE))
+            for k in t[1:]:
+                s &= set(mesh.neighbours(hg.VERTEX, verts[k], hg.FACE))
+            fid.append(s.pop())
+        nE = np.array([ncount(hg.EDGE, e) for e in eid])
+        nF = np.array([ncount(hg.FACE, f) for f in fid])
+        nV = np.array([ncount(hg.VERTEX, v) for v in verts])
+        cells.append(dict(u=rng.uniform(-1, 1, size), f=rng.uniform(-1, 1, size), r=np.zeros(size),
+                          c=np.zeros(csize), w=st, nE=nE, nF=nF, nV=nV))
+    dp = oracle.dp
+
+    def work(cd):
+        for _ in range(3):
+            ref.ref_sor_cell(dp(cd["u"]), dp(cd["f"]), L, dp(cd["w"]), 1.0)
+        ref.ref_apply_cell(dp(cd["r"]), dp(cd["u"]), L, dp(cd["w"]), 0)
+        ref.ref_restrict_cell(dp(cd["c"]), dp(cd["r"]), L - 1, dp(cd["nE"]), dp(cd["nF"]), dp(cd["nV"]))
+        ref.ref_prolongate_cell(dp(cd["c"]), dp(cd["u"]), L - 1, dp(cd["nE"]), dp(cd["nF"]), dp(cd["nV"]))
+        for _ in range(3):
+            ref.ref_sor_cell(dp(cd["u"]), dp(cd["f"]), L, dp(cd["w"]), 1.0)
+
+    times = []
+    with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as ex:
+        for i in range(warmup + steps):
+            t0 = time.perf_counter()
+            list(ex.map(work, cells))
+            if i >= warmup:
+                times.append(time.perf_counter() - t0)
+    return times
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_sample_text(L):
+    return ("finest-level cell-interior work of one V(3,3) cycle (6 lexicographic SOR sweeps, residual, restriction, "
+            "prolongation) on the 48 macro-cells of the level-%d cube with the reference's generated kernels "
+            "(oracle/_ref), threads over macro-cells; faces/edges/vertices and coarser levels not included "
+            "(<3%% and ~1/7 of the work)" % L)
+
+
+# ----------------------------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(v, pg):
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_setup(args)
+    L = args.level
+    out = None
+    if rank == 0:
+        from oracle import oracle
+        if oracle.ref_lib() is None:
+            out = {"impl": "reference", "unavailable": "oracle/_ref (reference kernels) was not built"}
+        else:
+            thr = host_threads()
+            times = reference_cpu_pass(L, args.steps, args.warmup, thr)
+            t = float(np.mean(times))
+            v = inner_dofs(L) / t / 1e9
+            out = {"impl": "reference", "metric": "GDoF/s", "value": v, "unit": "GDoF/s", "n_gpus": args.gpus,
+                   "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+                   "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                   "config": workload_config(L),
+                   "cpu_baseline": {"value": v, "unit": "GDoF/s", "cores": thr, "kind": "reference",
+                                    "sample": reference_sample_text(L)},
+                   "e2e": {"value": v, "unit": "GDoF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def workload_config(L):
+    return {"workload": "P1 Poisson GMG V(3,3) cycle, 48-tet unit cube (meshCuboid 2x2x2), level %d, FP64, "
+                        "multicolour SOR omega=1, linear transfers, CG on level 0" % L,
+            "level": L, "macro_cells": 48, "inner_dofs": inner_dofs(L),
+            "l2": "inputs larger than L2 (%.2f GB per vector)" % (inner_dofs(L) * 8 / 1e9),
+            "parallelism": "replicas"}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def load_traffic(kernel):
+    """Per-launch DRAM bytes of `kernel` at the benchmark level from profiles/<kernel>_traffic.json."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+def run_ours(args):
+    import torch
+    import hyteg_b200 as hg
+
+    world, rank, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    L = args.level
+    N_in = inner_dofs(L)
+    st = hg.PrimitiveStorage.cuboid((0, 0, 0), (1, 1, 1), 2, 2, 2, L)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    st.set_stream(stream.cuda_stream)
+
+    A = hg.P1ConstantLaplaceOperator(st, 0, L)
+    x = hg.P1Function("x", st, 0, L)
+    b = hg.P1Function("b", st, 0, L)
+    r = hg.P1Function("r", st, 0, L)
+    t = hg.P1Function("t", st, 0, L)
+    n = st.level_size(L)
+    rng = np.random.default_rng(42 + rank)
+    host_b = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    host_b.numpy()[:] = rng.uniform(-1.0, 1.0, n)
+    b.from_numpy(L, host_b.numpy())
+    b.communicate(L)
+    gmg = hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 50, 1e-16),
+                                      hg.P1toP1LinearRestriction(), hg.P1toP1LinearProlongation(), 0, L, 3, 3)
+    Inner = hg.Inner | hg.NeumannBoundary
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps * 1e-3
+
+    # --- standalone kernels on the seeded source vector ----------------------------------
+    x.from_numpy(L, host_b.numpy())
+    kern = {}
+    kern["apply"] = timed(lambda: A.apply(x, r, L, Inner), 5)
+    kern["residual"] = timed(lambda: A.residual(x, b, r, L, Inner), 5)
+    kern["sor_sweep"] = timed(lambda: A.smooth_sor(x, b, 1.0, L, Inner), 3)
+    kern["restrict"] = timed(lambda: hg.P1toP1LinearRestriction().restrict(r, L, Inner), 5)
+    kern["prolongate_add"] = timed(lambda: hg.P1toP1LinearProlongation().prolongateAndAdd(x, L - 1, Inner), 5)
+    kern["halo_refresh"] = timed(lambda: x.communicate(L), 5)
+    # dominant kernel alone: cell SOR (4 colour launches per sweep) and cell apply
+    t_sor_cells = timed(lambda: A.smooth_sor_primitives(x, b, 1.0, L, Inner, kinds=1 << hg.CELL, refresh=False), 3)
+    t_apply_cells = timed(lambda: A.apply_primitives(x, r, L, Inner, kinds=1 << hg.CELL, refresh=False), 5)
+    Nc = cell_inner_dofs(L)
+    kernels = {k: {"ms": v * 1e3, "gdofs": N_in / v / 1e9} for k, v in kern.items()}
+    for k in ("apply", "residual", "sor_sweep"):
+        kernels[k]["GBs_algorithmic"] = BYTES[k] * N_in / kern[k] / 1e9
+    kernels["cell_sor_colour_launch"] = {"ms": t_sor_cells / 4 * 1e3,
+                                         "GBs_algorithmic": BYTES["sor_sweep"] * Nc / 4 / (t_sor_cells / 4) / 1e9}
+    kernels["cell_apply_launch"] = {"ms": t_apply_cells * 1e3, "GBs_algorithmic": BYTES["apply"] * Nc / t_apply_cells / 1e9}
+
+    # --- time to 1e-8 relative residual, FP64 GMG from x = 0 -------------------------------
+    def rel_res():
+        A.residual(x, b, r, L, Inner)
+        return np.sqrt(r.dotGlobal(r, L, Inner))
+
+    x.interpolate(0.0, L, hg.All)
+    r0 = rel_res()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    cycles, rel, hist = 0, 1.0, []
+    while rel > 1e-8 and cycles < 50:
+        gmg.solve(A, x, b, L)
+        cycles += 1
+        rel = rel_res() / r0
+        hist.append(rel)
+    torch.cuda.synchronize()
+    t_solve = time.perf_counter() - t0
+    factors = [hist[i + 1] / hist[i] for i in range(len(hist) - 1)]
+
+    # --- the timed region: K V(3,3) cycles --------------------------------------------------
+    for _ in range(args.warmup):
+        gmg.solve(A, x, b, L)
+    launches0 = st.launch_count()
+    barrier(pg)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        for _ in range(args.steps):
+            gmg.solve(A, x, b, L)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    t_steps = e0.elapsed_time(e1) * 1e-3
+    launches = st.launch_count() - launches0
+    barrier(pg)
+    t_max = max_over_ranks(t_steps, pg)
+    ms = t_max / args.steps * 1e3
+    value = world * N_in * args.steps / t_max / 1e9
+
+    # --- end to end through the public API with host buffers --------------------------------
+    torch.cuda.synchronize()
+    barrier(pg)
+    e0, e1 = ev(), ev()
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.from_numpy(L, host_b.numpy())        # H2D of the step's input from pinned memory
+        gmg.solve(A, x, b, L)
+        A.residual(x, b, r, L, Inner)
+        _ = r.dotGlobal(r, L, Inner)           # D2H of the step's result (residual norm)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = max_over_ranks(e0.elapsed_time(e1) * 1e-3, pg)
+
+    peak, peak_kind = load_peaks()
+    t_launch = t_sor_cells / 4
+    achieved = BYTES["sor_sweep"] * Nc / 4 / t_launch / 1e9
+    traffic = load_traffic("cellSorKernel")
+    out = {
+        "metric": "GDoF/s", "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform[-1,1] right-hand side)",
+        "config": workload_config(L),
+        "roofline": {"kernel": "cellSorKernel<double> (one colour of the cell-interior SOR sweep)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": BYTES["sor_sweep"] * Nc / 4},
+        "e2e": {"value": world * N_in * args.steps / t_e2e / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": n * 8,
+                "d2h_bytes_per_step": 8},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "kernels": kernels,
+        "solve": {"precision": "fp64", "target_rel_residual": 1e-8, "cycles": cycles, "seconds": t_solve,
+                  "final_rel_residual": rel, "convergence_factors": factors},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        thr = host_threads()
+        times = reference_cpu_pass(L, 1, 0, thr)
+        if times:
+            out["cpu_baseline"] = {"value": inner_dofs(L) / times[0] / 1e9, "unit": "GDoF/s", "cores": thr,
+                                   "kind": "reference", "sample": reference_sample_text(L)}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    del gmg
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

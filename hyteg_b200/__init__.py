@@ -64,9 +64,12 @@ class HostMesh:
         return cls(h, max_level)
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            _capi.lib.hg_mesh_destroy(self._h)
-            self._h = None
+        try:
+            if getattr(self, "_h", None):
+                _capi.lib.hg_mesh_destroy(self._h)
+                self._h = None
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
 
     def counts(self):
         c = np.zeros(4, dtype=np.int32)
@@ -171,7 +174,10 @@ class PrimitiveStorage:
             self._h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
 
     @property
     def handle(self):
@@ -207,6 +213,11 @@ class PrimitiveStorage:
     def synchronize(self):
         call("hg_storage_synchronize", self._h)
 
+    def launch_count(self):
+        n = ctypes.c_ulonglong()
+        call("hg_storage_launch_count", self._h, ctypes.byref(n))
+        return n.value
+
     def level_size(self, level):
         n = ctypes.c_int64()
         call("hg_level_size", self._h, level, ctypes.byref(n))
@@ -234,9 +245,12 @@ class P1Function:
         self.id = h.value
 
     def __del__(self):
-        st = getattr(self, "storage", None)
-        if st is not None and st.handle:
-            _capi.lib.hg_function_destroy(st.handle, self.id)
+        try:
+            st = getattr(self, "storage", None)
+            if st is not None and st.handle:
+                _capi.lib.hg_function_destroy(st.handle, self.id)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
 
     def device_ptr(self, level):
         p = ctypes.c_void_p()
@@ -317,14 +331,22 @@ class _P1ConstantOperator:
         self.id = h.value
 
     def __del__(self):
-        st = getattr(self, "storage", None)
-        if st is not None and st.handle:
-            _capi.lib.hg_operator_destroy(st.handle, self.id)
+        try:
+            st = getattr(self, "storage", None)
+            if st is not None and st.handle:
+                _capi.lib.hg_operator_destroy(st.handle, self.id)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
 
     def apply(self, src, dst, level, flag, updateType=Replace):
         if src is dst:
             raise ValueError("apply: src and dst must be different functions")
         call("hg_apply", self.storage.handle, self.id, src.id, dst.id, level, flag, updateType)
+
+    def apply_primitives(self, src, dst, level, flag, updateType=Replace, kinds=15, refresh=True):
+        """Only the kernels of the selected primitive kinds (bit set over VERTEX..CELL)."""
+        call("hg_apply_primitives", self.storage.handle, self.id, src.id, dst.id, level, flag, updateType, kinds,
+             1 if refresh else 0)
 
     def residual(self, x, b, r, level, flag):
         """r = b - A x (fused apply + assign of GeometricMultigridSolver.hpp:185-186)."""
@@ -335,6 +357,11 @@ class _P1ConstantOperator:
 
     def smooth_sor_backwards(self, dst, rhs, relax, level, flag):
         call("hg_smooth_sor", self.storage.handle, self.id, dst.id, rhs.id, float(relax), level, flag, 1)
+
+    def smooth_sor_primitives(self, dst, rhs, relax, level, flag, kinds=15, refresh=True, backwards=False):
+        """The SOR phases of the selected primitive kinds only (bit set over VERTEX..CELL)."""
+        call("hg_smooth_sor_primitives", self.storage.handle, self.id, dst.id, rhs.id, float(relax), level, flag,
+             1 if backwards else 0, kinds, 1 if refresh else 0)
 
     def smooth_gs(self, dst, rhs, level, flag):
         self.smooth_sor(dst, rhs, 1.0, level, flag)
@@ -422,7 +449,10 @@ class GeometricMultigridSolver:
         call("hg_gmg_solve", self.storage.handle, self._handle(A), x.id, b.id, level)
 
     def __del__(self):
-        st = getattr(self, "storage", None)
-        if st is not None and st.handle:
-            for h in self._cache.values():
-                _capi.lib.hg_gmg_destroy(st.handle, h)
+        try:
+            st = getattr(self, "storage", None)
+            if st is not None and st.handle:
+                for h in self._cache.values():
+                    _capi.lib.hg_gmg_destroy(st.handle, h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass

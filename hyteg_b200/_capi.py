@@ -40,6 +40,7 @@ _SIGS = {
     "hg_storage_counts": (c_int, [c_void_p, P(c_int)]),
     "hg_storage_set_stream": (c_int, [c_void_p, c_void_p]),
     "hg_storage_synchronize": (c_int, [c_void_p]),
+    "hg_storage_launch_count": (c_int, [c_void_p, P(ctypes.c_ulonglong)]),
     "hg_storage_set_cell_coefficients": (c_int, [c_void_p, P(c_double), c_int]),
     "hg_primitive_vertices": (c_int, [c_void_p, c_int, c_int, P(c_int), P(c_double), P(c_int)]),
     "hg_primitive_neighbours": (c_int, [c_void_p, c_int, c_int, c_int, P(c_int), c_int, P(c_int)]),
@@ -73,8 +74,10 @@ _SIGS = {
     "hg_operator_create": (c_int, [c_void_p, c_int, c_int, c_int, P(c_int)]),
     "hg_operator_destroy": (c_int, [c_void_p, c_int]),
     "hg_apply": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_uint, c_int]),
+    "hg_apply_primitives": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_uint, c_int, c_int, c_int]),
     "hg_residual": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_uint]),
     "hg_smooth_sor": (c_int, [c_void_p, c_int, c_int, c_int, c_double, c_int, c_uint, c_int]),
+    "hg_smooth_sor_primitives": (c_int, [c_void_p, c_int, c_int, c_int, c_double, c_int, c_uint, c_int, c_int, c_int]),
     "hg_restrict": (c_int, [c_void_p, c_int, c_int, c_uint]),
     "hg_prolongate": (c_int, [c_void_p, c_int, c_int, c_uint, c_int]),
     "hg_cg_solve": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, P(c_int), P(c_double)]),

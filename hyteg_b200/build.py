@@ -1,6 +1,7 @@
 """Builds the in-tree shared library hyteg_b200/libhyteg_b200.so for sm_100a with nvcc.
 
-Usage: python -m hyteg_b200.build   (or build() from Python). Objects are compiled in
+Usage: python hyteg_b200/build.py   (run by path: importing the package would load the
+library before it is rebuilt). Objects are compiled in
 parallel into hyteg_b200/_build/ and only rebuilt when a source or header changed.
 """
 import concurrent.futures

@@ -131,6 +131,12 @@ int hg_storage_synchronize(hg_storage* h) {
   HG_CATCH
 }
 
+int hg_storage_launch_count(const hg_storage* h, unsigned long long* count) {
+  HG_TRY
+  *count = S(h).launches;
+  HG_CATCH
+}
+
 int hg_storage_set_cell_coefficients(hg_storage* h, const double* k, int ncells) {
   HG_TRY
   hg::Storage& s = S(h);
@@ -315,6 +321,15 @@ int hg_apply(hg_storage* h, int op, int src, int dst, int level, unsigned flag, 
   HG_CATCH
 }
 
+int hg_apply_primitives(hg_storage* h, int op, int src, int dst, int level, unsigned flag, int update, int kinds,
+                        int refresh) {
+  HG_TRY
+  hg::argCheck(update == 0 || update == 1, "update must be 0 (Replace) or 1 (Add)");
+  hg::argCheck(kinds > 0 && kinds < 16, "kinds must be a non-empty subset of {vertex, edge, face, cell}");
+  S(h).apply(op, src, dst, level, flag, update, kinds, refresh != 0);
+  HG_CATCH
+}
+
 int hg_residual(hg_storage* h, int op, int x, int b, int r, int level, unsigned flag) {
   HG_TRY
   S(h).residual(op, x, b, r, level, flag);
@@ -325,6 +340,15 @@ int hg_smooth_sor(hg_storage* h, int op, int dst, int rhs, double omega, int lev
   HG_TRY
   hg::argCheck(omega > 0.0 && omega < 2.0, "relaxation must lie in (0, 2)");
   S(h).smoothSor(op, dst, rhs, omega, level, flag, backwards != 0);
+  HG_CATCH
+}
+
+int hg_smooth_sor_primitives(hg_storage* h, int op, int dst, int rhs, double omega, int level, unsigned flag,
+                             int backwards, int kinds, int refresh) {
+  HG_TRY
+  hg::argCheck(omega > 0.0 && omega < 2.0, "relaxation must lie in (0, 2)");
+  hg::argCheck(kinds > 0 && kinds < 16, "kinds must be a non-empty subset of {vertex, edge, face, cell}");
+  S(h).smoothSor(op, dst, rhs, omega, level, flag, backwards != 0, kinds, refresh != 0);
   HG_CATCH
 }
 

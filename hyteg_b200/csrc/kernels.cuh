@@ -19,11 +19,8 @@ namespace dev {
 
 constexpr int kBlock = 256;
 
-struct CellBlock {
-  int cell, z, start, pad;
-};
 struct FaceBlock {
-  int face, start;
+  int face, start;  // rows [start, start + kFaceRows) of the face interior
 };
 struct LowBlock {
   int prim, start;
@@ -47,8 +44,7 @@ struct LevelDev {
   const unsigned char* cellType;
   const unsigned char* faceType;
   const unsigned char* lowType;
-  const CellBlock* cellBlocks;
-  int nCellBlocks;
+  int nCellBlocks;  // nCells * (N - 3) blocks (one per macro-cell and z-plane), 0 below level 2
   const FaceBlock* faceBlocks;
   int nFaceBlocks;
   const LowBlock* lowBlocks;
@@ -73,85 +69,127 @@ __device__ __forceinline__ int rowStart(int W, int y) { return y * (W + 1) - (y 
 __device__ __forceinline__ int64_t tetSize(int64_t w) { return w * (w + 1) * (w + 2) / 6; }
 __device__ __forceinline__ int triSize(int w) { return w * (w + 1) / 2; }
 
-// Row y of the offset `off` inside a triangular plane of width W.
-__device__ __forceinline__ int decodeRow(int W, int off) {
-  const float t = float(2 * W + 1);
-  int y = int((t - __fsqrt_rn(t * t - 8.0f * float(off))) * 0.5f);
-  y = max(y, 0);
-  if (rowStart(W, y) > off) --y;
-  if (rowStart(W, y + 1) <= off) ++y;
-  return y;
+// ---------------------------------------------------------------------------------------
+// Cell interiors. One block per (macro-cell, z-plane); the warps of a block walk the rows y
+// of the plane and the lanes the x positions of a row. All neighbour rows of a row are
+// addressed from six row bases computed once per row (cell layout of
+// indexing/MacroCellIndexing.hpp:40-52):
+//   r0  (0, y, z)     rN (0, y+1, z)    rS (0, y-1, z)
+//   rT  (0, y, z+1)   rTS (0, y-1, z+1)
+//   rB  (0, y, z-1)   rBN (0, y+1, z-1)
+// Consecutive blocks are neighbouring planes, so the z-1 / z+1 rows a block reads are those
+// its neighbours stream in: each value comes from HBM about once and from L2 about three times.
+// ---------------------------------------------------------------------------------------
+struct CellRow {
+  int r0, rN, rS, rT, rTS, rB, rBN;
+};
+
+__device__ __forceinline__ CellRow cellRow(int w, int z, int y) {
+  const int W = w - z;
+  CellRow r;
+  r.r0 = int(tetSize(w) - tetSize(W)) + rowStart(W, y);
+  r.rN = r.r0 + (W - y);
+  r.rS = r.r0 - (W - y + 1);
+  r.rT = r.r0 + triSize(W) - y;
+  r.rTS = r.rT - (W - y);
+  r.rB = r.r0 - triSize(W + 1) + y;
+  r.rBN = r.rB + (W + 1 - y);
+  return r;
 }
 
-// Absolute indices of the 15 stencil neighbours of the cell point with plane-local row y,
-// plane width W (= w - z) and absolute index c. Order: C E W N S NW SE TC TW TS TSE BC BE BN BNW.
-__device__ __forceinline__ void cellNeighbours(int64_t c, int W, int y, int64_t n[15]) {
-  const int64_t up = c + triSize(W) - y;           // (x, y, z+1)
-  const int64_t dn = c - triSize(W + 1) + y;       // (x, y, z-1)
-  n[0] = c;
-  n[1] = c + 1;
-  n[2] = c - 1;
-  n[3] = c + (W - y);
-  n[4] = c - (W - y + 1);
-  n[5] = n[3] - 1;
-  n[6] = n[4] + 1;
-  n[7] = up;
-  n[8] = up - 1;
-  n[9] = up - (W - y);
-  n[10] = n[9] + 1;
-  n[11] = dn;
-  n[12] = dn + 1;
-  n[13] = dn + (W + 1 - y);
-  n[14] = n[13] - 1;
+// sum_{k >= 1} w_k u(x + d_k) in the order E W N S NW SE TC TW TS TSE BC BE BN BNW
+template <class T, class LD>
+__device__ __forceinline__ T cellOffDiag(const T* wt, const CellRow& r, int x, LD ld) {
+  T s = wt[1] * ld(r.r0 + x + 1);
+  s += wt[2] * ld(r.r0 + x - 1);
+  s += wt[3] * ld(r.rN + x);
+  s += wt[4] * ld(r.rS + x);
+  s += wt[5] * ld(r.rN + x - 1);
+  s += wt[6] * ld(r.rS + x + 1);
+  s += wt[7] * ld(r.rT + x);
+  s += wt[8] * ld(r.rT + x - 1);
+  s += wt[9] * ld(r.rTS + x);
+  s += wt[10] * ld(r.rTS + x + 1);
+  s += wt[11] * ld(r.rB + x);
+  s += wt[12] * ld(r.rB + x + 1);
+  s += wt[13] * ld(r.rBN + x);
+  s += wt[14] * ld(r.rBN + x - 1);
+  return s;
 }
 
-// ---------------------------------------------------------------------------------------
-// Stencil application on cell interiors: dst = A src | dst += A src | dst = rhs - A src
-// ---------------------------------------------------------------------------------------
+// dst = A src | dst += A src | dst = rhs - A src on cell interiors. The weights live in shared
+// memory (broadcast reads) and every lane handles two points per iteration, so up to 30
+// independent loads per thread are in flight.
 template <class T, int MODE>
-__global__ void __launch_bounds__(kBlock) cellStencilKernel(LevelDev lv, const T* __restrict__ cellW,
-                                                            T* __restrict__ dst, const T* __restrict__ src,
-                                                            const T* __restrict__ rhs, unsigned mask) {
-  const CellBlock b = lv.cellBlocks[blockIdx.x];
-  if (!(lv.cellType[b.cell] & mask)) return;
-  const int W = lv.w - b.z;
-  const int off = b.start + threadIdx.x;
-  const int y = decodeRow(W, off);
-  const int x = off - rowStart(W, y);
-  if (y < 1 || x < 1 || x + y > W - 2) return;
-  const int64_t c = lv.cellOff[b.cell] + (tetSize(lv.w) - tetSize(W)) + off;
-  int64_t n[15];
-  cellNeighbours(c, W, y, n);
-  const T* wt = cellW + 16 * b.cell;
-  T s = wt[0] * __ldg(src + n[0]);
-#pragma unroll
-  for (int k = 1; k < 15; ++k) s += wt[k] * __ldg(src + n[k]);
-  if (MODE == MODE_REPLACE) dst[c] = s;
-  else if (MODE == MODE_ADD) dst[c] += s;
-  else dst[c] = rhs[c] - s;
+__global__ void __launch_bounds__(kBlock, 4) cellStencilKernel(LevelDev lv, const T* __restrict__ cellW,
+                                                               T* __restrict__ dst, const T* __restrict__ src,
+                                                               const T* __restrict__ rhs, unsigned mask) {
+  const int nPl = lv.N - 3;
+  const int c = blockIdx.x / nPl, z = 1 + blockIdx.x % nPl;
+  if (!(lv.cellType[c] & mask)) return;
+  __shared__ T wt[16];
+  if (threadIdx.x < 15) wt[threadIdx.x] = cellW[16 * c + threadIdx.x];
+  __syncthreads();
+  const int64_t base = lv.cellOff[c];
+  const T* __restrict__ u = src + base;
+  T* __restrict__ d = dst + base;
+  const T* __restrict__ f = rhs + base;
+  const int W = lv.w - z;
+  auto ld = [u](int i) { return __ldg(u + i); };
+  for (int y = 1 + (int)(threadIdx.x >> 5); y <= W - 3; y += kBlock / 32) {
+    const CellRow r = cellRow(lv.w, z, y);
+    const int len = W - 2 - y;
+    for (int x = 1 + (int)(threadIdx.x & 31); x <= len; x += 64) {
+      const int x2 = x + 32;
+      const bool two = x2 <= len;
+      const T s1 = wt[0] * ld(r.r0 + x) + cellOffDiag(wt, r, x, ld);
+      const T s2 = two ? wt[0] * ld(r.r0 + x2) + cellOffDiag(wt, r, x2, ld) : T(0);
+      if (MODE == MODE_REPLACE) {
+        d[r.r0 + x] = s1;
+        if (two) d[r.r0 + x2] = s2;
+      } else if (MODE == MODE_ADD) {
+        d[r.r0 + x] += s1;
+        if (two) d[r.r0 + x2] += s2;
+      } else {
+        d[r.r0 + x] = f[r.r0 + x] - s1;
+        if (two) d[r.r0 + x2] = f[r.r0 + x2] - s2;
+      }
+    }
+  }
 }
 
-// Multicolour SOR on cell interiors, colour = (x + 2y + 3z) mod 4.
+// Multicolour SOR on cell interiors, colour = (x + 2y + 3z) mod 4: the lanes of a warp step
+// over the x positions of the active colour only (every fourth point of a row), two per lane.
 template <class T>
-__global__ void __launch_bounds__(kBlock) cellSorKernel(LevelDev lv, const T* __restrict__ cellW, T* u,
-                                                        const T* __restrict__ rhs, unsigned mask, int colour,
-                                                        T omega) {
-  const CellBlock b = lv.cellBlocks[blockIdx.x];
-  if (!(lv.cellType[b.cell] & mask)) return;
-  const int W = lv.w - b.z;
-  const int off = b.start + threadIdx.x;
-  const int y = decodeRow(W, off);
-  const int x = off - rowStart(W, y);
-  if (y < 1 || x < 1 || x + y > W - 2) return;
-  if (((x + 2 * y + 3 * b.z) & 3) != colour) return;
-  const int64_t c = lv.cellOff[b.cell] + (tetSize(lv.w) - tetSize(W)) + off;
-  int64_t n[15];
-  cellNeighbours(c, W, y, n);
-  const T* wt = cellW + 16 * b.cell;
-  T s = rhs[c];
-#pragma unroll
-  for (int k = 1; k < 15; ++k) s -= wt[k] * u[n[k]];
-  u[c] = (T(1) - omega) * u[c] + (s * omega) / wt[0];
+__global__ void __launch_bounds__(kBlock, 4) cellSorKernel(LevelDev lv, const T* __restrict__ cellW, T* u,
+                                                           const T* __restrict__ rhs, unsigned mask, int colour,
+                                                           T omega, int cellBegin) {
+  const int nPl = lv.N - 3;
+  const int c = cellBegin + blockIdx.x / nPl, z = 1 + blockIdx.x % nPl;
+  if (!(lv.cellType[c] & mask)) return;
+  __shared__ T wt[16];
+  if (threadIdx.x < 15) wt[threadIdx.x] = cellW[16 * c + threadIdx.x];
+  __syncthreads();
+  const int64_t base = lv.cellOff[c];
+  T* uc = u + base;
+  const T* __restrict__ f = rhs + base;
+  const T om = omega, om1 = T(1) - omega, dinv = omega / wt[0];
+  const int W = lv.w - z;
+  auto ld = [uc](int i) { return uc[i]; };
+  for (int y = 1 + (int)(threadIdx.x >> 5); y <= W - 3; y += kBlock / 32) {
+    const CellRow r = cellRow(lv.w, z, y);
+    const int len = W - 2 - y;
+    const int x0 = 1 + (((colour - 2 * y - 3 * z - 1) % 4) + 4) % 4;
+    for (int x = x0 + 4 * (int)(threadIdx.x & 31); x <= len; x += 256) {
+      const int x2 = x + 128;
+      const bool two = x2 <= len;
+      const T s1 = f[r.r0 + x] - cellOffDiag(wt, r, x, ld);
+      const T s2 = two ? f[r.r0 + x2] - cellOffDiag(wt, r, x2, ld) : T(0);
+      uc[r.r0 + x] = om1 * uc[r.r0 + x] + (s1 * om) / wt[0];
+      if (two) uc[r.r0 + x2] = om1 * uc[r.r0 + x2] + (s2 * om) / wt[0];
+    }
+  }
+  (void)dinv;
 }
 
 // Full-weighting restriction at coarse cell-interior points: coarse = fine[2p] + 1/2 sum fine[2p+d]
@@ -159,78 +197,97 @@ __global__ void __launch_bounds__(kBlock) cellSorKernel(LevelDev lv, const T* __
 template <class T>
 __global__ void __launch_bounds__(kBlock) cellRestrictKernel(LevelDev lc, LevelDev lf, T* __restrict__ coarse,
                                                              const T* __restrict__ fine, unsigned mask) {
-  const CellBlock b = lc.cellBlocks[blockIdx.x];
-  if (!(lc.cellType[b.cell] & mask)) return;
-  const int W = lc.w - b.z;
-  const int off = b.start + threadIdx.x;
-  const int y = decodeRow(W, off);
-  const int x = off - rowStart(W, y);
-  if (y < 1 || x < 1 || x + y > W - 2) return;
-  const int zf = 2 * b.z, yf = 2 * y, xf = 2 * x;
-  const int Wf = lf.w - zf;
-  const int64_t cf = lf.cellOff[b.cell] + (tetSize(lf.w) - tetSize(Wf)) + rowStart(Wf, yf) + xf;
-  int64_t n[15];
-  cellNeighbours(cf, Wf, yf, n);
-  T s = T(0);
-#pragma unroll
-  for (int k = 1; k < 15; ++k) s += __ldg(fine + n[k]);
-  coarse[lc.cellOff[b.cell] + (tetSize(lc.w) - tetSize(W)) + off] = __ldg(fine + n[0]) + T(0.5) * s;
+  const int nPl = lc.N - 3;
+  const int c = blockIdx.x / nPl, z = 1 + blockIdx.x % nPl;
+  if (!(lc.cellType[c] & mask)) return;
+  const T* __restrict__ uf = fine + lf.cellOff[c];
+  T* __restrict__ uc = coarse + lc.cellOff[c];
+  const T one[15] = {T(1), T(1), T(1), T(1), T(1), T(1), T(1), T(1), T(1), T(1), T(1), T(1), T(1), T(1), T(1)};
+  const int W = lc.w - z;
+  auto ld = [uf](int i) { return __ldg(uf + i); };
+  for (int y = 1 + (int)(threadIdx.x >> 5); y <= W - 3; y += kBlock / 32) {
+    const CellRow rf = cellRow(lf.w, 2 * z, 2 * y);
+    const int rc = int(tetSize(lc.w) - tetSize(W)) + rowStart(W, y);
+    const int len = W - 2 - y;
+    for (int x = 1 + (int)(threadIdx.x & 31); x <= len; x += 32)
+      uc[rc + x] = ld(rf.r0 + 2 * x) + T(0.5) * cellOffDiag(one, rf, 2 * x, ld);
+  }
 }
 
-__device__ __forceinline__ int64_t cellIndexDev(int w, int x, int y, int z) {
+__device__ __forceinline__ int cellIndexDev(int w, int x, int y, int z) {
   const int W = w - z;
-  return (tetSize(w) - tetSize(W)) + rowStart(W, y) + x;
+  return int(tetSize(w) - tetSize(W)) + rowStart(W, y) + x;
 }
 
 // Linear prolongation at fine cell-interior points (prolongate_3D_macrocell_P1_push_additive.cpp):
 // even points copy the coarse value, every other point is the mean of the two coarse end
-// points of the coarse micro-edge it bisects.
+// points of the coarse micro-edge it bisects. The bisected direction depends on the parity of
+// (x, y, z); for one fine row only the x parity varies, so two row pairs are set up per row.
 template <class T, bool ADD>
 __global__ void __launch_bounds__(kBlock) cellProlongKernel(LevelDev lf, LevelDev lc, T* __restrict__ fine,
                                                             const T* __restrict__ coarse, unsigned mask) {
-  const CellBlock b = lf.cellBlocks[blockIdx.x];
-  if (!(lf.cellType[b.cell] & mask)) return;
-  const int W = lf.w - b.z;
-  const int off = b.start + threadIdx.x;
-  const int y = decodeRow(W, off);
-  const int x = off - rowStart(W, y);
-  if (y < 1 || x < 1 || x + y > W - 2) return;
-  const int z = b.z;
-  const int px = x & 1, py = y & 1, pz = z & 1;
-  int dx = 0, dy = 0, dz = 0;
-  const int code = px | (py << 1) | (pz << 2);
-  switch (code) {
-    case 1: dx = 1; break;
-    case 2: dy = 1; break;
-    case 4: dz = 1; break;
-    case 3: dx = -1; dy = 1; break;
-    case 5: dx = -1; dz = 1; break;
-    case 6: dy = -1; dz = 1; break;
-    case 7: dx = -1; dy = 1; dz = -1; break;
-    default: break;
+  const int nPl = lf.N - 3;
+  const int c = blockIdx.x / nPl, z = 1 + blockIdx.x % nPl;
+  if (!(lf.cellType[c] & mask)) return;
+  T* __restrict__ uf = fine + lf.cellOff[c];
+  const T* __restrict__ uc = coarse + lc.cellOff[c];
+  const int W = lf.w - z;
+  // directions of the bisected coarse micro-edge by parity code (x | y << 1 | z << 2)
+  const int DX[8] = {0, 1, 0, -1, 0, -1, 0, -1};
+  const int DY[8] = {0, 0, 1, 1, 0, 0, -1, 1};
+  const int DZ[8] = {0, 0, 0, 0, 1, 1, 1, -1};
+  for (int y = 1 + (int)(threadIdx.x >> 5); y <= W - 3; y += kBlock / 32) {
+    const int rf = int(tetSize(lf.w) - tetSize(W)) + rowStart(W, y);
+    const int len = W - 2 - y;
+    // for x parity p: coarse row base of end point a (x offset (x - dx) / 2) and of b = a + d
+    int ra[2], rb[2], dxp[2];
+    bool single[2];
+    for (int p = 0; p < 2; ++p) {
+      const int code = p | ((y & 1) << 1) | ((z & 1) << 2);
+      const int dx = DX[code], dy = DY[code], dz = DZ[code];
+      const int ay = (y - dy) >> 1, az = (z - dz) >> 1;
+      ra[p] = cellIndexDev(lc.w, 0, ay, az);
+      rb[p] = cellIndexDev(lc.w, 0, ay + dy, az + dz);
+      dxp[p] = dx;
+      single[p] = code == 0;
+    }
+    for (int x = 1 + (int)(threadIdx.x & 31); x <= len; x += 32) {
+      const int p = x & 1;
+      const int ax = (x - dxp[p]) >> 1;
+      const T v = single[p] ? __ldg(uc + ra[p] + ax)
+                            : T(0.5) * (__ldg(uc + ra[p] + ax) + __ldg(uc + rb[p] + ax + dxp[p]));
+      if (ADD) uf[rf + x] += v;
+      else uf[rf + x] = v;
+    }
   }
-  const int64_t base = lc.cellOff[b.cell];
-  T v;
-  if (code == 0) {
-    v = __ldg(coarse + base + cellIndexDev(lc.w, x >> 1, y >> 1, z >> 1));
-  } else {
-    const int ax = (x - dx) >> 1, ay = (y - dy) >> 1, az = (z - dz) >> 1;
-    v = T(0.5) * (__ldg(coarse + base + cellIndexDev(lc.w, ax, ay, az)) +
-                  __ldg(coarse + base + cellIndexDev(lc.w, ax + dx, ay + dy, az + dz)));
-  }
-  const int64_t c = lf.cellOff[b.cell] + (tetSize(lf.w) - tetSize(W)) + off;
-  if (ADD) fine[c] += v;
-  else fine[c] = v;
 }
 
 // ---------------------------------------------------------------------------------------
 // Face interiors: generic entries (layer, dx, dy, w); layer 0 is the face triangle, layer
 // 1+n the ghost layer of neighbour cell n (apply_3D_macroface_one_sided_*.cpp, called once
 // per neighbour cell in P1ConstantOperator.cpp:202-288, fused here into one sweep).
+// One block per (face, band of kFaceRows rows); for each row a warp turns the entries into
+// slot offsets once (shared memory), then every lane adds x.
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ int64_t faceSlot(int w, int layer, int x, int y) {
+constexpr int kFaceRows = 32;
+
+__device__ __forceinline__ int faceSlot(int w, int layer, int x, int y) {
   if (layer == 0) return rowStart(w, y) + x;
   return triSize(w) + (layer - 1) * triSize(w - 1) + rowStart(w - 1, y) + x;
+}
+
+template <class T>
+struct FaceShared {
+  FaceEnt<T> ent[16];
+  int off[kBlock / 32][16];
+};
+
+template <class T>
+__device__ __forceinline__ int loadFaceEntries(FaceShared<T>& sh, const StencilDev<T>& st, int face) {
+  const int ne = st.faceEntCount[face];
+  if (threadIdx.x < ne) sh.ent[threadIdx.x] = st.faceEnt[16 * face + threadIdx.x];
+  __syncthreads();
+  return ne;
 }
 
 template <class T, int MODE>
@@ -239,22 +296,26 @@ __global__ void __launch_bounds__(kBlock) faceStencilKernel(LevelDev lv, Stencil
                                                             unsigned mask) {
   const FaceBlock b = lv.faceBlocks[blockIdx.x];
   if (!(lv.faceType[b.face] & mask)) return;
-  __shared__ FaceEnt<T> ent[16];
-  const int ne = st.faceEntCount[b.face];
-  if (threadIdx.x < ne) ent[threadIdx.x] = st.faceEnt[16 * b.face + threadIdx.x];
-  __syncthreads();
-  const int w = lv.w;
-  const int off = b.start + threadIdx.x;
-  const int y = decodeRow(w, off);
-  const int x = off - rowStart(w, y);
-  if (y < 1 || x < 1 || x + y > w - 2) return;
+  __shared__ FaceShared<T> sh;
+  const int ne = loadFaceEntries(sh, st, b.face);
+  const int w = lv.w, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t base = lv.faceOff[b.face];
-  T s = T(0);
-  for (int k = 0; k < ne; ++k) s += ent[k].w * __ldg(src + base + faceSlot(w, ent[k].layer, x + ent[k].dx, y + ent[k].dy));
-  const int64_t c = base + off;
-  if (MODE == MODE_REPLACE) dst[c] = s;
-  else if (MODE == MODE_ADD) dst[c] += s;
-  else dst[c] = rhs[c] - s;
+  const T* __restrict__ u = src + base;
+  const int yEnd = min(b.start + kFaceRows, w - 2);
+  for (int y = b.start + warp; y < yEnd; y += kBlock / 32) {
+    if (lane < ne) sh.off[warp][lane] = faceSlot(w, sh.ent[lane].layer, sh.ent[lane].dx, y + sh.ent[lane].dy);
+    __syncwarp();
+    const int len = w - 2 - y, r0 = rowStart(w, y);
+    for (int x = 1 + lane; x <= len; x += 32) {
+      T s = T(0);
+      for (int k = 0; k < ne; ++k) s += sh.ent[k].w * __ldg(u + sh.off[warp][k] + x);
+      const int64_t i = base + r0 + x;
+      if (MODE == MODE_REPLACE) dst[i] = s;
+      else if (MODE == MODE_ADD) dst[i] += s;
+      else dst[i] = rhs[i] - s;
+    }
+    __syncwarp();
+  }
 }
 
 // Face SOR, colour = (x + 2y) mod 3; entry 0 is the diagonal.
@@ -263,21 +324,26 @@ __global__ void __launch_bounds__(kBlock) faceSorKernel(LevelDev lv, StencilDev<
                                                         unsigned mask, int colour, T omega) {
   const FaceBlock b = lv.faceBlocks[blockIdx.x];
   if (!(lv.faceType[b.face] & mask)) return;
-  __shared__ FaceEnt<T> ent[16];
-  const int ne = st.faceEntCount[b.face];
-  if (threadIdx.x < ne) ent[threadIdx.x] = st.faceEnt[16 * b.face + threadIdx.x];
-  __syncthreads();
-  const int w = lv.w;
-  const int off = b.start + threadIdx.x;
-  const int y = decodeRow(w, off);
-  const int x = off - rowStart(w, y);
-  if (y < 1 || x < 1 || x + y > w - 2) return;
-  if ((x + 2 * y) % 3 != colour) return;
+  __shared__ FaceShared<T> sh;
+  const int ne = loadFaceEntries(sh, st, b.face);
+  const int w = lv.w, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t base = lv.faceOff[b.face];
-  const int64_t c = base + off;
-  T s = rhs[c];
-  for (int k = 1; k < ne; ++k) s -= ent[k].w * u[base + faceSlot(w, ent[k].layer, x + ent[k].dx, y + ent[k].dy)];
-  u[c] = (T(1) - omega) * u[c] + (s * omega) / ent[0].w;
+  T* uf = u + base;
+  const T* __restrict__ f = rhs + base;
+  const T om = omega, om1 = T(1) - omega;
+  const int yEnd = min(b.start + kFaceRows, w - 2);
+  for (int y = b.start + warp; y < yEnd; y += kBlock / 32) {
+    if (lane < ne) sh.off[warp][lane] = faceSlot(w, sh.ent[lane].layer, sh.ent[lane].dx, y + sh.ent[lane].dy);
+    __syncwarp();
+    const int len = w - 2 - y, r0 = rowStart(w, y);
+    const int x0 = 1 + (((colour - 2 * y - 1) % 3) + 3) % 3;
+    for (int x = x0 + 3 * lane; x <= len; x += 96) {
+      T s = f[r0 + x];
+      for (int k = 1; k < ne; ++k) s -= sh.ent[k].w * uf[sh.off[warp][k] + x];
+      uf[r0 + x] = om1 * uf[r0 + x] + (s * om) / sh.ent[0].w;
+    }
+    __syncwarp();
+  }
 }
 
 // Restriction at coarse face-interior points from the fine face and its ghost layers: the fine
@@ -288,19 +354,23 @@ __global__ void __launch_bounds__(kBlock) faceRestrictKernel(LevelDev lc, LevelD
                                                              unsigned mask) {
   const FaceBlock b = lc.faceBlocks[blockIdx.x];
   if (!(lc.faceType[b.face] & mask)) return;
-  __shared__ FaceEnt<T> ent[16];
-  const int ne = stf.faceEntCount[b.face];
-  if (threadIdx.x < ne) ent[threadIdx.x] = stf.faceEnt[16 * b.face + threadIdx.x];
-  __syncthreads();
-  const int w = lc.w;
-  const int off = b.start + threadIdx.x;
-  const int y = decodeRow(w, off);
-  const int x = off - rowStart(w, y);
-  if (y < 1 || x < 1 || x + y > w - 2) return;
-  const int64_t basef = lf.faceOff[b.face];
-  T s = T(0);
-  for (int k = 1; k < ne; ++k) s += __ldg(fine + basef + faceSlot(lf.w, ent[k].layer, 2 * x + ent[k].dx, 2 * y + ent[k].dy));
-  coarse[lc.faceOff[b.face] + off] = __ldg(fine + basef + faceSlot(lf.w, 0, 2 * x, 2 * y)) + T(0.5) * s;
+  __shared__ FaceShared<T> sh;
+  const int ne = loadFaceEntries(sh, stf, b.face);
+  const int w = lc.w, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const T* __restrict__ uf = fine + lf.faceOff[b.face];
+  T* __restrict__ uc = coarse + lc.faceOff[b.face];
+  const int yEnd = min(b.start + kFaceRows, w - 2);
+  for (int y = b.start + warp; y < yEnd; y += kBlock / 32) {
+    if (lane < ne) sh.off[warp][lane] = faceSlot(lf.w, sh.ent[lane].layer, sh.ent[lane].dx, 2 * y + sh.ent[lane].dy);
+    __syncwarp();
+    const int len = w - 2 - y, r0 = rowStart(w, y);
+    for (int x = 1 + lane; x <= len; x += 32) {
+      T s = T(0);
+      for (int k = 1; k < ne; ++k) s += __ldg(uf + sh.off[warp][k] + 2 * x);
+      uc[r0 + x] = __ldg(uf + sh.off[warp][0] + 2 * x) + T(0.5) * s;
+    }
+    __syncwarp();
+  }
 }
 
 template <class T, bool ADD>
@@ -308,25 +378,32 @@ __global__ void __launch_bounds__(kBlock) faceProlongKernel(LevelDev lf, LevelDe
                                                             const T* __restrict__ coarse, unsigned mask) {
   const FaceBlock b = lf.faceBlocks[blockIdx.x];
   if (!(lf.faceType[b.face] & mask)) return;
-  const int w = lf.w;
-  const int off = b.start + threadIdx.x;
-  const int y = decodeRow(w, off);
-  const int x = off - rowStart(w, y);
-  if (y < 1 || x < 1 || x + y > w - 2) return;
-  const int64_t cb = lc.faceOff[b.face];
-  const int code = (x & 1) | ((y & 1) << 1);
-  T v;
-  if (code == 0) {
-    v = __ldg(coarse + cb + rowStart(lc.w, y >> 1) + (x >> 1));
-  } else {
-    const int dx = code == 1 ? 1 : (code == 3 ? -1 : 0);
-    const int dy = code == 1 ? 0 : 1;
-    const int ax = (x - dx) >> 1, ay = (y - dy) >> 1;
-    v = T(0.5) * (__ldg(coarse + cb + rowStart(lc.w, ay) + ax) + __ldg(coarse + cb + rowStart(lc.w, ay + dy) + ax + dx));
+  const int w = lf.w, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* __restrict__ uf = fine + lf.faceOff[b.face];
+  const T* __restrict__ uc = coarse + lc.faceOff[b.face];
+  const int yEnd = min(b.start + kFaceRows, w - 2);
+  for (int y = b.start + warp; y < yEnd; y += kBlock / 32) {
+    const int len = w - 2 - y, r0 = rowStart(w, y);
+    // bisected coarse micro-edge by parity (x | y << 1): (1,0), (0,1) or (-1,1)
+    int ra[2], rb[2], dxp[2];
+    for (int p = 0; p < 2; ++p) {
+      const int code = p | ((y & 1) << 1);
+      const int dx = code == 1 ? 1 : (code == 3 ? -1 : 0), dy = (code >= 2) ? 1 : 0;
+      const int ay = (y - dy) >> 1;
+      ra[p] = rowStart(lc.w, ay);
+      rb[p] = rowStart(lc.w, ay + dy);
+      dxp[p] = dx;
+    }
+    const bool evenRow = (y & 1) == 0;
+    for (int x = 1 + lane; x <= len; x += 32) {
+      const int p = x & 1;
+      const int ax = (x - dxp[p]) >> 1;
+      const T v = (evenRow && p == 0) ? __ldg(uc + ra[0] + ax)
+                                      : T(0.5) * (__ldg(uc + ra[p] + ax) + __ldg(uc + rb[p] + ax + dxp[p]));
+      if (ADD) uf[r0 + x] += v;
+      else uf[r0 + x] = v;
+    }
   }
-  const int64_t c = lf.faceOff[b.face] + off;
-  if (ADD) fine[c] += v;
-  else fine[c] = v;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -466,27 +543,29 @@ __global__ void __launch_bounds__(kBlock) dotKernel(LevelDev lv, const T* __rest
                                                     unsigned mask, double* partial) {
   double v = 0.0;
   int blk = blockIdx.x;
-  if (blk < lv.nCellBlocks) {
-    const CellBlock cb = lv.cellBlocks[blk];
-    if (lv.cellType[cb.cell] & mask) {
-      const int W = lv.w - cb.z;
-      const int off = cb.start + threadIdx.x;
-      const int y = decodeRow(W, off);
-      const int x = off - rowStart(W, y);
-      if (y >= 1 && x >= 1 && x + y <= W - 2) {
-        const int64_t c = lv.cellOff[cb.cell] + (tetSize(lv.w) - tetSize(W)) + off;
-        v = double(a[c]) * double(b[c]);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nCellGrid = lv.N >= 4 ? lv.nCells * (lv.N - 3) : 0;
+  if (blk < nCellGrid) {
+    const int nPl = lv.N - 3;
+    const int c = blk / nPl, z = 1 + blk % nPl;
+    if (lv.cellType[c] & mask) {
+      const T* __restrict__ pa = a + lv.cellOff[c];
+      const T* __restrict__ pb = b + lv.cellOff[c];
+      const int W = lv.w - z;
+      for (int y = 1 + warp; y <= W - 3; y += kBlock / 32) {
+        const int r0 = int(tetSize(lv.w) - tetSize(W)) + rowStart(W, y);
+        for (int x = 1 + lane; x <= W - 2 - y; x += 32) v += double(pa[r0 + x]) * double(pb[r0 + x]);
       }
     }
-  } else if ((blk -= lv.nCellBlocks) < lv.nFaceBlocks) {
+  } else if ((blk -= nCellGrid) < lv.nFaceBlocks) {
     const FaceBlock fb = lv.faceBlocks[blk];
     if (lv.faceType[fb.face] & mask) {
-      const int off = fb.start + threadIdx.x;
-      const int y = decodeRow(lv.w, off);
-      const int x = off - rowStart(lv.w, y);
-      if (y >= 1 && x >= 1 && x + y <= lv.w - 2) {
-        const int64_t c = lv.faceOff[fb.face] + off;
-        v = double(a[c]) * double(b[c]);
+      const T* __restrict__ pa = a + lv.faceOff[fb.face];
+      const T* __restrict__ pb = b + lv.faceOff[fb.face];
+      const int yEnd = min(fb.start + kFaceRows, lv.w - 2);
+      for (int y = fb.start + warp; y < yEnd; y += kBlock / 32) {
+        const int r0 = rowStart(lv.w, y);
+        for (int x = 1 + lane; x <= lv.w - 2 - y; x += 32) v += double(pa[r0 + x]) * double(pb[r0 + x]);
       }
     }
   } else {

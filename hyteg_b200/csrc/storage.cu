@@ -119,22 +119,11 @@ void Storage::buildLevel(int L) {
   ld.hostFaceType = faceType;
   ld.hostLowType = lowType;
 
-  std::vector<dev::CellBlock> cb;
-  if (N >= 4)
-    for (int c = 0; c < lv.nCells; ++c)
-      for (int z = 1; z <= N - 3; ++z) {
-        const int W = (int)(w - z);
-        const int a = W + 1 - 1;                                   // rowStart(W, 1)
-        const int e = (W - 2) * (W + 1) - ((W - 2) * (W - 1)) / 2;  // rowStart(W, W-2)
-        for (int s = a; s < e; s += dev::kBlock) cb.push_back({c, z, s, 0});
-      }
+  lv.nCellBlocks = N >= 4 ? lv.nCells * (int)(N - 3) : 0;
   std::vector<dev::FaceBlock> fb;
   if (N >= 3)
-    for (int f = 0; f < lv.nFaces; ++f) {
-      const int W = (int)w;
-      const int a = W, e = (W - 2) * (W + 1) - ((W - 2) * (W - 1)) / 2;
-      for (int s = a; s < e; s += dev::kBlock) fb.push_back({f, s});
-    }
+    for (int f = 0; f < lv.nFaces; ++f)
+      for (int y = 1; y < (int)w - 2; y += dev::kFaceRows) fb.push_back({f, y});
   std::vector<dev::LowBlock> lb;
   for (int p = 0; p < lv.nLow; ++p) {
     if (p == lv.nEdges) lv.nLowEdgeBlocks = (int)lb.size();
@@ -169,8 +158,6 @@ void Storage::buildLevel(int L) {
   lv.cellType = (const unsigned char*)upload(keep, cellType, stream);
   lv.faceType = (const unsigned char*)upload(keep, faceType, stream);
   lv.lowType = (const unsigned char*)upload(keep, lowType, stream);
-  lv.cellBlocks = (const dev::CellBlock*)upload(keep, cb, stream);
-  lv.nCellBlocks = (int)cb.size();
   lv.faceBlocks = (const dev::FaceBlock*)upload(keep, fb, stream);
   lv.nFaceBlocks = (int)fb.size();
   lv.lowBlocks = (const dev::LowBlock*)upload(keep, lb, stream);
@@ -386,37 +373,49 @@ const dev::StencilDev<float>& stencilOf<float>(Operator& o, int L) {
 }
 
 template <class T, int MODE>
-void Storage::stencilOp(Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask) {
+void Storage::stencilOp(Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask, int kinds) {
   const LevelData& ld = levels[L];
   const dev::StencilDev<T>& st = stencilOf<T>(o, L);
-  if (ld.lv.nCellBlocks) {
+  if (ld.lv.nCellBlocks && (kinds & (1 << KC))) {
     dev::cellStencilKernel<T, MODE><<<ld.lv.nCellBlocks, dev::kBlock, 0, stream>>>(ld.lv, st.cellW, dst, src, rhs, mask);
     ++launches;
   }
-  if (ld.lv.nFaceBlocks) {
+  if (ld.lv.nFaceBlocks && (kinds & (1 << KF))) {
     dev::faceStencilKernel<T, MODE><<<ld.lv.nFaceBlocks, dev::kBlock, 0, stream>>>(ld.lv, st, dst, src, rhs, mask);
     ++launches;
   }
-  if (ld.lv.nLowBlocks) {
+  const int nVertBlocks = ld.lv.nLowBlocks - ld.lv.nLowEdgeBlocks;
+  if ((kinds & (1 << KE)) && (kinds & (1 << KV)) && ld.lv.nLowBlocks) {
     dev::lowStencilKernel<T, MODE><<<ld.lv.nLowBlocks, dev::kBlock, 0, stream>>>(ld.lv, st, dst, src, rhs, mask, 0);
+    ++launches;
+  } else if ((kinds & (1 << KE)) && ld.lv.nLowEdgeBlocks) {
+    dev::lowStencilKernel<T, MODE><<<ld.lv.nLowEdgeBlocks, dev::kBlock, 0, stream>>>(ld.lv, st, dst, src, rhs, mask, 0);
+    ++launches;
+  } else if ((kinds & (1 << KV)) && nVertBlocks) {
+    dev::lowStencilKernel<T, MODE><<<nVertBlocks, dev::kBlock, 0, stream>>>(ld.lv, st, dst, src, rhs, mask,
+                                                                              ld.lv.nLowEdgeBlocks);
     ++launches;
   }
   cudaCheck(cudaGetLastError(), "stencil kernel");
 }
 
-void Storage::apply(int opId, int src, int dst, int L, unsigned mask, int update) {
+void Storage::apply(int opId, int src, int dst, int L, unsigned mask, int update, int kinds, bool refresh) {
   Operator& o = op(opId);
   argCheck(L >= o.minL && L <= o.maxL, "level outside the operator's level range");
   argCheck(src != dst, "apply: src and dst must differ");
   Function& fs = fn(src);
   argCheck(fs.prec == fn(dst).prec, "apply: precision mismatch");
-  communicate(src, L, kAllGroups);
+  if (refresh) communicate(src, L, kAllGroups);
   if (fs.prec == 8) {
-    if (update == 0) stencilOp<double, dev::MODE_REPLACE>(o, L, (double*)data(dst, L), (const double*)data(src, L), nullptr, mask);
-    else stencilOp<double, dev::MODE_ADD>(o, L, (double*)data(dst, L), (const double*)data(src, L), nullptr, mask);
+    if (update == 0)
+      stencilOp<double, dev::MODE_REPLACE>(o, L, (double*)data(dst, L), (const double*)data(src, L), nullptr, mask, kinds);
+    else
+      stencilOp<double, dev::MODE_ADD>(o, L, (double*)data(dst, L), (const double*)data(src, L), nullptr, mask, kinds);
   } else {
-    if (update == 0) stencilOp<float, dev::MODE_REPLACE>(o, L, (float*)data(dst, L), (const float*)data(src, L), nullptr, mask);
-    else stencilOp<float, dev::MODE_ADD>(o, L, (float*)data(dst, L), (const float*)data(src, L), nullptr, mask);
+    if (update == 0)
+      stencilOp<float, dev::MODE_REPLACE>(o, L, (float*)data(dst, L), (const float*)data(src, L), nullptr, mask, kinds);
+    else
+      stencilOp<float, dev::MODE_ADD>(o, L, (float*)data(dst, L), (const float*)data(src, L), nullptr, mask, kinds);
   }
 }
 
@@ -434,32 +433,36 @@ void Storage::residual(int opId, int x, int b, int r, int L, unsigned mask) {
 }
 
 template <class T>
-void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned mask, T omega, bool backwards) {
+void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned mask, T omega, bool backwards,
+                   int kinds, bool refresh) {
   const LevelData& ld = levels[L];
   const dev::StencilDev<T>& st = stencilOf<T>(o, L);
   const dev::LevelDev& lv = ld.lv;
   const int nVertBlocks = lv.nLowBlocks - lv.nLowEdgeBlocks;
+  auto comm = [&](int groups) {
+    if (refresh) communicate(dstId, L, groups);
+  };
   auto verts = [&]() {
-    if (nVertBlocks) {
+    if (nVertBlocks && (kinds & (1 << KV))) {
       dev::lowSorKernel<T><<<nVertBlocks, dev::kBlock, 0, stream>>>(lv, st, u, rhs, mask, -1, omega, lv.nLowEdgeBlocks);
       ++launches;
     }
   };
   auto edges = [&](int c) {
-    if (lv.nLowEdgeBlocks) {
+    if (lv.nLowEdgeBlocks && (kinds & (1 << KE))) {
       dev::lowSorKernel<T><<<lv.nLowEdgeBlocks, dev::kBlock, 0, stream>>>(lv, st, u, rhs, mask, c, omega, 0);
       ++launches;
     }
   };
   auto faces = [&](int c) {
-    if (lv.nFaceBlocks) {
+    if (lv.nFaceBlocks && (kinds & (1 << KF))) {
       dev::faceSorKernel<T><<<lv.nFaceBlocks, dev::kBlock, 0, stream>>>(lv, st, u, rhs, mask, c, omega);
       ++launches;
     }
   };
   auto cells = [&](int c) {
-    if (lv.nCellBlocks) {
-      dev::cellSorKernel<T><<<lv.nCellBlocks, dev::kBlock, 0, stream>>>(lv, st.cellW, u, rhs, mask, c, omega);
+    if (lv.nCellBlocks && (kinds & (1 << KC))) {
+      dev::cellSorKernel<T><<<lv.nCellBlocks, dev::kBlock, 0, stream>>>(lv, st.cellW, u, rhs, mask, c, omega, 0);
       ++launches;
     }
   };
@@ -467,30 +470,31 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
   // V -> E -> F -> C (backwards C -> F -> E -> V) with a refresh of the next phase's copies.
   // Only the copies the reference refreshes between phases are refreshed here, so ghost
   // values that reach a primitive from outside its closure keep their start-of-sweep value.
-  communicate(dstId, L, kAllGroups);
+  comm(kAllGroups);
   if (!backwards) {
     verts();
-    communicate(dstId, L, 1 << G_EDGE);           // Vertex -> Edge
+    comm(1 << G_EDGE);           // Vertex -> Edge
     edges(0);
     edges(1);
-    communicate(dstId, L, 1 << G_FACE_BOUNDARY);  // Edge -> Face
+    comm(1 << G_FACE_BOUNDARY);  // Edge -> Face
     for (int c = 0; c < 3; ++c) faces(c);
-    communicate(dstId, L, 1 << G_CELL);           // Face -> Cell
+    comm(1 << G_CELL);           // Face -> Cell
     for (int c = 0; c < 4; ++c) cells(c);
   } else {
     for (int c = 3; c >= 0; --c) cells(c);
-    communicate(dstId, L, 1 << G_FACE_GHOST);     // Cell -> Face
+    comm(1 << G_FACE_GHOST);     // Cell -> Face
     for (int c = 2; c >= 0; --c) faces(c);
-    communicate(dstId, L, 1 << G_EDGE);           // Face -> Edge
+    comm(1 << G_EDGE);           // Face -> Edge
     edges(1);
     edges(0);
-    communicate(dstId, L, 1 << G_VERT);           // Edge -> Vertex
+    comm(1 << G_VERT);           // Edge -> Vertex
     verts();
   }
   cudaCheck(cudaGetLastError(), "sor");
 }
 
-void Storage::smoothSor(int opId, int dst, int rhs, double omega, int L, unsigned mask, bool backwards) {
+void Storage::smoothSor(int opId, int dst, int rhs, double omega, int L, unsigned mask, bool backwards, int kinds,
+                        bool refresh) {
   Operator& o = op(opId);
   argCheck(L >= o.minL && L <= o.maxL, "level outside the operator's level range");
   argCheck(dst != rhs, "smooth_sor: dst and rhs must differ");
@@ -498,8 +502,11 @@ void Storage::smoothSor(int opId, int dst, int rhs, double omega, int L, unsigne
   argCheck(fd.prec == fn(rhs).prec, "smooth_sor: precision mismatch");
   for (auto& c : o.host[L - o.minL].cell)
     if (levels[L].lv.nCellBlocks && c[0] == 0.0) throw Error(HG_ERR_NUMERIC, "zero diagonal in cell stencil");
-  if (fd.prec == 8) sorT<double>(o, dst, L, (double*)data(dst, L), (const double*)data(rhs, L), mask, omega, backwards);
-  else sorT<float>(o, dst, L, (float*)data(dst, L), (const float*)data(rhs, L), mask, (float)omega, backwards);
+  if (fd.prec == 8)
+    sorT<double>(o, dst, L, (double*)data(dst, L), (const double*)data(rhs, L), mask, omega, backwards, kinds, refresh);
+  else
+    sorT<float>(o, dst, L, (float*)data(dst, L), (const float*)data(rhs, L), mask, (float)omega, backwards, kinds,
+                refresh);
 }
 
 // The fine-level face/edge/vertex stencil structure drives the restriction; it is taken from

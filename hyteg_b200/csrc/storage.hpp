@@ -81,17 +81,19 @@ struct Storage {
 
   int createOperator(int form, int minL, int maxL);
   Operator& op(int id);
-  void apply(int op, int src, int dst, int L, unsigned mask, int update);
+  void apply(int op, int src, int dst, int L, unsigned mask, int update, int kinds = 15, bool refresh = true);
   void residual(int op, int x, int b, int r, int L, unsigned mask);
-  void smoothSor(int op, int dst, int rhs, double omega, int L, unsigned mask, bool backwards);
+  void smoothSor(int op, int dst, int rhs, double omega, int L, unsigned mask, bool backwards, int kinds = 15,
+                 bool refresh = true);
   void restrictFn(int id, int Lf, unsigned mask);
   void prolongate(int id, int Lc, unsigned mask, bool add);
   const Operator& structure();
 
   template <class T, int MODE>
-  void stencilOp(Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask);
+  void stencilOp(Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask, int kinds = 15);
   template <class T>
-  void sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned mask, T omega, bool backwards);
+  void sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned mask, T omega, bool backwards, int kinds,
+            bool refresh);
   template <class T>
   void restrictT(int id, int Lf, unsigned mask);
   template <class T>

@@ -87,6 +87,8 @@ int hg_storage_counts(const hg_storage* s, int counts[4]);
 /* Use this CUDA stream (cudaStream_t) for all subsequent work; NULL = the storage's own stream. */
 int hg_storage_set_stream(hg_storage* s, void* stream);
 int hg_storage_synchronize(hg_storage* s);
+/* Number of device kernels this storage has launched so far. */
+int hg_storage_launch_count(const hg_storage* s, unsigned long long* count);
 /* Piecewise-constant diffusion coefficient per macro-cell (ncells values) for operators
  * created afterwards. */
 int hg_storage_set_cell_coefficients(hg_storage* s, const double* k, int ncells);
@@ -148,9 +150,19 @@ int hg_operator_create(hg_storage* s, int form, int min_level, int max_level, in
 int hg_operator_destroy(hg_storage* s, int op);
 /* update: 0 = Replace, 1 = Add */
 int hg_apply(hg_storage* s, int op, int src, int dst, int level, unsigned flag, int update);
+/* The per-primitive-kind kernels of hg_apply without (refresh = 0) or with (1) the preceding
+ * halo refresh: kinds is a bit set (1 << HG_VERTEX | 1 << HG_EDGE | 1 << HG_FACE | 1 << HG_CELL).
+ * Replaces the per-macro-primitive kernel calls of P1ConstantOperator
+ * (apply_cell_generated / apply_face3D_generated, P1ConstantOperator.cpp:202-336). */
+int hg_apply_primitives(hg_storage* s, int op, int src, int dst, int level, unsigned flag, int update, int kinds,
+                        int refresh);
 /* r = b - A x on the flagged primitives */
 int hg_residual(hg_storage* s, int op, int x, int b, int r, int level, unsigned flag);
 int hg_smooth_sor(hg_storage* s, int op, int dst, int rhs, double omega, int level, unsigned flag, int backwards);
+/* The phases of one SOR sweep restricted to the selected primitive kinds (bit set as in
+ * hg_apply_primitives), with (refresh = 1) or without the halo refreshes. */
+int hg_smooth_sor_primitives(hg_storage* s, int op, int dst, int rhs, double omega, int level, unsigned flag,
+                             int backwards, int kinds, int refresh);
 /* fn(src_level - 1) = R fn(src_level) */
 int hg_restrict(hg_storage* s, int fn, int src_level, unsigned flag);
 /* fn(src_level + 1) = P fn(src_level)   (add != 0: +=) */

@@ -348,9 +348,14 @@ void sorSweep(Oracle& o, int L, double* u, const double* f, double omega, bool m
         continue;
       }
       const Node& nj = d.nodes[j];
-      // values in the primitive's own closure are current; values reaching the primitive
-      // through ghost layers are those of the sweep's initial halo exchange
-      const bool current = inClosure(nj, ni) || (backwards && inClosure(ni, nj));
+      // Forward: values in the primitive's own closure are current (refreshed V->E->F->C
+      // between the phases); values reaching it through ghost layers keep the value of the
+      // sweep's initial halo exchange. Backward (C->F->E->V): the reference refreshes a
+      // primitive's ghosts from the higher-dimensional primitives that contain it, so only
+      // their values are current; the multicolour smoother refreshes every ghost slot from its
+      // owner, so every value owned by a higher-dimensional primitive is current.
+      bool current = inClosure(nj, ni);
+      if (backwards) current = current || (multicolour ? nj.kind > ni.kind : inClosure(ni, nj));
       s -= A.val[e] * (current ? u[j] : start[j]);
     }
     u[i] = (1.0 - omega) * u[i] + (s * omega) / diag;

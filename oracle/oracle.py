@@ -68,7 +68,7 @@ def ref_lib():
     d = P(c_double)
     r.ref_apply_cell.argtypes = [d, d, c_int, d, c_int]
     r.ref_sor_cell.argtypes = [d, d, c_int, d, c_double]
-    r.ref_apply_face.argtypes = [d, d, d, c_int, c_int64, c_int64, c_int64, d, c_int]
+    r.ref_apply_face.argtypes = [d, d, d, c_int, c_int64, c_int64, c_int64, d, P(c_int), c_int]
     r.ref_restrict_cell.argtypes = [d, d, c_int, d, d, d]
     r.ref_prolongate_cell.argtypes = [d, d, c_int, d, d, d]
     r.ref_p1_tet_diffusion.argtypes = [d, d]

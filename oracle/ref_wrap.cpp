@@ -26,12 +26,12 @@ static const int kOff[15][3] = {{0, 0, 0},  {1, 0, 0},  {-1, 0, 0}, {0, 1, 0},  
                                 {-1, 1, 0}, {1, -1, 0}, {0, 0, 1},  {-1, 0, 1}, {0, -1, 1},
                                 {1, -1, 1}, {0, 0, -1}, {1, 0, -1}, {0, 1, -1}, {-1, 1, -1}};
 
-// keepZero = false drops entries whose weight is exactly zero (one-sided face stencils only
-// contain the increments that stay inside the neighbour cell).
-static StencilMap toMap(const double* w, bool keepZero) {
+// present == nullptr keeps all 15 increments; otherwise only those with present[k] != 0 (the
+// one-sided face stencils contain the increments that stay inside the neighbour cell).
+static StencilMap toMap(const double* w, const int* present) {
   StencilMap m;
   for (int k = 0; k < 15; ++k)
-    if (keepZero || w[k] != 0.0) m[IndexIncrement(kOff[k][0], kOff[k][1], kOff[k][2])] = w[k];
+    if (!present || present[k]) m[IndexIncrement(kOff[k][0], kOff[k][1], kOff[k][2])] = w[k];
   return m;
 }
 
@@ -39,27 +39,27 @@ extern "C" {
 
 void ref_apply_cell(double* dst, const double* src, int level, const double* w15, int add) {
   if (add)
-    hyteg::vertexdof::macrocell::generated::apply_3D_macrocell_vertexdof_to_vertexdof_add(dst, src, level, toMap(w15, true));
+    hyteg::vertexdof::macrocell::generated::apply_3D_macrocell_vertexdof_to_vertexdof_add(dst, src, level, toMap(w15, nullptr));
   else
     hyteg::vertexdof::macrocell::generated::apply_3D_macrocell_vertexdof_to_vertexdof_replace(dst, src, level,
-                                                                                               toMap(w15, true));
+                                                                                               toMap(w15, nullptr));
 }
 
 void ref_sor_cell(double* dst, const double* rhs, int level, const double* w15, double relax) {
-  hyteg::vertexdof::macrocell::generated::sor_3D_macrocell_P1(dst, rhs, level, toMap(w15, true), relax);
+  hyteg::vertexdof::macrocell::generated::sor_3D_macrocell_P1(dst, rhs, level, toMap(w15, nullptr), relax);
 }
 
 // One-sided face apply with the ghost layer `srcGl` of a neighbour cell whose cell-local
 // vertex IDs of the face's vertices are (v0, v1, v2); w15 = that cell's contribution to the
 // face-point row in cell-local increments.
 void ref_apply_face(double* dst, const double* src, const double* srcGl, int level, int64_t v0, int64_t v1, int64_t v2,
-                    const double* w15, int add) {
+                    const double* w15, const int* present15, int add) {
   if (add)
     hyteg::vertexdof::macroface::generated::apply_3D_macroface_one_sided_vertexdof_to_vertexdof_add(
-        dst, src, srcGl, level, v0, v1, v2, toMap(w15, false));
+        dst, src, srcGl, level, v0, v1, v2, toMap(w15, present15));
   else
     hyteg::vertexdof::macroface::generated::apply_3D_macroface_one_sided_vertexdof_to_vertexdof_replace(
-        dst, src, srcGl, level, v0, v1, v2, toMap(w15, false));
+        dst, src, srcGl, level, v0, v1, v2, toMap(w15, present15));
 }
 
 void ref_restrict_cell(double* coarse, const double* fine, int coarseLevel, const double* nEdge6, const double* nFace4,
