@@ -213,6 +213,9 @@ class PrimitiveStorage:
     def synchronize(self):
         call("hg_storage_synchronize", self._h)
 
+    def set_l2_budget(self, nbytes):
+        call("hg_storage_set_l2_budget", self._h, int(nbytes))
+
     def launch_count(self):
         n = ctypes.c_ulonglong()
         call("hg_storage_launch_count", self._h, ctypes.byref(n))

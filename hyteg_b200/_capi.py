@@ -40,6 +40,7 @@ _SIGS = {
     "hg_storage_counts": (c_int, [c_void_p, P(c_int)]),
     "hg_storage_set_stream": (c_int, [c_void_p, c_void_p]),
     "hg_storage_synchronize": (c_int, [c_void_p]),
+    "hg_storage_set_l2_budget": (c_int, [c_void_p, c_int64]),
     "hg_storage_launch_count": (c_int, [c_void_p, P(ctypes.c_ulonglong)]),
     "hg_storage_set_cell_coefficients": (c_int, [c_void_p, P(c_double), c_int]),
     "hg_primitive_vertices": (c_int, [c_void_p, c_int, c_int, P(c_int), P(c_double), P(c_int)]),

@@ -131,6 +131,12 @@ int hg_storage_synchronize(hg_storage* h) {
   HG_CATCH
 }
 
+int hg_storage_set_l2_budget(hg_storage* h, int64_t bytes) {
+  HG_TRY
+  S(h).setL2Budget(bytes);
+  HG_CATCH
+}
+
 int hg_storage_launch_count(const hg_storage* h, unsigned long long* count) {
   HG_TRY
   *count = S(h).launches;

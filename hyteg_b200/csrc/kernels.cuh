@@ -192,6 +192,145 @@ __global__ void __launch_bounds__(kBlock, 4) cellSorKernel(LevelDev lv, const T*
   (void)dinv;
 }
 
+// ---------------------------------------------------------------------------------------
+// Register-blocked 2.5-D cell sweep (the kernel behind apply and residual on cell interiors).
+// A warp owns a strip of 30 x-columns (lanes 1..30; lanes 0 and 31 only carry the x-halo) by
+// kStripR rows and marches up z through a range of planes. Each lane keeps the rows
+// y0-1 .. y0+R of the planes z-1, z, z+1 of its own column in registers and has plane z+2
+// (and the second vector's rows of plane z+1) in flight while plane z is computed;
+// x-neighbours come from the adjacent lanes through warp shuffles. Addresses advance
+// incrementally: index(x, y, z+1) = index(x, y, z) + tri(w - z) - y.
+// Every value is loaded (R+2)/R times per sweep (the extra rows are the neighbouring strips'
+// rows, L1 hits). No shared memory, no block synchronisation.
+// ---------------------------------------------------------------------------------------
+constexpr int kStripR = 4;                          // rows per strip
+constexpr int kStripH = kStripR + 2;                // rows held per plane (with y-halo)
+constexpr int kStripX = 30;                         // computed columns per warp
+constexpr int kStripWarps = kBlock / 32;            // strips per block (stacked in y)
+constexpr int kStripZ = 32;                         // planes per work item
+constexpr int kStripRows = kStripR * kStripWarps;   // rows per block
+
+struct StripItem {
+  int cell, x0, y0, z0, z1, pad0, pad1, pad2;  // columns [x0, x0+30), rows [y0, y0+32), planes [z0, z1)
+};
+
+enum StripOp { STRIP_REPLACE = 0, STRIP_ADD = 1, STRIP_RESIDUAL = 2 };
+
+template <class T>
+__device__ __forceinline__ T shUp(T v) {  // value of lane - 1 (x - 1)
+  return __shfl_up_sync(0xffffffffu, v, 1);
+}
+template <class T>
+__device__ __forceinline__ T shDown(T v) {  // value of lane + 1 (x + 1)
+  return __shfl_down_sync(0xffffffffu, v, 1);
+}
+
+template <class T, int OP>
+__global__ void __launch_bounds__(kBlock, 2) cellStripKernel(LevelDev lv, const StripItem* __restrict__ items,
+                                                             const T* __restrict__ cellW, T* __restrict__ dst,
+                                                             const T* __restrict__ src, const T* __restrict__ rhs,
+                                                             unsigned mask) {
+  const StripItem it = items[blockIdx.x];
+  if (!(lv.cellType[it.cell] & mask)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int N = lv.N, w = lv.w;
+  const int x = it.x0 - 1 + lane;                    // lane 0: x0 - 1, lanes 1..30: x0 .. x0+29
+  const int y0 = it.y0 + warp * kStripR;
+  // last plane with an interior point in this strip: x + y + z <= N - 1 with x >= x0, y >= y0
+  const int zEnd = min(it.z1, N - it.x0 - y0);
+  if (it.z0 >= zEnd) return;
+  const int64_t base = lv.cellOff[it.cell];
+  const T* __restrict__ u = src + base;
+  const T* __restrict__ f = (OP == STRIP_ADD) ? dst + base : rhs + base;
+  constexpr bool kSecond = OP != STRIP_REPLACE;
+  T wt[15];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) wt[k] = __ldg(cellW + 16 * it.cell + k);
+  const bool computeLane = lane >= 1 && lane <= kStripX;
+  // index of (x, y0 - 1 + r) in plane p, advanced plane by plane
+  int idx[kStripH];
+  int p = it.z0 - 1;
+  {
+    const int W = w - p;
+    const int pb = int(tetSize(w) - tetSize(W));
+#pragma unroll
+    for (int r = 0; r < kStripH; ++r) idx[r] = pb + rowStart(W, y0 - 1 + r) + x;
+  }
+  // plane p exists at row y iff x + y <= N - p
+  auto load = [&](T (&v)[kStripH]) {
+#pragma unroll
+    for (int r = 0; r < kStripH; ++r) v[r] = (x + y0 - 1 + r <= N - p) ? __ldg(u + idx[r]) : T(0);
+  };
+  auto loadF = [&](T (&v)[kStripR]) {
+#pragma unroll
+    for (int r = 0; r < kStripR; ++r) v[r] = (x + y0 + r <= N - p) ? __ldg(f + idx[r + 1]) : T(0);
+  };
+  auto advance = [&]() {
+    const int t = triSize(w - p);
+#pragma unroll
+    for (int r = 0; r < kStripH; ++r) idx[r] += t - (y0 - 1 + r);
+    ++p;
+  };
+  T pm[kStripH], pc[kStripH], pp[kStripH], nx[kStripH], fc[kStripR], fn[kStripR];
+  load(pm);
+  advance();
+  load(pc);
+  if (kSecond) loadF(fc);
+  int idxc[kStripR];  // indices of the computed rows of plane z
+#pragma unroll
+  for (int r = 0; r < kStripR; ++r) idxc[r] = idx[r + 1];
+  advance();
+  load(pp);
+  for (int z = it.z0; z < zEnd; ++z) {
+    // p == z + 1 here: the second vector of plane z + 1, then plane z + 2 of the input
+    if (kSecond) loadF(fn);
+    int idxn[kStripR];
+#pragma unroll
+    for (int r = 0; r < kStripR; ++r) idxn[r] = idx[r + 1];
+    advance();
+    load(nx);
+#pragma unroll
+    for (int r = 0; r < kStripR; ++r) {
+      const int j = r + 1, y = y0 + r;
+      // shuffles are warp-uniform: every lane takes part, inactive lanes discard the result
+      const T E = shDown(pc[j]), Wv = shUp(pc[j]);
+      const T NW = shUp(pc[j + 1]), SE = shDown(pc[j - 1]);
+      const T TW = shUp(pp[j]), TSE = shDown(pp[j - 1]);
+      const T BE = shDown(pm[j]), BNW = shUp(pm[j + 1]);
+      if (computeLane && x + y + z <= N - 1) {
+        // four independent partial sums keep the FMA dependency chains short
+        T s0 = wt[1] * E, s1 = wt[3] * pc[j + 1], s2 = wt[7] * pp[j], s3 = wt[11] * pm[j];
+        s0 += wt[2] * Wv;
+        s1 += wt[4] * pc[j - 1];
+        s2 += wt[8] * TW;
+        s3 += wt[12] * BE;
+        s0 += wt[5] * NW;
+        s1 += wt[6] * SE;
+        s2 += wt[9] * pp[j - 1];
+        s3 += wt[13] * pm[j + 1];
+        s2 += wt[10] * TSE;
+        s3 += wt[14] * BNW;
+        const T a = wt[0] * pc[j] + ((s0 + s1) + (s2 + s3));
+        T* d = dst + base + idxc[r];
+        if (OP == STRIP_REPLACE) *d = a;
+        else if (OP == STRIP_ADD) *d = fc[r] + a;
+        else *d = fc[r] - a;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kStripH; ++r) {
+      pm[r] = pc[r];
+      pc[r] = pp[r];
+      pp[r] = nx[r];
+    }
+#pragma unroll
+    for (int r = 0; r < kStripR; ++r) {
+      idxc[r] = idxn[r];
+      if (kSecond) fc[r] = fn[r];
+    }
+  }
+}
+
 // Full-weighting restriction at coarse cell-interior points: coarse = fine[2p] + 1/2 sum fine[2p+d]
 // (restrict_3D_macrocell_P1_pull_additive.cpp; on interior points every weight is 1 or 1/2).
 template <class T>

@@ -164,9 +164,52 @@ void Storage::buildLevel(int L) {
   lv.nLowBlocks = (int)lb.size();
   ld.comm = (uint2*)upload(keep, comm, stream);
   ld.chunks = (dev::Chunk*)upload(keep, chunks, stream);
+  buildTiles(L);
   ld.nChunks = (int)chunks.size();
   ld.partial.alloc(sizeof(double) * std::max(1, lv.nCellBlocks + lv.nFaceBlocks + lv.nLowBlocks));
   cudaCheck(cudaStreamSynchronize(stream), "level upload");
+}
+
+// Cell-sweep work items: (cell, 30-column x 32-row block of strips, <= kStripZ planes), the
+// longest first inside groups of macro-cells whose two FP64 vectors fit into the L2 budget;
+// the SOR colours of a group run back to back so that their re-reads hit L2.
+void Storage::buildTiles(int L) {
+  LevelData& ld = levels[L];
+  const int64_t N = ld.lay->N, w = ld.lay->w;
+  const int nCells = ld.lv.nCells;
+  std::vector<dev::StripItem> items;
+  const int64_t cellBytes = tet(w) * 8;
+  ld.cellsPerGroup = (int)std::max<int64_t>(1, std::min<int64_t>(nCells, l2Budget / (2 * cellBytes)));
+  ld.tileGroupBegin.assign(1, 0);
+  for (int g0 = 0; N >= 4 && g0 < nCells; g0 += ld.cellsPerGroup) {
+    std::vector<dev::StripItem> grp;
+    for (int c = g0; c < std::min(nCells, g0 + ld.cellsPerGroup); ++c)
+      for (int y0 = 1; y0 <= N - 3; y0 += dev::kStripRows)
+        for (int x0 = 1; x0 <= N - 3; x0 += dev::kStripX) {
+          const int zmax = (int)N - 1 - x0 - y0;  // last plane with an interior point in the block
+          if (zmax < 1) continue;
+          for (int z0 = 1; z0 <= zmax; z0 += dev::kStripZ)
+            grp.push_back({c, x0, y0, z0, std::min(zmax + 1, z0 + dev::kStripZ), 0, 0, 0});
+        }
+    std::stable_sort(grp.begin(), grp.end(),
+                     [](const dev::StripItem& a, const dev::StripItem& b) { return (a.z1 - a.z0) > (b.z1 - b.z0); });
+    items.insert(items.end(), grp.begin(), grp.end());
+    ld.tileGroupBegin.push_back((int)items.size());
+  }
+  ld.tileBuf.reset(new DevBuf());
+  ld.tiles = (dev::StripItem*)ld.tileBuf->alloc(std::max<size_t>(items.size(), 1) * sizeof(dev::StripItem));
+  if (!items.empty())
+    cudaCheck(cudaMemcpyAsync(ld.tiles, items.data(), items.size() * sizeof(dev::StripItem), cudaMemcpyHostToDevice,
+                              stream),
+              "strip items");
+  ld.nTiles = (int)items.size();
+  cudaCheck(cudaStreamSynchronize(stream), "strip items sync");
+}
+
+void Storage::setL2Budget(int64_t bytes) {
+  argCheck(bytes > 0, "L2 budget must be positive");
+  l2Budget = bytes;
+  for (int L = 0; L <= maxLevel(); ++L) buildTiles(L);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -376,8 +419,10 @@ template <class T, int MODE>
 void Storage::stencilOp(Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask, int kinds) {
   const LevelData& ld = levels[L];
   const dev::StencilDev<T>& st = stencilOf<T>(o, L);
-  if (ld.lv.nCellBlocks && (kinds & (1 << KC))) {
-    dev::cellStencilKernel<T, MODE><<<ld.lv.nCellBlocks, dev::kBlock, 0, stream>>>(ld.lv, st.cellW, dst, src, rhs, mask);
+  if (ld.nTiles && (kinds & (1 << KC))) {
+    constexpr int op =
+        MODE == dev::MODE_REPLACE ? dev::STRIP_REPLACE : MODE == dev::MODE_ADD ? dev::STRIP_ADD : dev::STRIP_RESIDUAL;
+    dev::cellStripKernel<T, op><<<ld.nTiles, dev::kBlock, 0, stream>>>(ld.lv, ld.tiles, st.cellW, dst, src, rhs, mask);
     ++launches;
   }
   if (ld.lv.nFaceBlocks && (kinds & (1 << KF))) {
@@ -460,14 +505,20 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
       ++launches;
     }
   };
-  auto cells = [&](int c) {
-    if (lv.nCellBlocks && (kinds & (1 << KC))) {
-      dev::cellSorKernel<T><<<lv.nCellBlocks, dev::kBlock, 0, stream>>>(lv, st.cellW, u, rhs, mask, c, omega, 0);
-      ++launches;
+  // cell phase: the four colours run group by group (macro-cells whose vectors fit into the L2
+  // budget), so the re-reads of the later colours hit L2
+  auto cellPhase = [&](bool rev) {
+    if (!lv.nCellBlocks || !(kinds & (1 << KC))) return;
+    const int nPl = lv.N - 3;
+    for (int c0 = 0; c0 < lv.nCells; c0 += ld.cellsPerGroup) {
+      const int nc = std::min(ld.cellsPerGroup, lv.nCells - c0);
+      for (int k = 0; k < 4; ++k) {
+        const int c = rev ? 3 - k : k;
+        dev::cellSorKernel<T><<<nc * nPl, dev::kBlock, 0, stream>>>(lv, st.cellW, u, rhs, mask, c, omega, c0);
+        ++launches;
+      }
     }
   };
-  // P1Operator::smooth_sor (P1Operator.hpp:350-420): full halo refresh, then the phases
-  // V -> E -> F -> C (backwards C -> F -> E -> V) with a refresh of the next phase's copies.
   // Only the copies the reference refreshes between phases are refreshed here, so ghost
   // values that reach a primitive from outside its closure keep their start-of-sweep value.
   comm(kAllGroups);
@@ -479,9 +530,9 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
     comm(1 << G_FACE_BOUNDARY);  // Edge -> Face
     for (int c = 0; c < 3; ++c) faces(c);
     comm(1 << G_CELL);           // Face -> Cell
-    for (int c = 0; c < 4; ++c) cells(c);
+    cellPhase(false);
   } else {
-    for (int c = 3; c >= 0; --c) cells(c);
+    cellPhase(true);
     comm(1 << G_FACE_GHOST);     // Cell -> Face
     for (int c = 2; c >= 0; --c) faces(c);
     comm(1 << G_EDGE);           // Face -> Edge

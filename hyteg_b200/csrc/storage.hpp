@@ -32,6 +32,12 @@ struct LevelData {
   int64_t commBegin[G_COUNT] = {0, 0, 0, 0, 0}, commCount[G_COUNT] = {0, 0, 0, 0, 0};
   dev::Chunk* chunks = nullptr;
   int nChunks = 0;
+  // register-blocked cell sweep: work items grouped by macro-cell groups small enough to stay in L2
+  dev::StripItem* tiles = nullptr;
+  int nTiles = 0;
+  std::vector<int> tileGroupBegin;  // group g: items [tileGroupBegin[g], tileGroupBegin[g + 1])
+  int cellsPerGroup = 0;
+  std::unique_ptr<DevBuf> tileBuf;
   DevBuf partial;
   std::vector<unsigned char> hostCellType, hostFaceType, hostLowType;
   std::vector<std::unique_ptr<DevBuf>> keep;
@@ -67,6 +73,7 @@ struct Storage {
   int nextId = 1;
   int structureOp = -1;
   DevBuf scalars;            // device scratch for reductions
+  int64_t l2Budget = int64_t(1) << 62;  // bytes of L2 one SOR cell group may occupy (default: one group)
   unsigned long long launches = 0;  // kernels launched by this storage
 
   Function& fn(int id);
@@ -99,8 +106,11 @@ struct Storage {
   template <class T>
   void prolongT(int id, int Lc, unsigned mask, bool add);
 
+ void setL2Budget(int64_t bytes);
+
  private:
   void buildLevel(int L);
+  void buildTiles(int L);
 };
 
 struct Error : std::runtime_error {

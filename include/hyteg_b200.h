@@ -87,6 +87,9 @@ int hg_storage_counts(const hg_storage* s, int counts[4]);
 /* Use this CUDA stream (cudaStream_t) for all subsequent work; NULL = the storage's own stream. */
 int hg_storage_set_stream(hg_storage* s, void* stream);
 int hg_storage_synchronize(hg_storage* s);
+/* Bytes of L2 that one group of macro-cells may occupy during the cell phase of an SOR sweep
+ * (the four colour passes of a group run back to back); default: all macro-cells form one group. */
+int hg_storage_set_l2_budget(hg_storage* s, int64_t bytes);
 /* Number of device kernels this storage has launched so far. */
 int hg_storage_launch_count(const hg_storage* s, unsigned long long* count);
 /* Piecewise-constant diffusion coefficient per macro-cell (ncells values) for operators
