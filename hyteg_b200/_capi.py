@@ -72,6 +72,7 @@ _SIGS = {
     "hg_add": (c_int, [c_void_p, c_int, c_int, c_uint, c_int, P(c_double), P(c_int)]),
     "hg_copy_cast": (c_int, [c_void_p, c_int, c_int, c_int, c_uint, c_int]),
     "hg_dot": (c_int, [c_void_p, c_int, c_int, c_int, c_uint, P(c_double)]),
+    "hg_dot_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_uint, c_void_p]),
     "hg_operator_create": (c_int, [c_void_p, c_int, c_int, c_int, P(c_int)]),
     "hg_operator_destroy": (c_int, [c_void_p, c_int]),
     "hg_apply": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_uint, c_int]),

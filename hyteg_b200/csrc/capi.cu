@@ -10,10 +10,6 @@
 #include "solvers.hpp"
 #include "storage.hpp"
 
-struct hg_storage {
-  hg::Storage* s;
-};
-
 struct hg_mesh {
   hg::Discretization* d;
   std::map<std::pair<int, int>, hg::LevelStencils> stencils;  // (level, form)

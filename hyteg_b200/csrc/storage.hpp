@@ -122,3 +122,8 @@ void argCheck(bool ok, const std::string& msg);
 extern thread_local std::string g_lastError;
 
 }  // namespace hg
+
+// Opaque handle of the C-ABI (include/hyteg_b200.h).
+struct hg_storage {
+  hg::Storage* s;
+};

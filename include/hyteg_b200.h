@@ -147,6 +147,16 @@ int hg_add(hg_storage* s, int dst, int level, unsigned flag, int n, const double
 /* dst = (precision of dst) src, or dst += src when add != 0; src and dst may differ in precision */
 int hg_copy_cast(hg_storage* s, int dst, int src, int level, unsigned flag, int add);
 int hg_dot(hg_storage* s, int a, int b, int level, unsigned flag, double* out);
+/* hg_dot without any device allocation, for callers that may not allocate device memory while
+ * they run (e.g. a service that commits its device-memory budget at start-up). No counterpart in
+ * the reference. a, b: device pointers to one level buffer each (hg_function_device_ptr) of the
+ * given precision (8 or 4); result: device pointer to one double, written on the storage's
+ * stream (no synchronisation, no host copy). The scratch is a static device array of 65,536
+ * partial sums: levels that need more blocks are rejected with HG_ERR_ARG. The first call on a
+ * device looks up the array's device address, so make it before any stream capture. Every call
+ * shares the one array: calls that overlap on the GPU (other streams, other threads) race. */
+int hg_dot_noalloc(hg_storage* s, const void* a, const void* b, int precision, int level, unsigned flag,
+                   double* result);
 
 /* form: 0 = diffusion (Laplace, scaled by the per-cell coefficient), 1 = mass */
 int hg_operator_create(hg_storage* s, int form, int min_level, int max_level, int* op);
