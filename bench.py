@@ -5,8 +5,10 @@ Workload (one GPU): P1 Poisson on the unit cube split into 2x2x2 sub-cubes of 6 
 One step = one V(3,3) multigrid cycle (multicolour SOR, omega = 1, linear transfers, CG on
 level 0) on a seeded uniform[-1,1] right-hand side; value = finest inner DoFs per second.
 Also reported: standalone kernels (apply, residual, SOR sweep, restriction, prolongation),
-the roofline of the dominant kernel (cell SOR), the time to a 1e-8 relative residual, an
-end-to-end figure through host buffers, and the reference's own CPU kernels as baseline.
+the roofline of the dominant kernel (cell SOR), the time to a 1e-8 relative residual of FP64
+GMG against mixed precision (FP32 cycles inside FP64 defect correction) on the manufactured
+problem, the variable-coefficient case to 1e-10, an end-to-end figure through host buffers,
+and the reference's own CPU kernels as baseline.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--level L]
 
@@ -259,13 +261,83 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def load_traffic(kernel):
-    """Per-launch DRAM bytes of `kernel` at the benchmark level from profiles/<kernel>_traffic.json."""
+def load_traffic(kernel, L):
+    """Per-launch DRAM bytes (read + write) of `kernel` at level L, from the ncu summary
+    profiles/traffic.json ({kernel: {level: bytes}}), or None."""
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            return json.load(f).get(kernel)
-    except (OSError, ValueError):
+            return json.load(f).get(kernel, {}).get(str(L))
+    except (OSError, ValueError, AttributeError):
         return None
+
+
+def time_to_solution(hg, st, A, L, N_in, Inner):
+    """Manufactured problem -Lap u = 3 pi^2 u, u = sin(pi x) sin(pi y) sin(pi z), b = M I(f), x0 = 0:
+    FP64 V(3,3) cycles vs FP64 defect correction around FP32 V(3,3) cycles, each to a 1e-8
+    relative residual; then the variable-coefficient case k(x) = 1 + 0.5 sin(2 pi x) cos(2 pi y) z
+    (piecewise constant per macro-cell) to 1e-10. Errors are discrete L2 (RMS over inner DoFs)."""
+    import torch
+    M = hg.P1ConstantMassOperator(st, L, L)
+    f = hg.P1Function("f", st, L, L)
+    u = hg.P1Function("u", st, L, L)
+    e = hg.P1Function("e", st, L, L)
+    bm = hg.P1Function("bm", st, 0, L)
+    xs = hg.P1Function("xs", st, 0, L)
+    x64 = hg.P1Function("x64", st, L, L)
+    u.interpolate_sines(1.0, 1.0, L)
+    f.interpolate_sines(3 * np.pi ** 2, 1.0, L)
+    M.apply(f, bm, L, Inner)
+    del M, f
+
+    def rms(a, b_=None):
+        if b_ is not None:
+            e.assign([1.0, -1.0], [a, b_], L, Inner)
+            a = e
+        return float(np.sqrt(a.dotGlobal(a, L, Inner) / N_in))
+
+    def run(op, rhs, dtype, tol):
+        g = hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 50, 1e-16),
+                                        hg.P1toP1LinearRestriction(), hg.P1toP1LinearProlongation(), 0, L, 3, 3,
+                                        dtype=dtype)
+        xs.interpolate(0.0, L, hg.All)
+        g.solve_to(op, xs, rhs, L, tol, 2)       # warm-up: workspace allocation, first launches
+        xs.interpolate(0.0, L, hg.All)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it, rel, hist = g.solve_to(op, xs, rhs, L, tol, 100)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        del g
+        factors = [float(hist[0])] + [float(hist[i + 1] / hist[i]) for i in range(len(hist) - 1)]
+        return {"iterations": it, "seconds": dt, "final_rel_residual": rel, "convergence_factors": factors}
+
+    out = {"problem": "manufactured u = sin(pi x) sin(pi y) sin(pi z), b = M I(3 pi^2 u), x0 = 0, Dirichlet 0",
+           "target_rel_residual": 1e-8, "error_norm": "discrete L2 (RMS over inner DoFs)"}
+    r64 = run(A, bm, np.float64, 1e-8)
+    r64["err_vs_manufactured"] = rms(xs, u)
+    x64.assign([1.0], [xs], L, hg.All)
+    r32 = run(A, bm, np.float32, 1e-8)
+    r32["err_vs_manufactured"] = rms(xs, u)
+    r32["err_vs_fp64_solve"] = rms(xs, x64) / rms(x64)
+    out["fp64"], out["mixed"] = r64, r32
+    out["speedup_mixed_vs_fp64"] = r64["seconds"] / r32["seconds"]
+
+    # variable coefficient, 1e-10 (errors against the FP64 GPU solve)
+    mesh = st.host()
+    nc = mesh.counts()[3]
+    cent = np.array([np.mean([mesh.primitive(hg.VERTEX, v)[1] for v in mesh.primitive(hg.CELL, c)[0]], axis=0)
+                     for c in range(nc)])
+    st.set_cell_coefficients(1.0 + 0.5 * np.sin(2 * np.pi * cent[:, 0]) * np.cos(2 * np.pi * cent[:, 1]) * cent[:, 2])
+    Ak = hg.P1ConstantLaplaceOperator(st, 0, L)
+    v64 = run(Ak, bm, np.float64, 1e-10)
+    x64.assign([1.0], [xs], L, hg.All)
+    v32 = run(Ak, bm, np.float32, 1e-10)
+    v32["err_vs_fp64_solve"] = rms(xs, x64) / rms(x64)
+    out["variable_k"] = {"k": "1 + 0.5 sin(2 pi x) cos(2 pi y) z at macro-cell centroids", "target_rel_residual": 1e-10,
+                         "fp64": v64, "mixed": v32, "speedup_mixed_vs_fp64": v64["seconds"] / v32["seconds"]}
+    del Ak
+    st.set_cell_coefficients(np.ones(nc))
+    return out
 
 
 def run_ours(args):
@@ -320,35 +392,27 @@ def run_ours(args):
     kern["restrict"] = timed(lambda: hg.P1toP1LinearRestriction().restrict(r, L, Inner), 5)
     kern["prolongate_add"] = timed(lambda: hg.P1toP1LinearProlongation().prolongateAndAdd(x, L - 1, Inner), 5)
     kern["halo_refresh"] = timed(lambda: x.communicate(L), 5)
-    # dominant kernel alone: cell SOR (4 colour launches per sweep) and cell apply
-    t_sor_cells = timed(lambda: A.smooth_sor_primitives(x, b, 1.0, L, Inner, kinds=1 << hg.CELL, refresh=False), 3)
+    # dominant kernel alone: the cell phase of the SOR sweep (one single-pass launch plus the copy
+    # of the face/edge/vertex arrays into the exchanged buffer), and cell apply
+    t_sor_cells = timed(lambda: A.smooth_sor_primitives(x, b, 1.0, L, Inner, kinds=1 << hg.CELL, refresh=False), 4)
     t_apply_cells = timed(lambda: A.apply_primitives(x, r, L, Inner, kinds=1 << hg.CELL, refresh=False), 5)
+    st.set_sor_schedule(1)    # the four in-place colour passes, for comparison
+    t_sor_passes = timed(lambda: A.smooth_sor_primitives(x, b, 1.0, L, Inner, kinds=1 << hg.CELL, refresh=False), 2)
+    kern["sor_sweep_colour_passes"] = timed(lambda: A.smooth_sor(x, b, 1.0, L, Inner), 2)
+    st.set_sor_schedule(0)
     Nc = cell_inner_dofs(L)
     kernels = {k: {"ms": v * 1e3, "gdofs": N_in / v / 1e9} for k, v in kern.items()}
-    for k in ("apply", "residual", "sor_sweep"):
-        kernels[k]["GBs_algorithmic"] = BYTES[k] * N_in / kern[k] / 1e9
-    kernels["cell_sor_colour_launch"] = {"ms": t_sor_cells / 4 * 1e3,
-                                         "GBs_algorithmic": BYTES["sor_sweep"] * Nc / 4 / (t_sor_cells / 4) / 1e9}
+    for k in ("apply", "residual", "sor_sweep", "sor_sweep_colour_passes"):
+        kernels[k]["GBs_algorithmic"] = BYTES[k.replace("_colour_passes", "")] * N_in / kern[k] / 1e9
+    kernels["cell_sor_single_pass"] = {"ms": t_sor_cells * 1e3,
+                                       "GBs_algorithmic": BYTES["sor_sweep"] * Nc / t_sor_cells / 1e9}
+    kernels["cell_sor_colour_passes"] = {"ms": t_sor_passes * 1e3,
+                                         "GBs_algorithmic": BYTES["sor_sweep"] * Nc / t_sor_passes / 1e9}
     kernels["cell_apply_launch"] = {"ms": t_apply_cells * 1e3, "GBs_algorithmic": BYTES["apply"] * Nc / t_apply_cells / 1e9}
 
-    # --- time to 1e-8 relative residual, FP64 GMG from x = 0 -------------------------------
-    def rel_res():
-        A.residual(x, b, r, L, Inner)
-        return np.sqrt(r.dotGlobal(r, L, Inner))
-
-    x.interpolate(0.0, L, hg.All)
-    r0 = rel_res()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    cycles, rel, hist = 0, 1.0, []
-    while rel > 1e-8 and cycles < 50:
-        gmg.solve(A, x, b, L)
-        cycles += 1
-        rel = rel_res() / r0
-        hist.append(rel)
-    torch.cuda.synchronize()
-    t_solve = time.perf_counter() - t0
-    factors = [hist[i + 1] / hist[i] for i in range(len(hist) - 1)]
+    # --- time to solution: FP64 GMG vs mixed precision (FP32 cycles inside FP64 defect correction)
+    solve = time_to_solution(hg, st, A, L, N_in, Inner)
+    x.from_numpy(L, host_b.numpy())
 
     # --- the timed region: K V(3,3) cycles --------------------------------------------------
     for _ in range(args.warmup):
@@ -358,11 +422,13 @@ def run_ours(args):
     torch.cuda.synchronize()
     with Clocks(local) as clk:
         e0, e1 = ev(), ev()
+        torch.cuda.nvtx.range_push("timed_cycles")   # launch-list filter for ncu --nvtx-include
         e0.record(stream)
         for _ in range(args.steps):
             gmg.solve(A, x, b, L)
         e1.record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
     t_steps = e0.elapsed_time(e1) * 1e-3
     launches = st.launch_count() - launches0
     barrier(pg)
@@ -385,25 +451,24 @@ def run_ours(args):
     t_e2e = max_over_ranks(e0.elapsed_time(e1) * 1e-3, pg)
 
     peak, peak_kind = load_peaks()
-    t_launch = t_sor_cells / 4
-    achieved = BYTES["sor_sweep"] * Nc / 4 / t_launch / 1e9
-    traffic = load_traffic("cellSorKernel")
+    achieved = BYTES["sor_sweep"] * Nc / t_sor_cells / 1e9
+    traffic = load_traffic("cellSorWaveKernel<double>", L)
     out = {
         "metric": "GDoF/s", "value": value, "unit": "GDoF/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded uniform[-1,1] right-hand side)",
         "config": workload_config(L),
-        "roofline": {"kernel": "cellSorKernel<double> (one colour of the cell-interior SOR sweep)", "bound": "hbm",
+        "roofline": {"kernel": "cellSorWaveKernel<double> (cell-interior multicolour SOR sweep, one launch; timed "
+                               "with the copy of the non-cell arrays into the exchanged buffer)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": BYTES["sor_sweep"] * Nc / 4},
+                     "algorithmic_bytes_per_launch": BYTES["sor_sweep"] * Nc},
         "e2e": {"value": world * N_in * args.steps / t_e2e / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": n * 8,
                 "d2h_bytes_per_step": 8},
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "kernels": kernels,
-        "solve": {"precision": "fp64", "target_rel_residual": 1e-8, "cycles": cycles, "seconds": t_solve,
-                  "final_rel_residual": rel, "convergence_factors": factors},
+        "solve": solve,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         thr = host_threads()

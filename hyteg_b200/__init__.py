@@ -207,6 +207,10 @@ class PrimitiveStorage:
         if self._host is not None:
             self._host.set_cell_coefficients(k)
 
+    def set_sor_schedule(self, schedule):
+        """0: single-pass wavefront SOR (level buffers double-buffered), 1: in-place colour passes."""
+        call("hg_storage_set_sor_schedule", self._h, int(schedule))
+
     def set_stream(self, stream_ptr):
         call("hg_storage_set_stream", self._h, ctypes.c_void_p(stream_ptr))
 
@@ -284,6 +288,16 @@ class P1Function:
             self.from_numpy(level, cur)
         else:
             call("hg_interpolate_const", self.storage.handle, self.id, float(value), level, flag)
+
+    def interpolate_sines(self, amplitude, k, level, flag=All):
+        """amplitude * sin(k pi x) sin(k pi y) sin(k pi z), evaluated on the device."""
+        p = np.array([amplitude, k, 0.0, 0.0])
+        call("hg_interpolate_expr", self.storage.handle, self.id, level, flag, 0, dptr(p))
+
+    def interpolate_linear(self, a, b, c, d, level, flag=All):
+        """a + b x + c y + d z, evaluated on the device."""
+        p = np.array([a, b, c, d], dtype=np.float64)
+        call("hg_interpolate_expr", self.storage.handle, self.id, level, flag, 1, dptr(p))
 
     def assign(self, scalars, functions, level, flag=All):
         s = np.ascontiguousarray(scalars, dtype=np.float64)
@@ -450,6 +464,16 @@ class GeometricMultigridSolver:
 
     def solve(self, A, x, b, level):
         call("hg_gmg_solve", self.storage.handle, self._handle(A), x.id, b.id, level)
+
+    def solve_to(self, A, x, b, level, tol, max_iter=100):
+        """Iterate to a relative residual tol (FP64 x, b). An FP32 solver runs FP64 defect
+        correction around FP32 cycles. Returns (iterations, relative residual, history)."""
+        it = ctypes.c_int()
+        rel = ctypes.c_double()
+        hist = np.zeros(max_iter)
+        call("hg_gmg_solve_to", self.storage.handle, self._handle(A), x.id, b.id, level, float(tol), int(max_iter),
+             ctypes.byref(it), ctypes.byref(rel), dptr(hist), int(max_iter))
+        return it.value, rel.value, hist[: it.value].copy()
 
     def __del__(self):
         try:

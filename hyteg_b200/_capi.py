@@ -63,11 +63,13 @@ _SIGS = {
     "hg_mesh_low_stencil": (c_int, [c_void_p, c_int, c_int, c_int, c_int, P(c_int64), P(c_double), c_int, P(c_int)]),
     "hg_function_create": (c_int, [c_void_p, c_int, c_int, c_int, P(c_int)]),
     "hg_function_destroy": (c_int, [c_void_p, c_int]),
+    "hg_storage_set_sor_schedule": (c_int, [c_void_p, c_int]),
     "hg_function_device_ptr": (c_int, [c_void_p, c_int, c_int, P(c_void_p)]),
     "hg_function_upload": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64]),
     "hg_function_download": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64]),
     "hg_communicate": (c_int, [c_void_p, c_int, c_int]),
     "hg_interpolate_const": (c_int, [c_void_p, c_int, c_double, c_int, c_uint]),
+    "hg_interpolate_expr": (c_int, [c_void_p, c_int, c_int, c_uint, c_int, P(c_double)]),
     "hg_assign": (c_int, [c_void_p, c_int, c_int, c_uint, c_int, P(c_double), P(c_int)]),
     "hg_add": (c_int, [c_void_p, c_int, c_int, c_uint, c_int, P(c_double), P(c_int)]),
     "hg_copy_cast": (c_int, [c_void_p, c_int, c_int, c_int, c_uint, c_int]),
@@ -86,6 +88,8 @@ _SIGS = {
     "hg_gmg_create": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_double, c_int, P(c_int)]),
     "hg_gmg_destroy": (c_int, [c_void_p, c_int]),
     "hg_gmg_solve": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
+    "hg_gmg_solve_to": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_int, P(c_int), P(c_double), P(c_double),
+                                c_int]),
 }
 
 

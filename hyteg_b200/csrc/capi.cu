@@ -151,6 +151,13 @@ int hg_storage_set_cell_coefficients(hg_storage* h, const double* k, int ncells)
   HG_CATCH
 }
 
+int hg_storage_set_sor_schedule(hg_storage* h, int schedule) {
+  HG_TRY
+  hg::argCheck(schedule == 0 || schedule == 1, "SOR schedule must be 0 (single pass) or 1 (colour passes)");
+  S(h).sorSchedule = schedule;
+  HG_CATCH
+}
+
 int hg_primitive_vertices(const hg_storage* h, int kind, int prim, int ids[4], double coords[3], int* flag) {
   HG_TRY
   const auto& t = S(h).disc.topo();
@@ -274,6 +281,13 @@ int hg_communicate(hg_storage* h, int fn, int level) {
 int hg_interpolate_const(hg_storage* h, int fn, double value, int level, unsigned flag) {
   HG_TRY
   S(h).lincomb(fn, level, flag, 0, nullptr, nullptr, false, value);
+  HG_CATCH
+}
+
+int hg_interpolate_expr(hg_storage* h, int fn, int level, unsigned flag, int expr, const double params[4]) {
+  HG_TRY
+  hg::argCheck(params != nullptr, "null parameters");
+  S(h).interpolateExpr(fn, level, flag, expr, params);
   HG_CATCH
 }
 
@@ -663,6 +677,18 @@ int hg_mesh_low_stencil(const hg_mesh* m, int level, int form, int kind, int pri
     rel[k] = e[k].rel;
     w[k] = e[k].w;
   }
+  HG_CATCH
+}
+
+int hg_gmg_solve_to(hg_storage* h, int gmg, int x, int b, int level, double tol, int max_iter, int* iterations,
+                    double* rel_residual, double* history, int history_cap) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  auto it = s.gmgs.find(gmg);
+  hg::argCheck(it != s.gmgs.end(), "unknown multigrid handle");
+  hg::argCheck(tol > 0.0 && max_iter >= 0, "tolerance must be positive");
+  const int n = it->second->solveTo(x, b, level, tol, max_iter, rel_residual, history, history_cap);
+  if (iterations) *iterations = n;
   HG_CATCH
 }
 

@@ -193,6 +193,168 @@ __global__ void __launch_bounds__(kBlock, 4) cellSorKernel(LevelDev lv, const T*
 }
 
 // ---------------------------------------------------------------------------------------
+// Multicolour SOR on cell interiors in a single pass (z-wavefront, out of place).
+// The colour of (x, y, z) is (x + 2y + 3z) mod 4 and the sweep visits the colours in the
+// sequence seq = 0,1,2,3 (backwards: 3,2,1,0). At step s a block runs colour seq[k] on plane
+// s - 2k for k = 0..3. For every stencil offset a neighbour earlier in the sequence was updated
+// in an earlier step and a neighbour later in the sequence is updated in a later step, so the
+// result equals four separate colour sweeps over the whole cell, and the four stages of a step
+// touch disjoint data (they write the planes s, s-2, s-4, s-6 and read only those and the odd
+// planes between them) and need no barrier between them.
+// A block owns a 32 x 30 (x, y) tile of one macro-cell for all planes. It recomputes a shrinking
+// halo (stage k on the tile widened by 3 - k) from the start-of-sweep values, which makes the
+// tiles independent: they read uOld and write uNew, and the caller swaps the two buffers.
+// Planes s-7 .. s+1 of the tile widened by 4 (40 x 38) live in a 9-slot shared-memory ring;
+// plane s+2 is loaded into registers during step s and stored into the slot plane s-7 frees.
+// Rows are stored colour-split (x mod 4 major), so the points of one colour and each of their
+// x-neighbours are contiguous. Thread t < 380 owns the four columns 4(t mod 10) .. +3 of region
+// row t / 10: it loads and stores them and, in every stage, updates the one of them that
+// carries the stage's colour.
+// ---------------------------------------------------------------------------------------
+constexpr int kWaveTX = 32;                         // tile extent in x (multiple of 4)
+constexpr int kWaveTY = 30;                         // tile extent in y
+constexpr int kWaveH = 4;                           // halo loaded around the tile
+constexpr int kWaveRX = kWaveTX + 2 * kWaveH;       // region extent in x (40)
+constexpr int kWaveRY = kWaveTY + 2 * kWaveH;       // region extent in y (38)
+constexpr int kWaveQ = kWaveRX / 4;                 // column groups per region row (10)
+constexpr int kWavePlane = kWaveRX * kWaveRY;       // elements per plane slot
+constexpr int kWaveSlots = 9;
+constexpr int kWaveGroups = kWaveRY * kWaveQ;       // 380 column groups, one per thread
+constexpr int kWaveThreads = 384;
+constexpr int kWaveMaxN = 4096;                     // largest level size the shared-memory limit is set for
+
+struct WaveTile {
+  int cell, x0, y0, pEnd;  // tile origin; pEnd = N - x0 - y0, its last plane
+};
+
+// Dynamic shared memory of the kernel for level size N.
+template <class T>
+inline size_t waveSmemBytes(int N) {
+  return size_t(kWaveSlots) * kWavePlane * sizeof(T) + size_t(N + 2) * sizeof(int);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kWaveThreads, 2)
+    cellSorWaveKernel(LevelDev lv, const WaveTile* __restrict__ tiles, const T* __restrict__ cellW,
+                      const T* __restrict__ uOld, T* __restrict__ uNew, const T* __restrict__ rhs, unsigned mask,
+                      T omega, int backwards) {
+  extern __shared__ __align__(16) unsigned char waveSmem[];
+  T* sm = reinterpret_cast<T*>(waveSmem);
+  int* pbTab = reinterpret_cast<int*>(sm + kWaveSlots * kWavePlane);  // first index of plane p
+  const WaveTile tl = tiles[blockIdx.x];
+  const int N = lv.N, w = lv.w, tid = threadIdx.x;
+  const int64_t base = lv.cellOff[tl.cell];
+  const T* __restrict__ uo = uOld + base;
+  T* __restrict__ un = uNew + base;
+  const T* __restrict__ f = rhs + base;
+  const int xb = tl.x0 - kWaveH, yb = tl.y0 - kWaveH;  // region origin in cell coordinates
+  for (int p = tid; p <= N; p += kWaveThreads) pbTab[p] = int(tetSize(w) - tetSize(w - p));
+  // the thread's column group: region row gy, region columns 4 gx .. 4 gx + 3
+  const bool owner = tid < kWaveGroups;
+  const int gy = tid / kWaveQ, gx = tid - (tid / kWaveQ) * kWaveQ;
+  const int y = yb + gy, x4 = xb + 4 * gx;
+  const int Ay = y * (w + 1) - (y * (y + 1)) / 2;  // rowStart(w - p, y) = Ay - y p
+  const int so = gy * kWaveRX + gx;                 // slot offset of column j: so + j Q
+  __syncthreads();
+
+  if (!(lv.cellType[tl.cell] & mask)) {  // not smoothed: the tile is copied
+    if (owner && gy >= kWaveH && gy < kWaveH + kWaveTY && gx >= 1 && gx < kWaveQ - 1)
+      for (int p = 0; p <= tl.pEnd; ++p)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (x4 + j + y <= N - p) {
+            const int g = pbTab[p] + Ay - y * p + x4 + j;
+            un[g] = uo[g];
+          }
+    return;
+  }
+  T wt[15];
+#pragma unroll
+  for (int k = 0; k < 15; ++k) wt[k] = cellW[16 * tl.cell + k];
+  const T om1 = T(1) - omega, dinv = omega / wt[0];
+  const int qy = (-2 * y) & 3;
+  unsigned rowBits = 0;  // bit k: row gy lies in the region of stage k and y >= 1
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (owner && gy >= k + 1 && gy < kWaveRY - 1 - k && y >= 1) rowBits |= 1u << k;
+  const bool storer = owner && gy >= kWaveH && gy < kWaveH + kWaveTY && gx >= 1 && gx < kWaveQ - 1;
+
+  T stg[4];
+  auto loadRegs = [&](int p) {  // plane p of the thread's columns (points of the closed cell)
+    if (owner && p <= N && y >= 0 && y <= N - p) {
+      const int g = pbTab[p] + Ay - y * p + x4;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (x4 + j >= 0 && x4 + j + y <= N - p) stg[j] = uo[g + j];
+    }
+  };
+  auto storeRegs = [&](int p) {
+    if (owner && p <= N && y >= 0 && y <= N - p) {
+      T* s = sm + (p % kWaveSlots) * kWavePlane + so;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (x4 + j >= 0 && x4 + j + y <= N - p) s[j * kWaveQ] = stg[j];
+    }
+  };
+  auto stage = [&](int k, int p) {  // colour seq[k] on plane p, region = tile widened by 3 - k
+    if (!((rowBits >> k) & 1u)) return;
+    const int c = backwards ? 3 - k : k;
+    const int q = (c + qy + p) & 3;  // the group's column with colour c in row y of plane p
+    const int rx = 4 * gx + q, x = xb + rx;
+    if (rx < k + 1 || rx >= kWaveRX - 1 - k || x < 1 || x + y > N - 1 - p) return;
+    T* sP = sm + (p % kWaveSlots) * kWavePlane;
+    const T* sT = sm + ((p + 1) % kWaveSlots) * kWavePlane;
+    const T* sB = sm + ((p - 1) % kWaveSlots) * kWavePlane;
+    const int o = so + q * kWaveQ;
+    const int dE = q < 3 ? kWaveQ : 1 - 3 * kWaveQ;   // offset of x + 1
+    const int dW = q > 0 ? -kWaveQ : 3 * kWaveQ - 1;  // offset of x - 1
+    const T rh = f[pbTab[p] + Ay - y * p + x];
+    // three independent partial sums (this plane, the plane above, the plane below)
+    T a = wt[1] * sP[o + dE];
+    a += wt[2] * sP[o + dW];
+    a += wt[3] * sP[o + kWaveRX];
+    a += wt[4] * sP[o - kWaveRX];
+    a += wt[5] * sP[o + kWaveRX + dW];
+    a += wt[6] * sP[o - kWaveRX + dE];
+    T t = wt[7] * sT[o];
+    t += wt[8] * sT[o + dW];
+    t += wt[9] * sT[o - kWaveRX];
+    t += wt[10] * sT[o - kWaveRX + dE];
+    T b = wt[11] * sB[o];
+    b += wt[12] * sB[o + dE];
+    b += wt[13] * sB[o + kWaveRX];
+    b += wt[14] * sB[o + kWaveRX + dW];
+    sP[o] = om1 * sP[o] + (rh - (a + (t + b))) * dinv;
+  };
+  auto store = [&](int p) {  // the tile's points of plane p (interior and boundary) to uNew
+    if (!storer || y > N - p) return;
+    const T* s = sm + (p % kWaveSlots) * kWavePlane + so;
+    const int g = pbTab[p] + Ay - y * p + x4;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (x4 + j + y <= N - p) un[g + j] = s[j * kWaveQ];
+  };
+
+  loadRegs(0);
+  storeRegs(0);
+  loadRegs(1);
+  storeRegs(1);
+  const int sEnd = tl.pEnd + 6;
+  for (int s = 0; s <= sEnd; ++s) {
+    loadRegs(s + 2);
+    __syncthreads();  // the previous step's stores into the ring are visible
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int p = s - 2 * k;
+      if (p >= 1 && p <= N - 3) stage(k, p);
+    }
+    __syncthreads();  // plane s-7 is no longer read; plane s-6 is final
+    storeRegs(s + 2);
+    if (s >= 6 && s - 6 <= tl.pEnd) store(s - 6);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // Register-blocked 2.5-D cell sweep (the kernel behind apply and residual on cell interiors).
 // A warp owns a strip of 30 x-columns (lanes 1..30; lanes 0 and 31 only carry the x-halo) by
 // kStripR rows and marches up z through a range of planes. Each lane keeps the rows
@@ -609,6 +771,82 @@ __global__ void __launch_bounds__(kBlock) lowProlongKernel(LevelDev lf, LevelDev
   const int64_t c = lf.lowOff[b.prim] + x;
   if (ADD) fine[c] += v;
   else fine[c] = v;
+}
+
+// ---------------------------------------------------------------------------------------
+// Interpolation of built-in expressions at the owned DoFs (VertexDoFFunction::interpolate):
+//   expr 0: a * sin(k pi x) sin(k pi y) sin(k pi z)       (params a, k)
+//   expr 1: a + b x + c y + d z                           (params a, b, c, d)
+// Coordinates are the barycentric combination of the primitive's macro-vertices.
+// ---------------------------------------------------------------------------------------
+struct Geometry {
+  const double* vx;    // [nVerts][3]
+  const int* cellV;    // [nCells][4] (frame order)
+  const int* faceV;    // [nFaces][3]
+  const int* lowV;     // [nLow][2]: edges (v0, v1), vertices (v, v)
+};
+
+__device__ __forceinline__ double evalExpr(int expr, const double* p, double x, double y, double z) {
+  if (expr == 0) {
+    const double k = p[1] * 3.141592653589793;
+    return p[0] * sin(k * x) * sin(k * y) * sin(k * z);
+  }
+  return p[0] + p[1] * x + p[2] * y + p[3] * z;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) interpolateKernel(LevelDev lv, Geometry g, T* __restrict__ dst, unsigned mask,
+                                                            int expr, double p0, double p1, double p2, double p3) {
+  const double prm[4] = {p0, p1, p2, p3};
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double invN = 1.0 / lv.N;
+  int blk = blockIdx.x;
+  const int nCellGrid = lv.nCellBlocks;
+  if (blk < nCellGrid) {
+    const int nPl = lv.N - 3;
+    const int c = blk / nPl, z = 1 + blk % nPl;
+    if (!(lv.cellType[c] & mask)) return;
+    const int* cv = g.cellV + 4 * c;
+    const int W = lv.w - z;
+    T* d = dst + lv.cellOff[c];
+    for (int y = 1 + warp; y <= W - 3; y += kBlock / 32) {
+      const int r0 = int(tetSize(lv.w) - tetSize(W)) + rowStart(W, y);
+      for (int x = 1 + lane; x <= W - 2 - y; x += 32) {
+        const double b[4] = {double(lv.N - x - y - z), double(x), double(y), double(z)};
+        double q[3] = {0, 0, 0};
+        for (int k = 0; k < 4; ++k)
+          for (int e = 0; e < 3; ++e) q[e] += b[k] * g.vx[3 * cv[k] + e];
+        d[r0 + x] = T(evalExpr(expr, prm, q[0] * invN, q[1] * invN, q[2] * invN));
+      }
+    }
+  } else if ((blk -= nCellGrid) < lv.nFaceBlocks) {
+    const FaceBlock fb = lv.faceBlocks[blk];
+    if (!(lv.faceType[fb.face] & mask)) return;
+    const int* fv = g.faceV + 3 * fb.face;
+    T* d = dst + lv.faceOff[fb.face];
+    const int yEnd = min(fb.start + kFaceRows, lv.w - 2);
+    for (int y = fb.start + warp; y < yEnd; y += kBlock / 32) {
+      const int r0 = rowStart(lv.w, y);
+      for (int x = 1 + lane; x <= lv.w - 2 - y; x += 32) {
+        const double b[3] = {double(lv.N - x - y), double(x), double(y)};
+        double q[3] = {0, 0, 0};
+        for (int k = 0; k < 3; ++k)
+          for (int e = 0; e < 3; ++e) q[e] += b[k] * g.vx[3 * fv[k] + e];
+        d[r0 + x] = T(evalExpr(expr, prm, q[0] * invN, q[1] * invN, q[2] * invN));
+      }
+    }
+  } else {
+    blk -= lv.nFaceBlocks;
+    const LowBlock lb = lv.lowBlocks[blk];
+    if (!(lv.lowType[lb.prim] & mask)) return;
+    const int x = lb.start + threadIdx.x;
+    if (x >= lv.lowFirst[lb.prim] + lv.lowCount[lb.prim]) return;
+    const int* ev = g.lowV + 2 * lb.prim;
+    const double b0 = lb.prim < lv.nEdges ? double(lv.N - x) : double(lv.N), b1 = lb.prim < lv.nEdges ? double(x) : 0.0;
+    double q[3];
+    for (int e = 0; e < 3; ++e) q[e] = (b0 * g.vx[3 * ev[0] + e] + b1 * g.vx[3 * ev[1] + e]) * invN;
+    dst[lv.lowOff[lb.prim] + x] = T(evalExpr(expr, prm, q[0], q[1], q[2]));
+  }
 }
 
 // ---------------------------------------------------------------------------------------

@@ -57,21 +57,42 @@ Gmg::Gmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int post_, double
     : s(st), op(op_), minL(minL_), maxL(maxL_), pre(pre_), post(post_), omega(omega_), cycle(cycle_),
       coarseMaxIter(cmax), coarseTol(ctol), prec(prec_) {
   tmp = s.createFunction(minL, maxL, prec);
-  cp = s.createFunction(minL, minL, prec);
-  cz = s.createFunction(minL, minL, prec);
-  cap = s.createFunction(minL, minL, prec);
-  cr = s.createFunction(minL, minL, prec);
+  // the coarse-grid CG always runs in FP64
+  cp = s.createFunction(minL, minL, 8);
+  cz = s.createFunction(minL, minL, 8);
+  cap = s.createFunction(minL, minL, 8);
+  cr = s.createFunction(minL, minL, 8);
+  if (prec == 4) {
+    cx64 = s.createFunction(minL, minL, 8);
+    cb64 = s.createFunction(minL, minL, 8);
+    x32 = s.createFunction(minL, maxL, 4);
+    b32 = s.createFunction(minL, maxL, 4);
+    r64 = s.createFunction(maxL, maxL, 8);
+  }
 }
 
 Gmg::~Gmg() {
-  for (int id : {tmp, cp, cz, cap, cr}) s.fns.erase(id);
+  for (int id : {tmp, cp, cz, cap, cr, cx64, cb64, x32, b32, r64})
+    if (id >= 0) s.fns.erase(id);
+}
+
+void Gmg::coarseSolve(int x, int b, int L) {
+  if (prec == 8) {
+    cgSolve(s, op, x, b, L, coarseMaxIter, coarseTol, cp, cz, cap, cr, nullptr);
+    return;
+  }
+  // FP32 hierarchy: the coarse problem is solved in FP64 and the result rounded back
+  s.copyCast(cb64, b, L, HG_ALL, false);
+  s.copyCast(cx64, x, L, HG_ALL, false);
+  cgSolve(s, op, cx64, cb64, L, coarseMaxIter, coarseTol, cp, cz, cap, cr, nullptr);
+  s.copyCast(x, cx64, L, HG_ALL, false);
 }
 
 // GeometricMultigridSolver::solveRecursively (src/hyteg/solvers/GeometricMultigridSolver.hpp:136-235)
 void Gmg::solveRecursively(int x, int b, int L) {
   const unsigned flag = HG_INNER | HG_NEUMANN;
   if (L == minL) {
-    cgSolve(s, op, x, b, L, coarseMaxIter, coarseTol, cp, cz, cap, cr, nullptr);
+    coarseSolve(x, b, L);
     return;
   }
   for (int i = 0; i < pre; ++i) s.smoothSor(op, x, b, omega, L, flag, false);
@@ -84,6 +105,35 @@ void Gmg::solveRecursively(int x, int b, int L) {
   if (cycle == 1) solveRecursively(x, b, L - 1);
   s.prolongate(x, L - 1, flag, true);
   for (int i = 0; i < post; ++i) s.smoothSor(op, x, b, omega, L, flag, false);
+}
+
+int Gmg::solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap) {
+  const unsigned flag = HG_INNER | HG_NEUMANN;
+  argCheck(L >= minL && L <= maxL, "gmg: level outside the solver's range");
+  Function& fx = s.fn(x);
+  argCheck(fx.prec == 8 && s.fn(b).prec == 8, "solveTo: x and b must be FP64 functions");
+  const int r = prec == 8 ? tmp : r64;
+  s.residual(op, x, b, r, L, flag);
+  const double r0 = std::sqrt(s.dot(r, r, L, flag));
+  double rel = 1.0;
+  int it = 0;
+  while (it < maxIter && rel > tol && r0 > 0.0) {
+    if (prec == 8) {
+      solveRecursively(x, b, L);
+    } else {
+      // defect correction: FP32 cycle on A e = r (zero start), x += e in FP64
+      s.copyCast(b32, r, L, HG_ALL, false);
+      for (int l = minL; l <= L; ++l) s.lincomb(x32, l, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+      solveRecursively(x32, b32, L);
+      s.copyCast(x, x32, L, flag, true);
+    }
+    ++it;
+    s.residual(op, x, b, r, L, flag);
+    rel = std::sqrt(s.dot(r, r, L, flag)) / r0;
+    if (history && it <= historyCap) history[it - 1] = rel;
+  }
+  if (relRes) *relRes = r0 > 0.0 ? rel : 0.0;
+  return it;
 }
 
 void Gmg::solve(int x, int b, int L) {

@@ -15,6 +15,10 @@ struct Gmg {
   ~Gmg();
   void solve(int x, int b, int L);
   void solveRecursively(int x, int b, int L);
+  // Cycles (prec 8) or FP64 defect-correction steps around one FP32 cycle (prec 4; x, b FP64)
+  // until ||b - A x|| <= tol * ||b - A x0|| or maxIter; returns the iterations taken.
+  int solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap);
+  void coarseSolve(int x, int b, int L);
 
   Storage& s;
   int op, minL, maxL, pre, post;
@@ -23,6 +27,8 @@ struct Gmg {
   double coarseTol;
   int prec;
   int tmp, cp, cz, cap, cr;
+  // FP32 solvers: FP64 coarse-grid workspace and the FP32 correction / defect hierarchy
+  int cx64 = -1, cb64 = -1, x32 = -1, b32 = -1, r64 = -1;
 };
 
 }  // namespace hg

@@ -66,9 +66,38 @@ static unsigned char dofType(int meshFlag) {
 
 Storage::Storage(const Topology& topo, int maxLevel) : disc(topo, maxLevel) {
   cudaCheck(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "cudaStreamCreate");
+  cudaCheck(cudaFuncSetAttribute(dev::cellSorWaveKernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dev::waveSmemBytes<double>(dev::kWaveMaxN)),
+            "wave kernel shared memory");
+  cudaCheck(cudaFuncSetAttribute(dev::cellSorWaveKernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dev::waveSmemBytes<float>(dev::kWaveMaxN)),
+            "wave kernel shared memory");
   stream = ownStream;
   levels.resize(maxLevel + 1);
   for (int L = 0; L <= maxLevel; ++L) buildLevel(L);
+  {
+    const Topology& t = disc.topo();
+    std::vector<double> vx;
+    for (auto& v : t.verts)
+      for (int d = 0; d < 3; ++d) vx.push_back(v.x[d]);
+    std::vector<int> cv, fv, lv;
+    for (auto& c : t.cells)
+      for (int k = 0; k < 4; ++k) cv.push_back(c.v[k]);
+    for (auto& f : t.faces)
+      for (int k = 0; k < 3; ++k) fv.push_back(f.v[k]);
+    for (auto& e : t.edges) {
+      lv.push_back(e.v[0]);
+      lv.push_back(e.v[1]);
+    }
+    for (size_t v = 0; v < t.verts.size(); ++v) {
+      lv.push_back((int)v);
+      lv.push_back((int)v);
+    }
+    geom.vx = (const double*)upload(geomKeep, vx, stream);
+    geom.cellV = (const int*)upload(geomKeep, cv, stream);
+    geom.faceV = (const int*)upload(geomKeep, fv, stream);
+    geom.lowV = (const int*)upload(geomKeep, lv, stream);
+  }
   scalars.alloc(64 * sizeof(double));
   cudaCheck(cudaMemsetAsync(scalars.p, 0, 64 * sizeof(double), stream), "memset");
   cudaCheck(cudaStreamSynchronize(stream), "sync");
@@ -165,6 +194,23 @@ void Storage::buildLevel(int L) {
   ld.comm = (uint2*)upload(keep, comm, stream);
   ld.chunks = (dev::Chunk*)upload(keep, chunks, stream);
   buildTiles(L);
+  // single-pass SOR tiles: every (x, y) of the cell is in exactly one tile, tallest tiles first
+  {
+    std::vector<dev::WaveTile> wt;
+    if (N >= 4)
+      for (int c = 0; c < lv.nCells; ++c)
+        for (int y0 = 0; y0 <= N; y0 += dev::kWaveTY)
+          for (int x0 = 0; x0 + y0 <= N; x0 += dev::kWaveTX) wt.push_back({c, x0, y0, (int)N - x0 - y0});
+    std::stable_sort(wt.begin(), wt.end(), [](const dev::WaveTile& a, const dev::WaveTile& b) { return a.pEnd > b.pEnd; });
+    ld.waveTiles = (dev::WaveTile*)upload(keep, wt, stream);
+    ld.nWaveTiles = (int)wt.size();
+    int64_t first = lay.total;
+    for (int k : {KV, KE, KF})
+      for (int64_t o : lay.off[k]) first = std::min(first, o);
+    for (size_t c = 0; c < lay.off[KC].size(); ++c)
+      argCheck(lay.off[KC][c] + lay.size[KC][c] <= first, "cell arrays must precede the other primitives");
+    ld.nonCellBegin = first;
+  }
   ld.nChunks = (int)chunks.size();
   ld.partial.alloc(sizeof(double) * std::max(1, lv.nCellBlocks + lv.nFaceBlocks + lv.nLowBlocks));
   cudaCheck(cudaStreamSynchronize(stream), "level upload");
@@ -329,6 +375,22 @@ void Storage::dotAsync(int a, int b, int L, unsigned mask, double* dOut) {
   dev::reduceKernel<<<1, dev::kBlock, 0, stream>>>((const double*)ld.partial.p, nb, dOut);
   launches += 2;
   cudaCheck(cudaGetLastError(), "dot");
+}
+
+void Storage::interpolateExpr(int id, int L, unsigned mask, int expr, const double* p) {
+  argCheck(expr == 0 || expr == 1, "unknown expression");
+  Function& f = fn(id);
+  const LevelData& ld = levels[L];
+  const int nb = ld.lv.nCellBlocks + ld.lv.nFaceBlocks + ld.lv.nLowBlocks;
+  if (f.prec == 8)
+    dev::interpolateKernel<double><<<nb, dev::kBlock, 0, stream>>>(ld.lv, geom, (double*)data(id, L), mask, expr, p[0], p[1],
+                                                                   p[2], p[3]);
+  else
+    dev::interpolateKernel<float><<<nb, dev::kBlock, 0, stream>>>(ld.lv, geom, (float*)data(id, L), mask, expr, p[0], p[1],
+                                                                  p[2], p[3]);
+  ++launches;
+  cudaCheck(cudaGetLastError(), "interpolate");
+  communicate(id, L, kAllGroups);
 }
 
 double Storage::dot(int a, int b, int L, unsigned mask) {
@@ -509,6 +571,30 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
   // budget), so the re-reads of the later colours hit L2
   auto cellPhase = [&](bool rev) {
     if (!lv.nCellBlocks || !(kinds & (1 << KC))) return;
+    if (sorSchedule == 0 && ld.nWaveTiles) {
+      // one pass into the spare buffer of this level, which then becomes the function's buffer
+      Function& fd = fn(dstId);
+      std::unique_ptr<DevBuf>& cur = fd.levels[L - fd.minL];
+      std::unique_ptr<DevBuf>& sp = spare[{L, (int)sizeof(T)}];
+      if (!sp || sp->bytes != cur->bytes) {
+        sp.reset(new DevBuf());
+        sp->alloc(cur->bytes);
+        cudaCheck(cudaMemsetAsync(sp->p, 0, sp->bytes, stream), "spare memset");  // alignment padding stays zero
+      }
+      T* out = (T*)sp->p;
+      const size_t smem = dev::waveSmemBytes<T>(lv.N);
+      dev::cellSorWaveKernel<T><<<ld.nWaveTiles, dev::kWaveThreads, smem, stream>>>(lv, ld.waveTiles, st.cellW, u, out,
+                                                                                  rhs, mask, omega, rev ? 1 : 0);
+      ++launches;
+      const int64_t tail = ld.lay->total - ld.nonCellBegin;
+      if (tail > 0)
+        cudaCheck(cudaMemcpyAsync(out + ld.nonCellBegin, u + ld.nonCellBegin, tail * sizeof(T), cudaMemcpyDeviceToDevice,
+                                  stream),
+                  "sor tail copy");
+      std::swap(cur, sp);
+      u = out;
+      return;
+    }
     const int nPl = lv.N - 3;
     for (int c0 = 0; c0 < lv.nCells; c0 += ld.cellsPerGroup) {
       const int nc = std::min(ld.cellsPerGroup, lv.nCells - c0);

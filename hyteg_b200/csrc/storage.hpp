@@ -39,6 +39,10 @@ struct LevelData {
   int cellsPerGroup = 0;
   std::unique_ptr<DevBuf> tileBuf;
   DevBuf partial;
+  // single-pass SOR: one 32 x 32 (x, y) tile of a macro-cell per block, the tallest first
+  dev::WaveTile* waveTiles = nullptr;
+  int nWaveTiles = 0;
+  int64_t nonCellBegin = 0;  // first slot after the cell arrays (faces, edges, vertices follow)
   std::vector<unsigned char> hostCellType, hostFaceType, hostLowType;
   std::vector<std::unique_ptr<DevBuf>> keep;
 };
@@ -75,6 +79,12 @@ struct Storage {
   DevBuf scalars;            // device scratch for reductions
   int64_t l2Budget = int64_t(1) << 62;  // bytes of L2 one SOR cell group may occupy (default: one group)
   unsigned long long launches = 0;  // kernels launched by this storage
+  // Cell-phase schedule of the multicolour SOR: 0 = one wavefront pass that writes a second
+  // buffer which then replaces the level buffer, 1 = four in-place colour passes.
+  int sorSchedule = 0;
+  std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> spare;  // (level, precision) -> buffer
+  dev::Geometry geom{};              // macro-vertex coordinates and primitive vertex lists (device)
+  std::vector<std::unique_ptr<DevBuf>> geomKeep;
 
   Function& fn(int id);
   void* data(int id, int L);
@@ -84,6 +94,7 @@ struct Storage {
   void lincomb(int dst, int L, unsigned mask, int n, const double* a, const int* srcs, bool add, double constant);
   void copyCast(int dst, int src, int L, unsigned mask, bool add);
   void dotAsync(int a, int b, int L, unsigned mask, double* dOut);
+  void interpolateExpr(int id, int L, unsigned mask, int expr, const double* params);
   double dot(int a, int b, int L, unsigned mask);
 
   int createOperator(int form, int minL, int maxL);

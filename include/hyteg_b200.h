@@ -95,6 +95,10 @@ int hg_storage_launch_count(const hg_storage* s, unsigned long long* count);
 /* Piecewise-constant diffusion coefficient per macro-cell (ncells values) for operators
  * created afterwards. */
 int hg_storage_set_cell_coefficients(hg_storage* s, const double* k, int ncells);
+/* Cell-phase schedule of the multicolour SOR: 0 (default) = one pass per sweep (z-wavefront over
+ * the four colours, written to a second buffer of the level that then replaces the smoothed
+ * function's buffer), 1 = four in-place colour passes. Both give the same multicolour sweep. */
+int hg_storage_set_sor_schedule(hg_storage* s, int schedule);
 /* Topology export: for kind HG_VERTEX ids[0..2]=unused, coords[3]; HG_EDGE ids[2]; HG_FACE ids[3];
  * HG_CELL ids[4]; flag = mesh boundary flag. */
 int hg_primitive_vertices(const hg_storage* s, int kind, int prim, int ids[4], double coords[3], int* flag);
@@ -134,12 +138,19 @@ int hg_mesh_low_stencil(const hg_mesh* m, int level, int form, int kind, int pri
 /* precision: 8 = double, 4 = float */
 int hg_function_create(hg_storage* s, int min_level, int max_level, int precision, int* fn);
 int hg_function_destroy(hg_storage* s, int fn);
+/* The address of a level buffer is stable except across multicolour SOR on that level under
+ * schedule 0 (hg_storage_set_sor_schedule): the sweep writes the second buffer of the level and
+ * the two are exchanged, so re-query the address after smoothing (an even number of sweeps
+ * per level, as in a V(3,3) cycle, returns every buffer to its original address). */
 int hg_function_device_ptr(hg_storage* s, int fn, int level, void** ptr);
 /* Host <-> device copies of one level buffer (n elements of the function's precision). */
 int hg_function_upload(hg_storage* s, int fn, int level, const void* host, int64_t n);
 int hg_function_download(hg_storage* s, int fn, int level, void* host, int64_t n);
 int hg_communicate(hg_storage* s, int fn, int level);
 int hg_interpolate_const(hg_storage* s, int fn, double value, int level, unsigned flag);
+/* Built-in expressions at the flagged DoFs (then the halo is refreshed): expr 0 =
+ * p0 sin(p1 pi x) sin(p1 pi y) sin(p1 pi z); expr 1 = p0 + p1 x + p2 y + p3 z. */
+int hg_interpolate_expr(hg_storage* s, int fn, int level, unsigned flag, int expr, const double params[4]);
 /* dst = sum_i scalars[i] * srcs[i]   (n <= 3) */
 int hg_assign(hg_storage* s, int dst, int level, unsigned flag, int n, const double* scalars, const int* srcs);
 /* dst += sum_i scalars[i] * srcs[i]  (n <= 3) */
@@ -193,6 +204,12 @@ int hg_gmg_create(hg_storage* s, int op, int min_level, int max_level, int pre_s
 int hg_gmg_destroy(hg_storage* s, int gmg);
 /* One cycle: x <- MG(x, b) on max_level (x, b of the solver's precision). */
 int hg_gmg_solve(hg_storage* s, int gmg, int x, int b, int level);
+/* Iterate to ||b - A x|| <= tol ||b - A x0|| (at most max_iter iterations); x, b are FP64. An FP64
+ * solver repeats its cycle; an FP32 solver (precision 4) runs FP64 defect correction: r = b - A x
+ * in FP64, one FP32 cycle on A e = r from e = 0 (its coarse CG in FP64), x += e in FP64.
+ * history (nullable) receives the relative residual after each iteration. */
+int hg_gmg_solve_to(hg_storage* s, int gmg, int x, int b, int level, double tol, int max_iter, int* iterations,
+                    double* rel_residual, double* history, int history_cap);
 
 #ifdef __cplusplus
 }

@@ -122,3 +122,13 @@ def cube(max_level, nx=2):
     mesh = hg.HostMesh.cuboid((0, 0, 0), (1, 1, 1), nx, nx, nx, max_level)
     orc = oracle.Oracle(coords, tets, max_level)
     return coords, tets, mesh, orc
+
+
+def cell_coefficients(mesh, coords, tets, kfun):
+    """Per-macro-cell coefficient kfun(centroid) in the storage's cell order and in the order of
+    the oracle's tetrahedron list (the two orders differ; cells are matched by centroid)."""
+    nc = mesh.counts()[3]
+    cs = np.array([np.mean([mesh.primitive(hg.VERTEX, v)[1] for v in mesh.primitive(hg.CELL, c)[0]], axis=0)
+                   for c in range(nc)])
+    co = np.array([coords[t].mean(axis=0) for t in tets])
+    return kfun(cs), kfun(co)

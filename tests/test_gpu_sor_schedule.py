@@ -1,0 +1,107 @@
+"""The single-pass (z-wavefront, double-buffered) multicolour SOR against the four in-place
+colour passes and against the oracle, at levels where a macro-cell spans several 32 x 32 tiles
+(level 5: 3 tiles per cell, level 6: 10).
+
+Tolerances: FP64 1e-13 relative (max-norm over inner DoFs); FP32 1e-5 relative (the two
+schedules round the relaxation differently)."""
+import numpy as np
+import pytest
+
+import hyteg_b200 as hg
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def run_sor(st, L, x0, b0, dtype, schedule, sweeps, backwards, omega=1.3):
+    st.set_sor_schedule(schedule)
+    A = hg.P1ConstantLaplaceOperator(st, L, L)
+    x = hg.P1Function("x", st, L, L, dtype=dtype)
+    b = hg.P1Function("b", st, L, L, dtype=dtype)
+    x.from_numpy(L, x0)
+    b.from_numpy(L, b0)
+    for _ in range(sweeps):
+        if backwards:
+            A.smooth_sor_backwards(x, b, omega, L, hg.Inner)
+        else:
+            A.smooth_sor(x, b, omega, L, hg.Inner)
+    out = x.to_numpy(L).astype(np.float64)
+    st.set_sor_schedule(0)
+    return out
+
+
+@pytest.fixture(scope="module")
+def cube6():
+    if hg.device_count() == 0:
+        pytest.skip("no CUDA device")
+    st = hg.PrimitiveStorage.cuboid((0, 0, 0), (1, 1, 1), 2, 2, 2, 6)
+    mesh = hg.HostMesh.cuboid((0, 0, 0), (1, 1, 1), 2, 2, 2, 6)
+    return st, mesh
+
+
+@pytest.mark.parametrize("L", [5, 6])
+@pytest.mark.parametrize("backwards", [False, True])
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-13), (np.float32, 1e-5)])
+def test_single_pass_equals_colour_passes(cube6, L, backwards, dtype, tol):
+    st, mesh = cube6
+    n = st.level_size(L)
+    _, owned = mesh.slot_info(L)
+    rng = np.random.default_rng(L + 10 * backwards)
+    x0 = rng.uniform(-1, 1, n).astype(dtype)
+    b0 = rng.uniform(-1, 1, n).astype(dtype)
+    got = run_sor(st, L, x0, b0, dtype, 0, 2, backwards)
+    ref = run_sor(st, L, x0, b0, dtype, 1, 2, backwards)
+    m = owned == 1
+    assert np.abs(got[m] - ref[m]).max() / np.abs(ref[m]).max() < tol
+    # copies are refreshed identically under both schedules
+    used = owned >= 0
+    assert np.abs(got[used] - ref[used]).max() / np.abs(ref[used]).max() < tol
+
+
+def test_single_pass_matches_oracle_level5():
+    if hg.device_count() == 0:
+        pytest.skip("no CUDA device")
+    L = 5
+    coords, tets, mesh, orc = H.cube(L)
+    st = hg.PrimitiveStorage.cuboid((0, 0, 0), (1, 1, 1), 2, 2, 2, L)
+    xyz, owned = mesh.slot_info(L)
+    node = H.match_slots(xyz, orc.nodes(L)[0])
+    n = orc.n(L)
+    rng = np.random.default_rng(55)
+    u0, f0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    A = hg.P1ConstantLaplaceOperator(st, 0, L)
+    x, b = hg.P1Function("x", st, 0, L), hg.P1Function("b", st, 0, L)
+    x.from_numpy(L, H.scatter(node, u0))
+    b.from_numpy(L, H.scatter(node, f0))
+    for _ in range(2):
+        A.smooth_sor(x, b, 0.9, L, hg.Inner)
+    got = H.gather_owned(x.to_numpy(L), node, owned, n)
+    ref = orc.sor(L, u0, f0, 0.9, sweeps=2, multicolour=True)
+    inner = ~orc.dirichlet(L)
+    assert np.abs(got - ref)[inner].max() / np.abs(ref[inner]).max() < 1e-13
+
+
+def test_buffer_exchange_and_padding(cube6):
+    """The sweep exchanges the level buffer with the spare; an even number of sweeps restores the
+    original address, and alignment padding stays zero."""
+    st, mesh = cube6
+    L = 6
+    n = st.level_size(L)
+    _, owned = mesh.slot_info(L)
+    A = hg.P1ConstantLaplaceOperator(st, L, L)
+    x = hg.P1Function("x", st, L, L)
+    b = hg.P1Function("b", st, L, L)
+    rng = np.random.default_rng(3)
+    v = rng.uniform(-1, 1, n)
+    v[owned < 0] = 0.0
+    x.from_numpy(L, v)
+    b.from_numpy(L, rng.uniform(-1, 1, n))
+    p0 = x.device_ptr(L)
+    A.smooth_sor(x, b, 1.0, L, hg.Inner)
+    p1 = x.device_ptr(L)
+    A.smooth_sor(x, b, 1.0, L, hg.Inner)
+    p2 = x.device_ptr(L)
+    assert p1 != p0 and p2 == p0
+    out = x.to_numpy(L)
+    assert np.all(out[owned < 0] == 0.0)
+    assert np.all(np.isfinite(out))
