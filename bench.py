@@ -271,6 +271,28 @@ def load_traffic(kernel, L):
         return None
 
 
+def fp32_kernels(hg, st, A, x, b, L, Inner, N_in, Nc, timed):
+    """The same kernels on FP32 copies of the vectors (the arithmetic of the inner cycles of the
+    mixed-precision solve), and one FP32 V(3,3) cycle. Algorithmic bytes are half the FP64 ones."""
+    xf = hg.P1Function("xf", st, 0, L, dtype=np.float32)
+    bf = hg.P1Function("bf", st, 0, L, dtype=np.float32)
+    rf = hg.P1Function("rf", st, L, L, dtype=np.float32)
+    xf.copy_from(x, L)
+    bf.copy_from(b, L)
+    t = {"apply": timed(lambda: A.apply(xf, rf, L, Inner), 5),
+         "residual": timed(lambda: A.residual(xf, bf, rf, L, Inner), 5),
+         "sor_sweep": timed(lambda: A.smooth_sor(xf, bf, 1.0, L, Inner), 4)}
+    t_cells = timed(lambda: A.smooth_sor_primitives(xf, bf, 1.0, L, Inner, kinds=1 << hg.CELL, refresh=False), 4)
+    g = hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 50, 1e-16),
+                                    hg.P1toP1LinearRestriction(), hg.P1toP1LinearProlongation(), 0, L, 3, 3,
+                                    dtype=np.float32)
+    t_cycle = timed(lambda: g.solve(A, xf, bf, L), 3)
+    out = {k: {"ms": v * 1e3, "GBs_algorithmic": BYTES[k] / 2 * N_in / v / 1e9} for k, v in t.items()}
+    out["cell_sor_single_pass"] = {"ms": t_cells * 1e3, "GBs_algorithmic": BYTES["sor_sweep"] / 2 * Nc / t_cells / 1e9}
+    out["vcycle"] = {"ms": t_cycle * 1e3}
+    return out
+
+
 def time_to_solution(hg, st, A, L, N_in, Inner):
     """Manufactured problem -Lap u = 3 pi^2 u, u = sin(pi x) sin(pi y) sin(pi z), b = M I(f), x0 = 0:
     FP64 V(3,3) cycles vs FP64 defect correction around FP32 V(3,3) cycles, each to a 1e-8
@@ -409,6 +431,7 @@ def run_ours(args):
     kernels["cell_sor_colour_passes"] = {"ms": t_sor_passes * 1e3,
                                          "GBs_algorithmic": BYTES["sor_sweep"] * Nc / t_sor_passes / 1e9}
     kernels["cell_apply_launch"] = {"ms": t_apply_cells * 1e3, "GBs_algorithmic": BYTES["apply"] * Nc / t_apply_cells / 1e9}
+    kernels["fp32"] = fp32_kernels(hg, st, A, x, b, L, Inner, N_in, Nc, timed)
 
     # --- time to solution: FP64 GMG vs mixed precision (FP32 cycles inside FP64 defect correction)
     solve = time_to_solution(hg, st, A, L, N_in, Inner)

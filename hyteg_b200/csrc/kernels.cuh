@@ -201,25 +201,29 @@ __global__ void __launch_bounds__(kBlock, 4) cellSorKernel(LevelDev lv, const T*
 // result equals four separate colour sweeps over the whole cell, and the four stages of a step
 // touch disjoint data (they write the planes s, s-2, s-4, s-6 and read only those and the odd
 // planes between them) and need no barrier between them.
-// A block owns a 32 x 30 (x, y) tile of one macro-cell for all planes. It recomputes a shrinking
+// A block owns a 32 x 28 (x, y) tile of one macro-cell for all planes. It recomputes a shrinking
 // halo (stage k on the tile widened by 3 - k) from the start-of-sweep values, which makes the
 // tiles independent: they read uOld and write uNew, and the caller swaps the two buffers.
-// Planes s-7 .. s+1 of the tile widened by 4 (40 x 38) live in a 9-slot shared-memory ring;
-// plane s+2 is loaded into registers during step s and stored into the slot plane s-7 frees.
-// Rows are stored colour-split (x mod 4 major), so the points of one colour and each of their
-// x-neighbours are contiguous. Thread t < 380 owns the four columns 4(t mod 10) .. +3 of region
-// row t / 10: it loads and stores them and, in every stage, updates the one of them that
-// carries the stage's colour.
+// Planes s-7 .. s+1 of the tile widened by 4 (40 x 36 points) live in a 9-slot shared-memory
+// ring; plane s+2 is loaded into registers during step s and stored into the slot that plane
+// s-7 frees. Point (rx, ry) of the region sits at
+//   ry * 42 + ((rx mod 4 + 2 ry) mod 4) * 10 + rx / 4,
+// i.e. each row is split by x mod 4 and the split is rotated by 2y. The points of one colour then
+// occupy the same sub-row of every row, and with the row stride 42 (= 10 mod 16) the 16 lanes
+// of a half-warp never share a bank pair. Thread t < 360 owns the four columns 4(t mod 10) .. +3
+// of region row t / 10: it loads and stores them and, in every stage, updates the one of them
+// that carries the stage's colour.
 // ---------------------------------------------------------------------------------------
 constexpr int kWaveTX = 32;                         // tile extent in x (multiple of 4)
-constexpr int kWaveTY = 30;                         // tile extent in y
+constexpr int kWaveTY = 28;                         // tile extent in y (even)
 constexpr int kWaveH = 4;                           // halo loaded around the tile
 constexpr int kWaveRX = kWaveTX + 2 * kWaveH;       // region extent in x (40)
-constexpr int kWaveRY = kWaveTY + 2 * kWaveH;       // region extent in y (38)
+constexpr int kWaveRY = kWaveTY + 2 * kWaveH;       // region extent in y (36)
 constexpr int kWaveQ = kWaveRX / 4;                 // column groups per region row (10)
-constexpr int kWavePlane = kWaveRX * kWaveRY;       // elements per plane slot
+constexpr int kWaveS = 42;                          // shared-memory row stride (10 mod 16)
+constexpr int kWavePlane = kWaveRY * kWaveS;        // elements per plane slot
 constexpr int kWaveSlots = 9;
-constexpr int kWaveGroups = kWaveRY * kWaveQ;       // 380 column groups, one per thread
+constexpr int kWaveGroups = kWaveRY * kWaveQ;       // 360 column groups, one per thread
 constexpr int kWaveThreads = 384;
 constexpr int kWaveMaxN = 4096;                     // largest level size the shared-memory limit is set for
 
@@ -234,7 +238,7 @@ inline size_t waveSmemBytes(int N) {
 }
 
 template <class T>
-__global__ void __launch_bounds__(kWaveThreads, 2)
+__global__ void __launch_bounds__(kWaveThreads, sizeof(T) == 4 ? 3 : 2)
     cellSorWaveKernel(LevelDev lv, const WaveTile* __restrict__ tiles, const T* __restrict__ cellW,
                       const T* __restrict__ uOld, T* __restrict__ uNew, const T* __restrict__ rhs, unsigned mask,
                       T omega, int backwards) {
@@ -254,11 +258,13 @@ __global__ void __launch_bounds__(kWaveThreads, 2)
   const int gy = tid / kWaveQ, gx = tid - (tid / kWaveQ) * kWaveQ;
   const int y = yb + gy, x4 = xb + 4 * gx;
   const int Ay = y * (w + 1) - (y * (y + 1)) / 2;  // rowStart(w - p, y) = Ay - y p
-  const int so = gy * kWaveRX + gx;                 // slot offset of column j: so + j Q
+  const int rot = (2 * gy) & 3;                     // sub-row of column j: (j + rot) mod 4
+  const int so = gy * kWaveS + gx;
+  const bool storer = owner && gy >= kWaveH && gy < kWaveH + kWaveTY && gx >= 1 && gx < kWaveQ - 1;
   __syncthreads();
 
   if (!(lv.cellType[tl.cell] & mask)) {  // not smoothed: the tile is copied
-    if (owner && gy >= kWaveH && gy < kWaveH + kWaveTY && gx >= 1 && gx < kWaveQ - 1)
+    if (storer)
       for (int p = 0; p <= tl.pEnd; ++p)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
@@ -272,12 +278,10 @@ __global__ void __launch_bounds__(kWaveThreads, 2)
 #pragma unroll
   for (int k = 0; k < 15; ++k) wt[k] = cellW[16 * tl.cell + k];
   const T om1 = T(1) - omega, dinv = omega / wt[0];
-  const int qy = (-2 * y) & 3;
   unsigned rowBits = 0;  // bit k: row gy lies in the region of stage k and y >= 1
 #pragma unroll
   for (int k = 0; k < 4; ++k)
     if (owner && gy >= k + 1 && gy < kWaveRY - 1 - k && y >= 1) rowBits |= 1u << k;
-  const bool storer = owner && gy >= kWaveH && gy < kWaveH + kWaveTY && gx >= 1 && gx < kWaveQ - 1;
 
   T stg[4];
   auto loadRegs = [&](int p) {  // plane p of the thread's columns (points of the closed cell)
@@ -288,69 +292,79 @@ __global__ void __launch_bounds__(kWaveThreads, 2)
         if (x4 + j >= 0 && x4 + j + y <= N - p) stg[j] = uo[g + j];
     }
   };
-  auto storeRegs = [&](int p) {
+  auto storeRegs = [&](int p, int slot) {
     if (owner && p <= N && y >= 0 && y <= N - p) {
-      T* s = sm + (p % kWaveSlots) * kWavePlane + so;
+      T* s = sm + slot * kWavePlane + so;
 #pragma unroll
       for (int j = 0; j < 4; ++j)
-        if (x4 + j >= 0 && x4 + j + y <= N - p) s[j * kWaveQ] = stg[j];
+        if (x4 + j >= 0 && x4 + j + y <= N - p) s[((j + rot) & 3) * kWaveQ] = stg[j];
     }
   };
-  auto stage = [&](int k, int p) {  // colour seq[k] on plane p, region = tile widened by 3 - k
+  // colour seq[k] on plane p (ring slot sp, neighbours in slots st and sb); region = tile
+  // widened by 3 - k
+  auto stage = [&](int k, int p, int sp, int st, int sb) {
     if (!((rowBits >> k) & 1u)) return;
     const int c = backwards ? 3 - k : k;
-    const int q = (c + qy + p) & 3;  // the group's column with colour c in row y of plane p
+    const int q = (c - 2 * y + p) & 3;  // x mod 4 of colour c in row y of plane p
     const int rx = 4 * gx + q, x = xb + rx;
     if (rx < k + 1 || rx >= kWaveRX - 1 - k || x < 1 || x + y > N - 1 - p) return;
-    T* sP = sm + (p % kWaveSlots) * kWavePlane;
-    const T* sT = sm + ((p + 1) % kWaveSlots) * kWavePlane;
-    const T* sB = sm + ((p - 1) % kWaveSlots) * kWavePlane;
-    const int o = so + q * kWaveQ;
-    const int dE = q < 3 ? kWaveQ : 1 - 3 * kWaveQ;   // offset of x + 1
-    const int dW = q > 0 ? -kWaveQ : 3 * kWaveQ - 1;  // offset of x - 1
+    const int sg = (q + rot) & 3;  // its sub-row
+    const int e1 = sg < 3 ? kWaveQ : -3 * kWaveQ, w1 = sg > 0 ? -kWaveQ : 3 * kWaveQ;
+    const int n2 = sg < 2 ? 2 * kWaveQ : -2 * kWaveQ;
+    const int qe = q == 3 ? 1 : 0, qw = q == 0 ? 1 : 0;
+    const int dE = e1 + qe, dW = w1 - qw, dN = kWaveS + n2, dS = n2 - kWaveS;
+    const int dNW = kWaveS + e1 - qw, dSE = w1 - kWaveS + qe;
+    const int o = so + sg * kWaveQ;
+    T* sP = sm + sp * kWavePlane + o;
+    const T* sT = sm + st * kWavePlane + o;
+    const T* sB = sm + sb * kWavePlane + o;
     const T rh = f[pbTab[p] + Ay - y * p + x];
     // three independent partial sums (this plane, the plane above, the plane below)
-    T a = wt[1] * sP[o + dE];
-    a += wt[2] * sP[o + dW];
-    a += wt[3] * sP[o + kWaveRX];
-    a += wt[4] * sP[o - kWaveRX];
-    a += wt[5] * sP[o + kWaveRX + dW];
-    a += wt[6] * sP[o - kWaveRX + dE];
-    T t = wt[7] * sT[o];
-    t += wt[8] * sT[o + dW];
-    t += wt[9] * sT[o - kWaveRX];
-    t += wt[10] * sT[o - kWaveRX + dE];
-    T b = wt[11] * sB[o];
-    b += wt[12] * sB[o + dE];
-    b += wt[13] * sB[o + kWaveRX];
-    b += wt[14] * sB[o + kWaveRX + dW];
-    sP[o] = om1 * sP[o] + (rh - (a + (t + b))) * dinv;
+    T a = wt[1] * sP[dE];
+    a += wt[2] * sP[dW];
+    a += wt[3] * sP[dN];
+    a += wt[4] * sP[dS];
+    a += wt[5] * sP[dNW];
+    a += wt[6] * sP[dSE];
+    T t = wt[7] * sT[0];
+    t += wt[8] * sT[dW];
+    t += wt[9] * sT[dS];
+    t += wt[10] * sT[dSE];
+    T b = wt[11] * sB[0];
+    b += wt[12] * sB[dE];
+    b += wt[13] * sB[dN];
+    b += wt[14] * sB[dNW];
+    sP[0] = om1 * sP[0] + (rh - (a + (t + b))) * dinv;
   };
-  auto store = [&](int p) {  // the tile's points of plane p (interior and boundary) to uNew
+  auto store = [&](int p, int slot) {  // the tile's points of plane p (interior and boundary) to uNew
     if (!storer || y > N - p) return;
-    const T* s = sm + (p % kWaveSlots) * kWavePlane + so;
+    const T* s = sm + slot * kWavePlane + so;
     const int g = pbTab[p] + Ay - y * p + x4;
 #pragma unroll
     for (int j = 0; j < 4; ++j)
-      if (x4 + j + y <= N - p) un[g + j] = s[j * kWaveQ];
+      if (x4 + j + y <= N - p) un[g + j] = s[((j + rot) & 3) * kWaveQ];
   };
+  auto wrap = [](int v) { return v >= kWaveSlots ? v - kWaveSlots : v; };  // v in [0, 2 * slots)
 
   loadRegs(0);
-  storeRegs(0);
+  storeRegs(0, 0);
   loadRegs(1);
-  storeRegs(1);
+  storeRegs(1, 1);
   const int sEnd = tl.pEnd + 6;
+  int ss = 0;  // s mod 9
   for (int s = 0; s <= sEnd; ++s) {
     loadRegs(s + 2);
     __syncthreads();  // the previous step's stores into the ring are visible
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int p = s - 2 * k;
-      if (p >= 1 && p <= N - 3) stage(k, p);
+      const int sp = wrap(ss + kWaveSlots - 2 * k);  // slot of plane p
+      if (p >= 1 && p <= N - 3) stage(k, p, sp, wrap(sp + 1), wrap(sp + kWaveSlots - 1));
     }
     __syncthreads();  // plane s-7 is no longer read; plane s-6 is final
-    storeRegs(s + 2);
-    if (s >= 6 && s - 6 <= tl.pEnd) store(s - 6);
+    storeRegs(s + 2, wrap(ss + 2));
+    if (s >= 6 && s - 6 <= tl.pEnd) store(s - 6, wrap(ss + 3));  // (s - 6) mod 9 = (s + 3) mod 9
+    ss = wrap(ss + 1);
   }
 }
 
