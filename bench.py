@@ -43,6 +43,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--level", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--serving-requests", type=int, default=200,
+                   help="requests of the batched-serving measurement (0 skips it)")
     return p.parse_args()
 
 
@@ -271,6 +273,56 @@ def load_traffic(kernel, L):
         return None
 
 
+def serving_bench(hg, n_requests, seed=2024):
+    """Batched serving on a seeded request stream (config 5, bounded sample): k in U{1..4}
+    sub-cubes per direction (6..384 tets), level in U{3..6}, coefficient log-uniform in
+    [0.1, 10], right-hand side uniform[-1,1] from the request's seed, tolerance 1e-8, mixed
+    precision, Poisson arrivals. The same requests are first solved one after another with plain
+    FP64 cycles (one worker); the server then runs them at arrival rates of 2x, 4x and 8x that
+    sequential service rate (the last saturates it: its throughput is the server's capacity).
+    Latency = completion - arrival (server clock)."""
+    rng = np.random.default_rng(seed)
+    reqs = [(int(rng.integers(1, 5)), int(rng.integers(3, 7)), float(np.exp(rng.uniform(np.log(0.1), np.log(10.0)))),
+             int(rng.integers(1, 2 ** 62))) for _ in range(n_requests)]
+    shapes = sorted({(k, L) for k, L, _, _ in reqs})
+
+    def run(workers, precision, rate):
+        srv = hg.SolveServer(workers=workers, hbm_budget_bytes=64 << 30, precision=precision)
+        for k, L in shapes:
+            srv.prewarm(k, L)
+        arr = np.cumsum(rng.exponential(1.0 / rate, len(reqs))) if rate else np.zeros(len(reqs))
+        t0 = time.perf_counter()
+        ids = []
+        for (k, L, c, sd), ta in zip(reqs, arr):
+            d = ta - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(k, L, c, sd, 1e-8, 100))
+        for i in ids:
+            srv.wait(i)
+        res = [srv.result(i) for i in ids]
+        st = srv.stats()
+        srv.close()
+        lat = np.array([r["t_end"] - r["t_submit"] for r in res])
+        span = max(r["t_end"] for r in res) - min(r["t_submit"] for r in res)
+        dofs = sum(r["inner_dofs"] for r in res)
+        return {"requests": len(res), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3), "seconds": span, "gdofs": dofs / span / 1e9,
+                "max_rel_residual": max(r["rel_residual"] for r in res),
+                "mean_iterations": float(np.mean([r["iterations"] for r in res])), "peak_bytes": st["peak_bytes"],
+                "mean_setup_ms": float(np.mean([r["t_solve"] - r["t_start"] for r in res]) * 1e3),
+                "mean_solve_ms": float(np.mean([r["t_end"] - r["t_solve"] for r in res]) * 1e3)}
+
+    seq = run(1, 8, 0)  # all submitted at once, one worker: sequential FP64 solves
+    mu = seq["requests"] / seq["seconds"]
+    out = {"workload": "%d seeded requests: k in U{1..4}, level in U{3..6}, coefficient log-U[0.1,10], "
+                       "tol 1e-8, Poisson arrivals" % n_requests,
+           "sequential_fp64": seq}
+    for mult in (2.0, 4.0, 8.0):
+        out["mixed_rate_%gx" % mult] = dict(run(8, 4, mult * mu), arrival_rate_per_s=mult * mu)
+    return out
+
+
 def fp32_kernels(hg, st, A, x, b, L, Inner, N_in, Nc, timed):
     """The same kernels on FP32 copies of the vectors (the arithmetic of the inner cycles of the
     mixed-precision solve), and one FP32 V(3,3) cycle. Algorithmic bytes are half the FP64 ones."""
@@ -493,6 +545,8 @@ def run_ours(args):
         "kernels": kernels,
         "solve": solve,
     }
+    if world == 1 and args.serving_requests > 0:
+        out["serving"] = serving_bench(hg, args.serving_requests)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         thr = host_threads()
         times = reference_cpu_pass(L, 1, 0, thr)

@@ -299,6 +299,11 @@ class P1Function:
         p = np.array([a, b, c, d], dtype=np.float64)
         call("hg_interpolate_expr", self.storage.handle, self.id, level, flag, 1, dptr(p))
 
+    def fill_random(self, seed, level, flag=All, lo=-1.0, hi=1.0):
+        """Seeded uniform [lo, hi) values at the flagged DoFs (reproducible per topology)."""
+        call("hg_function_fill_random", self.storage.handle, self.id, level, flag, ctypes.c_uint64(seed), float(lo),
+             float(hi))
+
     def assign(self, scalars, functions, level, flag=All):
         s = np.ascontiguousarray(scalars, dtype=np.float64)
         f = np.ascontiguousarray([g.id for g in functions], dtype=np.int32)
@@ -465,6 +470,10 @@ class GeometricMultigridSolver:
     def solve(self, A, x, b, level):
         call("hg_gmg_solve", self.storage.handle, self._handle(A), x.id, b.id, level)
 
+    def set_graphs(self, A, enable):
+        """Replay cycles from captured CUDA graphs (default on; identical results)."""
+        call("hg_gmg_set_graphs", self.storage.handle, self._handle(A), 1 if enable else 0)
+
     def solve_to(self, A, x, b, level, tol, max_iter=100):
         """Iterate to a relative residual tol (FP64 x, b). An FP32 solver runs FP64 defect
         correction around FP32 cycles. Returns (iterations, relative residual, history)."""
@@ -481,5 +490,67 @@ class GeometricMultigridSolver:
             if st is not None and st.handle:
                 for h in self._cache.values():
                     _capi.lib.hg_gmg_destroy(st.handle, h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+
+
+class SolveServer:
+    """Continuous-batching server of P1 Poisson solves (hg_server_*): requests on the unit cube
+    split into k^3 sub-cubes of 6 tetrahedra at a refinement level, constant coefficient, seeded
+    uniform[-1,1] right-hand side, solved to a relative residual. precision 4 runs FP64 defect
+    correction around FP32 V(3,3) cycles, precision 8 plain FP64 V(3,3) cycles."""
+
+    def __init__(self, workers=8, hbm_budget_bytes=64 << 30, precision=4):
+        h = ctypes.c_void_p()
+        call("hg_server_create", int(workers), int(hbm_budget_bytes), int(precision), ctypes.byref(h))
+        self._h = h
+
+    def prewarm(self, k, level):
+        call("hg_server_prewarm", self._h, int(k), int(level))
+
+    def submit(self, k, level, coefficient=1.0, seed=0, tol=1e-8, max_iter=100, keep_solution=False):
+        i = ctypes.c_int64()
+        call("hg_server_submit", self._h, int(k), int(level), float(coefficient), ctypes.c_uint64(seed), float(tol),
+             int(max_iter), 1 if keep_solution else 0, ctypes.byref(i))
+        return i.value
+
+    def wait(self, rid, timeout=-1.0):
+        d = ctypes.c_int()
+        call("hg_server_wait", self._h, int(rid), float(timeout), ctypes.byref(d))
+        return bool(d.value)
+
+    def result(self, rid):
+        """dict(status, iterations, rel_residual, t_submit, t_start, t_solve, t_end, inner_dofs);
+        raises for a failed request."""
+        st, it = ctypes.c_int(), ctypes.c_int()
+        rel = ctypes.c_double()
+        t = np.zeros(4)
+        n = ctypes.c_int64()
+        call("hg_server_result", self._h, int(rid), ctypes.byref(st), ctypes.byref(it), ctypes.byref(rel), dptr(t),
+             ctypes.byref(n))
+        return {"status": st.value, "iterations": it.value, "rel_residual": rel.value, "t_submit": t[0],
+                "t_start": t[1], "t_solve": t[2], "t_end": t[3], "inner_dofs": n.value}
+
+    def solution(self, rid):
+        n = ctypes.c_int64()
+        call("hg_server_solution", self._h, int(rid), None, 0, ctypes.byref(n))
+        out = np.empty(n.value)
+        call("hg_server_solution", self._h, int(rid), dptr(out), n.value, ctypes.byref(n))
+        return out
+
+    def stats(self):
+        s = np.zeros(6, dtype=np.int64)
+        call("hg_server_stats", self._h, s.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+        keys = ("admitted", "completed", "failed", "resident_hierarchies", "resident_bytes", "peak_bytes")
+        return dict(zip(keys, (int(v) for v in s)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            call("hg_server_destroy", self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
         except (AttributeError, TypeError):  # interpreter shutdown
             pass

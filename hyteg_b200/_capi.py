@@ -88,6 +88,16 @@ _SIGS = {
     "hg_gmg_create": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_double, c_int, P(c_int)]),
     "hg_gmg_destroy": (c_int, [c_void_p, c_int]),
     "hg_gmg_solve": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
+    "hg_server_create": (c_int, [c_int, c_int64, c_int, P(c_void_p)]),
+    "hg_server_destroy": (c_int, [c_void_p]),
+    "hg_server_prewarm": (c_int, [c_void_p, c_int, c_int]),
+    "hg_server_submit": (c_int, [c_void_p, c_int, c_int, c_double, ctypes.c_uint64, c_double, c_int, c_int, P(c_int64)]),
+    "hg_server_wait": (c_int, [c_void_p, c_int64, c_double, P(c_int)]),
+    "hg_server_result": (c_int, [c_void_p, c_int64, P(c_int), P(c_int), P(c_double), P(c_double), P(c_int64)]),
+    "hg_server_solution": (c_int, [c_void_p, c_int64, P(c_double), c_int64, P(c_int64)]),
+    "hg_server_stats": (c_int, [c_void_p, P(c_int64)]),
+    "hg_function_fill_random": (c_int, [c_void_p, c_int, c_int, c_uint, ctypes.c_uint64, c_double, c_double]),
+    "hg_gmg_set_graphs": (c_int, [c_void_p, c_int, c_int]),
     "hg_gmg_solve_to": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_int, P(c_int), P(c_double), P(c_double),
                                 c_int]),
 }

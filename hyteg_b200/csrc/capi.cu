@@ -7,6 +7,7 @@
 #include <string>
 
 #include "../../include/hyteg_b200.h"
+#include "server.hpp"
 #include "solvers.hpp"
 #include "storage.hpp"
 
@@ -155,6 +156,7 @@ int hg_storage_set_sor_schedule(hg_storage* h, int schedule) {
   HG_TRY
   hg::argCheck(schedule == 0 || schedule == 1, "SOR schedule must be 0 (single pass) or 1 (colour passes)");
   S(h).sorSchedule = schedule;
+  ++S(h).generation;
   HG_CATCH
 }
 
@@ -677,6 +679,110 @@ int hg_mesh_low_stencil(const hg_mesh* m, int level, int form, int kind, int pri
     rel[k] = e[k].rel;
     w[k] = e[k].w;
   }
+  HG_CATCH
+}
+
+struct hg_server {
+  hg::Server* s;
+};
+
+int hg_server_create(int workers, int64_t hbm_budget_bytes, int precision, hg_server** out) {
+  HG_TRY
+  hg::argCheck(out != nullptr, "null output pointer");
+  if (hg_device_count() == 0) throw hg::Error(HG_ERR_CUDA, "no CUDA device visible");
+  std::unique_ptr<hg_server> h(new hg_server());
+  h->s = new hg::Server(workers, hbm_budget_bytes, precision);
+  *out = h.release();
+  HG_CATCH
+}
+
+int hg_server_destroy(hg_server* srv) {
+  HG_TRY
+  if (srv) {
+    delete srv->s;
+    delete srv;
+  }
+  HG_CATCH
+}
+
+static hg::Server& SV(hg_server* h) {
+  hg::argCheck(h != nullptr && h->s != nullptr, "null server");
+  return *h->s;
+}
+
+int hg_server_prewarm(hg_server* srv, int k, int level) {
+  HG_TRY
+  hg::argCheck(k >= 1 && k <= 16 && level >= 2 && level <= 8, "shape out of range");
+  SV(srv).prewarm(k, level);
+  HG_CATCH
+}
+
+int hg_server_submit(hg_server* srv, int k, int level, double coefficient, uint64_t seed, double tol, int max_iter,
+                     int keep_solution, int64_t* id) {
+  HG_TRY
+  hg::argCheck(id != nullptr, "null id pointer");
+  *id = SV(srv).submit(k, level, coefficient, seed, tol, max_iter, keep_solution != 0);
+  HG_CATCH
+}
+
+int hg_server_wait(hg_server* srv, int64_t id, double timeout_seconds, int* done) {
+  HG_TRY
+  const bool d = SV(srv).wait(id, timeout_seconds);
+  if (done) *done = d ? 1 : 0;
+  HG_CATCH
+}
+
+int hg_server_result(hg_server* srv, int64_t id, int* status, int* iterations, double* rel_residual, double times[4],
+                     int64_t* inner_dofs) {
+  HG_TRY
+  auto r = SV(srv).request(id);
+  if (status) *status = r->status;
+  if (iterations) *iterations = r->iterations;
+  if (rel_residual) *rel_residual = r->relResidual;
+  if (times) {
+    times[0] = r->tSubmit;
+    times[1] = r->tStart;
+    times[2] = r->tSolve;
+    times[3] = r->tEnd;
+  }
+  if (inner_dofs) *inner_dofs = r->innerDofs;
+  if (r->status < 0) throw hg::Error(HG_ERR_STATE, "request failed: " + r->error);
+  HG_CATCH
+}
+
+int hg_server_solution(hg_server* srv, int64_t id, double* host, int64_t n, int64_t* size) {
+  HG_TRY
+  auto r = SV(srv).request(id);
+  hg::argCheck(r->status == 2, "request has not completed");
+  hg::argCheck(r->keepSolution, "request was submitted without keep_solution");
+  if (size) *size = (int64_t)r->solution.size();
+  if (host) {
+    hg::argCheck(n >= (int64_t)r->solution.size(), "host buffer too small");
+    std::copy(r->solution.begin(), r->solution.end(), host);
+  }
+  HG_CATCH
+}
+
+int hg_server_stats(hg_server* srv, int64_t stats[6]) {
+  HG_TRY
+  hg::argCheck(stats != nullptr, "null stats");
+  SV(srv).stats(stats);
+  HG_CATCH
+}
+
+int hg_function_fill_random(hg_storage* h, int fn, int level, unsigned flag, uint64_t seed, double lo, double hi) {
+  HG_TRY
+  hg::argCheck(lo <= hi, "lo must not exceed hi");
+  S(h).fillRandom(fn, level, flag, seed, lo, hi);
+  HG_CATCH
+}
+
+int hg_gmg_set_graphs(hg_storage* h, int gmg, int enable) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  auto it = s.gmgs.find(gmg);
+  hg::argCheck(it != s.gmgs.end(), "unknown multigrid handle");
+  it->second->setGraphs(enable != 0);
   HG_CATCH
 }
 

@@ -741,6 +741,103 @@ __global__ void __launch_bounds__(kBlock) lowStencilKernel(LevelDev lv, StencilD
   else dst[c] = rhs[c] - s;
 }
 
+// ---------------------------------------------------------------------------------------
+// Coarse-grid CG in one block (CGSolver.hpp:69-150 with the identity preconditioner) for a
+// level whose DoFs all sit on vertices and edges (levels 0 and 1). The halo refresh, stencil,
+// dot products and updates of every iteration run on the device, so a multigrid cycle needs no
+// host synchronisation. Vector updates touch the owned DoFs; the copies of the source of every
+// apply, and of x at the end, are refreshed from their owners. r, p and ap are workspace level
+// buffers; info[0] = iterations, info[1] = final residual norm.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ double blockSum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    red[32] = t;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+static __global__ void __launch_bounds__(kBlock) coarseCgKernel(LevelDev lv, StencilDev<double> st, const uint2* __restrict__ comm,
+                                                        int64_t nComm, double* x, const double* __restrict__ b,
+                                                        double* r, double* p, double* ap, unsigned mask, int maxIter,
+                                                        double tol, double* info) {
+  __shared__ double red[33];
+  const int tid = threadIdx.x;
+  auto refresh = [&](double* v) {
+    __syncthreads();
+    for (int64_t i = tid; i < nComm; i += blockDim.x) {
+      const uint2 t = comm[i];
+      v[t.x] = v[t.y];
+    }
+    __syncthreads();
+  };
+  // visit every owned DoF of the flagged vertices and edges: f(slot)
+  auto forOwned = [&](auto f) {
+    for (int blk = 0; blk < lv.nLowBlocks; ++blk) {
+      const LowBlock lb = lv.lowBlocks[blk];
+      if (!(lv.lowType[lb.prim] & mask)) continue;
+      for (int xx = lb.start + tid; xx < lb.start + (int)blockDim.x && xx < lv.lowFirst[lb.prim] + lv.lowCount[lb.prim];
+           xx += blockDim.x)
+        f(lb.prim, lv.lowOff[lb.prim] + xx);
+    }
+  };
+  auto apply = [&](double* dst, double* src) {  // dst = A src on the flagged DoFs
+    refresh(src);
+    forOwned([&](int prim, int64_t c) {
+      double s = 0;
+      for (int k = st.lowEntOff[prim]; k < st.lowEntOff[prim + 1]; ++k) s += st.lowEntW[k] * src[c + st.lowEntRel[k]];
+      dst[c] = s;
+    });
+    __syncthreads();
+  };
+  auto dot = [&](const double* u, const double* v) {
+    double s = 0;
+    forOwned([&](int, int64_t c) { s += u[c] * v[c]; });
+    return blockSum(s, red);
+  };
+  // r = b - A x; p = z = r (identity preconditioner)
+  apply(p, x);
+  forOwned([&](int, int64_t c) {
+    r[c] = b[c] - p[c];
+    p[c] = r[c];
+  });
+  __syncthreads();
+  double prsold = dot(r, r);
+  double res = sqrt(prsold);
+  int it = 0;
+  if (res >= tol) {
+    for (int i = 0; i < maxIter; ++i) {
+      it = i + 1;
+      apply(ap, p);
+      const double alpha = prsold / dot(p, ap);
+      forOwned([&](int, int64_t c) {
+        x[c] += alpha * p[c];
+        r[c] -= alpha * ap[c];
+      });
+      __syncthreads();
+      const double rsnew = dot(r, r);
+      res = sqrt(rsnew);
+      if (res < tol) break;
+      const double beta = rsnew / prsold;
+      forOwned([&](int, int64_t c) { p[c] = r[c] + beta * p[c]; });
+      __syncthreads();
+      prsold = rsnew;
+    }
+  }
+  refresh(x);
+  if (tid == 0 && info) {
+    info[0] = it;
+    info[1] = res;
+  }
+}
+
 // colour < 0: all points; otherwise x mod 2 == colour (edges are 1-D chains)
 template <class T>
 __global__ void __launch_bounds__(kBlock) lowSorKernel(LevelDev lv, StencilDev<T> st, T* u, const T* __restrict__ rhs,
@@ -909,6 +1006,29 @@ __global__ void __launch_bounds__(kBlock) castKernel(const Chunk* __restrict__ c
     const int64_t j = ch.start + i;
     if (add) dst[j] += TD(src[j]);
     else dst[j] = TD(src[j]);
+  }
+}
+
+// Seeded uniform values in [lo, hi) at every slot of the flagged primitives' arrays; the value
+// depends only on (seed, slot index), so a level buffer of one topology is reproducible.
+// splitmix64 (Steele, Lea, Flood 2014) of the slot index mixed with the seed; 53 bits -> [0, 1).
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) randomFillKernel(const Chunk* __restrict__ chunks, unsigned mask, T* dst,
+                                                           uint64_t seed, double lo, double hi) {
+  const Chunk ch = chunks[blockIdx.x];
+  if (!(ch.type & mask)) return;
+  const uint64_t s = splitmix64(seed);
+  for (int i = threadIdx.x; i < ch.len; i += blockDim.x) {
+    const int64_t j = ch.start + i;
+    const double u = double(splitmix64(s ^ uint64_t(j)) >> 11) * (1.0 / 9007199254740992.0);
+    dst[j] = T(lo + (hi - lo) * u);
   }
 }
 

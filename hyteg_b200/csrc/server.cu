@@ -1,0 +1,291 @@
+// Continuous-batching solve server: worker threads, admission by device footprint, resident
+// hierarchies per shape (see server.hpp). Every request's work runs on the stream of its own
+// storage; the only synchronisations are per stream (convergence checks of that request).
+#include "server.hpp"
+
+#include <algorithm>
+#include <cmath>
+
+#include "../../include/hyteg_b200.h"
+#include "solvers.hpp"
+#include "storage.hpp"
+#include "topology.hpp"
+
+namespace hg {
+
+ServerSlot::~ServerSlot() = default;
+
+Server::Server(int workers, int64_t budgetBytes, int precision)
+    : precision_(precision), budget_(budgetBytes), t0_(std::chrono::steady_clock::now()) {
+  argCheck(workers >= 1 && workers <= 256, "workers must be in [1, 256]");
+  argCheck(budgetBytes > 0, "HBM budget must be positive");
+  argCheck(precision == 4 || precision == 8, "precision must be 4 (mixed) or 8 (FP64)");
+  int device = 0;
+  cudaCheck(cudaGetDevice(&device), "cudaGetDevice");
+  for (int i = 0; i < workers; ++i)
+    threads_.emplace_back([this, device]() {
+      cudaSetDevice(device);
+      worker();
+    });
+}
+
+Server::~Server() {
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    stopping_ = true;
+    for (auto& r : queue_) {
+      r->status = -1;
+      r->error = "server stopped before the request was admitted";
+    }
+    queue_.clear();
+  }
+  cv_.notify_all();
+  doneCv_.notify_all();
+  for (auto& t : threads_) t.join();
+  idle_.clear();
+}
+
+double Server::now() const {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+}
+
+int64_t Server::estimate(int k, int level) const {
+  auto it = measured_.find({k, level});
+  if (it != measured_.end()) return it->second;
+  // not built yet: level buffer of the finest level times the bytes per slot of the functions,
+  // spare buffers and tables (FP64 x, b; FP32 or FP64 multigrid workspace), plus the hierarchy
+  const int64_t m = int64_t(k) << level;
+  const int64_t slots = 6 * k * k * k * ((m / k + 1) * (m / k + 2) * (m / k + 3) / 6) + 64 * m * m;
+  const int64_t perSlot = precision_ == 4 ? 56 : 48;
+  return slots * perSlot;
+}
+
+int64_t Server::submit(int k, int level, double coefficient, uint64_t seed, double tol, int maxIter,
+                       bool keepSolution) {
+  argCheck(k >= 1 && k <= 16, "sub-cubes per direction must be in [1, 16]");
+  argCheck(level >= 2 && level <= 8, "level must be in [2, 8]");
+  argCheck(coefficient > 0.0 && std::isfinite(coefficient), "coefficient must be positive");
+  argCheck(tol > 0.0 && maxIter >= 1, "tolerance must be positive and max_iter at least 1");
+  auto r = std::make_shared<ServerRequest>();
+  r->k = k;
+  r->level = level;
+  r->coefficient = coefficient;
+  r->seed = seed;
+  r->tol = tol;
+  r->maxIter = maxIter;
+  r->keepSolution = keepSolution;
+  const int64_t m = (int64_t(k) << level) - 1;
+  r->innerDofs = m * m * m;
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    argCheck(!stopping_, "server is stopping");
+    r->id = nextId_++;
+    r->tSubmit = now();
+    all_[r->id] = r;
+    queue_.push_back(r);
+  }
+  cv_.notify_all();
+  return r->id;
+}
+
+std::unique_ptr<ServerSlot> Server::buildSlot(int k, int level) {
+  std::unique_ptr<ServerSlot> s(new ServerSlot());
+  s->k = k;
+  s->level = level;
+  const double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+  Topology t = meshCuboid(lo, hi, k, k, k);
+  t.setBoundaryFlags(1, 0);
+  s->st.reset(new Storage(t, level));
+  Storage& st = *s->st;
+  s->x = st.createFunction(0, level, 8);
+  s->b = st.createFunction(0, level, 8);
+  s->op = st.createOperator(0, 0, level);
+  s->gmg = st.nextId++;
+  st.gmgs[s->gmg].reset(new Gmg(st, s->op, 0, level, 3, 3, 1.0, 0, 200, 1e-16, precision_));
+  // one iteration so that the smoother's spare buffers exist before the footprint is taken
+  st.fillRandom(s->b, level, HG_INNER, 0, -1.0, 1.0);
+  double rel = 0;
+  st.gmgs[s->gmg]->solveTo(s->x, s->b, level, 1e-30, 1, &rel, nullptr, 0);
+  cudaCheck(cudaStreamSynchronize(st.stream), "slot build");
+  s->bytes = st.deviceBytes();
+  return s;
+}
+
+void Server::prewarm(int k, int level) {
+  std::unique_ptr<ServerSlot> s = buildSlot(k, level);
+  std::lock_guard<std::mutex> lk(mu_);
+  measured_[{k, level}] = s->bytes;
+  if (active_ + resident_ + s->bytes > budget_) throw Error(HG_ERR_OOM, "prewarm exceeds the HBM budget");
+  resident_ += s->bytes;
+  peak_ = std::max(peak_, active_ + resident_);
+  s->lastUse = ++useClock_;
+  idle_.push_back(std::move(s));
+}
+
+void Server::run(ServerRequest& r, ServerSlot& s) {
+  Storage& st = *s.st;
+  const int L = r.level;
+  // constant coefficient: scale every macro-cell and re-assemble the stencils in place (no device
+  // allocation or release, which would synchronise the whole device and stall the other requests)
+  auto& cells = const_cast<Topology&>(st.disc.topo()).cells;
+  if (cells.empty() || cells[0].k != r.coefficient) {
+    for (auto& c : cells) c.k = r.coefficient;
+    st.reassembleOperator(s.op);
+  }
+  r.tSolve = now();
+  st.fillRandom(s.b, L, HG_INNER, r.seed, -1.0, 1.0);
+  st.lincomb(s.x, L, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+  double rel = 0;
+  r.iterations = st.gmgs[s.gmg]->solveTo(s.x, s.b, L, r.tol, r.maxIter, &rel, nullptr, 0);
+  r.relResidual = rel;
+  if (r.keepSolution) {
+    r.solution.resize((size_t)st.levels[L].lay->total);
+    cudaCheck(cudaMemcpyAsync(r.solution.data(), st.data(s.x, L), r.solution.size() * sizeof(double),
+                              cudaMemcpyDeviceToHost, st.stream),
+              "solution download");
+  }
+  cudaCheck(cudaStreamSynchronize(st.stream), "request sync");
+}
+
+void Server::worker() {
+  for (;;) {
+    std::shared_ptr<ServerRequest> r;
+    std::unique_ptr<ServerSlot> slot;
+    std::vector<std::unique_ptr<ServerSlot>> evict;
+    int64_t est = 0;
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      for (;;) {
+        if (stopping_) return;
+        if (!queue_.empty()) {
+          std::shared_ptr<ServerRequest> h = queue_.front();
+          auto same = std::find_if(idle_.begin(), idle_.end(), [&](const std::unique_ptr<ServerSlot>& s) {
+            return s->k == h->k && s->level == h->level;
+          });
+          if (same != idle_.end()) {  // a resident hierarchy of this shape is free
+            slot = std::move(*same);
+            idle_.erase(same);
+            resident_ -= slot->bytes;
+            active_ += slot->bytes;
+            r = h;
+            queue_.pop_front();
+            break;
+          }
+          est = estimate(h->k, h->level);
+          while (active_ + resident_ + est > budget_ && !idle_.empty()) {  // release LRU idle hierarchies
+            auto lru = std::min_element(idle_.begin(), idle_.end(),
+                                        [](const std::unique_ptr<ServerSlot>& a, const std::unique_ptr<ServerSlot>& b) {
+                                          return a->lastUse < b->lastUse;
+                                        });
+            resident_ -= (*lru)->bytes;
+            evict.push_back(std::move(*lru));
+            idle_.erase(lru);
+          }
+          if (active_ + resident_ + est <= budget_) {
+            active_ += est;
+            r = h;
+            queue_.pop_front();
+            break;
+          }
+          if (active_ == 0 && idle_.empty()) {  // cannot fit even on an empty device budget
+            h->status = -1;
+            h->error = "request exceeds the HBM budget";
+            h->tEnd = now();
+            ++failed_;
+            queue_.pop_front();
+            doneCv_.notify_all();
+            continue;
+          }
+          if (!evict.empty()) break;  // free the evicted memory, then look again
+        }
+        cv_.wait(lk);
+      }
+      if (r) {
+        r->status = 1;
+        r->tStart = now();
+        ++admitted_;
+        peak_ = std::max(peak_, active_ + resident_);
+      }
+    }
+    evict.clear();
+    if (!r) continue;
+    std::string err;
+    if (!slot) {
+      try {
+        slot = buildSlot(r->k, r->level);
+      } catch (const std::exception& e) {
+        err = e.what();
+      }
+      std::lock_guard<std::mutex> lk(mu_);
+      if (slot) {
+        active_ += slot->bytes - est;
+        measured_[{r->k, r->level}] = slot->bytes;
+        peak_ = std::max(peak_, active_ + resident_);
+      } else {
+        active_ -= est;
+      }
+    }
+    if (slot && err.empty()) {
+      try {
+        run(*r, *slot);
+      } catch (const std::exception& e) {
+        err = e.what();
+      }
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      r->tEnd = now();
+      if (err.empty()) {
+        r->status = 2;
+        ++completed_;
+      } else {
+        r->status = -1;
+        r->error = err;
+        ++failed_;
+      }
+      if (slot) {
+        active_ -= slot->bytes;
+        if (err.empty()) {
+          slot->lastUse = ++useClock_;
+          resident_ += slot->bytes;
+          idle_.push_back(std::move(slot));
+        }
+      }
+    }
+    slot.reset();  // a failed hierarchy is released
+    cv_.notify_all();
+    doneCv_.notify_all();
+  }
+}
+
+bool Server::wait(int64_t id, double timeoutSeconds) {
+  std::unique_lock<std::mutex> lk(mu_);
+  auto it = all_.find(id);
+  argCheck(it != all_.end(), "unknown request id");
+  std::shared_ptr<ServerRequest> r = it->second;
+  auto pred = [&]() { return r->status == 2 || r->status < 0; };
+  if (timeoutSeconds < 0) {
+    doneCv_.wait(lk, pred);
+    return true;
+  }
+  return doneCv_.wait_for(lk, std::chrono::duration<double>(timeoutSeconds), pred);
+}
+
+std::shared_ptr<ServerRequest> Server::request(int64_t id) {
+  std::lock_guard<std::mutex> lk(mu_);
+  auto it = all_.find(id);
+  argCheck(it != all_.end(), "unknown request id");
+  return it->second;
+}
+
+void Server::stats(int64_t out[6]) {
+  std::lock_guard<std::mutex> lk(mu_);
+  out[0] = admitted_;
+  out[1] = completed_;
+  out[2] = failed_;
+  out[3] = (int64_t)idle_.size();
+  out[4] = resident_;
+  out[5] = peak_;
+}
+
+}  // namespace hg

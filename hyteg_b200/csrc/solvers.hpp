@@ -1,6 +1,11 @@
 // Solver drivers (host C++) used behind the C-ABI.
 #pragma once
 
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
 namespace hg {
 
 struct Storage;
@@ -19,6 +24,21 @@ struct Gmg {
   // until ||b - A x|| <= tol * ||b - A x0|| or maxIter; returns the iterations taken.
   int solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap);
   void coarseSolve(int x, int b, int L);
+  // One cycle x <- MG(x, b) on level L: replayed from a captured CUDA graph when the coarse solve
+  // runs on the device and pre + post is even (every smoothed buffer returns to its address).
+  void runCycle(int x, int b, int L);
+  void setGraphs(bool on);
+  bool deviceCoarse() const;  // the coarse level has vertex and edge DoFs only
+
+  struct Captured {
+    std::vector<uintptr_t> sig;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches = 0;
+  };
+  bool graphs = true;
+  std::vector<Captured> captured;
+  std::vector<std::vector<uintptr_t>> warm;  // signatures that ran eagerly once
+  std::vector<uintptr_t> signature(int x, int b, int L);
 
   Storage& s;
   int op, minL, maxL, pre, post;

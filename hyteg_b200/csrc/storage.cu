@@ -255,6 +255,7 @@ void Storage::buildTiles(int L) {
 void Storage::setL2Budget(int64_t bytes) {
   argCheck(bytes > 0, "L2 budget must be positive");
   l2Budget = bytes;
+  ++generation;
   for (int L = 0; L <= maxLevel(); ++L) buildTiles(L);
 }
 
@@ -393,6 +394,37 @@ void Storage::interpolateExpr(int id, int L, unsigned mask, int expr, const doub
   communicate(id, L, kAllGroups);
 }
 
+void Storage::fillRandom(int id, int L, unsigned mask, uint64_t seed, double lo, double hi) {
+  Function& f = fn(id);
+  const LevelData& ld = levels[L];
+  if (ld.nChunks) {
+    if (f.prec == 8)
+      dev::randomFillKernel<double><<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (double*)data(id, L), seed, lo, hi);
+    else
+      dev::randomFillKernel<float><<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (float*)data(id, L), seed, lo, hi);
+    ++launches;
+    cudaCheck(cudaGetLastError(), "random fill");
+  }
+  communicate(id, L, kAllGroups);
+}
+
+int64_t Storage::deviceBytes() const {
+  int64_t b = (int64_t)scalars.bytes;
+  for (auto& g : geomKeep) b += (int64_t)g->bytes;
+  for (const LevelData& ld : levels) {
+    for (auto& k : ld.keep) b += (int64_t)k->bytes;
+    if (ld.tileBuf) b += (int64_t)ld.tileBuf->bytes;
+    b += (int64_t)ld.partial.bytes;
+  }
+  for (auto& f : fns)
+    for (auto& l : f.second->levels) b += (int64_t)l->bytes;
+  for (auto& o : ops)
+    for (auto& k : o.second->keep) b += (int64_t)k->bytes;
+  for (auto& sp : spare)
+    if (sp.second) b += (int64_t)sp.second->bytes;
+  return b;
+}
+
 double Storage::dot(int a, int b, int L, unsigned mask) {
   double* d = (double*)scalars.p;
   dotAsync(a, b, L, mask, d);
@@ -440,6 +472,44 @@ static dev::StencilDev<T> packStencil(std::vector<std::unique_ptr<DevBuf>>& keep
   d.lowEntRel = (const int64_t*)upload(keep, rel, stream);
   d.lowEntW = (const T*)upload(keep, wv, stream);
   return d;
+}
+
+// New stencil values into the device arrays of an existing operator (same topology, so the same
+// sizes and index arrays): no device allocation or release, only copies on this stream.
+template <class T>
+static void refillStencil(const dev::StencilDev<T>& d, const LevelStencils& st, cudaStream_t stream) {
+  std::vector<T> cellW;
+  for (auto& c : st.cell)
+    for (int k = 0; k < 16; ++k) cellW.push_back(T(c[k]));
+  std::vector<dev::FaceEnt<T>> fe(st.face.size() * 16);
+  for (size_t f = 0; f < st.face.size(); ++f)
+    for (size_t k = 0; k < st.face[f].size(); ++k)
+      fe[16 * f + k] = {T(st.face[f][k].w), st.face[f][k].layer, st.face[f][k].dx, st.face[f][k].dy};
+  std::vector<T> wv;
+  for (auto& e : st.edge)
+    for (auto& x : e) wv.push_back(T(x.w));
+  for (auto& v : st.vert)
+    for (auto& x : v) wv.push_back(T(x.w));
+  if (!cellW.empty())
+    cudaCheck(cudaMemcpyAsync((void*)d.cellW, cellW.data(), cellW.size() * sizeof(T), cudaMemcpyHostToDevice, stream),
+              "stencil refill");
+  if (!fe.empty())
+    cudaCheck(cudaMemcpyAsync((void*)d.faceEnt, fe.data(), fe.size() * sizeof(fe[0]), cudaMemcpyHostToDevice, stream),
+              "stencil refill");
+  if (!wv.empty())
+    cudaCheck(cudaMemcpyAsync((void*)d.lowEntW, wv.data(), wv.size() * sizeof(T), cudaMemcpyHostToDevice, stream),
+              "stencil refill");
+  cudaCheck(cudaStreamSynchronize(stream), "stencil refill");
+}
+
+void Storage::reassembleOperator(int id) {
+  Operator& o = op(id);
+  for (int L = o.minL; L <= o.maxL; ++L) {
+    LevelStencils h = assembleStencils(disc, L, (FormKind)o.form);
+    refillStencil<double>(o.d[L - o.minL], h, stream);
+    refillStencil<float>(o.f[L - o.minL], h, stream);
+    o.host[L - o.minL] = std::move(h);
+  }
 }
 
 int Storage::createOperator(int form, int minL, int maxL) {

@@ -82,6 +82,7 @@ struct Storage {
   // Cell-phase schedule of the multicolour SOR: 0 = one wavefront pass that writes a second
   // buffer which then replaces the level buffer, 1 = four in-place colour passes.
   int sorSchedule = 0;
+  unsigned long long generation = 0;  // bumped when level tables or schedules change (captured graphs)
   std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> spare;  // (level, precision) -> buffer
   dev::Geometry geom{};              // macro-vertex coordinates and primitive vertex lists (device)
   std::vector<std::unique_ptr<DevBuf>> geomKeep;
@@ -95,9 +96,15 @@ struct Storage {
   void copyCast(int dst, int src, int L, unsigned mask, bool add);
   void dotAsync(int a, int b, int L, unsigned mask, double* dOut);
   void interpolateExpr(int id, int L, unsigned mask, int expr, const double* params);
+  // Seeded uniform [lo, hi) values at the flagged primitives' DoFs, then a full halo refresh.
+  void fillRandom(int id, int L, unsigned mask, uint64_t seed, double lo, double hi);
+  // Device memory held by this storage (level tables, functions, operators, spare buffers).
+  int64_t deviceBytes() const;
   double dot(int a, int b, int L, unsigned mask);
 
   int createOperator(int form, int minL, int maxL);
+  // Re-assemble an operator's stencils from the current cell coefficients into its device arrays.
+  void reassembleOperator(int id);
   Operator& op(int id);
   void apply(int op, int src, int dst, int L, unsigned mask, int update, int kinds = 15, bool refresh = true);
   void residual(int op, int x, int b, int r, int L, unsigned mask);

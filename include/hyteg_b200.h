@@ -169,6 +169,39 @@ int hg_dot(hg_storage* s, int a, int b, int level, unsigned flag, double* out);
 int hg_dot_noalloc(hg_storage* s, const void* a, const void* b, int precision, int level, unsigned flag,
                    double* result);
 
+/* ---------------------------------------------------------------------------------------
+ * Solve server (continuous batching). No counterpart in the reference, which solves one
+ * problem per program run; this serves a stream of independent P1 Poisson solves.
+ * A request is the unit cube split into k x k x k sub-cubes of 6 tetrahedra (meshCuboid),
+ * refined to `level`, Dirichlet 0 on the boundary, constant coefficient, right-hand side
+ * uniform[-1,1] at the inner DoFs from `seed` (hg_function_fill_random), x0 = 0, solved to the
+ * relative residual `tol` with V(3,3) cycles (precision 8) or FP64 defect correction around
+ * FP32 V(3,3) cycles (precision 4). `workers` threads admit queued requests in arrival order
+ * while the request's device footprint fits `hbm_budget_bytes`; each admitted request runs on
+ * a resident hierarchy of its shape with its own CUDA stream, concurrently with the others.
+ * --------------------------------------------------------------------------------------- */
+typedef struct hg_server hg_server;
+int hg_server_create(int workers, int64_t hbm_budget_bytes, int precision, hg_server** out);
+int hg_server_destroy(hg_server* srv);
+/* Build one resident hierarchy of shape (k, level) ahead of the first request. */
+int hg_server_prewarm(hg_server* srv, int k, int level);
+int hg_server_submit(hg_server* srv, int k, int level, double coefficient, uint64_t seed, double tol, int max_iter,
+                     int keep_solution, int64_t* id);
+/* Block until the request has finished (timeout < 0: no limit); *done = 1 when it has. */
+int hg_server_wait(hg_server* srv, int64_t id, double timeout_seconds, int* done);
+/* status: 0 queued, 1 running, 2 done, -1 failed (message in hg_last_error after this call
+ * returns HG_ERR_STATE); times: submit, admission, start of the iteration (after the stencils
+ * and the right-hand side are set up), end, in seconds since hg_server_create. */
+int hg_server_result(hg_server* srv, int64_t id, int* status, int* iterations, double* rel_residual, double times[4],
+                     int64_t* inner_dofs);
+/* Level buffer of the solution (requests submitted with keep_solution); *size = elements. */
+int hg_server_solution(hg_server* srv, int64_t id, double* host, int64_t n, int64_t* size);
+/* admitted, completed, failed, resident idle hierarchies, their bytes, peak bytes in use. */
+int hg_server_stats(hg_server* srv, int64_t stats[6]);
+/* Seeded uniform [lo, hi) values at the DoFs of the flagged primitives, then a halo refresh; the
+ * values depend only on (seed, slot), so equal topologies give equal vectors. */
+int hg_function_fill_random(hg_storage* s, int fn, int level, unsigned flag, uint64_t seed, double lo, double hi);
+
 /* form: 0 = diffusion (Laplace, scaled by the per-cell coefficient), 1 = mass */
 int hg_operator_create(hg_storage* s, int form, int min_level, int max_level, int* op);
 int hg_operator_destroy(hg_storage* s, int op);
@@ -208,6 +241,12 @@ int hg_gmg_solve(hg_storage* s, int gmg, int x, int b, int level);
  * solver repeats its cycle; an FP32 solver (precision 4) runs FP64 defect correction: r = b - A x
  * in FP64, one FP32 cycle on A e = r from e = 0 (its coarse CG in FP64), x += e in FP64.
  * history (nullable) receives the relative residual after each iteration. */
+/* Cycles are captured as CUDA graphs and replayed (default on) when the coarse level has only
+ * vertex and edge DoFs (its CG then runs on the device in one block) and pre + post smoothing
+ * steps are even. The first cycle with a given set of buffers runs eagerly, the second is
+ * captured; any change of a buffer address (for example an odd number of SOR sweeps on one of
+ * the functions elsewhere) selects or captures another graph. Results are identical either way. */
+int hg_gmg_set_graphs(hg_storage* s, int gmg, int enable);
 int hg_gmg_solve_to(hg_storage* s, int gmg, int x, int b, int level, double tol, int max_iter, int* iterations,
                     double* rel_residual, double* history, int history_cap);
 
