@@ -677,7 +677,11 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
   };
   // Only the copies the reference refreshes between phases are refreshed here, so ghost
   // values that reach a primitive from outside its closure keep their start-of-sweep value.
-  comm(kAllGroups);
+  // At the start only the groups read before their own refresh in this sweep are brought up to
+  // date (forward: vertex ghosts and face ghost layers; backward: cell closures and face
+  // boundary rows); the other groups are refreshed again before any phase reads them, so
+  // refreshing them here as well would not change a single value that is read.
+  comm(backwards ? (1 << G_CELL) | (1 << G_FACE_BOUNDARY) : (1 << G_VERT) | (1 << G_FACE_GHOST));
   if (!backwards) {
     verts();
     comm(1 << G_EDGE);           // Vertex -> Edge
