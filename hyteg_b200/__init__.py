@@ -494,6 +494,68 @@ class GeometricMultigridSolver:
             pass
 
 
+class P2Function:
+    """P2 (quadratic) function on levels [minLevel, maxLevel] (P2Function.hpp of the reference).
+    Its DoFs on level L are the vertex DoFs of level L + 1 (micro-vertices at even lattice
+    coordinates, micro-edge midpoints at the others), held by a vertex-DoF function `v` of
+    levels [minLevel + 1, maxLevel + 1]; level arguments here are P2 levels."""
+
+    def __init__(self, name, storage, minLevel, maxLevel, dtype=np.float64):
+        self.name = name
+        self.storage = storage
+        self.minLevel, self.maxLevel = minLevel, maxLevel
+        self.v = P1Function(name, storage, minLevel + 1, maxLevel + 1, dtype=dtype)
+        self.id = self.v.id
+        self.dtype = self.v.dtype
+
+    def to_numpy(self, level):
+        return self.v.to_numpy(level + 1)
+
+    def from_numpy(self, level, a):
+        self.v.from_numpy(level + 1, a)
+
+    def communicate(self, level):
+        self.v.communicate(level + 1)
+
+    def fill_random(self, seed, level, flag=All, lo=-1.0, hi=1.0):
+        self.v.fill_random(seed, level + 1, flag, lo, hi)
+
+    def interpolate(self, value, level, flag=All):
+        self.v.interpolate(value, level + 1, flag)
+
+    def assign(self, scalars, functions, level, flag=All):
+        self.v.assign(scalars, [f.v for f in functions], level + 1, flag)
+
+    def dotGlobal(self, other, level, flag=All):
+        return self.v.dotGlobal(other.v, level + 1, flag)
+
+
+class P2ConstantLaplaceOperator:
+    """P2ConstantLaplaceOperator (P2ConstantOperator.hpp:154-157): element-wise P2 Laplace with
+    the per-macro-cell coefficient, on levels [minLevel, maxLevel] (the storage needs
+    maxLevel + 1)."""
+
+    def __init__(self, storage, minLevel, maxLevel):
+        self.storage = storage
+        h = ctypes.c_int()
+        call("hg_p2_operator_create", storage.handle, 0, minLevel, maxLevel, ctypes.byref(h))
+        self.id = h.value
+
+    def apply(self, src, dst, level, flag=Inner):
+        call("hg_p2_apply", self.storage.handle, self.id, src.id, dst.id, level, flag)
+
+    def residual(self, x, b, r, level, flag=Inner):
+        call("hg_p2_residual", self.storage.handle, self.id, x.id, b.id, r.id, level, flag)
+
+    def __del__(self):
+        try:
+            st = getattr(self, "storage", None)
+            if st is not None and st.handle:
+                _capi.lib.hg_p2_operator_destroy(st.handle, self.id)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+
+
 class SolveServer:
     """Continuous-batching server of P1 Poisson solves (hg_server_*): requests on the unit cube
     split into k^3 sub-cubes of 6 tetrahedra at a refinement level, constant coefficient, seeded

@@ -88,6 +88,10 @@ _SIGS = {
     "hg_gmg_create": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_int, c_double, c_int, P(c_int)]),
     "hg_gmg_destroy": (c_int, [c_void_p, c_int]),
     "hg_gmg_solve": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
+    "hg_p2_operator_create": (c_int, [c_void_p, c_int, c_int, c_int, P(c_int)]),
+    "hg_p2_operator_destroy": (c_int, [c_void_p, c_int]),
+    "hg_p2_apply": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_uint]),
+    "hg_p2_residual": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_uint]),
     "hg_server_create": (c_int, [c_int, c_int64, c_int, P(c_void_p)]),
     "hg_server_destroy": (c_int, [c_void_p]),
     "hg_server_prewarm": (c_int, [c_void_p, c_int, c_int]),

@@ -682,6 +682,31 @@ int hg_mesh_low_stencil(const hg_mesh* m, int level, int form, int kind, int pri
   HG_CATCH
 }
 
+int hg_p2_operator_create(hg_storage* h, int form, int min_level, int max_level, int* op) {
+  HG_TRY
+  hg::argCheck(op != nullptr, "null output pointer");
+  *op = S(h).createP2Operator(form, min_level, max_level);
+  HG_CATCH
+}
+
+int hg_p2_operator_destroy(hg_storage* h, int op) {
+  HG_TRY
+  S(h).p2ops.erase(op);
+  HG_CATCH
+}
+
+int hg_p2_apply(hg_storage* h, int op, int src, int dst, int level, unsigned flag) {
+  HG_TRY
+  S(h).p2Apply(op, src, dst, -1, level, flag, 0);
+  HG_CATCH
+}
+
+int hg_p2_residual(hg_storage* h, int op, int x, int b, int r, int level, unsigned flag) {
+  HG_TRY
+  S(h).p2Apply(op, x, r, b, level, flag, 2);
+  HG_CATCH
+}
+
 struct hg_server {
   hg::Server* s;
 };

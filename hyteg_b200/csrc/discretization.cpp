@@ -341,6 +341,81 @@ void Discretization::buildLevel(int L) {
 // ---------------------------------------------------------------------------------------
 // Element matrices
 // ---------------------------------------------------------------------------------------
+const int kP2Edge[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+const int kMicroCellTable[6][4][3] = {
+    {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}}, {{1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {1, 0, 1}},
+    {{1, 0, 0}, {0, 1, 0}, {1, 0, 1}, {0, 0, 1}}, {{1, 1, 0}, {1, 1, 1}, {0, 1, 1}, {1, 0, 1}},
+    {{1, 0, 1}, {0, 1, 1}, {0, 0, 1}, {0, 1, 0}}, {{0, 1, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}},
+};
+const int kMicroCellWidth[6] = {0, 1, 1, 2, 1, 1};
+
+void elementP2Laplace(const double p[4][3], double K[100]) {
+  double J[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) J[r][c] = p[c + 1][r] - p[0][r];
+  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                     J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  // gradients of the barycentric coordinates: rows of J^-1 (lambda_1..3), lambda_0 = 1 - sum
+  const double cof[3][3] = {{J[1][1] * J[2][2] - J[1][2] * J[2][1], J[0][2] * J[2][1] - J[0][1] * J[2][2],
+                             J[0][1] * J[1][2] - J[0][2] * J[1][1]},
+                            {J[1][2] * J[2][0] - J[1][0] * J[2][2], J[0][0] * J[2][2] - J[0][2] * J[2][0],
+                             J[0][2] * J[1][0] - J[0][0] * J[1][2]},
+                            {J[1][0] * J[2][1] - J[1][1] * J[2][0], J[0][1] * J[2][0] - J[0][0] * J[2][1],
+                             J[0][0] * J[1][1] - J[0][1] * J[1][0]}};
+  double G[4][3];
+  for (int d = 0; d < 3; ++d) {
+    for (int i = 0; i < 3; ++i) G[i + 1][d] = cof[i][d] / det;
+    G[0][d] = -(G[1][d] + G[2][d] + G[3][d]);
+  }
+  double gg[4][4];
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) gg[a][b] = G[a][0] * G[b][0] + G[a][1] * G[b][1] + G[a][2] * G[b][2];
+  const double vol = std::fabs(det) / 6.0;
+  auto m2 = [vol](int a, int b) { return vol * (a == b ? 2.0 : 1.0) / 20.0; };  // int lambda_a lambda_b
+  auto m1l = [vol](int a, int x) { return vol * ((a == x ? 2.0 : 1.0) / 5.0 - 0.25); };  // int (4 l_a - 1) l_x
+  // node i: vertex a (i < 4) with gradient (4 l_a - 1) G_a, or edge (a, b) with 4 (l_b G_a + l_a G_b)
+  for (int i = 0; i < 10; ++i)
+    for (int j = 0; j < 10; ++j) {
+      double v;
+      if (i < 4 && j < 4) {
+        v = gg[i][j] * vol * (4.0 * (i == j ? 2.0 : 1.0) / 5.0 - 1.0);
+      } else if (i < 4 || j < 4) {
+        const int a = i < 4 ? i : j, e = (i < 4 ? j : i) - 4;
+        const int c = kP2Edge[e][0], d = kP2Edge[e][1];
+        v = 4.0 * (gg[a][c] * m1l(a, d) + gg[a][d] * m1l(a, c));
+      } else {
+        const int a = kP2Edge[i - 4][0], b = kP2Edge[i - 4][1], c = kP2Edge[j - 4][0], d = kP2Edge[j - 4][1];
+        v = 16.0 * (gg[a][c] * m2(b, d) + gg[a][d] * m2(b, c) + gg[b][c] * m2(a, d) + gg[b][d] * m2(a, c));
+      }
+      K[10 * i + j] = v;
+    }
+}
+
+std::vector<double> p2CellElements(const Topology& topo, int L) {
+  const int64_t N = int64_t(1) << L;
+  std::vector<double> out(topo.cells.size() * 600, 0.0);
+  for (size_t c = 0; c < topo.cells.size(); ++c) {
+    const auto& ce = topo.cells[c];
+    double V[4][3];
+    for (int i = 0; i < 4; ++i)
+      for (int d = 0; d < 3; ++d) V[i][d] = topo.verts[ce.v[i]].x[d];
+    for (int t = 0; t < 6; ++t) {
+      double P[4][3];
+      for (int m = 0; m < 4; ++m)
+        for (int d = 0; d < 3; ++d)
+          P[m][d] = V[0][d] + ((V[1][d] - V[0][d]) * kMicroCellTable[t][m][0] +
+                               (V[2][d] - V[0][d]) * kMicroCellTable[t][m][1] +
+                               (V[3][d] - V[0][d]) * kMicroCellTable[t][m][2]) /
+                                  (double)N;
+      double K[100];
+      elementP2Laplace(P, K);
+      for (int i = 0; i < 100; ++i) out[c * 600 + t * 100 + i] = ce.k * K[i];
+    }
+  }
+  return out;
+}
+
 void elementLaplace(const double p[4][3], double K[16]) {
   double J[3][3];
   for (int r = 0; r < 3; ++r)

@@ -126,4 +126,19 @@ void elementMass(const double p[4][3], double K[16]);
 
 LevelStencils assembleStencils(const Discretization& d, int L, FormKind form);
 
+// P2 (quadratic) space of level L, stored as the vertex-DoF lattice of level L + 1: the
+// micro-vertices of level L sit at even coordinates, the midpoints of its micro-edges at the
+// seven other parity classes (the reference's X, Y, Z, XY, XZ, YZ, XYZ edge orientations,
+// edgedofspace/EdgeDoFOrientation.hpp:29-39). Local nodes of a micro-tetrahedron: its four
+// vertices, then the midpoints of the edges (0,1),(0,2),(0,3),(1,2),(1,3),(2,3).
+extern const int kP2Edge[6][2];
+extern const int kMicroCellTable[6][4][3];
+extern const int kMicroCellWidth[6];
+// P2 Laplace element matrix (10 x 10, row major) from the barycentric moments
+// int lambda_a lambda_b = |T| (1 + delta_ab) / 20 (p2_tet_diffusion of the reference's forms).
+void elementP2Laplace(const double p[4][3], double K[100]);
+// Element matrices of the six micro-cell types of level L in every macro-cell, scaled by the
+// cell's coefficient: [cell][type][10][10].
+std::vector<double> p2CellElements(const Topology& topo, int L);
+
 }  // namespace hg

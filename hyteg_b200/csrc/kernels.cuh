@@ -838,6 +838,74 @@ static __global__ void __launch_bounds__(kBlock) coarseCgKernel(LevelDev lv, Ste
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// P2 operator of level L on the vertex-DoF lattice of level L + 1 (size M = 2N per edge).
+// Node (X, Y, Z) of a macro-cell is local node j of the level-L micro-cell (t, a) exactly when
+// (X, Y, Z) = 2a + off[t][j]; its parity class (X, Y, Z mod 2) fixes the candidates (t, j).
+// A thread owns one node of the closed macro-cell and sums, over the candidate micro-cells that
+// lie inside the cell, row j of that micro-cell's 10 x 10 element matrix times the ten nodal
+// values (gather form of the element-by-element product; deterministic). Interior nodes get
+// their final value; nodes on the cell's faces, edges and vertices get this cell's share in the
+// cell's closure slots, which p2AddKernel sums into the owning primitive.
+// ---------------------------------------------------------------------------------------
+struct P2Tables {
+  signed char off[6][10][3];   // lattice offset of local node j of micro-cell type t from 2a
+  unsigned char nCand[8];      // candidates per parity class
+  unsigned char cand[8][24][2];  // (t, j)
+  unsigned char widthRed[6];   // micro-cells of type t: a_x + a_y + a_z < N - widthRed[t]
+};
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(kBlock) p2CellKernel(LevelDev lv, P2Tables tb, const T* __restrict__ K,
+                                                       T* __restrict__ dst, const T* __restrict__ src,
+                                                       const T* __restrict__ rhs, unsigned mask) {
+  const int M = lv.N, N = M / 2, nPl = M + 1, w = lv.w;
+  const int c = blockIdx.x / nPl, Z = blockIdx.x % nPl;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t base = lv.cellOff[c];
+  const bool cellOn = (lv.cellType[c] & mask) != 0;
+  const T* Kc = K + (int64_t)c * 600;
+  const int pb = int(tetSize(w) - tetSize(w - Z));
+  for (int Y = warp; Y <= M - Z; Y += kBlock / 32) {
+    const int r0 = pb + rowStart(w - Z, Y);
+    for (int X = lane; X <= M - Z - Y; X += 32) {
+      const int pc = (X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2);
+      T s = T(0);
+      for (int k = 0; k < tb.nCand[pc]; ++k) {
+        const int t = tb.cand[pc][k][0], j = tb.cand[pc][k][1];
+        const int ax = (X - tb.off[t][j][0]) >> 1, ay = (Y - tb.off[t][j][1]) >> 1, az = (Z - tb.off[t][j][2]) >> 1;
+        if (ax < 0 || ay < 0 || az < 0 || ax + ay + az >= N - tb.widthRed[t]) continue;
+        const T* Kr = Kc + t * 100 + j * 10;
+#pragma unroll
+        for (int m = 0; m < 10; ++m) {
+          const int qx = 2 * ax + tb.off[t][m][0], qy = 2 * ay + tb.off[t][m][1], qz = 2 * az + tb.off[t][m][2];
+          const int W = w - qz;
+          s += Kr[m] * __ldg(src + base + int(tetSize(w) - tetSize(W)) + rowStart(W, qy) + qx);
+        }
+      }
+      const int64_t i = base + r0 + X;
+      const bool interior = X >= 1 && Y >= 1 && Z >= 1 && X + Y + Z <= M - 1;
+      if (!interior) dst[i] = s;
+      else if (cellOn) dst[i] = MODE == MODE_RESIDUAL ? rhs[i] - s : s;
+    }
+  }
+}
+
+// Sums the cells' shares of every DoF owned by a face, edge or vertex (the copies of that DoF in
+// the closure slots of its cells) into the owner slot: dst = sum, or rhs - sum for a residual.
+template <class T, int MODE>
+__global__ void __launch_bounds__(kBlock) p2AddKernel(const int64_t* __restrict__ owner, const int* __restrict__ ptr,
+                                                      const int64_t* __restrict__ copies,
+                                                      const unsigned char* __restrict__ type, int n, T* dst,
+                                                      const T* __restrict__ rhs, unsigned mask) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !(type[i] & mask)) return;
+  T v = T(0);
+  for (int k = ptr[i]; k < ptr[i + 1]; ++k) v += dst[copies[k]];
+  const int64_t o = owner[i];
+  dst[o] = MODE == MODE_RESIDUAL ? rhs[o] - v : v;
+}
+
 // colour < 0: all points; otherwise x mod 2 == colour (edges are 1-D chains)
 template <class T>
 __global__ void __launch_bounds__(kBlock) lowSorKernel(LevelDev lv, StencilDev<T> st, T* u, const T* __restrict__ rhs,

@@ -502,6 +502,147 @@ static void refillStencil(const dev::StencilDev<T>& d, const LevelStencils& st, 
   cudaCheck(cudaStreamSynchronize(stream), "stencil refill");
 }
 
+int Storage::createP2Operator(int form, int minL, int maxL) {
+  argCheck(form == FORM_LAPLACE, "P2 operators: only the Laplace form is available");
+  argCheck(minL >= 0 && maxL + 1 <= maxLevel() && minL <= maxL,
+           "P2 level range needs the storage's levels up to max_level + 1");
+  std::unique_ptr<P2Operator> o(new P2Operator());
+  o->form = form;
+  o->minL = minL;
+  o->maxL = maxL;
+  for (int L = minL; L <= maxL; ++L) {
+    const std::vector<double> K = p2CellElements(disc.topo(), L);
+    std::vector<float> Kf(K.begin(), K.end());
+    o->kd.emplace_back(new DevBuf());
+    o->kd.back()->alloc(K.size() * sizeof(double));
+    cudaCheck(cudaMemcpyAsync(o->kd.back()->p, K.data(), K.size() * sizeof(double), cudaMemcpyHostToDevice, stream),
+              "P2 upload");
+    o->kf.emplace_back(new DevBuf());
+    o->kf.back()->alloc(Kf.size() * sizeof(float));
+    cudaCheck(cudaMemcpyAsync(o->kf.back()->p, Kf.data(), Kf.size() * sizeof(float), cudaMemcpyHostToDevice, stream),
+              "P2 upload");
+    cudaCheck(cudaStreamSynchronize(stream), "P2 upload");
+  }
+  const int id = nextId++;
+  p2ops[id] = std::move(o);
+  return id;
+}
+
+static dev::P2Tables p2Tables() {
+  dev::P2Tables tb{};
+  for (int t = 0; t < 6; ++t) {
+    tb.widthRed[t] = (unsigned char)kMicroCellWidth[t];
+    for (int j = 0; j < 10; ++j)
+      for (int d = 0; d < 3; ++d)
+        tb.off[t][j][d] = (signed char)(j < 4 ? 2 * kMicroCellTable[t][j][d]
+                                              : kMicroCellTable[t][kP2Edge[j - 4][0]][d] +
+                                                    kMicroCellTable[t][kP2Edge[j - 4][1]][d]);
+  }
+  for (int t = 0; t < 6; ++t)
+    for (int j = 0; j < 10; ++j) {
+      const int pc = (tb.off[t][j][0] & 1) | ((tb.off[t][j][1] & 1) << 1) | ((tb.off[t][j][2] & 1) << 2);
+      argCheck(tb.nCand[pc] < 24, "P2 candidate table overflow");
+      tb.cand[pc][tb.nCand[pc]][0] = (unsigned char)t;
+      tb.cand[pc][tb.nCand[pc]][1] = (unsigned char)j;
+      ++tb.nCand[pc];
+    }
+  return tb;
+}
+
+void Storage::p2Apply(int opId, int src, int dst, int rhs, int L, unsigned mask, int mode) {
+  auto it = p2ops.find(opId);
+  argCheck(it != p2ops.end(), "unknown P2 operator handle");
+  P2Operator& o = *it->second;
+  argCheck(L >= o.minL && L <= o.maxL, "level outside the P2 operator's level range");
+  argCheck(src != dst && (mode == 0 || (rhs != dst && rhs != src)), "P2 apply: distinct functions required");
+  const int Lf = L + 1;
+  Function& fs = fn(src);
+  argCheck(fs.prec == fn(dst).prec && (mode == 0 || fn(rhs).prec == fs.prec), "P2 apply: precision mismatch");
+  const LevelData& ld = levels[Lf];
+  // additive table of this lattice level (built once): owner <- closure copies in its cells
+  if ((int)p2add.size() <= Lf) p2add.resize(maxLevel() + 1);
+  P2Additive& ad = p2add[Lf];
+  if (!ad.built) {
+    std::map<int64_t, std::vector<int64_t>> byOwner;
+    const auto& cd = ld.lay->commDst[G_CELL];
+    const auto& cs = ld.lay->commSrc[G_CELL];
+    for (size_t i = 0; i < cd.size(); ++i) byOwner[cs[i]].push_back(cd[i]);
+    std::vector<int64_t> own, cp;
+    std::vector<int> ptr{0};
+    std::vector<unsigned char> ty;
+    auto typeOf = [&](int64_t slot) {  // DoF type of the primitive whose array holds the slot
+      for (int k : {KF, KE, KV})
+        for (size_t pr = 0; pr < ld.lay->off[k].size(); ++pr)
+          if (slot >= ld.lay->off[k][pr] && slot < ld.lay->off[k][pr] + ld.lay->size[k][pr])
+            return k == KF ? ld.hostFaceType[pr] : k == KE ? ld.hostLowType[pr] : ld.hostLowType[ld.lv.nEdges + pr];
+      throw Error(HG_ERR_INTERNAL, "owner slot outside the face, edge and vertex arrays");
+    };
+    for (auto& kv : byOwner) {
+      own.push_back(kv.first);
+      for (int64_t c : kv.second) cp.push_back(c);
+      ptr.push_back((int)cp.size());
+      ty.push_back(typeOf(kv.first));
+    }
+    ad.n = (int)own.size();
+    ad.owner.alloc(std::max<size_t>(1, own.size()) * sizeof(int64_t));
+    ad.ptr.alloc(ptr.size() * sizeof(int));
+    ad.copies.alloc(std::max<size_t>(1, cp.size()) * sizeof(int64_t));
+    ad.type.alloc(std::max<size_t>(1, ty.size()));
+    if (!own.empty()) {
+      cudaCheck(cudaMemcpyAsync(ad.owner.p, own.data(), own.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream), "p2 add");
+      cudaCheck(cudaMemcpyAsync(ad.copies.p, cp.data(), cp.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream), "p2 add");
+      cudaCheck(cudaMemcpyAsync(ad.type.p, ty.data(), ty.size(), cudaMemcpyHostToDevice, stream), "p2 add");
+    }
+    cudaCheck(cudaMemcpyAsync(ad.ptr.p, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice, stream), "p2 add");
+    cudaCheck(cudaStreamSynchronize(stream), "p2 add");
+    ad.built = true;
+  }
+  communicate(src, Lf, 1 << G_CELL);  // the closure copies of every cell hold the owners' values
+  static const dev::P2Tables tb = p2Tables();
+  const int nb = ld.lv.nCells * (ld.lv.N + 1);
+  const int na = (ad.n + dev::kBlock - 1) / dev::kBlock;
+  if (fs.prec == 8) {
+    const double* K = (const double*)o.kd[L - o.minL]->p;
+    double* d = (double*)data(dst, Lf);
+    const double* sr = (const double*)data(src, Lf);
+    const double* r = mode ? (const double*)data(rhs, Lf) : nullptr;
+    if (mode == 0) {
+      dev::p2CellKernel<double, dev::MODE_REPLACE><<<nb, dev::kBlock, 0, stream>>>(ld.lv, tb, K, d, sr, r, mask);
+      if (ad.n)
+        dev::p2AddKernel<double, dev::MODE_REPLACE><<<na, dev::kBlock, 0, stream>>>(
+            (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
+            ad.n, d, r, mask);
+    } else {
+      dev::p2CellKernel<double, dev::MODE_RESIDUAL><<<nb, dev::kBlock, 0, stream>>>(ld.lv, tb, K, d, sr, r, mask);
+      if (ad.n)
+        dev::p2AddKernel<double, dev::MODE_RESIDUAL><<<na, dev::kBlock, 0, stream>>>(
+            (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
+            ad.n, d, r, mask);
+    }
+  } else {
+    const float* K = (const float*)o.kf[L - o.minL]->p;
+    float* d = (float*)data(dst, Lf);
+    const float* sr = (const float*)data(src, Lf);
+    const float* r = mode ? (const float*)data(rhs, Lf) : nullptr;
+    if (mode == 0) {
+      dev::p2CellKernel<float, dev::MODE_REPLACE><<<nb, dev::kBlock, 0, stream>>>(ld.lv, tb, K, d, sr, r, mask);
+      if (ad.n)
+        dev::p2AddKernel<float, dev::MODE_REPLACE><<<na, dev::kBlock, 0, stream>>>(
+            (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
+            ad.n, d, r, mask);
+    } else {
+      dev::p2CellKernel<float, dev::MODE_RESIDUAL><<<nb, dev::kBlock, 0, stream>>>(ld.lv, tb, K, d, sr, r, mask);
+      if (ad.n)
+        dev::p2AddKernel<float, dev::MODE_RESIDUAL><<<na, dev::kBlock, 0, stream>>>(
+            (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
+            ad.n, d, r, mask);
+    }
+  }
+  launches += ad.n ? 2 : 1;
+  cudaCheck(cudaGetLastError(), "P2 apply");
+  communicate(dst, Lf, kAllGroups);
+}
+
 void Storage::reassembleOperator(int id) {
   Operator& o = op(id);
   for (int L = o.minL; L <= o.maxL; ++L) {

@@ -60,6 +60,19 @@ struct Operator {
   std::vector<std::unique_ptr<DevBuf>> keep;
 };
 
+// P2 operator: element matrices of the six micro-cell types per macro-cell and level.
+struct P2Operator {
+  int form = 0, minL = 0, maxL = 0;
+  std::vector<std::unique_ptr<DevBuf>> kd, kf;  // per level: [cell][type][10][10] in FP64 / FP32
+};
+
+// Cell-closure copies of every DoF owned by a face, edge or vertex of one lattice level.
+struct P2Additive {
+  bool built = false;
+  int n = 0;
+  DevBuf owner, ptr, copies, type;
+};
+
 struct Gmg;
 
 struct Storage {
@@ -74,6 +87,8 @@ struct Storage {
   std::map<int, std::unique_ptr<Function>> fns;
   std::map<int, std::unique_ptr<Operator>> ops;
   std::map<int, std::unique_ptr<Gmg>> gmgs;
+  std::map<int, std::unique_ptr<P2Operator>> p2ops;
+  std::deque<P2Additive> p2add;  // per lattice level
   int nextId = 1;
   int structureOp = -1;
   DevBuf scalars;            // device scratch for reductions
@@ -103,6 +118,10 @@ struct Storage {
   double dot(int a, int b, int L, unsigned mask);
 
   int createOperator(int form, int minL, int maxL);
+  // P2 operators on levels [minL, maxL]; the P2 DoFs of level L are the vertex DoFs of level L+1.
+  int createP2Operator(int form, int minL, int maxL);
+  // dst = A2 src (mode 0) or dst = rhs - A2 src (mode 2) at the flagged DoFs of P2 level L.
+  void p2Apply(int op, int src, int dst, int rhs, int L, unsigned mask, int mode);
   // Re-assemble an operator's stencils from the current cell coefficients into its device arrays.
   void reassembleOperator(int id);
   Operator& op(int id);

@@ -170,6 +170,24 @@ int hg_dot_noalloc(hg_storage* s, const void* a, const void* b, int precision, i
                    double* result);
 
 /* ---------------------------------------------------------------------------------------
+ * P2 (quadratic Lagrange) operators. The P2 DoFs of level L (micro-vertices and micro-edge
+ * midpoints of level L) are exactly the vertex DoFs of level L + 1, so a P2 function of levels
+ * [a, b] is a function of levels [a + 1, b + 1] created with hg_function_create; its values at
+ * even lattice coordinates are the vertex DoFs, the other seven parity classes the edge DoFs of
+ * the reference's seven edge orientations (edgedofspace/EdgeDoFOrientation.hpp:29-39). The
+ * reference stores the same values in separate vertex-DoF and edge-DoF arrays
+ * (P2Function.hpp): a host adapter converts between the two layouts.
+ * Replaces P2ConstantLaplaceOperator = P2ConstantOperator<P2FenicsForm<p2_diffusion,
+ * p2_tet_diffusion>> (p2functionspace/P2ConstantOperator.hpp:154-157); form 0 only.
+ * --------------------------------------------------------------------------------------- */
+int hg_p2_operator_create(hg_storage* s, int form, int min_level, int max_level, int* op);
+int hg_p2_operator_destroy(hg_storage* s, int op);
+/* dst = A src at the flagged P2 DoFs of `level` (P2ConstantOperator.cpp:98-117, Replace). */
+int hg_p2_apply(hg_storage* s, int op, int src, int dst, int level, unsigned flag);
+/* r = b - A x at the flagged P2 DoFs of `level`. */
+int hg_p2_residual(hg_storage* s, int op, int x, int b, int r, int level, unsigned flag);
+
+/* ---------------------------------------------------------------------------------------
  * Solve server (continuous batching). No counterpart in the reference, which solves one
  * problem per program run; this serves a stream of independent P1 Poisson solves.
  * A request is the unit cube split into k x k x k sub-cubes of 6 tetrahedra (meshCuboid),

@@ -87,6 +87,55 @@ void massElement(const double p[4][3], double K[4][4]) {
     for (int j = 0; j < 4; ++j) K[i][j] = vol * (i == j ? 2.0 : 1.0) / 20.0;
 }
 
+// P2 Laplace element matrix of a tetrahedron (vertices p[4]). Local nodes: the vertices 0..3,
+// then the edge midpoints (0,1),(0,2),(0,3),(1,2),(1,3),(2,3). Basis: lambda_a (2 lambda_a - 1)
+// and 4 lambda_a lambda_b; the gradients are linear in lambda, so the 4-point degree-2 rule
+// (points (a,b,b,b), a = (5 + 3 sqrt5)/20, b = (5 - sqrt5)/20) integrates the products exactly.
+static const int kP2Edge[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+
+void p2LaplaceElement(const double p[4][3], double K[10][10]) {
+  double J[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) J[r][c] = p[c + 1][r] - p[0][r];
+  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  // rows of J^-1 are the gradients of lambda_1..3
+  double inv[3][3];
+  inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+  inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+  inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+  inv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
+  inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+  inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+  inv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+  inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+  inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+  double G[4][3];
+  for (int d = 0; d < 3; ++d) {
+    G[1][d] = inv[0][d];
+    G[2][d] = inv[1][d];
+    G[3][d] = inv[2][d];
+    G[0][d] = -(G[1][d] + G[2][d] + G[3][d]);
+  }
+  const double vol = std::fabs(det) / 6.0;
+  const double qa = (5.0 + 3.0 * std::sqrt(5.0)) / 20.0, qb = (5.0 - std::sqrt(5.0)) / 20.0;
+  for (int i = 0; i < 10; ++i)
+    for (int j = 0; j < 10; ++j) K[i][j] = 0.0;
+  for (int q = 0; q < 4; ++q) {
+    double l[4] = {qb, qb, qb, qb};
+    l[q] = qa;
+    double g[10][3];
+    for (int a = 0; a < 4; ++a)
+      for (int d = 0; d < 3; ++d) g[a][d] = (4.0 * l[a] - 1.0) * G[a][d];
+    for (int e = 0; e < 6; ++e) {
+      const int a = kP2Edge[e][0], b = kP2Edge[e][1];
+      for (int d = 0; d < 3; ++d) g[4 + e][d] = 4.0 * (l[b] * G[a][d] + l[a] * G[b][d]);
+    }
+    for (int i = 0; i < 10; ++i)
+      for (int j = 0; j < 10; ++j) K[i][j] += 0.25 * vol * (g[i][0] * g[j][0] + g[i][1] * g[j][1] + g[i][2] * g[j][2]);
+  }
+}
+
 struct Node {
   Key key;
   int kind, id;           // owner primitive (0 vertex, 1 edge, 2 face, 3 cell) and its ID
@@ -103,6 +152,8 @@ struct Csr {
 
 struct LevelData {
   int64_t N = 1;
+  Csr P2;                    // P2 Laplace of this level on the nodes of the next finer level
+  bool haveP2 = false;
   std::vector<Node> nodes;
   std::unordered_map<Key, int64_t, KeyHash> index;
   Csr A[2];                  // 0: diffusion (per-cell coefficient), 1: mass
@@ -310,6 +361,52 @@ void buildMatrix(Oracle& o, int L, int form) {
     A.ptr.push_back((int64_t)A.col.size());
   }
   d.haveA[form] = true;
+}
+
+// P2 Laplace of level L assembled over the level-L micro-tetrahedra, on the node set of level
+// L + 1 (micro-vertices of level L at even coordinates, micro-edge midpoints at the others).
+void buildP2Matrix(Oracle& o, int L) {
+  LevelData& d = o.lv[L];
+  const LevelData& f = o.lv[L + 1];
+  const int64_t N = d.N;
+  std::vector<std::map<int64_t, double>> rows(f.nodes.size());
+  for (size_t ci = 0; ci < o.cells.size(); ++ci)
+    for (int t = 0; t < 6; ++t) {
+      const int64_t width = N - kMicroWidthReduction[t];
+      for (int64_t z = 0; z < width; ++z)
+        for (int64_t y = 0; y + z < width; ++y)
+          for (int64_t x = 0; x + y + z < width; ++x) {
+            int64_t v[4][3];
+            double p[4][3];
+            for (int m = 0; m < 4; ++m) {
+              v[m][0] = x + kMicro[t][m][0];
+              v[m][1] = y + kMicro[t][m][1];
+              v[m][2] = z + kMicro[t][m][2];
+              o.coordOf(o.keyOf((int)ci, N, v[m][0], v[m][1], v[m][2]), N, p[m]);
+            }
+            int64_t id[10];
+            for (int m = 0; m < 4; ++m) id[m] = f.index.at(o.keyOf((int)ci, 2 * N, 2 * v[m][0], 2 * v[m][1], 2 * v[m][2]));
+            for (int e = 0; e < 6; ++e) {
+              const int a = kP2Edge[e][0], b = kP2Edge[e][1];
+              id[4 + e] = f.index.at(
+                  o.keyOf((int)ci, 2 * N, v[a][0] + v[b][0], v[a][1] + v[b][1], v[a][2] + v[b][2]));
+            }
+            double K[10][10];
+            p2LaplaceElement(p, K);
+            for (int a = 0; a < 10; ++a)
+              for (int b = 0; b < 10; ++b) rows[id[a]][id[b]] += o.k[ci] * K[a][b];
+          }
+    }
+  Csr& A = d.P2;
+  A.ptr.assign(1, 0);
+  for (auto& r : rows) {
+    for (auto& kv : r) {
+      A.col.push_back(kv.first);
+      A.val.push_back(kv.second);
+    }
+    A.ptr.push_back((int64_t)A.col.size());
+  }
+  d.haveP2 = true;
 }
 
 const Csr& matrix(Oracle& o, int L, int form) {
@@ -552,6 +649,29 @@ void orc_gmg(void* h, int L, int minL, double* x, const double* b, int cycles, i
     }
   }
   std::copy(xs[L].begin(), xs[L].end(), x);
+}
+
+// y = A2 u for the P2 Laplace of level L; u and y are indexed by the nodes of level L + 1.
+void orc_p2_apply(void* h, int L, const double* u, double* y) {
+  Oracle& o = *(Oracle*)h;
+  if (!o.lv[L].haveP2) buildP2Matrix(o, L);
+  const Csr& A = o.lv[L].P2;
+  const int64_t n = (int64_t)A.ptr.size() - 1;
+  for (int64_t i = 0; i < n; ++i) {
+    double s = 0.0;
+    for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) s += A.val[k] * u[A.col[k]];
+    y[i] = s;
+  }
+}
+
+void orc_p2_element_laplace(const double* coords12, double* K100) {
+  double p[4][3];
+  for (int m = 0; m < 4; ++m)
+    for (int d = 0; d < 3; ++d) p[m][d] = coords12[3 * m + d];
+  double K[10][10];
+  p2LaplaceElement(p, K);
+  for (int i = 0; i < 10; ++i)
+    for (int j = 0; j < 10; ++j) K100[10 * i + j] = K[i][j];
 }
 
 void orc_element_laplace(const double* coords12, double* K16) {

@@ -41,6 +41,8 @@ def _load_oracle():
                            c_int, c_double, P(c_double)]),
         "orc_element_laplace": (None, [P(c_double), P(c_double)]),
         "orc_element_mass": (None, [P(c_double), P(c_double)]),
+        "orc_p2_apply": (None, [c_void_p, c_int, P(c_double), P(c_double)]),
+        "orc_p2_element_laplace": (None, [P(c_double), P(c_double)]),
         "orc_cell_local_stencil": (None, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, P(c_double)]),
     }
     for name, (res, args) in sig.items():
@@ -73,8 +75,9 @@ def ref_lib():
     r.ref_prolongate_cell.argtypes = [d, d, c_int, d, d, d]
     r.ref_p1_tet_diffusion.argtypes = [d, d]
     r.ref_p1_tet_mass.argtypes = [d, d]
+    r.ref_p2_tet_diffusion.argtypes = [d, d]
     for f in (r.ref_apply_cell, r.ref_sor_cell, r.ref_apply_face, r.ref_restrict_cell, r.ref_prolongate_cell,
-              r.ref_p1_tet_diffusion, r.ref_p1_tet_mass):
+              r.ref_p1_tet_diffusion, r.ref_p1_tet_mass, r.ref_p2_tet_diffusion):
         f.restype = None
     return r
 
@@ -163,10 +166,26 @@ class Oracle:
                       dp(res))
         return x, res
 
+    def p2_apply(self, L, u):
+        """P2 Laplace of level L applied to u; u and the result are indexed by the nodes of level
+        L + 1 (the oracle must hold level L + 1)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        y = np.zeros(self.n(L + 1))
+        lib().orc_p2_apply(self.h, L, dp(u), dp(y))
+        return y
+
     def cell_local_stencil(self, L, cell, x, y, z, form=0):
         out = np.zeros(15)
         lib().orc_cell_local_stencil(self.h, L, cell, x, y, z, form, dp(out))
         return out
+
+
+def p2_element_laplace(coords4x3):
+    """P2 Laplace element matrix (vertices, then edges (0,1),(0,2),(0,3),(1,2),(1,3),(2,3))."""
+    c = np.ascontiguousarray(coords4x3, dtype=np.float64).reshape(12)
+    K = np.zeros(100)
+    lib().orc_p2_element_laplace(dp(c), dp(K))
+    return K.reshape(10, 10)
 
 
 def element_laplace(coords4x3):

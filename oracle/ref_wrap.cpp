@@ -8,6 +8,7 @@
 #include "hyteg/fenics/ufc.h"
 #include "hyteg/forms/form_fenics_generated/p1_tet_diffusion.h"
 #include "hyteg/forms/form_fenics_generated/p1_tet_mass.h"
+#include "hyteg/forms/form_fenics_generated/p2_tet_diffusion.h"
 #include "hyteg/gridtransferoperators/generatedKernels/prolongate_3D_macrocell_P1_push_additive.hpp"
 #include "hyteg/gridtransferoperators/generatedKernels/restrict_3D_macrocell_P1_pull_additive.hpp"
 #include "hyteg/p1functionspace/generatedKernels/apply_3D_macrocell_vertexdof_to_vertexdof_add.hpp"
@@ -85,6 +86,12 @@ void ref_p1_tet_diffusion(const double* coords12, double* K16) {
 void ref_p1_tet_mass(const double* coords12, double* K16) {
   p1_tet_mass_cell_integral_0_otherwise f;
   f.tabulate_tensor(K16, nullptr, coords12, 0);
+}
+
+// P2 Laplace element matrix of the reference's FEniCS form (10 x 10, UFC local node order).
+void ref_p2_tet_diffusion(const double* coords12, double* K100) {
+  p2_tet_diffusion_cell_integral_0_otherwise f;
+  f.tabulate_tensor(K100, nullptr, coords12, 0);
 }
 
 }  // extern "C"

@@ -1,0 +1,89 @@
+"""P2 Laplace apply and residual on the device against the oracle's globally assembled P2
+matrix (48-tet cube, P2 levels 0-3 = vertex lattices 1-4; 3x3x3 cube for coarse levels with
+inner DoFs on every primitive kind).
+
+Tolerances: 1e-13 relative in FP64 and 2e-5 in FP32 (max-norm over inner DoFs); Dirichlet DoFs
+are not written."""
+import numpy as np
+import pytest
+
+import hyteg_b200 as hg
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def setup(nx, Lmax):
+    if hg.device_count() == 0:
+        pytest.skip("no CUDA device")
+    coords, tets, mesh, orc = H.cube(Lmax + 1, nx=nx)
+    st = hg.PrimitiveStorage.cuboid((0, 0, 0), (1, 1, 1), nx, nx, nx, Lmax + 1)
+    maps = {}
+    for L in range(Lmax + 1):
+        xyz, owned = mesh.slot_info(L + 1)
+        maps[L] = (H.match_slots(xyz, orc.nodes(L + 1)[0]), owned)
+    return st, orc, maps
+
+
+@pytest.fixture(scope="module")
+def cube2():
+    return setup(2, 3)
+
+
+@pytest.fixture(scope="module")
+def cube3():
+    return setup(3, 1)
+
+
+def rel(a, b, m):
+    return np.abs(a[m] - b[m]).max() / np.abs(b[m]).max()
+
+
+def run_apply(env, L, dtype, residual, seed):
+    st, orc, maps = env
+    node, owned = maps[L]
+    n = orc.n(L + 1)
+    rng = np.random.default_rng(seed)
+    u, f, d0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    Lmax = max(maps)
+    A = hg.P2ConstantLaplaceOperator(st, 0, Lmax)
+    x, b, y = (hg.P2Function(nm, st, 0, Lmax, dtype=dtype) for nm in ("x", "b", "y"))
+    x.from_numpy(L, H.scatter(node, u).astype(dtype))
+    b.from_numpy(L, H.scatter(node, f).astype(dtype))
+    y.from_numpy(L, H.scatter(node, d0).astype(dtype))
+    if residual:
+        A.residual(x, b, y, L, hg.Inner)
+    else:
+        A.apply(x, y, L, hg.Inner)
+    got = H.gather_owned(y.to_numpy(L).astype(np.float64), node, owned, n)
+    uu = u.astype(dtype).astype(np.float64)
+    ref = orc.p2_apply(L, uu)
+    if residual:
+        ref = f.astype(dtype).astype(np.float64) - ref
+    inner = ~orc.dirichlet(L + 1)
+    # copies of every DoF are consistent with its owner after the operation
+    full = y.to_numpy(L).astype(np.float64)
+    used = owned >= 0
+    assert np.array_equal(full[used], got[node[used]])
+    return got, ref, inner, d0.astype(dtype).astype(np.float64)
+
+
+@pytest.mark.parametrize("L", [0, 1, 2, 3])
+@pytest.mark.parametrize("residual", [False, True])
+def test_p2_apply_fp64(cube2, L, residual):
+    got, ref, inner, d0 = run_apply(cube2, L, np.float64, residual, 10 * L + residual)
+    assert rel(got, ref, inner) < 1e-13
+    assert np.array_equal(got[~inner], d0[~inner])
+
+
+@pytest.mark.parametrize("L", [1, 3])
+def test_p2_apply_fp32(cube2, L):
+    got, ref, inner, _ = run_apply(cube2, L, np.float32, False, 77)
+    assert rel(got, ref, inner) < 2e-5
+
+
+@pytest.mark.parametrize("L", [0, 1])
+def test_p2_apply_inner_vertices_and_edges(cube3, L):
+    # the 3x3x3 cube has inner macro-vertices and inner macro-edges: sums over up to 24 cells
+    got, ref, inner, _ = run_apply(cube3, L, np.float64, False, 5 + L)
+    assert rel(got, ref, inner) < 1e-13

@@ -239,3 +239,32 @@ def test_gmg_convergence_bound_of_reference_test(multicolour, oracle_mod):
         r = res2(u)
         assert r / last < 3.2e-2
         last = r
+
+
+def test_p2_element_matches_reference_form(ref, oracle_mod):
+    # p2_tet_diffusion of the reference's FEniCS forms; UFC numbers the edges
+    # (2,3),(1,3),(1,2),(0,3),(0,2),(0,1), the oracle (0,1),(0,2),(0,3),(1,2),(1,3),(2,3)
+    perm = [0, 1, 2, 3, 9, 8, 7, 6, 5, 4]
+    rng = np.random.default_rng(12)
+    for _ in range(5):
+        c = rng.uniform(-1, 1, (4, 3))
+        K = oracle_mod.p2_element_laplace(c)
+        R = np.zeros(100)
+        ref.ref_p2_tet_diffusion(oracle_mod.dp(np.ascontiguousarray(c.reshape(12))), oracle_mod.dp(R))
+        R = R.reshape(10, 10)[np.ix_(perm, perm)]
+        assert np.abs(K - R).max() <= 1e-13 * np.abs(R).max()
+
+
+@pytest.mark.parametrize("name", ["regular_octahedron_8el", "pyramid_4el", "pyramid_tilted_4el"])
+def test_p2_laplace_annihilates_constants_and_linears(name, oracle_mod):
+    m = meshes()[name]
+    L = 2
+    o = oracle_mod.Oracle(np.array(m["coords"]), np.array(m["tets"], dtype=np.int32), L + 1)
+    xyz, info = o.nodes(L + 1)
+    inner = ~info[:, 2].astype(bool)
+    for u in (np.ones(len(xyz)), 1.0 + 2.0 * xyz[:, 0] - xyz[:, 1] + 0.5 * xyz[:, 2]):
+        y = o.p2_apply(L, u)
+        assert np.abs(y[inner]).max() < 1e-12
+    rng = np.random.default_rng(1)
+    a, b = rng.uniform(-1, 1, len(xyz)), rng.uniform(-1, 1, len(xyz))
+    assert abs(a @ o.p2_apply(L, b) - b @ o.p2_apply(L, a)) < 1e-11
