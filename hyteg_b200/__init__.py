@@ -547,6 +547,12 @@ class P2ConstantLaplaceOperator:
     def residual(self, x, b, r, level, flag=Inner):
         call("hg_p2_residual", self.storage.handle, self.id, x.id, b.id, r.id, level, flag)
 
+    def smooth_sor(self, dst, rhs, relax, level, flag=Inner | NeumannBoundary):
+        call("hg_p2_smooth_sor", self.storage.handle, self.id, dst.id, rhs.id, float(relax), level, flag, 0)
+
+    def smooth_sor_backwards(self, dst, rhs, relax, level, flag=Inner | NeumannBoundary):
+        call("hg_p2_smooth_sor", self.storage.handle, self.id, dst.id, rhs.id, float(relax), level, flag, 1)
+
     def __del__(self):
         try:
             st = getattr(self, "storage", None)

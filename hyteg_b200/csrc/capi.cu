@@ -707,6 +707,12 @@ int hg_p2_residual(hg_storage* h, int op, int x, int b, int r, int level, unsign
   HG_CATCH
 }
 
+int hg_p2_smooth_sor(hg_storage* h, int op, int x, int b, double omega, int level, unsigned flag, int backwards) {
+  HG_TRY
+  S(h).p2Sor(op, x, b, omega, level, flag, backwards != 0);
+  HG_CATCH
+}
+
 struct hg_server {
   hg::Server* s;
 };

@@ -855,10 +855,15 @@ struct P2Tables {
   unsigned char widthRed[6];   // micro-cells of type t: a_x + a_y + a_z < N - widthRed[t]
 };
 
+constexpr int MODE_DIAG = 3;  // P2: sum of the element diagonals (the matrix diagonal)
+
+// colour, sel: when sel >= 0 only nodes whose colour (low 7 bits of the per-slot colour byte)
+// is sel are computed (one pass of the multicolour SOR); bit 7 of the byte marks owned slots.
 template <class T, int MODE>
 __global__ void __launch_bounds__(kBlock) p2CellKernel(LevelDev lv, P2Tables tb, const T* __restrict__ K,
                                                        T* __restrict__ dst, const T* __restrict__ src,
-                                                       const T* __restrict__ rhs, unsigned mask) {
+                                                       const T* __restrict__ rhs, unsigned mask,
+                                                       const unsigned char* __restrict__ colour, int sel) {
   const int M = lv.N, N = M / 2, nPl = M + 1, w = lv.w;
   const int c = blockIdx.x / nPl, Z = blockIdx.x % nPl;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -869,6 +874,8 @@ __global__ void __launch_bounds__(kBlock) p2CellKernel(LevelDev lv, P2Tables tb,
   for (int Y = warp; Y <= M - Z; Y += kBlock / 32) {
     const int r0 = pb + rowStart(w - Z, Y);
     for (int X = lane; X <= M - Z - Y; X += 32) {
+      const int64_t i = base + r0 + X;
+      if (sel >= 0 && (colour[i] & 0x7f) != sel) continue;
       const int pc = (X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2);
       T s = T(0);
       for (int k = 0; k < tb.nCand[pc]; ++k) {
@@ -876,6 +883,10 @@ __global__ void __launch_bounds__(kBlock) p2CellKernel(LevelDev lv, P2Tables tb,
         const int ax = (X - tb.off[t][j][0]) >> 1, ay = (Y - tb.off[t][j][1]) >> 1, az = (Z - tb.off[t][j][2]) >> 1;
         if (ax < 0 || ay < 0 || az < 0 || ax + ay + az >= N - tb.widthRed[t]) continue;
         const T* Kr = Kc + t * 100 + j * 10;
+        if (MODE == MODE_DIAG) {
+          s += Kr[j];
+          continue;
+        }
 #pragma unroll
         for (int m = 0; m < 10; ++m) {
           const int qx = 2 * ax + tb.off[t][m][0], qy = 2 * ay + tb.off[t][m][1], qz = 2 * az + tb.off[t][m][2];
@@ -883,7 +894,6 @@ __global__ void __launch_bounds__(kBlock) p2CellKernel(LevelDev lv, P2Tables tb,
           s += Kr[m] * __ldg(src + base + int(tetSize(w) - tetSize(W)) + rowStart(W, qy) + qx);
         }
       }
-      const int64_t i = base + r0 + X;
       const bool interior = X >= 1 && Y >= 1 && Z >= 1 && X + Y + Z <= M - 1;
       if (!interior) dst[i] = s;
       else if (cellOn) dst[i] = MODE == MODE_RESIDUAL ? rhs[i] - s : s;
@@ -897,9 +907,11 @@ template <class T, int MODE>
 __global__ void __launch_bounds__(kBlock) p2AddKernel(const int64_t* __restrict__ owner, const int* __restrict__ ptr,
                                                       const int64_t* __restrict__ copies,
                                                       const unsigned char* __restrict__ type, int n, T* dst,
-                                                      const T* __restrict__ rhs, unsigned mask) {
+                                                      const T* __restrict__ rhs, unsigned mask,
+                                                      const unsigned char* __restrict__ colour, int sel) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !(type[i] & mask)) return;
+  if (sel >= 0 && (colour[owner[i]] & 0x7f) != sel) return;
   T v = T(0);
   for (int k = ptr[i]; k < ptr[i + 1]; ++k) v += dst[copies[k]];
   const int64_t o = owner[i];
@@ -1074,6 +1086,21 @@ __global__ void __launch_bounds__(kBlock) castKernel(const Chunk* __restrict__ c
     const int64_t j = ch.start + i;
     if (add) dst[j] += TD(src[j]);
     else dst[j] = TD(src[j]);
+  }
+}
+
+// One colour pass of the P2 multicolour SOR on the owned DoFs of the flagged primitives:
+// x += omega (b - Ax) / diag, with Ax (in ax) computed for this colour from the pass's start values.
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2SorUpdateKernel(const Chunk* __restrict__ chunks, unsigned mask,
+                                                            const unsigned char* __restrict__ colour, int sel, T* x,
+                                                            const T* __restrict__ b, const T* __restrict__ ax,
+                                                            const T* __restrict__ diag, T omega) {
+  const Chunk ch = chunks[blockIdx.x];
+  if (!(ch.type & mask)) return;
+  for (int i = threadIdx.x; i < ch.len; i += blockDim.x) {
+    const int64_t j = ch.start + i;
+    if (colour[j] == (0x80 | sel)) x[j] += omega * (b[j] - ax[j]) / diag[j];
   }
 }
 

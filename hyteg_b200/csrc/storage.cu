@@ -549,98 +549,174 @@ static dev::P2Tables p2Tables() {
   return tb;
 }
 
-void Storage::p2Apply(int opId, int src, int dst, int rhs, int L, unsigned mask, int mode) {
-  auto it = p2ops.find(opId);
+P2Additive& Storage::p2Additive(int Lf) {
+  if ((int)p2add.size() <= Lf) p2add.resize(maxLevel() + 1);
+  P2Additive& ad = p2add[Lf];
+  if (ad.built) return ad;
+  const LevelData& ld = levels[Lf];
+  // owner <- its copies in the closure slots of its cells (the cell-closure halo group)
+  std::map<int64_t, std::vector<int64_t>> byOwner;
+  const auto& cd = ld.lay->commDst[G_CELL];
+  const auto& cs = ld.lay->commSrc[G_CELL];
+  for (size_t i = 0; i < cd.size(); ++i) byOwner[cs[i]].push_back(cd[i]);
+  std::vector<int64_t> own, cp;
+  std::vector<int> ptr{0};
+  std::vector<unsigned char> ty;
+  auto typeOf = [&](int64_t slot) {  // DoF type of the primitive whose array holds the slot
+    for (int k : {KF, KE, KV})
+      for (size_t pr = 0; pr < ld.lay->off[k].size(); ++pr)
+        if (slot >= ld.lay->off[k][pr] && slot < ld.lay->off[k][pr] + ld.lay->size[k][pr])
+          return k == KF ? ld.hostFaceType[pr] : k == KE ? ld.hostLowType[pr] : ld.hostLowType[ld.lv.nEdges + pr];
+    throw Error(HG_ERR_INTERNAL, "owner slot outside the face, edge and vertex arrays");
+  };
+  for (auto& kv : byOwner) {
+    own.push_back(kv.first);
+    for (int64_t c : kv.second) cp.push_back(c);
+    ptr.push_back((int)cp.size());
+    ty.push_back(typeOf(kv.first));
+  }
+  ad.n = (int)own.size();
+  ad.owner.alloc(std::max<size_t>(1, own.size()) * sizeof(int64_t));
+  ad.ptr.alloc(ptr.size() * sizeof(int));
+  ad.copies.alloc(std::max<size_t>(1, cp.size()) * sizeof(int64_t));
+  ad.type.alloc(std::max<size_t>(1, ty.size()));
+  if (!own.empty()) {
+    cudaCheck(cudaMemcpyAsync(ad.owner.p, own.data(), own.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream), "p2 add");
+    cudaCheck(cudaMemcpyAsync(ad.copies.p, cp.data(), cp.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream), "p2 add");
+    cudaCheck(cudaMemcpyAsync(ad.type.p, ty.data(), ty.size(), cudaMemcpyHostToDevice, stream), "p2 add");
+  }
+  cudaCheck(cudaMemcpyAsync(ad.ptr.p, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice, stream), "p2 add");
+  // colour of every slot (the colour of the DoF it holds; bit 7 set on the owner slot): from the
+  // DoF's barycentric weights in ascending vertex-ID order (b0, b1, b2, b3), parity class
+  // p = (b1 & 1) | (b2 & 1) << 1 | (b3 & 1) << 2; p = 0 (micro-vertices of the coarse level) is
+  // split into ((b1 >> 1) + 2 (b2 >> 1) + 3 (b3 >> 1)) mod 4, the others are colours 3 + p
+  std::vector<unsigned char> col((size_t)ld.lay->total, 0x7f);
+  for (int k = 0; k < 4; ++k)
+    for (size_t pr = 0; pr < ld.lay->off[k].size(); ++pr)
+      for (int64_t loc = 0; loc < ld.lay->size[k][pr]; ++loc) {
+        const Bary b = disc.slotBary(Lf, k, (int)pr, loc);
+        int64_t w[4] = {0, 0, 0, 0};
+        for (int i = 0; i < b.n; ++i) w[i] = b.b[i];
+        const int par = int(w[1] & 1) | (int(w[2] & 1) << 1) | (int(w[3] & 1) << 2);
+        int c = par ? 3 + par : int(((w[1] >> 1) + 2 * (w[2] >> 1) + 3 * (w[3] >> 1)) % 4);
+        const Slot o = disc.owner(Lf, b);
+        if (o.kind == k && o.prim == (int)pr && o.local == loc) c |= 0x80;
+        col[(size_t)(ld.lay->off[k][pr] + loc)] = (unsigned char)c;
+      }
+  ad.colour.alloc(col.size());
+  cudaCheck(cudaMemcpyAsync(ad.colour.p, col.data(), col.size(), cudaMemcpyHostToDevice, stream), "p2 colour");
+  cudaCheck(cudaStreamSynchronize(stream), "p2 add");
+  ad.built = true;
+  return ad;
+}
+
+static const dev::P2Tables& p2TablesOnce() {
+  static const dev::P2Tables tb = p2Tables();
+  return tb;
+}
+
+// Cell gather + additive owner sums for one P2 level: dst = A src, rhs - A src or diag(A), on the
+// flagged DoFs of colour `sel` (all when sel < 0). The copies of dst are not refreshed here.
+template <class T, int MODE>
+void Storage::p2Launch(P2Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask, int sel) {
+  const int Lf = L + 1;
+  const LevelData& ld = levels[Lf];
+  P2Additive& ad = p2Additive(Lf);
+  const T* K = (const T*)(sizeof(T) == 8 ? o.kd[L - o.minL]->p : o.kf[L - o.minL]->p);
+  const int nb = ld.lv.nCells * (ld.lv.N + 1);
+  const unsigned char* col = (const unsigned char*)ad.colour.p;
+  dev::p2CellKernel<T, MODE><<<nb, dev::kBlock, 0, stream>>>(ld.lv, p2TablesOnce(), K, dst, src, rhs, mask, col, sel);
+  ++launches;
+  if (ad.n) {
+    constexpr int AM = MODE == dev::MODE_RESIDUAL ? dev::MODE_RESIDUAL : dev::MODE_REPLACE;
+    dev::p2AddKernel<T, AM><<<(ad.n + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, stream>>>(
+        (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
+        ad.n, dst, rhs, mask, col, sel);
+    ++launches;
+  }
+  cudaCheck(cudaGetLastError(), "P2 kernels");
+}
+
+P2Operator& Storage::p2op(int id) {
+  auto it = p2ops.find(id);
   argCheck(it != p2ops.end(), "unknown P2 operator handle");
-  P2Operator& o = *it->second;
+  return *it->second;
+}
+
+void Storage::p2Apply(int opId, int src, int dst, int rhs, int L, unsigned mask, int mode) {
+  P2Operator& o = p2op(opId);
   argCheck(L >= o.minL && L <= o.maxL, "level outside the P2 operator's level range");
   argCheck(src != dst && (mode == 0 || (rhs != dst && rhs != src)), "P2 apply: distinct functions required");
   const int Lf = L + 1;
   Function& fs = fn(src);
   argCheck(fs.prec == fn(dst).prec && (mode == 0 || fn(rhs).prec == fs.prec), "P2 apply: precision mismatch");
-  const LevelData& ld = levels[Lf];
-  // additive table of this lattice level (built once): owner <- closure copies in its cells
-  if ((int)p2add.size() <= Lf) p2add.resize(maxLevel() + 1);
-  P2Additive& ad = p2add[Lf];
-  if (!ad.built) {
-    std::map<int64_t, std::vector<int64_t>> byOwner;
-    const auto& cd = ld.lay->commDst[G_CELL];
-    const auto& cs = ld.lay->commSrc[G_CELL];
-    for (size_t i = 0; i < cd.size(); ++i) byOwner[cs[i]].push_back(cd[i]);
-    std::vector<int64_t> own, cp;
-    std::vector<int> ptr{0};
-    std::vector<unsigned char> ty;
-    auto typeOf = [&](int64_t slot) {  // DoF type of the primitive whose array holds the slot
-      for (int k : {KF, KE, KV})
-        for (size_t pr = 0; pr < ld.lay->off[k].size(); ++pr)
-          if (slot >= ld.lay->off[k][pr] && slot < ld.lay->off[k][pr] + ld.lay->size[k][pr])
-            return k == KF ? ld.hostFaceType[pr] : k == KE ? ld.hostLowType[pr] : ld.hostLowType[ld.lv.nEdges + pr];
-      throw Error(HG_ERR_INTERNAL, "owner slot outside the face, edge and vertex arrays");
-    };
-    for (auto& kv : byOwner) {
-      own.push_back(kv.first);
-      for (int64_t c : kv.second) cp.push_back(c);
-      ptr.push_back((int)cp.size());
-      ty.push_back(typeOf(kv.first));
-    }
-    ad.n = (int)own.size();
-    ad.owner.alloc(std::max<size_t>(1, own.size()) * sizeof(int64_t));
-    ad.ptr.alloc(ptr.size() * sizeof(int));
-    ad.copies.alloc(std::max<size_t>(1, cp.size()) * sizeof(int64_t));
-    ad.type.alloc(std::max<size_t>(1, ty.size()));
-    if (!own.empty()) {
-      cudaCheck(cudaMemcpyAsync(ad.owner.p, own.data(), own.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream), "p2 add");
-      cudaCheck(cudaMemcpyAsync(ad.copies.p, cp.data(), cp.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream), "p2 add");
-      cudaCheck(cudaMemcpyAsync(ad.type.p, ty.data(), ty.size(), cudaMemcpyHostToDevice, stream), "p2 add");
-    }
-    cudaCheck(cudaMemcpyAsync(ad.ptr.p, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice, stream), "p2 add");
-    cudaCheck(cudaStreamSynchronize(stream), "p2 add");
-    ad.built = true;
-  }
   communicate(src, Lf, 1 << G_CELL);  // the closure copies of every cell hold the owners' values
-  static const dev::P2Tables tb = p2Tables();
-  const int nb = ld.lv.nCells * (ld.lv.N + 1);
-  const int na = (ad.n + dev::kBlock - 1) / dev::kBlock;
   if (fs.prec == 8) {
-    const double* K = (const double*)o.kd[L - o.minL]->p;
-    double* d = (double*)data(dst, Lf);
-    const double* sr = (const double*)data(src, Lf);
     const double* r = mode ? (const double*)data(rhs, Lf) : nullptr;
-    if (mode == 0) {
-      dev::p2CellKernel<double, dev::MODE_REPLACE><<<nb, dev::kBlock, 0, stream>>>(ld.lv, tb, K, d, sr, r, mask);
-      if (ad.n)
-        dev::p2AddKernel<double, dev::MODE_REPLACE><<<na, dev::kBlock, 0, stream>>>(
-            (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
-            ad.n, d, r, mask);
-    } else {
-      dev::p2CellKernel<double, dev::MODE_RESIDUAL><<<nb, dev::kBlock, 0, stream>>>(ld.lv, tb, K, d, sr, r, mask);
-      if (ad.n)
-        dev::p2AddKernel<double, dev::MODE_RESIDUAL><<<na, dev::kBlock, 0, stream>>>(
-            (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
-            ad.n, d, r, mask);
-    }
+    if (mode == 0)
+      p2Launch<double, dev::MODE_REPLACE>(o, L, (double*)data(dst, Lf), (const double*)data(src, Lf), r, mask, -1);
+    else
+      p2Launch<double, dev::MODE_RESIDUAL>(o, L, (double*)data(dst, Lf), (const double*)data(src, Lf), r, mask, -1);
   } else {
-    const float* K = (const float*)o.kf[L - o.minL]->p;
-    float* d = (float*)data(dst, Lf);
-    const float* sr = (const float*)data(src, Lf);
     const float* r = mode ? (const float*)data(rhs, Lf) : nullptr;
-    if (mode == 0) {
-      dev::p2CellKernel<float, dev::MODE_REPLACE><<<nb, dev::kBlock, 0, stream>>>(ld.lv, tb, K, d, sr, r, mask);
-      if (ad.n)
-        dev::p2AddKernel<float, dev::MODE_REPLACE><<<na, dev::kBlock, 0, stream>>>(
-            (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
-            ad.n, d, r, mask);
-    } else {
-      dev::p2CellKernel<float, dev::MODE_RESIDUAL><<<nb, dev::kBlock, 0, stream>>>(ld.lv, tb, K, d, sr, r, mask);
-      if (ad.n)
-        dev::p2AddKernel<float, dev::MODE_RESIDUAL><<<na, dev::kBlock, 0, stream>>>(
-            (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
-            ad.n, d, r, mask);
-    }
+    if (mode == 0)
+      p2Launch<float, dev::MODE_REPLACE>(o, L, (float*)data(dst, Lf), (const float*)data(src, Lf), r, mask, -1);
+    else
+      p2Launch<float, dev::MODE_RESIDUAL>(o, L, (float*)data(dst, Lf), (const float*)data(src, Lf), r, mask, -1);
   }
-  launches += ad.n ? 2 : 1;
-  cudaCheck(cudaGetLastError(), "P2 apply");
   communicate(dst, Lf, kAllGroups);
+}
+
+// Diagonal of a P2 operator level as a function of that level (built once per precision).
+int Storage::p2Diagonal(int opId, int L, int prec) {
+  P2Operator& o = p2op(opId);
+  auto key = std::make_pair(L, prec);
+  auto it = o.diag.find(key);
+  if (it != o.diag.end()) return it->second;
+  const int Lf = L + 1;
+  const int d = createFunction(Lf, Lf, prec);
+  if (prec == 8)
+    p2Launch<double, dev::MODE_DIAG>(o, L, (double*)data(d, Lf), nullptr, nullptr, HG_ALL, -1);
+  else
+    p2Launch<float, dev::MODE_DIAG>(o, L, (float*)data(d, Lf), nullptr, nullptr, HG_ALL, -1);
+  communicate(d, Lf, kAllGroups);
+  o.diag[key] = d;
+  return d;
+}
+
+template <class T>
+void Storage::p2SorT(P2Operator& o, int opId, int x, int b, int L, unsigned mask, T omega, bool backwards) {
+  const int Lf = L + 1;
+  const int prec = (int)sizeof(T);
+  const int dg = p2Diagonal(opId, L, prec);
+  auto key = std::make_pair(Lf, prec);
+  if (!p2scratch.count(key)) p2scratch[key] = createFunction(Lf, Lf, prec);
+  const int ax = p2scratch[key];
+  const LevelData& ld = levels[Lf];
+  P2Additive& ad = p2Additive(Lf);
+  for (int k = 0; k < 11; ++k) {
+    const int c = backwards ? 10 - k : k;
+    communicate(x, Lf, 1 << G_CELL);
+    p2Launch<T, dev::MODE_REPLACE>(o, L, (T*)data(ax, Lf), (const T*)data(x, Lf), nullptr, mask, c);
+    dev::p2SorUpdateKernel<T><<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (const unsigned char*)ad.colour.p, c,
+                                                                     (T*)data(x, Lf), (const T*)data(b, Lf),
+                                                                     (const T*)data(ax, Lf), (const T*)data(dg, Lf), omega);
+    ++launches;
+  }
+  cudaCheck(cudaGetLastError(), "P2 SOR");
+  communicate(x, Lf, kAllGroups);
+}
+
+void Storage::p2Sor(int opId, int x, int b, double omega, int L, unsigned mask, bool backwards) {
+  P2Operator& o = p2op(opId);
+  argCheck(L >= o.minL && L <= o.maxL, "level outside the P2 operator's level range");
+  argCheck(x != b, "P2 SOR: x and b must differ");
+  Function& fx = fn(x);
+  argCheck(fx.prec == fn(b).prec, "P2 SOR: precision mismatch");
+  if (fx.prec == 8)
+    p2SorT<double>(o, opId, x, b, L, mask, omega, backwards);
+  else
+    p2SorT<float>(o, opId, x, b, L, mask, (float)omega, backwards);
 }
 
 void Storage::reassembleOperator(int id) {

@@ -64,6 +64,7 @@ struct Operator {
 struct P2Operator {
   int form = 0, minL = 0, maxL = 0;
   std::vector<std::unique_ptr<DevBuf>> kd, kf;  // per level: [cell][type][10][10] in FP64 / FP32
+  std::map<std::pair<int, int>, int> diag;      // (level, precision) -> diagonal function
 };
 
 // Cell-closure copies of every DoF owned by a face, edge or vertex of one lattice level.
@@ -71,6 +72,7 @@ struct P2Additive {
   bool built = false;
   int n = 0;
   DevBuf owner, ptr, copies, type;
+  DevBuf colour;  // per slot: SOR colour of the DoF (0..10), bit 7 on its owner slot
 };
 
 struct Gmg;
@@ -122,6 +124,17 @@ struct Storage {
   int createP2Operator(int form, int minL, int maxL);
   // dst = A2 src (mode 0) or dst = rhs - A2 src (mode 2) at the flagged DoFs of P2 level L.
   void p2Apply(int op, int src, int dst, int rhs, int L, unsigned mask, int mode);
+  // Multicolour SOR on P2 level L (11 colours; each pass updates one colour from the values
+  // at the start of the pass).
+  void p2Sor(int op, int x, int b, double omega, int L, unsigned mask, bool backwards);
+  P2Operator& p2op(int id);
+  P2Additive& p2Additive(int Lf);
+  int p2Diagonal(int op, int L, int prec);
+  std::map<std::pair<int, int>, int> p2scratch;  // (lattice level, precision) -> scratch function
+  template <class T, int MODE>
+  void p2Launch(P2Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask, int sel);
+  template <class T>
+  void p2SorT(P2Operator& o, int opId, int x, int b, int L, unsigned mask, T omega, bool backwards);
   // Re-assemble an operator's stencils from the current cell coefficients into its device arrays.
   void reassembleOperator(int id);
   Operator& op(int id);

@@ -186,6 +186,12 @@ int hg_p2_operator_destroy(hg_storage* s, int op);
 int hg_p2_apply(hg_storage* s, int op, int src, int dst, int level, unsigned flag);
 /* r = b - A x at the flagged P2 DoFs of `level`. */
 int hg_p2_residual(hg_storage* s, int op, int x, int b, int r, int level, unsigned flag);
+/* One multicolour SOR sweep on P2 level `level` (P2ConstantOperator.cpp:1171-1235 smooth_sor).
+ * Colours: the DoF's barycentric weights in ascending vertex-ID order (b0..b3) give the parity
+ * class p = (b1&1) | (b2&1)<<1 | (b3&1)<<2; p = 0 is split into ((b1>>1) + 2(b2>>1) + 3(b3>>1))
+ * mod 4, the edge DoFs form colours 3 + p. A pass updates one colour, every DoF of it from the
+ * values at the start of the pass: x += omega (b - A x) / diag(A). backwards reverses the order. */
+int hg_p2_smooth_sor(hg_storage* s, int op, int x, int b, double omega, int level, unsigned flag, int backwards);
 
 /* ---------------------------------------------------------------------------------------
  * Solve server (continuous batching). No counterpart in the reference, which solves one

@@ -664,6 +664,40 @@ void orc_p2_apply(void* h, int L, const double* u, double* y) {
   }
 }
 
+// Multicolour SOR on P2 level L in the GPU's colour order: colour of a node from its
+// barycentric weights in ascending vertex order; a pass updates all non-Dirichlet nodes of one
+// colour from the values at the start of the pass.
+void orc_p2_sor(void* h, int L, double* u, const double* f, double omega, int sweeps, int backwards) {
+  Oracle& o = *(Oracle*)h;
+  if (!o.lv[L].haveP2) buildP2Matrix(o, L);
+  const Csr& A = o.lv[L].P2;
+  const LevelData& F = o.lv[L + 1];
+  const int64_t n = (int64_t)F.nodes.size();
+  std::vector<int> col(n);
+  std::vector<double> diag(n, 0.0);
+  for (int64_t i = 0; i < n; ++i) {
+    const Key& k = F.nodes[i].key;
+    const int64_t w1 = k[3], w2 = k[5], w3 = k[7];
+    const int par = int(w1 & 1) | (int(w2 & 1) << 1) | (int(w3 & 1) << 2);
+    col[i] = par ? 3 + par : int(((w1 >> 1) + 2 * (w2 >> 1) + 3 * (w3 >> 1)) % 4);
+    for (int64_t q = A.ptr[i]; q < A.ptr[i + 1]; ++q)
+      if (A.col[q] == i) diag[i] += A.val[q];
+  }
+  std::vector<double> r(n);
+  for (int s = 0; s < sweeps; ++s)
+    for (int kk = 0; kk < 11; ++kk) {
+      const int c = backwards ? 10 - kk : kk;
+      for (int64_t i = 0; i < n; ++i) {
+        if (col[i] != c || F.nodes[i].dirichlet) continue;
+        double t = f[i];
+        for (int64_t q = A.ptr[i]; q < A.ptr[i + 1]; ++q) t -= A.val[q] * u[A.col[q]];
+        r[i] = t;
+      }
+      for (int64_t i = 0; i < n; ++i)
+        if (col[i] == c && !F.nodes[i].dirichlet) u[i] += omega * r[i] / diag[i];
+    }
+}
+
 void orc_p2_element_laplace(const double* coords12, double* K100) {
   double p[4][3];
   for (int m = 0; m < 4; ++m)

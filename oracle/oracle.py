@@ -43,6 +43,7 @@ def _load_oracle():
         "orc_element_mass": (None, [P(c_double), P(c_double)]),
         "orc_p2_apply": (None, [c_void_p, c_int, P(c_double), P(c_double)]),
         "orc_p2_element_laplace": (None, [P(c_double), P(c_double)]),
+        "orc_p2_sor": (None, [c_void_p, c_int, P(c_double), P(c_double), c_double, c_int, c_int]),
         "orc_cell_local_stencil": (None, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, P(c_double)]),
     }
     for name, (res, args) in sig.items():
@@ -173,6 +174,13 @@ class Oracle:
         y = np.zeros(self.n(L + 1))
         lib().orc_p2_apply(self.h, L, dp(u), dp(y))
         return y
+
+    def p2_sor(self, L, u, f, omega, sweeps=1, backwards=False):
+        """Multicolour SOR on P2 level L (nodes of level L + 1), the GPU's colour order."""
+        u = np.ascontiguousarray(u, dtype=np.float64).copy()
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        lib().orc_p2_sor(self.h, L, dp(u), dp(f), omega, sweeps, 1 if backwards else 0)
+        return u
 
     def cell_local_stencil(self, L, cell, x, y, z, form=0):
         out = np.zeros(15)

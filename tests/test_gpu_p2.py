@@ -87,3 +87,41 @@ def test_p2_apply_inner_vertices_and_edges(cube3, L):
     # the 3x3x3 cube has inner macro-vertices and inner macro-edges: sums over up to 24 cells
     got, ref, inner, _ = run_apply(cube3, L, np.float64, False, 5 + L)
     assert rel(got, ref, inner) < 1e-13
+
+
+@pytest.mark.parametrize("L", [0, 1, 2, 3])
+@pytest.mark.parametrize("backwards", [False, True])
+def test_p2_multicolour_sor(cube2, L, backwards):
+    st, orc, maps = cube2
+    node, owned = maps[L]
+    n = orc.n(L + 1)
+    rng = np.random.default_rng(30 + L + 7 * backwards)
+    u0, f0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    A = hg.P2ConstantLaplaceOperator(st, 0, 3)
+    x, b = hg.P2Function("x", st, 0, 3), hg.P2Function("b", st, 0, 3)
+    x.from_numpy(L, H.scatter(node, u0))
+    b.from_numpy(L, H.scatter(node, f0))
+    for _ in range(2):
+        (A.smooth_sor_backwards if backwards else A.smooth_sor)(x, b, 0.8, L)
+    got = H.gather_owned(x.to_numpy(L), node, owned, n)
+    ref = orc.p2_sor(L, u0, f0, 0.8, sweeps=2, backwards=backwards)
+    inner = ~orc.dirichlet(L + 1)
+    assert rel(got, ref, inner) < 1e-13
+    assert np.array_equal(got[~inner], u0[~inner])
+
+
+def test_p2_sor_fp32(cube2):
+    st, orc, maps = cube2
+    L = 3
+    node, owned = maps[L]
+    n = orc.n(L + 1)
+    rng = np.random.default_rng(99)
+    u0, f0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    A = hg.P2ConstantLaplaceOperator(st, 0, 3)
+    x, b = hg.P2Function("x", st, 0, 3, dtype=np.float32), hg.P2Function("b", st, 0, 3, dtype=np.float32)
+    x.from_numpy(L, H.scatter(node, u0).astype(np.float32))
+    b.from_numpy(L, H.scatter(node, f0).astype(np.float32))
+    A.smooth_sor(x, b, 1.0, L)
+    got = H.gather_owned(x.to_numpy(L).astype(np.float64), node, owned, n)
+    ref = orc.p2_sor(L, u0.astype(np.float32).astype(np.float64), f0.astype(np.float32).astype(np.float64), 1.0)
+    assert rel(got, ref, ~orc.dirichlet(L + 1)) < 2e-5
