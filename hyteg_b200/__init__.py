@@ -562,6 +562,24 @@ class P2ConstantLaplaceOperator:
             pass
 
 
+class P2toP2QuadraticProlongation:
+    """P2toP2QuadraticProlongation: quadratic interpolation from P2 level `level` to level + 1."""
+
+    def prolongate(self, f, level, flag=All):
+        call("hg_p2_prolongate", f.storage.handle, f.id, level, flag, 0)
+
+    def prolongateAndAdd(self, f, level, flag=All):
+        call("hg_p2_prolongate", f.storage.handle, f.id, level, flag, 1)
+
+
+class P2toP2QuadraticRestriction:
+    """P2toP2QuadraticRestriction: transpose of the quadratic prolongation, from P2 level
+    `level` to level - 1."""
+
+    def restrict(self, f, level, flag=All):
+        call("hg_p2_restrict", f.storage.handle, f.id, level, flag)
+
+
 class SolveServer:
     """Continuous-batching server of P1 Poisson solves (hg_server_*): requests on the unit cube
     split into k^3 sub-cubes of 6 tetrahedra at a refinement level, constant coefficient, seeded

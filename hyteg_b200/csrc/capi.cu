@@ -713,6 +713,18 @@ int hg_p2_smooth_sor(hg_storage* h, int op, int x, int b, double omega, int leve
   HG_CATCH
 }
 
+int hg_p2_prolongate(hg_storage* h, int fn, int level, unsigned flag, int add) {
+  HG_TRY
+  S(h).p2Prolongate(fn, level, flag, add != 0);
+  HG_CATCH
+}
+
+int hg_p2_restrict(hg_storage* h, int fn, int level, unsigned flag) {
+  HG_TRY
+  S(h).p2Restrict(fn, level, flag);
+  HG_CATCH
+}
+
 struct hg_server {
   hg::Server* s;
 };

@@ -901,6 +901,113 @@ __global__ void __launch_bounds__(kBlock) p2CellKernel(LevelDev lv, P2Tables tb,
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// P2 quadratic transfers between P2 levels L and L + 1 (vertex lattices L + 1 and L + 2).
+// A fine node Q of a macro-cell lies at Q / 4 in level-L micro-cell units; with a0 = Q >> 2
+// and r = Q & 3, the candidates of class r are the micro-cells (type t, anchor a0 - delta)
+// containing it, each with the ten values of the coarse P2 basis at the point. The first
+// candidate inside the macro-cell is used (P2 is continuous, so any containing micro-cell gives
+// the same interpolant). Fine nodes at even coordinates are coarse nodes (injection).
+// ---------------------------------------------------------------------------------------
+constexpr int kP2TrCand = 24;
+struct P2TransferDev {
+  const unsigned char* nCand;  // [64]
+  const unsigned char* cand;   // [64][24]: delta (bits 3..5) << 3 | type
+};
+
+template <class T>
+__device__ __forceinline__ int p2PickCandidate(const P2TransferDev& tr, const P2Tables& tb, int r, int ax0, int ay0,
+                                               int az0, int N, int& ax, int& ay, int& az) {
+  for (int k = 0; k < tr.nCand[r]; ++k) {
+    const int c = tr.cand[r * kP2TrCand + k], t = c & 7, d = c >> 3;
+    ax = ax0 - (d & 1);
+    ay = ay0 - ((d >> 1) & 1);
+    az = az0 - ((d >> 2) & 1);
+    if (ax >= 0 && ay >= 0 && az >= 0 && ax + ay + az < N - tb.widthRed[t]) return k;
+  }
+  return -1;
+}
+
+// fine = P coarse on every node of the closed macro-cells (closure slots included)
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2ProlongKernel(LevelDev lvc, LevelDev lvf, P2Tables tb, P2TransferDev tr,
+                                                          const T* __restrict__ wts, const T* __restrict__ coarse,
+                                                          T* __restrict__ fine) {
+  const int Mf = lvf.N, Mc = lvc.N, N = Mc / 2, nPl = Mf + 1, wf = lvf.w, wc = lvc.w;
+  const int c = blockIdx.x / nPl, Z = blockIdx.x % nPl;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const T* cc = coarse + lvc.cellOff[c];
+  T* ff = fine + lvf.cellOff[c];
+  auto cidx = [wc](int x, int y, int z) { return int(tetSize(wc) - tetSize(wc - z)) + rowStart(wc - z, y) + x; };
+  const int pb = int(tetSize(wf) - tetSize(wf - Z));
+  for (int Y = warp; Y <= Mf - Z; Y += kBlock / 32)
+    for (int X = lane; X <= Mf - Z - Y; X += 32) {
+      T v;
+      if (((X | Y | Z) & 1) == 0) {
+        v = cc[cidx(X >> 1, Y >> 1, Z >> 1)];
+      } else {
+        const int r = (X & 3) | ((Y & 3) << 2) | ((Z & 3) << 4);
+        int ax, ay, az;
+        const int k = p2PickCandidate<T>(tr, tb, r, X >> 2, Y >> 2, Z >> 2, N, ax, ay, az);
+        v = T(0);
+        if (k >= 0) {
+          const int t = tr.cand[r * kP2TrCand + k] & 7;
+          const T* w = wts + (r * kP2TrCand + k) * 10;
+#pragma unroll
+          for (int m = 0; m < 10; ++m)
+            v += w[m] * cc[cidx(2 * ax + tb.off[t][m][0], 2 * ay + tb.off[t][m][1], 2 * az + tb.off[t][m][2])];
+        }
+      }
+      ff[pb + rowStart(wf - Z, Y) + X] = v;
+    }
+}
+
+// coarse += P^T (fine / multiplicity) over every node of the closed macro-cells: each cell adds
+// its share (a DoF on a face, edge or vertex is split evenly among its cells) into its own
+// coarse closure slots; the owners are summed afterwards. coarse must be zero on entry.
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2RestrictKernel(LevelDev lvc, LevelDev lvf, P2Tables tb, P2TransferDev tr,
+                                                           const T* __restrict__ wts, const T* __restrict__ fine,
+                                                           const unsigned char* __restrict__ mult, T* coarse) {
+  const int Mf = lvf.N, Mc = lvc.N, N = Mc / 2, nPl = Mf + 1, wf = lvf.w, wc = lvc.w;
+  const int c = blockIdx.x / nPl, Z = blockIdx.x % nPl;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* cc = coarse + lvc.cellOff[c];
+  const int64_t fb = lvf.cellOff[c];
+  auto cidx = [wc](int x, int y, int z) { return int(tetSize(wc) - tetSize(wc - z)) + rowStart(wc - z, y) + x; };
+  const int pb = int(tetSize(wf) - tetSize(wf - Z));
+  for (int Y = warp; Y <= Mf - Z; Y += kBlock / 32)
+    for (int X = lane; X <= Mf - Z - Y; X += 32) {
+      const int64_t i = fb + pb + rowStart(wf - Z, Y) + X;
+      const T v = fine[i] / T(mult[i]);
+      if (((X | Y | Z) & 1) == 0) {
+        atomicAdd(cc + cidx(X >> 1, Y >> 1, Z >> 1), v);
+      } else {
+        const int r = (X & 3) | ((Y & 3) << 2) | ((Z & 3) << 4);
+        int ax, ay, az;
+        const int k = p2PickCandidate<T>(tr, tb, r, X >> 2, Y >> 2, Z >> 2, N, ax, ay, az);
+        if (k < 0) continue;
+        const int t = tr.cand[r * kP2TrCand + k] & 7;
+        const T* w = wts + (r * kP2TrCand + k) * 10;
+#pragma unroll
+        for (int m = 0; m < 10; ++m)
+          if (w[m] != T(0))
+            atomicAdd(cc + cidx(2 * ax + tb.off[t][m][0], 2 * ay + tb.off[t][m][1], 2 * az + tb.off[t][m][2]), w[m] * v);
+      }
+    }
+}
+
+// owner <- its first cell-closure copy (values that every cell computes alike)
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2PickKernel(const int64_t* __restrict__ owner, const int* __restrict__ ptr,
+                                                       const int64_t* __restrict__ copies,
+                                                       const unsigned char* __restrict__ type, int n, T* dst,
+                                                       unsigned mask) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !(type[i] & mask)) return;
+  dst[owner[i]] = dst[copies[ptr[i]]];
+}
+
 // Sums the cells' shares of every DoF owned by a face, edge or vertex (the copies of that DoF in
 // the closure slots of its cells) into the owner slot: dst = sum, or rhs - sum for a residual.
 template <class T, int MODE>

@@ -605,6 +605,11 @@ P2Additive& Storage::p2Additive(int Lf) {
       }
   ad.colour.alloc(col.size());
   cudaCheck(cudaMemcpyAsync(ad.colour.p, col.data(), col.size(), cudaMemcpyHostToDevice, stream), "p2 colour");
+  std::vector<unsigned char> mult((size_t)ld.lay->total, 1);
+  for (size_t i = 0; i + 1 < ptr.size(); ++i)
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k) mult[(size_t)cp[k]] = (unsigned char)(ptr[i + 1] - ptr[i]);
+  ad.mult.alloc(mult.size());
+  cudaCheck(cudaMemcpyAsync(ad.mult.p, mult.data(), mult.size(), cudaMemcpyHostToDevice, stream), "p2 mult");
   cudaCheck(cudaStreamSynchronize(stream), "p2 add");
   ad.built = true;
   return ad;
@@ -717,6 +722,139 @@ void Storage::p2Sor(int opId, int x, int b, double omega, int L, unsigned mask, 
     p2SorT<double>(o, opId, x, b, L, mask, omega, backwards);
   else
     p2SorT<float>(o, opId, x, b, L, mask, (float)omega, backwards);
+}
+
+// Fine node Q of a macro-cell at Q / 4 level-L units: class r = (Q_x & 3) | (Q_y & 3) << 2 |
+// (Q_z & 3) << 4. For every micro-cell (type t, anchor (Q >> 2) - delta) containing the point,
+// its barycentric coordinates in quarters (exact: the micro-cells are unimodular) give the coarse
+// P2 basis values lambda (2 lambda - 1) at the vertices and 4 lambda_i lambda_j at the edges.
+static void buildP2Transfer(P2Transfer& tr, cudaStream_t stream) {
+  std::vector<unsigned char> nc(64, 0), cand(64 * dev::kP2TrCand, 0);
+  std::vector<double> w(64 * dev::kP2TrCand * 10, 0.0);
+  for (int r = 0; r < 64; ++r) {
+    const int f4[3] = {r & 3, (r >> 2) & 3, (r >> 4) & 3};
+    for (int d = 0; d < 8; ++d)
+      for (int t = 0; t < 6; ++t) {
+        const int* v0 = kMicroCellTable[t][0];
+        int B[3][3];  // columns v_m - v0
+        for (int m = 1; m < 4; ++m)
+          for (int k = 0; k < 3; ++k) B[k][m - 1] = kMicroCellTable[t][m][k] - v0[k];
+        const int det = B[0][0] * (B[1][1] * B[2][2] - B[1][2] * B[2][1]) - B[0][1] * (B[1][0] * B[2][2] - B[1][2] * B[2][0]) +
+                        B[0][2] * (B[1][0] * B[2][1] - B[1][1] * B[2][0]);
+        const int inv[3][3] = {{(B[1][1] * B[2][2] - B[1][2] * B[2][1]) * det, (B[0][2] * B[2][1] - B[0][1] * B[2][2]) * det,
+                                (B[0][1] * B[1][2] - B[0][2] * B[1][1]) * det},
+                               {(B[1][2] * B[2][0] - B[1][0] * B[2][2]) * det, (B[0][0] * B[2][2] - B[0][2] * B[2][0]) * det,
+                                (B[0][2] * B[1][0] - B[0][0] * B[1][2]) * det},
+                               {(B[1][0] * B[2][1] - B[1][1] * B[2][0]) * det, (B[0][1] * B[2][0] - B[0][0] * B[2][1]) * det,
+                                (B[0][0] * B[1][1] - B[0][1] * B[1][0]) * det}};  // det = +-1, so inv = adj * det
+        int q[3];
+        for (int k = 0; k < 3; ++k) q[k] = f4[k] + 4 * ((d >> k) & 1) - 4 * v0[k];  // 4 (point - v0)
+        int l4[4];
+        l4[1] = inv[0][0] * q[0] + inv[0][1] * q[1] + inv[0][2] * q[2];
+        l4[2] = inv[1][0] * q[0] + inv[1][1] * q[1] + inv[1][2] * q[2];
+        l4[3] = inv[2][0] * q[0] + inv[2][1] * q[1] + inv[2][2] * q[2];
+        l4[0] = 4 - l4[1] - l4[2] - l4[3];
+        if (l4[0] < 0 || l4[1] < 0 || l4[2] < 0 || l4[3] < 0) continue;
+        argCheck(det == 1 || det == -1, "micro-cell is not unimodular");
+        if (nc[r] >= dev::kP2TrCand) continue;
+        const int k = nc[r]++;
+        cand[r * dev::kP2TrCand + k] = (unsigned char)((d << 3) | t);
+        double* wr = &w[(size_t)(r * dev::kP2TrCand + k) * 10];
+        for (int m = 0; m < 4; ++m) {
+          const double l = l4[m] / 4.0;
+          wr[m] = l * (2.0 * l - 1.0);
+        }
+        for (int e = 0; e < 6; ++e) wr[4 + e] = 4.0 * (l4[kP2Edge[e][0]] / 4.0) * (l4[kP2Edge[e][1]] / 4.0);
+      }
+  }
+  std::vector<float> wfl(w.begin(), w.end());
+  tr.nCand.alloc(nc.size());
+  tr.cand.alloc(cand.size());
+  tr.wd.alloc(w.size() * sizeof(double));
+  tr.wf.alloc(wfl.size() * sizeof(float));
+  cudaCheck(cudaMemcpyAsync(tr.nCand.p, nc.data(), nc.size(), cudaMemcpyHostToDevice, stream), "p2 transfer");
+  cudaCheck(cudaMemcpyAsync(tr.cand.p, cand.data(), cand.size(), cudaMemcpyHostToDevice, stream), "p2 transfer");
+  cudaCheck(cudaMemcpyAsync(tr.wd.p, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, stream), "p2 transfer");
+  cudaCheck(cudaMemcpyAsync(tr.wf.p, wfl.data(), wfl.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "p2 transfer");
+  cudaCheck(cudaStreamSynchronize(stream), "p2 transfer");
+  tr.built = true;
+}
+
+int Storage::p2Scratch(int Lf, int prec) {
+  auto key = std::make_pair(Lf, prec);
+  if (!p2scratch.count(key)) p2scratch[key] = createFunction(Lf, Lf, prec);
+  return p2scratch[key];
+}
+
+void Storage::p2Prolongate(int id, int Lc, unsigned mask, bool add) {
+  Function& f = fn(id);
+  const int Lcf = Lc + 1, Lff = Lc + 2;  // lattice levels
+  argCheck(Lcf >= f.minL && Lff <= f.maxL, "P2 prolongation: levels outside the function's range");
+  if (!p2tr.built) buildP2Transfer(p2tr, stream);
+  const LevelData& lc = levels[Lcf];
+  const LevelData& lf = levels[Lff];
+  P2Additive& ad = p2Additive(Lff);
+  communicate(id, Lcf, 1 << G_CELL);
+  const int out = add ? p2Scratch(Lff, f.prec) : id;
+  const dev::P2TransferDev tr{(const unsigned char*)p2tr.nCand.p, (const unsigned char*)p2tr.cand.p};
+  const int nb = lf.lv.nCells * (lf.lv.N + 1), na = (ad.n + dev::kBlock - 1) / dev::kBlock;
+  if (f.prec == 8) {
+    dev::p2ProlongKernel<double><<<nb, dev::kBlock, 0, stream>>>(lc.lv, lf.lv, p2TablesOnce(), tr, (const double*)p2tr.wd.p,
+                                                               (const double*)data(id, Lcf), (double*)data(out, Lff));
+    if (ad.n)
+      dev::p2PickKernel<double><<<na, dev::kBlock, 0, stream>>>((const int64_t*)ad.owner.p, (const int*)ad.ptr.p,
+                                                              (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
+                                                              ad.n, (double*)data(out, Lff), add ? HG_ALL : mask);
+  } else {
+    dev::p2ProlongKernel<float><<<nb, dev::kBlock, 0, stream>>>(lc.lv, lf.lv, p2TablesOnce(), tr, (const float*)p2tr.wf.p,
+                                                              (const float*)data(id, Lcf), (float*)data(out, Lff));
+    if (ad.n)
+      dev::p2PickKernel<float><<<na, dev::kBlock, 0, stream>>>((const int64_t*)ad.owner.p, (const int*)ad.ptr.p,
+                                                             (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
+                                                             ad.n, (float*)data(out, Lff), add ? HG_ALL : mask);
+  }
+  launches += ad.n ? 2 : 1;
+  cudaCheck(cudaGetLastError(), "P2 prolongation");
+  if (add) {
+    const double one = 1.0;
+    lincomb(id, Lff, mask, 1, &one, &out, true, 0.0);
+  }
+  communicate(id, Lff, kAllGroups);
+}
+
+void Storage::p2Restrict(int id, int Lf, unsigned mask) {
+  Function& f = fn(id);
+  const int Lff = Lf + 1, Lcf = Lf;  // lattice levels: fine P2 level Lf, coarse Lf - 1
+  argCheck(Lf >= 1 && Lcf >= f.minL && Lff <= f.maxL, "P2 restriction: levels outside the function's range");
+  if (!p2tr.built) buildP2Transfer(p2tr, stream);
+  const LevelData& lc = levels[Lcf];
+  const LevelData& lf = levels[Lff];
+  P2Additive& adf = p2Additive(Lff);
+  P2Additive& adc = p2Additive(Lcf);
+  communicate(id, Lff, 1 << G_CELL);
+  cudaCheck(cudaMemsetAsync(data(id, Lcf), 0, (size_t)lc.lay->total * f.prec, stream), "P2 restriction");
+  const dev::P2TransferDev tr{(const unsigned char*)p2tr.nCand.p, (const unsigned char*)p2tr.cand.p};
+  const int nb = lf.lv.nCells * (lf.lv.N + 1), na = (adc.n + dev::kBlock - 1) / dev::kBlock;
+  if (f.prec == 8) {
+    dev::p2RestrictKernel<double><<<nb, dev::kBlock, 0, stream>>>(lc.lv, lf.lv, p2TablesOnce(), tr,
+                                                                (const double*)p2tr.wd.p, (const double*)data(id, Lff),
+                                                                (const unsigned char*)adf.mult.p, (double*)data(id, Lcf));
+    if (adc.n)
+      dev::p2AddKernel<double, dev::MODE_REPLACE><<<na, dev::kBlock, 0, stream>>>(
+          (const int64_t*)adc.owner.p, (const int*)adc.ptr.p, (const int64_t*)adc.copies.p,
+          (const unsigned char*)adc.type.p, adc.n, (double*)data(id, Lcf), nullptr, mask, nullptr, -1);
+  } else {
+    dev::p2RestrictKernel<float><<<nb, dev::kBlock, 0, stream>>>(lc.lv, lf.lv, p2TablesOnce(), tr,
+                                                               (const float*)p2tr.wf.p, (const float*)data(id, Lff),
+                                                               (const unsigned char*)adf.mult.p, (float*)data(id, Lcf));
+    if (adc.n)
+      dev::p2AddKernel<float, dev::MODE_REPLACE><<<na, dev::kBlock, 0, stream>>>(
+          (const int64_t*)adc.owner.p, (const int*)adc.ptr.p, (const int64_t*)adc.copies.p,
+          (const unsigned char*)adc.type.p, adc.n, (float*)data(id, Lcf), nullptr, mask, nullptr, -1);
+  }
+  launches += adc.n ? 2 : 1;
+  cudaCheck(cudaGetLastError(), "P2 restriction");
+  communicate(id, Lcf, kAllGroups);
 }
 
 void Storage::reassembleOperator(int id) {

@@ -73,6 +73,13 @@ struct P2Additive {
   int n = 0;
   DevBuf owner, ptr, copies, type;
   DevBuf colour;  // per slot: SOR colour of the DoF (0..10), bit 7 on its owner slot
+  DevBuf mult;    // per slot: number of macro-cells holding the DoF (1 for cell-owned)
+};
+
+// Candidate micro-cells and coarse P2 basis values for the fine nodes of the 64 residue classes.
+struct P2Transfer {
+  bool built = false;
+  DevBuf nCand, cand, wd, wf;
 };
 
 struct Gmg;
@@ -131,6 +138,12 @@ struct Storage {
   P2Additive& p2Additive(int Lf);
   int p2Diagonal(int op, int L, int prec);
   std::map<std::pair<int, int>, int> p2scratch;  // (lattice level, precision) -> scratch function
+  P2Transfer p2tr;
+  // Quadratic prolongation from P2 level Lc to Lc + 1 of function id (fine = P coarse, or += with
+  // add) and its transpose, the restriction from P2 level Lf to Lf - 1.
+  void p2Prolongate(int id, int Lc, unsigned mask, bool add);
+  void p2Restrict(int id, int Lf, unsigned mask);
+  int p2Scratch(int Lf, int prec);
   template <class T, int MODE>
   void p2Launch(P2Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask, int sel);
   template <class T>

@@ -192,6 +192,11 @@ int hg_p2_residual(hg_storage* s, int op, int x, int b, int r, int level, unsign
  * mod 4, the edge DoFs form colours 3 + p. A pass updates one colour, every DoF of it from the
  * values at the start of the pass: x += omega (b - A x) / diag(A). backwards reverses the order. */
 int hg_p2_smooth_sor(hg_storage* s, int op, int x, int b, double omega, int level, unsigned flag, int backwards);
+/* Quadratic prolongation of fn from P2 level `level` to level + 1 (P2toP2QuadraticProlongation,
+ * gridtransferoperators/P2toP2QuadraticProlongation.hpp), add != 0: prolongateAndAdd; and its
+ * transpose, the restriction from P2 level `level` to level - 1 (P2toP2QuadraticRestriction). */
+int hg_p2_prolongate(hg_storage* s, int fn, int level, unsigned flag, int add);
+int hg_p2_restrict(hg_storage* s, int fn, int level, unsigned flag);
 
 /* ---------------------------------------------------------------------------------------
  * Solve server (continuous batching). No counterpart in the reference, which solves one

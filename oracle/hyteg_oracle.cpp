@@ -154,6 +154,8 @@ struct LevelData {
   int64_t N = 1;
   Csr P2;                    // P2 Laplace of this level on the nodes of the next finer level
   bool haveP2 = false;
+  Csr P2prol;                // P2 prolongation from this level to the next (rows: nodes of level + 2)
+  bool haveP2prol = false;
   std::vector<Node> nodes;
   std::unordered_map<Key, int64_t, KeyHash> index;
   Csr A[2];                  // 0: diffusion (per-cell coefficient), 1: mass
@@ -649,6 +651,89 @@ void orc_gmg(void* h, int L, int minL, double* x, const double* b, int cycles, i
     }
   }
   std::copy(xs[L].begin(), xs[L].end(), x);
+}
+
+// Quadratic prolongation from P2 level Lc to Lc + 1: every point of the lattice Lc + 2 inside a
+// level-Lc micro-cell has barycentric coordinates l / 4 (l_m >= 0 integers, sum 4) there; its
+// row holds the coarse P2 basis values (l(2l-1) at the vertices, 4 l_i l_j at the edges).
+void buildP2Prolongation(Oracle& o, int Lc) {
+  LevelData& d = o.lv[Lc];
+  const LevelData& cL = o.lv[Lc + 1];
+  const LevelData& fL = o.lv[Lc + 2];
+  const int64_t N = d.N;
+  std::vector<std::map<int64_t, double>> rows(fL.nodes.size());
+  std::vector<char> done(fL.nodes.size(), 0);
+  for (size_t ci = 0; ci < o.cells.size(); ++ci)
+    for (int t = 0; t < 6; ++t) {
+      const int64_t width = N - kMicroWidthReduction[t];
+      for (int64_t z = 0; z < width; ++z)
+        for (int64_t y = 0; y + z < width; ++y)
+          for (int64_t x = 0; x + y + z < width; ++x) {
+            int64_t v[4][3];
+            for (int m = 0; m < 4; ++m) {
+              v[m][0] = x + kMicro[t][m][0];
+              v[m][1] = y + kMicro[t][m][1];
+              v[m][2] = z + kMicro[t][m][2];
+            }
+            int64_t cid[10];
+            for (int m = 0; m < 4; ++m) cid[m] = cL.index.at(o.keyOf((int)ci, 2 * N, 2 * v[m][0], 2 * v[m][1], 2 * v[m][2]));
+            for (int e = 0; e < 6; ++e) {
+              const int a = kP2Edge[e][0], b = kP2Edge[e][1];
+              cid[4 + e] = cL.index.at(o.keyOf((int)ci, 2 * N, v[a][0] + v[b][0], v[a][1] + v[b][1], v[a][2] + v[b][2]));
+            }
+            for (int l1 = 0; l1 <= 4; ++l1)
+              for (int l2 = 0; l1 + l2 <= 4; ++l2)
+                for (int l3 = 0; l1 + l2 + l3 <= 4; ++l3) {
+                  const int l[4] = {4 - l1 - l2 - l3, l1, l2, l3};
+                  int64_t q[3] = {0, 0, 0};
+                  for (int m = 0; m < 4; ++m)
+                    for (int k = 0; k < 3; ++k) q[k] += l[m] * v[m][k];
+                  const int64_t fi = fL.index.at(o.keyOf((int)ci, 4 * N, q[0], q[1], q[2]));
+                  if (done[fi]) continue;
+                  done[fi] = 1;
+                  for (int m = 0; m < 4; ++m) {
+                    const double lm = l[m] / 4.0, wv = lm * (2.0 * lm - 1.0);
+                    if (wv != 0.0) rows[fi][cid[m]] += wv;
+                  }
+                  for (int e = 0; e < 6; ++e) {
+                    const double wv = 4.0 * (l[kP2Edge[e][0]] / 4.0) * (l[kP2Edge[e][1]] / 4.0);
+                    if (wv != 0.0) rows[fi][cid[4 + e]] += wv;
+                  }
+                }
+          }
+    }
+  Csr& P = d.P2prol;
+  P.ptr.assign(1, 0);
+  for (auto& r : rows) {
+    for (auto& kv : r) {
+      P.col.push_back(kv.first);
+      P.val.push_back(kv.second);
+    }
+    P.ptr.push_back((int64_t)P.col.size());
+  }
+  d.haveP2prol = true;
+}
+
+// fine (nodes of level Lc + 2) = P coarse (nodes of level Lc + 1), or += with add
+void orc_p2_prolongate(void* h, int Lc, const double* coarse, double* fine, int add) {
+  Oracle& o = *(Oracle*)h;
+  if (!o.lv[Lc].haveP2prol) buildP2Prolongation(o, Lc);
+  const Csr& P = o.lv[Lc].P2prol;
+  for (size_t i = 0; i + 1 < P.ptr.size(); ++i) {
+    double s = 0.0;
+    for (int64_t k = P.ptr[i]; k < P.ptr[i + 1]; ++k) s += P.val[k] * coarse[P.col[k]];
+    fine[i] = add ? fine[i] + s : s;
+  }
+}
+
+// coarse (nodes of level Lf) = P^T fine (nodes of level Lf + 1): restriction from P2 level Lf
+void orc_p2_restrict(void* h, int Lf, const double* fine, double* coarse) {
+  Oracle& o = *(Oracle*)h;
+  if (!o.lv[Lf - 1].haveP2prol) buildP2Prolongation(o, Lf - 1);
+  const Csr& P = o.lv[Lf - 1].P2prol;
+  for (size_t j = 0; j < o.lv[Lf].nodes.size(); ++j) coarse[j] = 0.0;
+  for (size_t i = 0; i + 1 < P.ptr.size(); ++i)
+    for (int64_t k = P.ptr[i]; k < P.ptr[i + 1]; ++k) coarse[P.col[k]] += P.val[k] * fine[i];
 }
 
 // y = A2 u for the P2 Laplace of level L; u and y are indexed by the nodes of level L + 1.

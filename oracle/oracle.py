@@ -44,6 +44,8 @@ def _load_oracle():
         "orc_p2_apply": (None, [c_void_p, c_int, P(c_double), P(c_double)]),
         "orc_p2_element_laplace": (None, [P(c_double), P(c_double)]),
         "orc_p2_sor": (None, [c_void_p, c_int, P(c_double), P(c_double), c_double, c_int, c_int]),
+        "orc_p2_prolongate": (None, [c_void_p, c_int, P(c_double), P(c_double), c_int]),
+        "orc_p2_restrict": (None, [c_void_p, c_int, P(c_double), P(c_double)]),
         "orc_cell_local_stencil": (None, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, P(c_double)]),
     }
     for name, (res, args) in sig.items():
@@ -181,6 +183,20 @@ class Oracle:
         f = np.ascontiguousarray(f, dtype=np.float64)
         lib().orc_p2_sor(self.h, L, dp(u), dp(f), omega, sweeps, 1 if backwards else 0)
         return u
+
+    def p2_prolongate(self, Lc, coarse, fine=None, add=False):
+        """P2 quadratic prolongation from P2 level Lc (nodes of level Lc + 1) to Lc + 1."""
+        coarse = np.ascontiguousarray(coarse, dtype=np.float64)
+        fine = np.zeros(self.n(Lc + 2)) if fine is None else np.ascontiguousarray(fine, dtype=np.float64).copy()
+        lib().orc_p2_prolongate(self.h, Lc, dp(coarse), dp(fine), 1 if add else 0)
+        return fine
+
+    def p2_restrict(self, Lf, fine):
+        """Transpose of the P2 prolongation: P2 level Lf (nodes of Lf + 1) to Lf - 1 (nodes of Lf)."""
+        fine = np.ascontiguousarray(fine, dtype=np.float64)
+        coarse = np.zeros(self.n(Lf))
+        lib().orc_p2_restrict(self.h, Lf, dp(fine), dp(coarse))
+        return coarse
 
     def cell_local_stencil(self, L, cell, x, y, z, form=0):
         out = np.zeros(15)

@@ -125,3 +125,37 @@ def test_p2_sor_fp32(cube2):
     got = H.gather_owned(x.to_numpy(L).astype(np.float64), node, owned, n)
     ref = orc.p2_sor(L, u0.astype(np.float32).astype(np.float64), f0.astype(np.float32).astype(np.float64), 1.0)
     assert rel(got, ref, ~orc.dirichlet(L + 1)) < 2e-5
+
+
+@pytest.mark.parametrize("Lc", [0, 1, 2])
+@pytest.mark.parametrize("add", [False, True])
+def test_p2_prolongation(cube2, Lc, add):
+    st, orc, maps = cube2
+    nc, nf = orc.n(Lc + 1), orc.n(Lc + 2)
+    rng = np.random.default_rng(40 + Lc + 3 * add)
+    c0, f0 = rng.uniform(-1, 1, nc), rng.uniform(-1, 1, nf)
+    f = hg.P2Function("f", st, 0, 3)
+    f.from_numpy(Lc, H.scatter(maps[Lc][0], c0))
+    f.from_numpy(Lc + 1, H.scatter(maps[Lc + 1][0], f0))
+    P = hg.P2toP2QuadraticProlongation()
+    (P.prolongateAndAdd if add else P.prolongate)(f, Lc, hg.Inner)
+    got = H.gather_owned(f.to_numpy(Lc + 1), maps[Lc + 1][0], maps[Lc + 1][1], nf)
+    ref = orc.p2_prolongate(Lc, c0, f0, add=add)
+    inner = ~orc.dirichlet(Lc + 2)
+    assert rel(got, ref, inner) < 1e-13
+    assert np.array_equal(got[~inner], f0[~inner])
+
+
+@pytest.mark.parametrize("Lf", [1, 2, 3])
+def test_p2_restriction(cube2, Lf):
+    st, orc, maps = cube2
+    nc, nf = orc.n(Lf), orc.n(Lf + 1)
+    rng = np.random.default_rng(60 + Lf)
+    fine = rng.uniform(-1, 1, nf)
+    f = hg.P2Function("f", st, 0, 3)
+    f.from_numpy(Lf, H.scatter(maps[Lf][0], fine))
+    hg.P2toP2QuadraticRestriction().restrict(f, Lf, hg.Inner)
+    got = H.gather_owned(f.to_numpy(Lf - 1), maps[Lf - 1][0], maps[Lf - 1][1], nc)
+    ref = orc.p2_restrict(Lf, fine)
+    inner = ~orc.dirichlet(Lf)
+    assert rel(got, ref, inner) < 1e-13
