@@ -580,6 +580,38 @@ class P2toP2QuadraticRestriction:
         call("hg_p2_restrict", f.storage.handle, f.id, level, flag)
 
 
+class P2GeometricMultigridSolver:
+    """GeometricMultigridSolver for P2ConstantLaplaceOperator: multicolour P2 SOR, quadratic
+    transfers, CG on the coarsest level (FP64)."""
+
+    def __init__(self, storage, A, minLevel, maxLevel, preSmoothSteps=3, postSmoothSteps=3, relax=1.0,
+                 coarseMaxIter=1000, coarseTolerance=1e-16):
+        self.storage = storage
+        h = ctypes.c_int()
+        call("hg_p2_gmg_create", storage.handle, A.id, minLevel, maxLevel, preSmoothSteps, postSmoothSteps,
+             float(relax), int(coarseMaxIter), float(coarseTolerance), ctypes.byref(h))
+        self.id = h.value
+
+    def solve(self, x, b, level):
+        call("hg_p2_gmg_solve", self.storage.handle, self.id, x.id, b.id, level)
+
+    def solve_to(self, x, b, level, tol, max_iter=100):
+        it = ctypes.c_int()
+        rel = ctypes.c_double()
+        hist = np.zeros(max_iter)
+        call("hg_p2_gmg_solve_to", self.storage.handle, self.id, x.id, b.id, level, float(tol), int(max_iter),
+             ctypes.byref(it), ctypes.byref(rel), dptr(hist), int(max_iter))
+        return it.value, rel.value, hist[: it.value].copy()
+
+    def __del__(self):
+        try:
+            st = getattr(self, "storage", None)
+            if st is not None and st.handle:
+                _capi.lib.hg_p2_gmg_destroy(st.handle, self.id)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+
+
 class SolveServer:
     """Continuous-batching server of P1 Poisson solves (hg_server_*): requests on the unit cube
     split into k^3 sub-cubes of 6 tetrahedra at a refinement level, constant coefficient, seeded

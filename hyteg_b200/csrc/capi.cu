@@ -725,6 +725,48 @@ int hg_p2_restrict(hg_storage* h, int fn, int level, unsigned flag) {
   HG_CATCH
 }
 
+int hg_p2_gmg_create(hg_storage* h, int op, int min_level, int max_level, int pre_smooth, int post_smooth,
+                     double omega, int coarse_max_iter, double coarse_tol, int* gmg) {
+  HG_TRY
+  hg::argCheck(gmg != nullptr && pre_smooth >= 0 && post_smooth >= 0 && coarse_max_iter >= 0, "invalid arguments");
+  hg::Storage& s = S(h);
+  const int id = s.nextId++;
+  s.p2gmgs[id].reset(
+      new hg::P2Gmg(s, op, min_level, max_level, pre_smooth, post_smooth, omega, coarse_max_iter, coarse_tol));
+  *gmg = id;
+  HG_CATCH
+}
+
+int hg_p2_gmg_destroy(hg_storage* h, int gmg) {
+  HG_TRY
+  S(h).p2gmgs.erase(gmg);
+  HG_CATCH
+}
+
+static hg::P2Gmg& P2G(hg_storage* h, int gmg) {
+  auto& m = S(h).p2gmgs;
+  auto it = m.find(gmg);
+  hg::argCheck(it != m.end(), "unknown P2 multigrid handle");
+  return *it->second;
+}
+
+int hg_p2_gmg_solve(hg_storage* h, int gmg, int x, int b, int level) {
+  HG_TRY
+  hg::P2Gmg& g = P2G(h, gmg);
+  hg::argCheck(level >= g.minL && level <= g.maxL, "level outside the solver's range");
+  g.solveRecursively(x, b, level);
+  HG_CATCH
+}
+
+int hg_p2_gmg_solve_to(hg_storage* h, int gmg, int x, int b, int level, double tol, int max_iter, int* iterations,
+                       double* rel_residual, double* history, int history_cap) {
+  HG_TRY
+  hg::argCheck(tol > 0.0 && max_iter >= 0, "tolerance must be positive");
+  const int n = P2G(h, gmg).solveTo(x, b, level, tol, max_iter, rel_residual, history, history_cap);
+  if (iterations) *iterations = n;
+  HG_CATCH
+}
+
 struct hg_server {
   hg::Server* s;
 };

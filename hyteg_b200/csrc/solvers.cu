@@ -247,4 +247,86 @@ void Gmg::solve(int x, int b, int L) {
   runCycle(x, b, L);
 }
 
+P2Gmg::P2Gmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int post_, double omega_, int cmax, double ctol)
+    : s(st), op(op_), minL(minL_), maxL(maxL_), pre(pre_), post(post_), omega(omega_), coarseMaxIter(cmax),
+      coarseTol(ctol) {
+  P2Operator& o = s.p2op(op);
+  argCheck(minL >= o.minL && maxL <= o.maxL && minL <= maxL, "P2 multigrid: levels outside the operator's range");
+  tmp = s.createFunction(minL + 1, maxL + 1, 8);
+  cp = s.createFunction(minL + 1, minL + 1, 8);
+  cz = s.createFunction(minL + 1, minL + 1, 8);
+  cap = s.createFunction(minL + 1, minL + 1, 8);
+  cr = s.createFunction(minL + 1, minL + 1, 8);
+}
+
+P2Gmg::~P2Gmg() {
+  for (int id : {tmp, cp, cz, cap, cr}) s.fns.erase(id);
+}
+
+// CGSolver (CGSolver.hpp:69-150, identity preconditioner) with the P2 operator of level L.
+int P2Gmg::coarseCg(int x, int b, int L) {
+  const unsigned flag = HG_INNER | HG_NEUMANN | HG_FREESLIP;
+  const int Lf = L + 1;
+  const double one = 1.0;
+  s.p2Apply(op, x, cr, b, L, flag, 2);  // r = b - A x
+  s.lincomb(cp, Lf, flag, 1, &one, &cr, false, 0.0);
+  double rs = s.dot(cr, cr, Lf, flag);
+  if (std::sqrt(rs) < coarseTol) return 0;
+  int it = 0;
+  for (int i = 0; i < coarseMaxIter; ++i) {
+    it = i + 1;
+    s.p2Apply(op, cp, cap, -1, L, flag, 0);
+    const double alpha = rs / s.dot(cp, cap, Lf, flag);
+    s.lincomb(x, Lf, flag, 1, &alpha, &cp, true, 0.0);
+    const double malpha = -alpha;
+    s.lincomb(cr, Lf, flag, 1, &malpha, &cap, true, 0.0);
+    const double rsn = s.dot(cr, cr, Lf, flag);
+    if (std::sqrt(rsn) < coarseTol) break;
+    const double sc[2] = {1.0, rsn / rs};
+    const int src[2] = {cr, cp};
+    s.lincomb(cp, Lf, flag, 2, sc, src, false, 0.0);
+    rs = rsn;
+  }
+  return it;
+}
+
+// GeometricMultigridSolver::solveRecursively (GeometricMultigridSolver.hpp:136-235) with the P2
+// pieces: SOR, r = b - A x, restriction, coarse-grid correction, prolongation and add.
+void P2Gmg::solveRecursively(int x, int b, int L) {
+  const unsigned flag = HG_INNER | HG_NEUMANN;
+  if (L == minL) {
+    coarseCg(x, b, L);
+    return;
+  }
+  for (int i = 0; i < pre; ++i) s.p2Sor(op, x, b, omega, L, flag, false);
+  s.p2Apply(op, x, tmp, b, L, flag, 2);
+  s.p2Restrict(tmp, L, flag);
+  const double one = 1.0;
+  s.lincomb(b, L, flag, 1, &one, &tmp, false, 0.0);  // lattice level L = P2 level L - 1
+  s.lincomb(x, L, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+  solveRecursively(x, b, L - 1);
+  s.p2Prolongate(x, L - 1, flag, true);
+  for (int i = 0; i < post; ++i) s.p2Sor(op, x, b, omega, L, flag, false);
+}
+
+int P2Gmg::solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap) {
+  const unsigned flag = HG_INNER | HG_NEUMANN;
+  argCheck(L >= minL && L <= maxL, "P2 multigrid: level outside the solver's range");
+  argCheck(s.fn(x).prec == 8 && s.fn(b).prec == 8, "P2 multigrid: FP64 functions required");
+  const int Lf = L + 1;
+  s.p2Apply(op, x, tmp, b, L, flag, 2);
+  const double r0 = std::sqrt(s.dot(tmp, tmp, Lf, flag));
+  double rel = 1.0;
+  int it = 0;
+  while (it < maxIter && rel > tol && r0 > 0.0) {
+    solveRecursively(x, b, L);
+    ++it;
+    s.p2Apply(op, x, tmp, b, L, flag, 2);
+    rel = std::sqrt(s.dot(tmp, tmp, Lf, flag)) / r0;
+    if (history && it <= historyCap) history[it - 1] = rel;
+  }
+  if (relRes) *relRes = r0 > 0.0 ? rel : 0.0;
+  return it;
+}
+
 }  // namespace hg

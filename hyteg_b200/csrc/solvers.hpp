@@ -51,4 +51,22 @@ struct Gmg {
   int cx64 = -1, cb64 = -1, x32 = -1, b32 = -1, r64 = -1;
 };
 
+// P2 geometric multigrid on P2 levels [minL, maxL] (the P2 DoFs of level L are the vertex DoFs
+// of level L + 1): multicolour P2 SOR, quadratic transfers, CG on the coarsest level; FP64.
+struct P2Gmg {
+  P2Gmg(Storage& s, int op, int minL, int maxL, int pre, int post, double omega, int coarseMaxIter,
+        double coarseTol);
+  ~P2Gmg();
+  void solveRecursively(int x, int b, int L);
+  int solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap);
+  int coarseCg(int x, int b, int L);
+
+  Storage& s;
+  int op, minL, maxL, pre, post;
+  double omega;
+  int coarseMaxIter;
+  double coarseTol;
+  int tmp, cp, cz, cap, cr;
+};
+
 }  // namespace hg

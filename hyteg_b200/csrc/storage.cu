@@ -104,6 +104,7 @@ Storage::Storage(const Topology& topo, int maxLevel) : disc(topo, maxLevel) {
 }
 
 Storage::~Storage() {
+  p2gmgs.clear();
   gmgs.clear();
   ops.clear();
   fns.clear();

@@ -83,6 +83,7 @@ struct P2Transfer {
 };
 
 struct Gmg;
+struct P2Gmg;
 
 struct Storage {
   Storage(const Topology& topo, int maxLevel);
@@ -97,6 +98,7 @@ struct Storage {
   std::map<int, std::unique_ptr<Operator>> ops;
   std::map<int, std::unique_ptr<Gmg>> gmgs;
   std::map<int, std::unique_ptr<P2Operator>> p2ops;
+  std::map<int, std::unique_ptr<P2Gmg>> p2gmgs;
   std::deque<P2Additive> p2add;  // per lattice level
   int nextId = 1;
   int structureOp = -1;

@@ -197,6 +197,15 @@ int hg_p2_smooth_sor(hg_storage* s, int op, int x, int b, double omega, int leve
  * transpose, the restriction from P2 level `level` to level - 1 (P2toP2QuadraticRestriction). */
 int hg_p2_prolongate(hg_storage* s, int fn, int level, unsigned flag, int add);
 int hg_p2_restrict(hg_storage* s, int fn, int level, unsigned flag);
+/* P2 geometric multigrid (GeometricMultigridSolver with P2ConstantLaplaceOperator, the P2 SOR
+ * above, the quadratic transfers and CG on min_level), FP64. x, b: P2 functions covering
+ * [min_level, max_level]. solve: one cycle; solve_to: cycles to the relative residual tol. */
+int hg_p2_gmg_create(hg_storage* s, int op, int min_level, int max_level, int pre_smooth, int post_smooth,
+                     double omega, int coarse_max_iter, double coarse_tol, int* gmg);
+int hg_p2_gmg_destroy(hg_storage* s, int gmg);
+int hg_p2_gmg_solve(hg_storage* s, int gmg, int x, int b, int level);
+int hg_p2_gmg_solve_to(hg_storage* s, int gmg, int x, int b, int level, double tol, int max_iter, int* iterations,
+                       double* rel_residual, double* history, int history_cap);
 
 /* ---------------------------------------------------------------------------------------
  * Solve server (continuous batching). No counterpart in the reference, which solves one

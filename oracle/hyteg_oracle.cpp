@@ -783,6 +783,47 @@ void orc_p2_sor(void* h, int L, double* u, const double* f, double omega, int sw
     }
 }
 
+// CG on the non-Dirichlet rows of the P2 Laplace of level L (Dirichlet values of x kept).
+int orc_p2_cg(void* h, int L, double* x, const double* b, int maxIter, double tol) {
+  Oracle& o = *(Oracle*)h;
+  if (!o.lv[L].haveP2) buildP2Matrix(o, L);
+  const Csr& A = o.lv[L].P2;
+  const LevelData& F = o.lv[L + 1];
+  const int64_t n = (int64_t)F.nodes.size();
+  auto mv = [&](const std::vector<double>& u, std::vector<double>& y) {
+    for (int64_t i = 0; i < n; ++i) {
+      double t = 0.0;
+      if (!F.nodes[i].dirichlet)
+        for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) t += A.val[k] * u[A.col[k]];
+      y[i] = t;
+    }
+  };
+  std::vector<double> xv(x, x + n), r(n), p(n), ap(n);
+  mv(xv, ap);
+  for (int64_t i = 0; i < n; ++i) r[i] = F.nodes[i].dirichlet ? 0.0 : b[i] - ap[i];
+  for (int64_t i = 0; i < n; ++i) p[i] = F.nodes[i].dirichlet ? 0.0 : r[i];
+  auto dot = [&](const std::vector<double>& a, const std::vector<double>& c) {
+    double t = 0.0;
+    for (int64_t i = 0; i < n; ++i) t += a[i] * c[i];
+    return t;
+  };
+  double rs = dot(r, r);
+  int it = 0;
+  for (; it < maxIter && std::sqrt(rs) >= tol; ++it) {
+    mv(p, ap);
+    const double alpha = rs / dot(p, ap);
+    for (int64_t i = 0; i < n; ++i) {
+      xv[i] += alpha * p[i];
+      r[i] -= alpha * ap[i];
+    }
+    const double rn = dot(r, r);
+    for (int64_t i = 0; i < n; ++i) p[i] = r[i] + rn / rs * p[i];
+    rs = rn;
+  }
+  std::copy(xv.begin(), xv.end(), x);
+  return it;
+}
+
 void orc_p2_element_laplace(const double* coords12, double* K100) {
   double p[4][3];
   for (int m = 0; m < 4; ++m)

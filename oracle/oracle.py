@@ -46,6 +46,7 @@ def _load_oracle():
         "orc_p2_sor": (None, [c_void_p, c_int, P(c_double), P(c_double), c_double, c_int, c_int]),
         "orc_p2_prolongate": (None, [c_void_p, c_int, P(c_double), P(c_double), c_int]),
         "orc_p2_restrict": (None, [c_void_p, c_int, P(c_double), P(c_double)]),
+        "orc_p2_cg": (c_int, [c_void_p, c_int, P(c_double), P(c_double), c_int, c_double]),
         "orc_cell_local_stencil": (None, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, P(c_double)]),
     }
     for name, (res, args) in sig.items():
@@ -197,6 +198,13 @@ class Oracle:
         coarse = np.zeros(self.n(Lf))
         lib().orc_p2_restrict(self.h, Lf, dp(fine), dp(coarse))
         return coarse
+
+    def p2_cg(self, L, x, b, max_iter=10000, tol=1e-13):
+        """CG solution of the P2 Laplace system of level L (Dirichlet values of x kept)."""
+        x = np.ascontiguousarray(x, dtype=np.float64).copy()
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        lib().orc_p2_cg(self.h, L, dp(x), dp(b), max_iter, tol)
+        return x
 
     def cell_local_stencil(self, L, cell, x, y, z, form=0):
         out = np.zeros(15)

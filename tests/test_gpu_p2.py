@@ -159,3 +159,25 @@ def test_p2_restriction(cube2, Lf):
     ref = orc.p2_restrict(Lf, fine)
     inner = ~orc.dirichlet(Lf)
     assert rel(got, ref, inner) < 1e-13
+
+
+def test_p2_multigrid_solves_to_oracle_solution(cube2):
+    st, orc, maps = cube2
+    L = 3
+    node, owned = maps[L]
+    n = orc.n(L + 1)
+    rng = np.random.default_rng(123)
+    bg = rng.uniform(-1, 1, n)
+    inner = ~orc.dirichlet(L + 1)
+    bg[~inner] = 0.0
+    A = hg.P2ConstantLaplaceOperator(st, 0, 3)
+    x, b = hg.P2Function("x", st, 0, 3), hg.P2Function("b", st, 0, 3)
+    b.from_numpy(L, H.scatter(node, bg))
+    gmg = hg.P2GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
+    it, relres, hist = gmg.solve_to(x, b, L, 1e-10, 60)
+    assert relres <= 1e-10
+    factors = hist[1:] / hist[:-1]
+    assert factors.max() < 0.6, factors
+    ref = orc.p2_cg(L, np.zeros(n), bg, 20000, 1e-14)
+    got = H.gather_owned(x.to_numpy(L), node, owned, n)
+    assert rel(got, ref, inner) < 1e-8
