@@ -323,6 +323,26 @@ def serving_bench(hg, n_requests, seed=2024):
     return out
 
 
+def p2_kernels(hg, st, L2, timed):
+    """P2 Laplace on P2 level L2 of the same cube (its DoFs are the vertex lattice L2 + 1):
+    apply, multicolour SOR sweep, one P2 V(3,3) cycle; FP64. Algorithmic bytes of the apply:
+    16 per inner P2 DoF (read x, write y)."""
+    Inner = hg.Inner | hg.NeumannBoundary
+    n_in = inner_dofs(L2 + 1)
+    A = hg.P2ConstantLaplaceOperator(st, 0, L2)
+    x, b, y = (hg.P2Function(nm, st, 0, L2) for nm in ("p2x", "p2b", "p2y"))
+    x.fill_random(5, L2, hg.Inner)
+    b.fill_random(6, L2, hg.Inner)
+    t_apply = timed(lambda: A.apply(x, y, L2, hg.Inner), 5)
+    t_sor = timed(lambda: A.smooth_sor(x, b, 1.0, L2, Inner), 3)
+    g = hg.P2GeometricMultigridSolver(st, A, 0, L2, 3, 3, 1.0)
+    t_cycle = timed(lambda: g.solve(x, b, L2), 2)
+    return {"p2_level": L2, "inner_dofs": n_in,
+            "apply": {"ms": t_apply * 1e3, "gdofs": n_in / t_apply / 1e9, "GBs_algorithmic": 16 * n_in / t_apply / 1e9},
+            "sor_sweep": {"ms": t_sor * 1e3, "gdofs": n_in / t_sor / 1e9},
+            "vcycle": {"ms": t_cycle * 1e3, "gdofs": n_in / t_cycle / 1e9}}
+
+
 def fp32_kernels(hg, st, A, x, b, L, Inner, N_in, Nc, timed):
     """The same kernels on FP32 copies of the vectors (the arithmetic of the inner cycles of the
     mixed-precision solve), and one FP32 V(3,3) cycle. Algorithmic bytes are half the FP64 ones."""
@@ -484,6 +504,8 @@ def run_ours(args):
                                          "GBs_algorithmic": BYTES["sor_sweep"] * Nc / t_sor_passes / 1e9}
     kernels["cell_apply_launch"] = {"ms": t_apply_cells * 1e3, "GBs_algorithmic": BYTES["apply"] * Nc / t_apply_cells / 1e9}
     kernels["fp32"] = fp32_kernels(hg, st, A, x, b, L, Inner, N_in, Nc, timed)
+    if L >= 3:
+        kernels["p2"] = p2_kernels(hg, st, L - 2, timed)
 
     # --- time to solution: FP64 GMG vs mixed precision (FP32 cycles inside FP64 defect correction)
     solve = time_to_solution(hg, st, A, L, N_in, Inner)

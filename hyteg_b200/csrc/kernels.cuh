@@ -870,7 +870,14 @@ __global__ void __launch_bounds__(kBlock) p2CellKernel(LevelDev lv, P2Tables tb,
   const int64_t base = lv.cellOff[c];
   const bool cellOn = (lv.cellType[c] & mask) != 0;
   const T* Kc = K + (int64_t)c * 600;
-  const int pb = int(tetSize(w) - tetSize(w - Z));
+  // first index of the planes Z-2 .. Z+2 (the ones a micro-cell around a node of plane Z reaches)
+  int pbz[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    const int z = Z - 2 + d;
+    pbz[d] = (z >= 0 && z <= M) ? int(tetSize(w) - tetSize(w - z)) : 0;
+  }
+  const int pb = pbz[2];
   for (int Y = warp; Y <= M - Z; Y += kBlock / 32) {
     const int r0 = pb + rowStart(w - Z, Y);
     for (int X = lane; X <= M - Z - Y; X += 32) {
@@ -890,8 +897,7 @@ __global__ void __launch_bounds__(kBlock) p2CellKernel(LevelDev lv, P2Tables tb,
 #pragma unroll
         for (int m = 0; m < 10; ++m) {
           const int qx = 2 * ax + tb.off[t][m][0], qy = 2 * ay + tb.off[t][m][1], qz = 2 * az + tb.off[t][m][2];
-          const int W = w - qz;
-          s += Kr[m] * __ldg(src + base + int(tetSize(w) - tetSize(W)) + rowStart(W, qy) + qx);
+          s += Kr[m] * __ldg(src + base + pbz[qz - Z + 2] + rowStart(w - qz, qy) + qx);
         }
       }
       const bool interior = X >= 1 && Y >= 1 && Z >= 1 && X + Y + Z <= M - 1;
