@@ -612,6 +612,43 @@ class P2GeometricMultigridSolver:
             pass
 
 
+class P2P1TaylorHoodStokesOperator:
+    """P2P1TaylorHoodStokesOperator: velocity = three P2Functions, pressure = a P1Function whose
+    level L is the pressure of P2 level L. apply(u, p, v, q, level): v = A u + D^T p, q = D u."""
+
+    def __init__(self, storage, minLevel, maxLevel):
+        self.storage = storage
+        h = ctypes.c_int()
+        call("hg_p2p1_stokes_create", storage.handle, minLevel, maxLevel, ctypes.byref(h))
+        self.id = h.value
+
+    def apply(self, u, p, v, q, level, flagVelocity=Inner | NeumannBoundary, flagPressure=All):
+        ui = (ctypes.c_int * 3)(*[f.id for f in u])
+        vi = (ctypes.c_int * 3)(*[f.id for f in v])
+        call("hg_p2p1_stokes_apply", self.storage.handle, self.id, ui, p.id, vi, q.id, level, flagVelocity,
+             flagPressure)
+
+    def minres(self, u, p, f, g, level, nu=2, max_iter=500, tol=1e-8):
+        """MinResSolver with the block-diagonal preconditioner (symmetric P2 V(nu, nu) per velocity
+        component, lumped P1 mass on the pressure). Returns (iterations, relative residual, history)."""
+        ui = (ctypes.c_int * 3)(*[x.id for x in u])
+        fi = (ctypes.c_int * 3)(*[x.id for x in f])
+        it = ctypes.c_int()
+        rel = ctypes.c_double()
+        hist = np.zeros(max_iter)
+        call("hg_p2p1_stokes_minres", self.storage.handle, self.id, ui, p.id, fi, g.id, level, int(nu), int(max_iter),
+             float(tol), ctypes.byref(it), ctypes.byref(rel), dptr(hist), int(max_iter))
+        return it.value, rel.value, hist[: it.value].copy()
+
+    def __del__(self):
+        try:
+            st = getattr(self, "storage", None)
+            if st is not None and st.handle:
+                _capi.lib.hg_p2_operator_destroy(st.handle, self.id)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+
+
 class SolveServer:
     """Continuous-batching server of P1 Poisson solves (hg_server_*): requests on the unit cube
     split into k^3 sub-cubes of 6 tetrahedra at a refinement level, constant coefficient, seeded

@@ -100,6 +100,10 @@ _SIGS = {
     "hg_p2_gmg_solve": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
     "hg_p2_gmg_solve_to": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_int, P(c_int), P(c_double),
                                    P(c_double), c_int]),
+    "hg_p2p1_stokes_create": (c_int, [c_void_p, c_int, c_int, P(c_int)]),
+    "hg_p2p1_stokes_apply": (c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), c_int, c_int, c_uint, c_uint]),
+    "hg_p2p1_stokes_minres": (c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), c_int, c_int, c_int, c_int, c_double,
+                                      P(c_int), P(c_double), P(c_double), c_int]),
     "hg_server_create": (c_int, [c_int, c_int64, c_int, P(c_void_p)]),
     "hg_server_destroy": (c_int, [c_void_p]),
     "hg_server_prewarm": (c_int, [c_void_p, c_int, c_int]),

@@ -767,6 +767,31 @@ int hg_p2_gmg_solve_to(hg_storage* h, int gmg, int x, int b, int level, double t
   HG_CATCH
 }
 
+int hg_p2p1_stokes_create(hg_storage* h, int min_level, int max_level, int* op) {
+  HG_TRY
+  hg::argCheck(op != nullptr, "null output pointer");
+  *op = S(h).createStokesOperator(min_level, max_level);
+  HG_CATCH
+}
+
+int hg_p2p1_stokes_apply(hg_storage* h, int op, const int u[3], int p, const int v[3], int q, int level,
+                         unsigned flag_velocity, unsigned flag_pressure) {
+  HG_TRY
+  hg::argCheck(u && v, "null function lists");
+  S(h).stokesApply(op, u, p, v, q, level, flag_velocity, flag_pressure);
+  HG_CATCH
+}
+
+int hg_p2p1_stokes_minres(hg_storage* h, int op, const int u[3], int p, const int f[3], int g, int level, int nu,
+                          int max_iter, double tol, int* iterations, double* rel_residual, double* history,
+                          int history_cap) {
+  HG_TRY
+  hg::argCheck(u && f && tol > 0.0 && max_iter >= 0 && nu >= 0, "invalid arguments");
+  const int n = hg::stokesMinres(S(h), op, u, p, f, g, level, nu, max_iter, tol, rel_residual, history, history_cap);
+  if (iterations) *iterations = n;
+  HG_CATCH
+}
+
 struct hg_server {
   hg::Server* s;
 };

@@ -392,6 +392,65 @@ void elementP2Laplace(const double p[4][3], double K[100]) {
     }
 }
 
+void elementP2P1Div(const double p[4][3], double D[3][40]) {
+  double J[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) J[r][c] = p[c + 1][r] - p[0][r];
+  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) -
+                     J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  const double cof[3][3] = {{J[1][1] * J[2][2] - J[1][2] * J[2][1], J[0][2] * J[2][1] - J[0][1] * J[2][2],
+                             J[0][1] * J[1][2] - J[0][2] * J[1][1]},
+                            {J[1][2] * J[2][0] - J[1][0] * J[2][2], J[0][0] * J[2][2] - J[0][2] * J[2][0],
+                             J[0][2] * J[1][0] - J[0][0] * J[1][2]},
+                            {J[1][0] * J[2][1] - J[1][1] * J[2][0], J[0][1] * J[2][0] - J[0][0] * J[2][1],
+                             J[0][0] * J[1][1] - J[0][1] * J[1][0]}};
+  double G[4][3];
+  for (int d = 0; d < 3; ++d) {
+    for (int i = 0; i < 3; ++i) G[i + 1][d] = cof[i][d] / det;
+    G[0][d] = -(G[1][d] + G[2][d] + G[3][d]);
+  }
+  const double vol = std::fabs(det) / 6.0;
+  // int lambda_i (4 lambda_a - 1) = |T| ((1 + delta_ia) / 5 - 1/4); int lambda_i lambda_b = |T| (1 + delta_ib) / 20
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 10; ++j) {
+        double v;
+        if (j < 4) {
+          v = G[j][k] * vol * ((i == j ? 2.0 : 1.0) / 5.0 - 0.25);
+        } else {
+          const int a = kP2Edge[j - 4][0], b = kP2Edge[j - 4][1];
+          v = 4.0 * vol / 20.0 * (G[a][k] * (i == b ? 2.0 : 1.0) + G[b][k] * (i == a ? 2.0 : 1.0));
+        }
+        D[k][10 * i + j] = -v;
+      }
+}
+
+std::vector<double> p2p1CellDiv(const Topology& topo, int L) {
+  const int64_t N = int64_t(1) << L;
+  std::vector<double> out(topo.cells.size() * 6 * 120, 0.0);
+  for (size_t c = 0; c < topo.cells.size(); ++c) {
+    const auto& ce = topo.cells[c];
+    double V[4][3];
+    for (int i = 0; i < 4; ++i)
+      for (int d = 0; d < 3; ++d) V[i][d] = topo.verts[ce.v[i]].x[d];
+    for (int t = 0; t < 6; ++t) {
+      double P[4][3];
+      for (int m = 0; m < 4; ++m)
+        for (int d = 0; d < 3; ++d)
+          P[m][d] = V[0][d] + ((V[1][d] - V[0][d]) * kMicroCellTable[t][m][0] +
+                               (V[2][d] - V[0][d]) * kMicroCellTable[t][m][1] +
+                               (V[3][d] - V[0][d]) * kMicroCellTable[t][m][2]) /
+                                  (double)N;
+      double D[3][40];
+      elementP2P1Div(P, D);
+      for (int k = 0; k < 3; ++k)
+        for (int i = 0; i < 40; ++i) out[(c * 6 + t) * 120 + k * 40 + i] = D[k][i];
+    }
+  }
+  return out;
+}
+
 std::vector<double> p2CellElements(const Topology& topo, int L) {
   const int64_t N = int64_t(1) << L;
   std::vector<double> out(topo.cells.size() * 600, 0.0);

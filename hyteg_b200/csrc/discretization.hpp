@@ -140,5 +140,11 @@ void elementP2Laplace(const double p[4][3], double K[100]);
 // Element matrices of the six micro-cell types of level L in every macro-cell, scaled by the
 // cell's coefficient: [cell][type][10][10].
 std::vector<double> p2CellElements(const Topology& topo, int L);
+// Taylor-Hood divergence element (P2ToP1ConstantDivOperator, p2_to_p1_tet_div_tet of the
+// reference's forms): D[k][4 i + ...] = -int psi_i d(phi_j)/dx_k for P1 vertex i and P2 node j,
+// stored as D[k][10 i + j]; the gradient block (P1ToP2ConstantDivTOperator) is its transpose.
+void elementP2P1Div(const double p[4][3], double D[3][40]);
+// [cell][type][3][40] for the six micro-cell types of level L.
+std::vector<double> p2p1CellDiv(const Topology& topo, int L);
 
 }  // namespace hg

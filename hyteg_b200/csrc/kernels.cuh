@@ -1014,6 +1014,86 @@ __global__ void __launch_bounds__(kBlock) p2PickKernel(const int64_t* __restrict
   dst[owner[i]] = dst[copies[ptr[i]]];
 }
 
+// ---------------------------------------------------------------------------------------
+// Taylor-Hood coupling blocks between the P1 pressure lattice (level L) and the P2 velocity
+// lattice (level L + 1); element matrices D[cell][type][k][4][10] (pressure vertex i, velocity
+// node j). p2DivKernel: q = sum_k D_k u_k at the pressure nodes (a pressure node (x, y, z) is
+// vertex i of micro-cell (t, (x, y, z) - v_t,i)). p2DivTKernel: v_k = D_k^T p at the velocity
+// nodes (same candidates as the P2 operator). Both write final values at cell-interior nodes
+// and this cell's share at the closure nodes; p2AddKernel sums the shares into the owners.
+// ---------------------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2DivKernel(LevelDev lvp, LevelDev lvv, P2Tables tb, const T* __restrict__ D,
+                                                      T* __restrict__ q, const T* __restrict__ u0,
+                                                      const T* __restrict__ u1, const T* __restrict__ u2,
+                                                      unsigned mask) {
+  const int N = lvp.N, nPl = N + 1, wp = lvp.w, wv = lvv.w;
+  const int c = blockIdx.x / nPl, z = blockIdx.x % nPl;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t vb = lvv.cellOff[c];
+  const T* Dc = D + (int64_t)c * 720;
+  const bool cellOn = (lvp.cellType[c] & mask) != 0;
+  auto vidx = [wv](int x, int y, int zz) { return int(tetSize(wv) - tetSize(wv - zz)) + rowStart(wv - zz, y) + x; };
+  const int pb = int(tetSize(wp) - tetSize(wp - z));
+  for (int y = warp; y <= N - z; y += kBlock / 32)
+    for (int x = lane; x <= N - z - y; x += 32) {
+      T s = T(0);
+      for (int t = 0; t < 6; ++t)
+        for (int i = 0; i < 4; ++i) {
+          const int ax = x - (tb.off[t][i][0] >> 1), ay = y - (tb.off[t][i][1] >> 1), az = z - (tb.off[t][i][2] >> 1);
+          if (ax < 0 || ay < 0 || az < 0 || ax + ay + az >= N - tb.widthRed[t]) continue;
+          const T* Dr = Dc + t * 120 + i * 10;
+#pragma unroll
+          for (int j = 0; j < 10; ++j) {
+            const int64_t g = vb + vidx(2 * ax + tb.off[t][j][0], 2 * ay + tb.off[t][j][1], 2 * az + tb.off[t][j][2]);
+            s += Dr[j] * __ldg(u0 + g) + Dr[40 + j] * __ldg(u1 + g) + Dr[80 + j] * __ldg(u2 + g);
+          }
+        }
+      const int64_t o = lvp.cellOff[c] + pb + rowStart(wp - z, y) + x;
+      const bool interior = x >= 1 && y >= 1 && z >= 1 && x + y + z <= N - 1;
+      if (!interior || cellOn) q[o] = s;
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2DivTKernel(LevelDev lvv, LevelDev lvp, P2Tables tb, const T* __restrict__ D,
+                                                       T* __restrict__ v0, T* __restrict__ v1, T* __restrict__ v2,
+                                                       const T* __restrict__ p, unsigned mask) {
+  const int M = lvv.N, N = M / 2, nPl = M + 1, wv = lvv.w, wp = lvp.w;
+  const int c = blockIdx.x / nPl, Z = blockIdx.x % nPl;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t pbase = lvp.cellOff[c];
+  const T* Dc = D + (int64_t)c * 720;
+  const bool cellOn = (lvv.cellType[c] & mask) != 0;
+  auto pidx = [wp](int x, int y, int z) { return int(tetSize(wp) - tetSize(wp - z)) + rowStart(wp - z, y) + x; };
+  const int pb = int(tetSize(wv) - tetSize(wv - Z));
+  for (int Y = warp; Y <= M - Z; Y += kBlock / 32)
+    for (int X = lane; X <= M - Z - Y; X += 32) {
+      const int pc = (X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2);
+      T s0 = T(0), s1 = T(0), s2 = T(0);
+      for (int k = 0; k < tb.nCand[pc]; ++k) {
+        const int t = tb.cand[pc][k][0], j = tb.cand[pc][k][1];
+        const int ax = (X - tb.off[t][j][0]) >> 1, ay = (Y - tb.off[t][j][1]) >> 1, az = (Z - tb.off[t][j][2]) >> 1;
+        if (ax < 0 || ay < 0 || az < 0 || ax + ay + az >= N - tb.widthRed[t]) continue;
+        const T* Dt = Dc + t * 120;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const T pv = __ldg(p + pbase + pidx(ax + (tb.off[t][i][0] >> 1), ay + (tb.off[t][i][1] >> 1), az + (tb.off[t][i][2] >> 1)));
+          s0 += Dt[i * 10 + j] * pv;
+          s1 += Dt[40 + i * 10 + j] * pv;
+          s2 += Dt[80 + i * 10 + j] * pv;
+        }
+      }
+      const int64_t o = lvv.cellOff[c] + pb + rowStart(wv - Z, Y) + X;
+      const bool interior = X >= 1 && Y >= 1 && Z >= 1 && X + Y + Z <= M - 1;
+      if (!interior || cellOn) {
+        v0[o] = s0;
+        v1[o] = s1;
+        v2[o] = s2;
+      }
+    }
+}
+
 // Sums the cells' shares of every DoF owned by a face, edge or vertex (the copies of that DoF in
 // the closure slots of its cells) into the owner slot: dst = sum, or rhs - sum for a residual.
 template <class T, int MODE>
@@ -1187,6 +1267,17 @@ __global__ void __launch_bounds__(kBlock) lincombKernel(const Chunk* __restrict_
     if (nsrc > 1) v += T(a1) * s1[j];
     if (nsrc > 2) v += T(a2) * s2[j];
     dst[j] = v;
+  }
+}
+
+// dst = a / b on the flagged primitives' slots (the inverse of a lumped / diagonal operator)
+static __global__ void __launch_bounds__(kBlock) divideKernel(const Chunk* __restrict__ chunks, unsigned mask, double* dst,
+                                                      const double* __restrict__ a, const double* __restrict__ b) {
+  const Chunk ch = chunks[blockIdx.x];
+  if (!(ch.type & mask)) return;
+  for (int i = threadIdx.x; i < ch.len; i += blockDim.x) {
+    const int64_t j = ch.start + i;
+    dst[j] = a[j] / b[j];
   }
 }
 

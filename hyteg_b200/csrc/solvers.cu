@@ -306,7 +306,142 @@ void P2Gmg::solveRecursively(int x, int b, int L) {
   s.lincomb(x, L, HG_ALL, 0, nullptr, nullptr, false, 0.0);
   solveRecursively(x, b, L - 1);
   s.p2Prolongate(x, L - 1, flag, true);
-  for (int i = 0; i < post; ++i) s.p2Sor(op, x, b, omega, L, flag, false);
+  for (int i = 0; i < post; ++i) s.p2Sor(op, x, b, omega, L, flag, symmetric);
+}
+
+int stokesMinres(Storage& s, int op, const int u[3], int p, const int f[3], int g, int L, int nu, int maxIter,
+                 double tol, double* relRes, double* history, int historyCap) {
+  const unsigned fv = HG_INNER | HG_NEUMANN, fp = HG_ALL;
+  const int Lv = L + 1, Lp = L;
+  std::vector<int> made;
+  auto fnV = [&](int minL) {
+    const int id = s.createFunction(minL, Lv, 8);
+    made.push_back(id);
+    return id;
+  };
+  auto fnP = [&]() {
+    const int id = s.createFunction(Lp, Lp, 8);
+    made.push_back(id);
+    return id;
+  };
+  struct Blk {
+    int u[3];
+    int p;
+  };
+  auto blk = [&]() {
+    Blk b;
+    for (int k = 0; k < 3; ++k) b.u[k] = fnV(Lv);
+    b.p = fnP();
+    return b;
+  };
+  Blk x{{u[0], u[1], u[2]}, p}, rhs{{f[0], f[1], f[2]}, g};
+  Blk vPrev = blk(), v = blk(), vNext = blk(), z = blk(), wPrev = blk(), w = blk(), wNext = blk(), az = blk();
+  auto dot = [&](const Blk& a, const Blk& b) {
+    double t = s.dot(a.p, b.p, Lp, fp);
+    for (int k = 0; k < 3; ++k) t += s.dot(a.u[k], b.u[k], Lv, fv);
+    return t;
+  };
+  // dst = sum_i a_i src_i (up to three terms) on the unknowns of every block
+  auto comb = [&](const Blk& dst, int n, const double* a, const Blk* src, bool add) {
+    for (int k = 0; k < 3; ++k) {
+      int ids[3];
+      for (int i = 0; i < n; ++i) ids[i] = src[i].u[k];
+      s.lincomb(dst.u[k], Lv, fv, n, a, ids, add, 0.0);
+    }
+    int ids[3];
+    for (int i = 0; i < n; ++i) ids[i] = src[i].p;
+    s.lincomb(dst.p, Lp, fp, n, a, ids, add, 0.0);
+  };
+  auto applyK = [&](const Blk& src, const Blk& dst) { s.stokesApply(op, src.u, src.p, dst.u, dst.p, L, fv, fp); };
+  // preconditioner: velocity V-cycles (symmetric), pressure / lumped mass; zero-mean pressure
+  const int mass = s.createOperator(FORM_MASS, Lp, Lp);
+  const int ones = fnP(), lumped = fnP();
+  s.lincomb(ones, Lp, fp, 0, nullptr, nullptr, false, 1.0);
+  s.apply(mass, ones, lumped, Lp, fp, 0);
+  const double nP = s.dot(ones, ones, Lp, fp);
+  P2Gmg mg(s, op, 0, L, nu, nu, 1.0, 1000, 1e-14);
+  mg.symmetric = true;
+  const int px = fnV(1), pb = fnV(1);
+  auto precond = [&](const Blk& src, const Blk& dst) {
+    const double one = 1.0;
+    for (int k = 0; k < 3; ++k) {
+      s.lincomb(pb, Lv, fv, 1, &one, &src.u[k], false, 0.0);
+      for (int l = 1; l <= Lv; ++l) s.lincomb(px, l, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+      mg.solveRecursively(px, pb, L);
+      s.lincomb(dst.u[k], Lv, fv, 1, &one, &px, false, 0.0);
+    }
+    s.divideBy(dst.p, src.p, lumped, Lp, fp);
+    const double mean = s.dot(dst.p, ones, Lp, fp) / nP;
+    s.lincomb(dst.p, Lp, fp, 1, &one, &dst.p, false, -mean);
+  };
+  // v1 = f - K x, z1 = M^-1 v1, gamma1 = sqrt(<z1, v1>)
+  applyK(x, az);
+  {
+    const double a[2] = {1.0, -1.0};
+    const Blk src[2] = {rhs, az};
+    comb(v, 2, a, src, false);
+  }
+  precond(v, z);
+  double gamma = std::sqrt(std::max(dot(z, v), 0.0)), gammaPrev = 1.0;
+  const double gamma1 = gamma;
+  double eta = gamma, c = 1.0, cPrev = 1.0, sn = 0.0, snPrev = 0.0;
+  int it = 0;
+  double rel = gamma1 > 0.0 ? 1.0 : 0.0;
+  while (it < maxIter && rel > tol && gamma > 0.0) {
+    ++it;
+    {  // z_j = z_j / gamma_j
+      const double a = 1.0 / gamma;
+      comb(z, 1, &a, &z, false);
+    }
+    applyK(z, az);
+    const double delta = dot(az, z);
+    {  // v_{j+1} = A z_j - delta / gamma_j v_j - gamma_j / gamma_{j-1} v_{j-1}
+      const double a[3] = {1.0, -delta / gamma, -gamma / gammaPrev};
+      const Blk src[3] = {az, v, vPrev};
+      comb(vNext, it == 1 ? 2 : 3, a, src, false);
+    }
+    precond(vNext, az);  // az now holds z_{j+1}
+    const double gammaNext = std::sqrt(std::max(dot(az, vNext), 0.0));
+    const double a0 = c * delta - cPrev * sn * gamma;
+    const double a1 = std::sqrt(a0 * a0 + gammaNext * gammaNext);
+    const double a2 = sn * delta + cPrev * c * gamma;
+    const double a3 = snPrev * gamma;
+    cPrev = c;
+    snPrev = sn;
+    c = a0 / a1;
+    sn = gammaNext / a1;
+    {  // w_{j+1} = (z_j - a3 w_{j-1} - a2 w_j) / a1
+      const double a[3] = {1.0 / a1, -a3 / a1, -a2 / a1};
+      const Blk src[3] = {z, wPrev, w};
+      comb(wNext, 3, a, src, false);
+    }
+    {  // x += c eta w_{j+1}
+      const double a = c * eta;
+      comb(x, 1, &a, &wNext, true);
+    }
+    eta = -sn * eta;
+    rel = std::fabs(eta) / gamma1;
+    if (history && it <= historyCap) history[it - 1] = rel;
+    // rotate: v_{j-1} <- v_j <- v_{j+1}, w_{j-1} <- w_j <- w_{j+1}, z <- z_{j+1}
+    std::swap(vPrev, v);
+    std::swap(v, vNext);
+    std::swap(wPrev, w);
+    std::swap(w, wNext);
+    std::swap(z, az);
+    gammaPrev = gamma;
+    gamma = gammaNext;
+  }
+  {
+    const double one = 1.0;
+    const double mean = s.dot(x.p, ones, Lp, fp) / nP;
+    s.lincomb(x.p, Lp, fp, 1, &one, &x.p, false, -mean);
+  }
+  for (int k = 0; k < 3; ++k) s.communicate(x.u[k], Lv, (1 << G_COUNT) - 1);
+  s.communicate(x.p, Lp, (1 << G_COUNT) - 1);
+  s.ops.erase(mass);
+  for (int id : made) s.fns.erase(id);
+  if (relRes) *relRes = rel;
+  return it;
 }
 
 int P2Gmg::solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap) {

@@ -67,6 +67,16 @@ struct P2Gmg {
   int coarseMaxIter;
   double coarseTol;
   int tmp, cp, cz, cap, cr;
+  bool symmetric = false;  // post-smoothing with backward sweeps (a symmetric cycle)
 };
+
+// MinResSolver (solvers/MinresSolver.hpp:63-125) for the P2-P1 Taylor-Hood Stokes system on
+// level L, preconditioned block-diagonally: one symmetric P2 V(nu, nu) cycle from zero per velocity
+// component and the inverse lumped P1 mass on the pressure. Velocity DoFs flagged
+// Inner | Neumann are unknowns (the Dirichlet values of u are kept), every pressure DoF is an
+// unknown; the pressure is returned with zero mean. Returns the iterations; relRes is the
+// preconditioned residual norm relative to the initial one.
+int stokesMinres(Storage& s, int op, const int u[3], int p, const int f[3], int g, int L, int nu, int maxIter,
+                 double tol, double* relRes, double* history, int historyCap);
 
 }  // namespace hg

@@ -343,6 +343,16 @@ void Storage::lincomb(int dst, int L, unsigned mask, int n, const double* a, con
   cudaCheck(cudaGetLastError(), "lincomb");
 }
 
+void Storage::divideBy(int dst, int a, int b, int L, unsigned mask) {
+  argCheck(fn(dst).prec == 8 && fn(a).prec == 8 && fn(b).prec == 8, "divide: FP64 functions required");
+  const LevelData& ld = levels[L];
+  if (!ld.nChunks) return;
+  dev::divideKernel<<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (double*)data(dst, L),
+                                                             (const double*)data(a, L), (const double*)data(b, L));
+  ++launches;
+  cudaCheck(cudaGetLastError(), "divide");
+}
+
 void Storage::copyCast(int dst, int src, int L, unsigned mask, bool add) {
   Function& fd = fn(dst);
   Function& fs = fn(src);
@@ -856,6 +866,88 @@ void Storage::p2Restrict(int id, int Lf, unsigned mask) {
   launches += adc.n ? 2 : 1;
   cudaCheck(cudaGetLastError(), "P2 restriction");
   communicate(id, Lcf, kAllGroups);
+}
+
+int Storage::createStokesOperator(int minL, int maxL) {
+  const int id = createP2Operator(FORM_LAPLACE, minL, maxL);
+  P2Operator& o = p2op(id);
+  for (int L = minL; L <= maxL; ++L) {
+    const std::vector<double> D = p2p1CellDiv(disc.topo(), L);
+    std::vector<float> Df(D.begin(), D.end());
+    o.dd.emplace_back(new DevBuf());
+    o.dd.back()->alloc(D.size() * sizeof(double));
+    cudaCheck(cudaMemcpyAsync(o.dd.back()->p, D.data(), D.size() * sizeof(double), cudaMemcpyHostToDevice, stream),
+              "div upload");
+    o.df.emplace_back(new DevBuf());
+    o.df.back()->alloc(Df.size() * sizeof(float));
+    cudaCheck(cudaMemcpyAsync(o.df.back()->p, Df.data(), Df.size() * sizeof(float), cudaMemcpyHostToDevice, stream),
+              "div upload");
+    cudaCheck(cudaStreamSynchronize(stream), "div upload");
+  }
+  return id;
+}
+
+template <class T>
+static void stokesCoupling(Storage& st, P2Operator& o, const int u[3], int p, const int v[3], int q, int L,
+                           unsigned maskV, unsigned maskP) {
+  const int Lv = L + 1, Lp = L;
+  const LevelData& lvv = st.levels[Lv];
+  const LevelData& lvp = st.levels[Lp];
+  const T* D = (const T*)(sizeof(T) == 8 ? o.dd[L - o.minL]->p : o.df[L - o.minL]->p);
+  const int prec = (int)sizeof(T);
+  // v_k += D_k^T p: shares into three scratch functions, owner sums, then added where flagged
+  int sc[3];
+  for (int k = 0; k < 3; ++k) {
+    auto key = std::make_pair(Lv, 16 + 8 * k + prec);  // three distinct scratch buffers per level
+    if (!st.p2scratch.count(key)) st.p2scratch[key] = st.createFunction(Lv, Lv, prec);
+    sc[k] = st.p2scratch[key];
+  }
+  st.communicate(p, Lp, 1 << G_CELL);
+  P2Additive& adv = st.p2Additive(Lv);
+  dev::p2DivTKernel<T><<<lvv.lv.nCells * (lvv.lv.N + 1), dev::kBlock, 0, st.stream>>>(
+      lvv.lv, lvp.lv, p2TablesOnce(), D, (T*)st.data(sc[0], Lv), (T*)st.data(sc[1], Lv), (T*)st.data(sc[2], Lv),
+      (const T*)st.data(p, Lp), maskV);
+  ++st.launches;
+  for (int k = 0; k < 3; ++k) {
+    if (adv.n)
+      dev::p2AddKernel<T, dev::MODE_REPLACE><<<(adv.n + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, st.stream>>>(
+          (const int64_t*)adv.owner.p, (const int*)adv.ptr.p, (const int64_t*)adv.copies.p,
+          (const unsigned char*)adv.type.p, adv.n, (T*)st.data(sc[k], Lv), nullptr, maskV, nullptr, -1);
+    const double one = 1.0;
+    st.lincomb(v[k], Lv, maskV, 1, &one, &sc[k], true, 0.0);
+    st.communicate(v[k], Lv, (1 << G_COUNT) - 1);
+    st.launches += adv.n ? 1 : 0;
+  }
+  // q = sum_k D_k u_k
+  for (int k = 0; k < 3; ++k) st.communicate(u[k], Lv, 1 << G_CELL);
+  P2Additive& adp = st.p2Additive(Lp);
+  dev::p2DivKernel<T><<<lvp.lv.nCells * (lvp.lv.N + 1), dev::kBlock, 0, st.stream>>>(
+      lvp.lv, lvv.lv, p2TablesOnce(), D, (T*)st.data(q, Lp), (const T*)st.data(u[0], Lv), (const T*)st.data(u[1], Lv),
+      (const T*)st.data(u[2], Lv), maskP);
+  ++st.launches;
+  if (adp.n) {
+    dev::p2AddKernel<T, dev::MODE_REPLACE><<<(adp.n + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, st.stream>>>(
+        (const int64_t*)adp.owner.p, (const int*)adp.ptr.p, (const int64_t*)adp.copies.p,
+        (const unsigned char*)adp.type.p, adp.n, (T*)st.data(q, Lp), nullptr, maskP, nullptr, -1);
+    ++st.launches;
+  }
+  cudaCheck(cudaGetLastError(), "Stokes coupling");
+  st.communicate(q, Lp, (1 << G_COUNT) - 1);
+}
+
+void Storage::stokesApply(int opId, const int u[3], int p, const int v[3], int q, int L, unsigned maskV,
+                          unsigned maskP) {
+  P2Operator& o = p2op(opId);
+  argCheck(!o.dd.empty(), "not a Stokes operator");
+  argCheck(L >= o.minL && L <= o.maxL, "level outside the Stokes operator's level range");
+  const int prec = fn(p).prec;
+  for (int k = 0; k < 3; ++k) argCheck(fn(u[k]).prec == prec && fn(v[k]).prec == prec, "Stokes: precision mismatch");
+  argCheck(fn(q).prec == prec, "Stokes: precision mismatch");
+  for (int k = 0; k < 3; ++k) p2Apply(opId, u[k], v[k], -1, L, maskV, 0);
+  if (prec == 8)
+    stokesCoupling<double>(*this, o, u, p, v, q, L, maskV, maskP);
+  else
+    stokesCoupling<float>(*this, o, u, p, v, q, L, maskV, maskP);
 }
 
 void Storage::reassembleOperator(int id) {

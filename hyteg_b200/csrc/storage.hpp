@@ -65,6 +65,7 @@ struct P2Operator {
   int form = 0, minL = 0, maxL = 0;
   std::vector<std::unique_ptr<DevBuf>> kd, kf;  // per level: [cell][type][10][10] in FP64 / FP32
   std::map<std::pair<int, int>, int> diag;      // (level, precision) -> diagonal function
+  std::vector<std::unique_ptr<DevBuf>> dd, df;  // Taylor-Hood divergence per level: [cell][type][3][4][10]
 };
 
 // Cell-closure copies of every DoF owned by a face, edge or vertex of one lattice level.
@@ -120,6 +121,8 @@ struct Storage {
   void communicate(int id, int L, int groupMask);
   void lincomb(int dst, int L, unsigned mask, int n, const double* a, const int* srcs, bool add, double constant);
   void copyCast(int dst, int src, int L, unsigned mask, bool add);
+  // dst = a / b elementwise on the flagged primitives' slots (FP64)
+  void divideBy(int dst, int a, int b, int L, unsigned mask);
   void dotAsync(int a, int b, int L, unsigned mask, double* dOut);
   void interpolateExpr(int id, int L, unsigned mask, int expr, const double* params);
   // Seeded uniform [lo, hi) values at the flagged primitives' DoFs, then a full halo refresh.
@@ -145,6 +148,12 @@ struct Storage {
   // add) and its transpose, the restriction from P2 level Lf to Lf - 1.
   void p2Prolongate(int id, int Lc, unsigned mask, bool add);
   void p2Restrict(int id, int Lf, unsigned mask);
+  // P2-P1 Taylor-Hood Stokes (P2P1TaylorHoodStokesOperator): velocity P2 functions u[3], v[3],
+  // pressure P1 functions p, q (level L of the pressure = P2 level L):
+  //   v_k = A u_k + D_k^T p   (velocity DoFs flagged by maskV)
+  //   q   = sum_k D_k u_k     (pressure DoFs flagged by maskP)
+  int createStokesOperator(int minL, int maxL);
+  void stokesApply(int op, const int u[3], int p, const int v[3], int q, int L, unsigned maskV, unsigned maskP);
   int p2Scratch(int Lf, int prec);
   template <class T, int MODE>
   void p2Launch(P2Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask, int sel);

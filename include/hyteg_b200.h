@@ -197,6 +197,23 @@ int hg_p2_smooth_sor(hg_storage* s, int op, int x, int b, double omega, int leve
  * transpose, the restriction from P2 level `level` to level - 1 (P2toP2QuadraticRestriction). */
 int hg_p2_prolongate(hg_storage* s, int fn, int level, unsigned flag, int add);
 int hg_p2_restrict(hg_storage* s, int fn, int level, unsigned flag);
+/* P2-P1 Taylor-Hood Stokes operator (P2P1TaylorHoodStokesOperator, composites/
+ * P2P1TaylorHoodStokesOperator.hpp:33-84): the P2 Laplace per velocity component and the
+ * divergence blocks P2ToP1ConstantDivOperator / P1ToP2ConstantDivTOperator (p2_to_p1_tet_div_tet,
+ * p1_to_p2_tet_divt_tet). Velocity: three P2 functions; pressure: a P1 function whose level L is
+ * the pressure of P2 level L. Destroy with hg_p2_operator_destroy.
+ * apply: v_k = A u_k + D_k^T p at the velocity DoFs of flag_velocity, q = sum_k D_k u_k at the
+ * pressure DoFs of flag_pressure.
+ * minres: MinResSolver (solvers/MinresSolver.hpp:63-125) on level L with a block-diagonal
+ * preconditioner (one symmetric P2 V(nu, nu) cycle per velocity component, inverse lumped P1
+ * mass for the pressure) to the relative preconditioned residual tol; the Dirichlet values of u
+ * are kept, the pressure is returned with zero mean. */
+int hg_p2p1_stokes_create(hg_storage* s, int min_level, int max_level, int* op);
+int hg_p2p1_stokes_apply(hg_storage* s, int op, const int u[3], int p, const int v[3], int q, int level,
+                         unsigned flag_velocity, unsigned flag_pressure);
+int hg_p2p1_stokes_minres(hg_storage* s, int op, const int u[3], int p, const int f[3], int g, int level, int nu,
+                          int max_iter, double tol, int* iterations, double* rel_residual, double* history,
+                          int history_cap);
 /* P2 geometric multigrid (GeometricMultigridSolver with P2ConstantLaplaceOperator, the P2 SOR
  * above, the quadratic transfers and CG on min_level), FP64. x, b: P2 functions covering
  * [min_level, max_level]. solve: one cycle; solve_to: cycles to the relative residual tol. */

@@ -136,6 +136,52 @@ void p2LaplaceElement(const double p[4][3], double K[10][10]) {
   }
 }
 
+// Taylor-Hood divergence element: D[k][i][j] = -int psi_i d(phi_j)/dx_k (P1 vertex i, P2 node j),
+// by the 4-point degree-2 rule (the integrand is quadratic).
+void p2p1DivElement(const double p[4][3], double D[3][4][10]) {
+  double J[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) J[r][c] = p[c + 1][r] - p[0][r];
+  const double det = J[0][0] * (J[1][1] * J[2][2] - J[1][2] * J[2][1]) - J[0][1] * (J[1][0] * J[2][2] - J[1][2] * J[2][0]) +
+                     J[0][2] * (J[1][0] * J[2][1] - J[1][1] * J[2][0]);
+  double inv[3][3];
+  inv[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / det;
+  inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / det;
+  inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / det;
+  inv[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / det;
+  inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / det;
+  inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / det;
+  inv[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / det;
+  inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / det;
+  inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / det;
+  double G[4][3];
+  for (int d = 0; d < 3; ++d) {
+    G[1][d] = inv[0][d];
+    G[2][d] = inv[1][d];
+    G[3][d] = inv[2][d];
+    G[0][d] = -(G[1][d] + G[2][d] + G[3][d]);
+  }
+  const double vol = std::fabs(det) / 6.0;
+  const double qa = (5.0 + 3.0 * std::sqrt(5.0)) / 20.0, qb = (5.0 - std::sqrt(5.0)) / 20.0;
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 10; ++j) D[k][i][j] = 0.0;
+  for (int q = 0; q < 4; ++q) {
+    double l[4] = {qb, qb, qb, qb};
+    l[q] = qa;
+    double g[10][3];
+    for (int a = 0; a < 4; ++a)
+      for (int d = 0; d < 3; ++d) g[a][d] = (4.0 * l[a] - 1.0) * G[a][d];
+    for (int e = 0; e < 6; ++e) {
+      const int a = kP2Edge[e][0], b = kP2Edge[e][1];
+      for (int d = 0; d < 3; ++d) g[4 + e][d] = 4.0 * (l[b] * G[a][d] + l[a] * G[b][d]);
+    }
+    for (int k = 0; k < 3; ++k)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 10; ++j) D[k][i][j] -= 0.25 * vol * l[i] * g[j][k];
+  }
+}
+
 struct Node {
   Key key;
   int kind, id;           // owner primitive (0 vertex, 1 edge, 2 face, 3 cell) and its ID
@@ -152,6 +198,8 @@ struct Csr {
 
 struct LevelData {
   int64_t N = 1;
+  Csr Div[3];                // Taylor-Hood divergence: rows nodes of this level, columns of the next
+  bool haveDiv = false;
   Csr P2;                    // P2 Laplace of this level on the nodes of the next finer level
   bool haveP2 = false;
   Csr P2prol;                // P2 prolongation from this level to the next (rows: nodes of level + 2)
@@ -712,6 +760,89 @@ void buildP2Prolongation(Oracle& o, int Lc) {
     P.ptr.push_back((int64_t)P.col.size());
   }
   d.haveP2prol = true;
+}
+
+void buildDiv(Oracle& o, int L) {
+  LevelData& d = o.lv[L];
+  const LevelData& f = o.lv[L + 1];
+  const int64_t N = d.N;
+  std::vector<std::map<int64_t, double>> rows[3];
+  for (auto& r : rows) r.resize(d.nodes.size());
+  for (size_t ci = 0; ci < o.cells.size(); ++ci)
+    for (int t = 0; t < 6; ++t) {
+      const int64_t width = N - kMicroWidthReduction[t];
+      for (int64_t z = 0; z < width; ++z)
+        for (int64_t y = 0; y + z < width; ++y)
+          for (int64_t x = 0; x + y + z < width; ++x) {
+            int64_t v[4][3];
+            double p[4][3];
+            int64_t pid[4], vid[10];
+            for (int m = 0; m < 4; ++m) {
+              v[m][0] = x + kMicro[t][m][0];
+              v[m][1] = y + kMicro[t][m][1];
+              v[m][2] = z + kMicro[t][m][2];
+              const Key k = o.keyOf((int)ci, N, v[m][0], v[m][1], v[m][2]);
+              o.coordOf(k, N, p[m]);
+              pid[m] = d.index.at(k);
+              vid[m] = f.index.at(o.keyOf((int)ci, 2 * N, 2 * v[m][0], 2 * v[m][1], 2 * v[m][2]));
+            }
+            for (int e = 0; e < 6; ++e) {
+              const int a = kP2Edge[e][0], b = kP2Edge[e][1];
+              vid[4 + e] = f.index.at(o.keyOf((int)ci, 2 * N, v[a][0] + v[b][0], v[a][1] + v[b][1], v[a][2] + v[b][2]));
+            }
+            double D[3][4][10];
+            p2p1DivElement(p, D);
+            for (int k = 0; k < 3; ++k)
+              for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 10; ++j) rows[k][pid[i]][vid[j]] += D[k][i][j];
+          }
+    }
+  for (int k = 0; k < 3; ++k) {
+    Csr& A = d.Div[k];
+    A.ptr.assign(1, 0);
+    for (auto& r : rows[k]) {
+      for (auto& kv : r) {
+        A.col.push_back(kv.first);
+        A.val.push_back(kv.second);
+      }
+      A.ptr.push_back((int64_t)A.col.size());
+    }
+  }
+  d.haveDiv = true;
+}
+
+void orc_p2_apply(void* h, int L, const double* u, double* y);
+
+// Taylor-Hood Stokes on P2 level L (velocity: nodes of level L + 1, pressure: nodes of level L):
+// v_k = A2 u_k + D_k^T p and q = sum_k D_k u_k, every row.
+void orc_stokes_apply(void* h, int L, const double* u0, const double* u1, const double* u2, const double* p, double* v0,
+                      double* v1, double* v2, double* q) {
+  Oracle& o = *(Oracle*)h;
+  if (!o.lv[L].haveDiv) buildDiv(o, L);
+  const double* u[3] = {u0, u1, u2};
+  double* v[3] = {v0, v1, v2};
+  for (int k = 0; k < 3; ++k) orc_p2_apply(h, L, u[k], v[k]);
+  const int64_t np = (int64_t)o.lv[L].nodes.size();
+  for (int64_t i = 0; i < np; ++i) q[i] = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    const Csr& D = o.lv[L].Div[k];
+    for (int64_t i = 0; i < np; ++i)
+      for (int64_t m = D.ptr[i]; m < D.ptr[i + 1]; ++m) {
+        q[i] += D.val[m] * u[k][D.col[m]];
+        v[k][D.col[m]] += D.val[m] * p[i];
+      }
+  }
+}
+
+void orc_p2p1_div_element(const double* coords12, double* D120) {
+  double p[4][3];
+  for (int m = 0; m < 4; ++m)
+    for (int d = 0; d < 3; ++d) p[m][d] = coords12[3 * m + d];
+  double D[3][4][10];
+  p2p1DivElement(p, D);
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 10; ++j) D120[40 * k + 10 * i + j] = D[k][i][j];
 }
 
 // fine (nodes of level Lc + 2) = P coarse (nodes of level Lc + 1), or += with add

@@ -47,6 +47,8 @@ def _load_oracle():
         "orc_p2_prolongate": (None, [c_void_p, c_int, P(c_double), P(c_double), c_int]),
         "orc_p2_restrict": (None, [c_void_p, c_int, P(c_double), P(c_double)]),
         "orc_p2_cg": (c_int, [c_void_p, c_int, P(c_double), P(c_double), c_int, c_double]),
+        "orc_stokes_apply": (None, [c_void_p, c_int] + [P(c_double)] * 8),
+        "orc_p2p1_div_element": (None, [P(c_double), P(c_double)]),
         "orc_cell_local_stencil": (None, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, P(c_double)]),
     }
     for name, (res, args) in sig.items():
@@ -80,8 +82,11 @@ def ref_lib():
     r.ref_p1_tet_diffusion.argtypes = [d, d]
     r.ref_p1_tet_mass.argtypes = [d, d]
     r.ref_p2_tet_diffusion.argtypes = [d, d]
+    r.ref_p2_to_p1_div.argtypes = [d, c_int, d]
+    r.ref_p1_to_p2_divt.argtypes = [d, c_int, d]
     for f in (r.ref_apply_cell, r.ref_sor_cell, r.ref_apply_face, r.ref_restrict_cell, r.ref_prolongate_cell,
-              r.ref_p1_tet_diffusion, r.ref_p1_tet_mass, r.ref_p2_tet_diffusion):
+              r.ref_p1_tet_diffusion, r.ref_p1_tet_mass, r.ref_p2_tet_diffusion, r.ref_p2_to_p1_div,
+              r.ref_p1_to_p2_divt):
         f.restype = None
     return r
 
@@ -206,6 +211,16 @@ class Oracle:
         lib().orc_p2_cg(self.h, L, dp(x), dp(b), max_iter, tol)
         return x
 
+    def stokes_apply(self, L, u, p):
+        """Taylor-Hood Stokes of P2 level L: u = three velocity vectors (nodes of level L + 1), p the
+        pressure (nodes of level L); returns (v, q) with v_k = A u_k + D_k^T p, q = sum_k D_k u_k."""
+        u = [np.ascontiguousarray(x, dtype=np.float64) for x in u]
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        v = [np.zeros(self.n(L + 1)) for _ in range(3)]
+        q = np.zeros(self.n(L))
+        lib().orc_stokes_apply(self.h, L, dp(u[0]), dp(u[1]), dp(u[2]), dp(p), dp(v[0]), dp(v[1]), dp(v[2]), dp(q))
+        return v, q
+
     def cell_local_stencil(self, L, cell, x, y, z, form=0):
         out = np.zeros(15)
         lib().orc_cell_local_stencil(self.h, L, cell, x, y, z, form, dp(out))
@@ -218,6 +233,14 @@ def p2_element_laplace(coords4x3):
     K = np.zeros(100)
     lib().orc_p2_element_laplace(dp(c), dp(K))
     return K.reshape(10, 10)
+
+
+def p2p1_div_element(coords4x3):
+    """Taylor-Hood divergence element [3][4][10] (P1 vertex, P2 node in the oracle's order)."""
+    c = np.ascontiguousarray(coords4x3, dtype=np.float64).reshape(12)
+    D = np.zeros(120)
+    lib().orc_p2p1_div_element(dp(c), dp(D))
+    return D.reshape(3, 4, 10)
 
 
 def element_laplace(coords4x3):

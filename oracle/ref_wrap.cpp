@@ -9,6 +9,8 @@
 #include "hyteg/forms/form_fenics_generated/p1_tet_diffusion.h"
 #include "hyteg/forms/form_fenics_generated/p1_tet_mass.h"
 #include "hyteg/forms/form_fenics_generated/p2_tet_diffusion.h"
+#include "hyteg/forms/form_fenics_generated/p2_to_p1_tet_div_tet.h"
+#include "hyteg/forms/form_fenics_generated/p1_to_p2_tet_divt_tet.h"
 #include "hyteg/gridtransferoperators/generatedKernels/prolongate_3D_macrocell_P1_push_additive.hpp"
 #include "hyteg/gridtransferoperators/generatedKernels/restrict_3D_macrocell_P1_pull_additive.hpp"
 #include "hyteg/p1functionspace/generatedKernels/apply_3D_macrocell_vertexdof_to_vertexdof_add.hpp"
@@ -86,6 +88,34 @@ void ref_p1_tet_diffusion(const double* coords12, double* K16) {
 void ref_p1_tet_mass(const double* coords12, double* K16) {
   p1_tet_mass_cell_integral_0_otherwise f;
   f.tabulate_tensor(K16, nullptr, coords12, 0);
+}
+
+// Divergence P2 -> P1 (component k; 4 x 10) and its transpose form P1 -> P2 (10 x 4) of the
+// reference's FEniCS forms (P2P1TaylorHoodStokesOperator div / divT), UFC local node order.
+void ref_p2_to_p1_div(const double* coords12, int k, double* A40) {
+  if (k == 0) {
+    p2_to_p1_tet_div_tet_cell_integral_0_otherwise f;
+    f.tabulate_tensor(A40, nullptr, coords12, 0);
+  } else if (k == 1) {
+    p2_to_p1_tet_div_tet_cell_integral_1_otherwise f;
+    f.tabulate_tensor(A40, nullptr, coords12, 0);
+  } else {
+    p2_to_p1_tet_div_tet_cell_integral_2_otherwise f;
+    f.tabulate_tensor(A40, nullptr, coords12, 0);
+  }
+}
+
+void ref_p1_to_p2_divt(const double* coords12, int k, double* A40) {
+  if (k == 0) {
+    p1_to_p2_tet_divt_tet_cell_integral_0_otherwise f;
+    f.tabulate_tensor(A40, nullptr, coords12, 0);
+  } else if (k == 1) {
+    p1_to_p2_tet_divt_tet_cell_integral_1_otherwise f;
+    f.tabulate_tensor(A40, nullptr, coords12, 0);
+  } else {
+    p1_to_p2_tet_divt_tet_cell_integral_2_otherwise f;
+    f.tabulate_tensor(A40, nullptr, coords12, 0);
+  }
 }
 
 // P2 Laplace element matrix of the reference's FEniCS form (10 x 10, UFC local node order).

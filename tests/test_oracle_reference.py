@@ -268,3 +268,22 @@ def test_p2_laplace_annihilates_constants_and_linears(name, oracle_mod):
     rng = np.random.default_rng(1)
     a, b = rng.uniform(-1, 1, len(xyz)), rng.uniform(-1, 1, len(xyz))
     assert abs(a @ o.p2_apply(L, b) - b @ o.p2_apply(L, a)) < 1e-11
+
+
+def test_p2p1_divergence_element_matches_reference_forms(ref, oracle_mod):
+    # p2_to_p1_tet_div_tet (div) and p1_to_p2_tet_divt_tet (its transpose) of the reference's forms
+    perm = [0, 1, 2, 3, 9, 8, 7, 6, 5, 4]
+    rng = np.random.default_rng(13)
+    for _ in range(4):
+        c = rng.uniform(-1, 1, (4, 3))
+        D = oracle_mod.p2p1_div_element(c)
+        cc = np.ascontiguousarray(c.reshape(12))
+        for k in range(3):
+            A = np.zeros(40)
+            ref.ref_p2_to_p1_div(oracle_mod.dp(cc), k, oracle_mod.dp(A))
+            A = A.reshape(4, 10)[:, perm]
+            B = np.zeros(40)
+            ref.ref_p1_to_p2_divt(oracle_mod.dp(cc), k, oracle_mod.dp(B))
+            B = B.reshape(10, 4)[perm, :]
+            assert np.abs(D[k] - A).max() <= 1e-13 * np.abs(A).max()
+            assert np.abs(D[k].T - B).max() <= 1e-13 * np.abs(B).max()
