@@ -343,6 +343,35 @@ def p2_kernels(hg, st, L2, timed):
             "vcycle": {"ms": t_cycle * 1e3, "gdofs": n_in / t_cycle / 1e9}}
 
 
+def stokes_bench(hg, st, L2):
+    """P2-P1 Taylor-Hood lid-driven cavity on P2 level L2 of the same cube (velocity on the
+    vertex lattice L2 + 1, pressure on L2): MINRES to 1e-8 with the block-diagonal multigrid
+    preconditioner (symmetric P2 V(2,2) per velocity component, lumped P1 mass), the V-cycles in
+    FP64 and in FP32 (mixed); residual and update in FP64."""
+    import torch
+    xyz, _ = st.host().slot_info(L2 + 1)
+    lid = np.where(np.abs(xyz[:, 2] - 1.0) < 1e-12, 1.0, 0.0)
+    S = hg.P2P1TaylorHoodStokesOperator(st, 0, L2)
+    out = {"p2_level": L2, "velocity_dofs": 3 * inner_dofs(L2 + 1), "pressure_dofs": (2 * 2 ** L2 + 1) ** 3,
+           "problem": "lid-driven cavity, u = (1,0,0) on z = 1, no slip elsewhere, zero-mean pressure"}
+    sol = {}
+    for name, dt in (("fp64", np.float64), ("mixed", np.float32)):
+        u = [hg.P2Function("su%d" % k, st, 0, L2) for k in range(3)]
+        f = [hg.P2Function("sf%d" % k, st, 0, L2) for k in range(3)]
+        p, g = hg.P1Function("sp", st, 0, L2), hg.P1Function("sg", st, 0, L2)
+        u[0].from_numpy(L2, lid)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it, rel, _ = S.minres(u, p, f, g, L2, nu=2, max_iter=500, tol=1e-8, precondition_dtype=dt)
+        torch.cuda.synchronize()
+        out[name] = {"iterations": it, "seconds": time.perf_counter() - t0, "rel_residual": rel}
+        sol[name] = [x.to_numpy(L2) for x in u]
+    out["speedup_mixed_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
+    out["max_velocity_difference_mixed_vs_fp64"] = float(max(np.abs(a - b).max() for a, b in zip(sol["fp64"],
+                                                                                                   sol["mixed"])))
+    return out
+
+
 def fp32_kernels(hg, st, A, x, b, L, Inner, N_in, Nc, timed):
     """The same kernels on FP32 copies of the vectors (the arithmetic of the inner cycles of the
     mixed-precision solve), and one FP32 V(3,3) cycle. Algorithmic bytes are half the FP64 ones."""
@@ -506,6 +535,7 @@ def run_ours(args):
     kernels["fp32"] = fp32_kernels(hg, st, A, x, b, L, Inner, N_in, Nc, timed)
     if L >= 3:
         kernels["p2"] = p2_kernels(hg, st, L - 2, timed)
+        kernels["stokes"] = stokes_bench(hg, st, min(L - 2, 4))
 
     # --- time to solution: FP64 GMG vs mixed precision (FP32 cycles inside FP64 defect correction)
     solve = time_to_solution(hg, st, A, L, N_in, Inner)

@@ -628,16 +628,18 @@ class P2P1TaylorHoodStokesOperator:
         call("hg_p2p1_stokes_apply", self.storage.handle, self.id, ui, p.id, vi, q.id, level, flagVelocity,
              flagPressure)
 
-    def minres(self, u, p, f, g, level, nu=2, max_iter=500, tol=1e-8):
+    def minres(self, u, p, f, g, level, nu=2, max_iter=500, tol=1e-8, precondition_dtype=np.float64):
         """MinResSolver with the block-diagonal preconditioner (symmetric P2 V(nu, nu) per velocity
-        component, lumped P1 mass on the pressure). Returns (iterations, relative residual, history)."""
+        component, lumped P1 mass on the pressure); precondition_dtype float32 runs the V-cycles in
+        FP32 inside the FP64 iteration. Returns (iterations, relative residual, history)."""
         ui = (ctypes.c_int * 3)(*[x.id for x in u])
         fi = (ctypes.c_int * 3)(*[x.id for x in f])
         it = ctypes.c_int()
         rel = ctypes.c_double()
         hist = np.zeros(max_iter)
-        call("hg_p2p1_stokes_minres", self.storage.handle, self.id, ui, p.id, fi, g.id, level, int(nu), int(max_iter),
-             float(tol), ctypes.byref(it), ctypes.byref(rel), dptr(hist), int(max_iter))
+        prec = {np.dtype(np.float64): 8, np.dtype(np.float32): 4}[np.dtype(precondition_dtype)]
+        call("hg_p2p1_stokes_minres_mixed", self.storage.handle, self.id, ui, p.id, fi, g.id, level, int(nu),
+             int(max_iter), float(tol), prec, ctypes.byref(it), ctypes.byref(rel), dptr(hist), int(max_iter))
         return it.value, rel.value, hist[: it.value].copy()
 
     def __del__(self):

@@ -104,6 +104,8 @@ _SIGS = {
     "hg_p2p1_stokes_apply": (c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), c_int, c_int, c_uint, c_uint]),
     "hg_p2p1_stokes_minres": (c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), c_int, c_int, c_int, c_int, c_double,
                                       P(c_int), P(c_double), P(c_double), c_int]),
+    "hg_p2p1_stokes_minres_mixed": (c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), c_int, c_int, c_int, c_int,
+                                            c_double, c_int, P(c_int), P(c_double), P(c_double), c_int]),
     "hg_server_create": (c_int, [c_int, c_int64, c_int, P(c_void_p)]),
     "hg_server_destroy": (c_int, [c_void_p]),
     "hg_server_prewarm": (c_int, [c_void_p, c_int, c_int]),

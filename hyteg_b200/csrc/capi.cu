@@ -792,6 +792,17 @@ int hg_p2p1_stokes_minres(hg_storage* h, int op, const int u[3], int p, const in
   HG_CATCH
 }
 
+int hg_p2p1_stokes_minres_mixed(hg_storage* h, int op, const int u[3], int p, const int f[3], int g, int level, int nu,
+                                int max_iter, double tol, int precondition_precision, int* iterations,
+                                double* rel_residual, double* history, int history_cap) {
+  HG_TRY
+  hg::argCheck(u && f && tol > 0.0 && max_iter >= 0 && nu >= 0, "invalid arguments");
+  const int n = hg::stokesMinres(S(h), op, u, p, f, g, level, nu, max_iter, tol, rel_residual, history, history_cap,
+                                 precondition_precision);
+  if (iterations) *iterations = n;
+  HG_CATCH
+}
+
 struct hg_server {
   hg::Server* s;
 };

@@ -247,20 +247,27 @@ void Gmg::solve(int x, int b, int L) {
   runCycle(x, b, L);
 }
 
-P2Gmg::P2Gmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int post_, double omega_, int cmax, double ctol)
+P2Gmg::P2Gmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int post_, double omega_, int cmax, double ctol,
+             int prec_)
     : s(st), op(op_), minL(minL_), maxL(maxL_), pre(pre_), post(post_), omega(omega_), coarseMaxIter(cmax),
-      coarseTol(ctol) {
+      coarseTol(ctol), prec(prec_) {
   P2Operator& o = s.p2op(op);
   argCheck(minL >= o.minL && maxL <= o.maxL && minL <= maxL, "P2 multigrid: levels outside the operator's range");
-  tmp = s.createFunction(minL + 1, maxL + 1, 8);
+  argCheck(prec == 8 || prec == 4, "P2 multigrid: precision must be 8 or 4");
+  tmp = s.createFunction(minL + 1, maxL + 1, prec);
   cp = s.createFunction(minL + 1, minL + 1, 8);
   cz = s.createFunction(minL + 1, minL + 1, 8);
   cap = s.createFunction(minL + 1, minL + 1, 8);
   cr = s.createFunction(minL + 1, minL + 1, 8);
+  if (prec == 4) {
+    cx64 = s.createFunction(minL + 1, minL + 1, 8);
+    cb64 = s.createFunction(minL + 1, minL + 1, 8);
+  }
 }
 
 P2Gmg::~P2Gmg() {
-  for (int id : {tmp, cp, cz, cap, cr}) s.fns.erase(id);
+  for (int id : {tmp, cp, cz, cap, cr, cx64, cb64})
+    if (id >= 0) s.fns.erase(id);
 }
 
 // CGSolver (CGSolver.hpp:69-150, identity preconditioner) with the P2 operator of level L.
@@ -295,7 +302,14 @@ int P2Gmg::coarseCg(int x, int b, int L) {
 void P2Gmg::solveRecursively(int x, int b, int L) {
   const unsigned flag = HG_INNER | HG_NEUMANN;
   if (L == minL) {
-    coarseCg(x, b, L);
+    if (prec == 8) {
+      coarseCg(x, b, L);
+    } else {  // FP32 cycle: the coarse problem in FP64, rounded back
+      s.copyCast(cb64, b, L + 1, HG_ALL, false);
+      s.copyCast(cx64, x, L + 1, HG_ALL, false);
+      coarseCg(cx64, cb64, L);
+      s.copyCast(x, cx64, L + 1, HG_ALL, false);
+    }
     return;
   }
   for (int i = 0; i < pre; ++i) s.p2Sor(op, x, b, omega, L, flag, false);
@@ -310,7 +324,7 @@ void P2Gmg::solveRecursively(int x, int b, int L) {
 }
 
 int stokesMinres(Storage& s, int op, const int u[3], int p, const int f[3], int g, int L, int nu, int maxIter,
-                 double tol, double* relRes, double* history, int historyCap) {
+                 double tol, double* relRes, double* history, int historyCap, int precondPrec) {
   const unsigned fv = HG_INNER | HG_NEUMANN, fp = HG_ALL;
   const int Lv = L + 1, Lp = L;
   std::vector<int> made;
@@ -359,17 +373,22 @@ int stokesMinres(Storage& s, int op, const int u[3], int p, const int f[3], int 
   s.lincomb(ones, Lp, fp, 0, nullptr, nullptr, false, 1.0);
   s.apply(mass, ones, lumped, Lp, fp, 0);
   const double nP = s.dot(ones, ones, Lp, fp);
-  P2Gmg mg(s, op, 0, L, nu, nu, 1.0, 1000, 1e-14);
+  argCheck(precondPrec == 8 || precondPrec == 4, "preconditioner precision must be 8 or 4");
+  P2Gmg mg(s, op, 0, L, nu, nu, 1.0, 1000, 1e-14, precondPrec);
   mg.symmetric = true;
-  const int px = fnV(1), pb = fnV(1);
+  // the V-cycle's own x and b (FP32 for a mixed-precision preconditioner; cast at level L)
+  const int px = s.createFunction(1, Lv, precondPrec), pb = s.createFunction(1, Lv, precondPrec);
+  made.push_back(px);
+  made.push_back(pb);
   auto precond = [&](const Blk& src, const Blk& dst) {
     const double one = 1.0;
     for (int k = 0; k < 3; ++k) {
-      s.lincomb(pb, Lv, fv, 1, &one, &src.u[k], false, 0.0);
+      s.copyCast(pb, src.u[k], Lv, fv, false);
       for (int l = 1; l <= Lv; ++l) s.lincomb(px, l, HG_ALL, 0, nullptr, nullptr, false, 0.0);
       mg.solveRecursively(px, pb, L);
-      s.lincomb(dst.u[k], Lv, fv, 1, &one, &px, false, 0.0);
+      s.copyCast(dst.u[k], px, Lv, fv, false);
     }
+    (void)one;
     s.divideBy(dst.p, src.p, lumped, Lp, fp);
     const double mean = s.dot(dst.p, ones, Lp, fp) / nP;
     s.lincomb(dst.p, Lp, fp, 1, &one, &dst.p, false, -mean);

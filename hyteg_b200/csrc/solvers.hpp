@@ -55,7 +55,7 @@ struct Gmg {
 // of level L + 1): multicolour P2 SOR, quadratic transfers, CG on the coarsest level; FP64.
 struct P2Gmg {
   P2Gmg(Storage& s, int op, int minL, int maxL, int pre, int post, double omega, int coarseMaxIter,
-        double coarseTol);
+        double coarseTol, int prec = 8);
   ~P2Gmg();
   void solveRecursively(int x, int b, int L);
   int solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap);
@@ -67,6 +67,8 @@ struct P2Gmg {
   int coarseMaxIter;
   double coarseTol;
   int tmp, cp, cz, cap, cr;
+  int prec = 8;                      // precision of the cycle (4: FP32 hierarchy, coarse CG in FP64)
+  int cx64 = -1, cb64 = -1;          // FP64 coarse-level copies for an FP32 cycle
   bool symmetric = false;  // post-smoothing with backward sweeps (a symmetric cycle)
 };
 
@@ -77,6 +79,6 @@ struct P2Gmg {
 // unknown; the pressure is returned with zero mean. Returns the iterations; relRes is the
 // preconditioned residual norm relative to the initial one.
 int stokesMinres(Storage& s, int op, const int u[3], int p, const int f[3], int g, int L, int nu, int maxIter,
-                 double tol, double* relRes, double* history, int historyCap);
+                 double tol, double* relRes, double* history, int historyCap, int precondPrec = 8);
 
 }  // namespace hg

@@ -214,6 +214,12 @@ int hg_p2p1_stokes_apply(hg_storage* s, int op, const int u[3], int p, const int
 int hg_p2p1_stokes_minres(hg_storage* s, int op, const int u[3], int p, const int f[3], int g, int level, int nu,
                           int max_iter, double tol, int* iterations, double* rel_residual, double* history,
                           int history_cap);
+/* The same with the preconditioner's V-cycles in FP32 (precondition_precision 4: FP32 storage and
+ * arithmetic inside the cycles, coarse CG in FP64) while MINRES, the operator and the residual
+ * stay FP64; precondition_precision 8 equals hg_p2p1_stokes_minres. */
+int hg_p2p1_stokes_minres_mixed(hg_storage* s, int op, const int u[3], int p, const int f[3], int g, int level, int nu,
+                                int max_iter, double tol, int precondition_precision, int* iterations,
+                                double* rel_residual, double* history, int history_cap);
 /* P2 geometric multigrid (GeometricMultigridSolver with P2ConstantLaplaceOperator, the P2 SOR
  * above, the quadratic transfers and CG on min_level), FP64. x, b: P2 functions covering
  * [min_level, max_level]. solve: one cycle; solve_to: cycles to the relative residual tol. */

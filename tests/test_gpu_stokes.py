@@ -134,3 +134,26 @@ def test_minres_converges_on_level_2(env):
         vv = v[k].to_numpy(L)
         assert np.abs(vv[maps[L + 1][1] == 1]).max() < 1e-6
     assert np.abs(q.to_numpy(L)).max() < 1e-6
+
+
+def test_minres_with_fp32_preconditioner_matches_fp64(env):
+    st, orc, maps = env
+    L = 2
+    S = hg.P2P1TaylorHoodStokesOperator(st, 0, LMAX)
+    xyz = maps[L + 1][2]
+    lid = np.where(np.abs(xyz[:, 2] - 1.0) < 1e-12, 1.0, 0.0)
+    out = {}
+    for dt in (np.float64, np.float32):
+        u, p = funcs(st)
+        f, g = funcs(st)
+        u[0].from_numpy(L, lid)
+        it, relres, _ = S.minres(u, p, f, g, L, nu=2, max_iter=300, tol=1e-10, precondition_dtype=dt)
+        assert relres <= 1e-10
+        out[dt] = (it, [x.to_numpy(L) for x in u], p.to_numpy(L))
+    (i64, u64, p64), (i32, u32, p32) = out[np.float64], out[np.float32]
+    assert i32 <= i64 + 10
+    m = maps[L + 1][1] == 1
+    for k in range(3):
+        assert np.abs(u32[k][m] - u64[k][m]).max() < 1e-8
+    mp = maps[L][1] == 1
+    assert np.abs(p32[mp] - p64[mp]).max() / np.abs(p64[mp]).max() < 1e-7
