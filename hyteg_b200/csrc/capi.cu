@@ -160,6 +160,16 @@ int hg_storage_set_sor_schedule(hg_storage* h, int schedule) {
   HG_CATCH
 }
 
+int hg_storage_autotune_sor(hg_storage* h, int min_level, int max_level, int precision, int reps, double* ms,
+                            int* chosen) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  s.autotuneSor(min_level, max_level, precision, reps, ms);
+  if (chosen)
+    for (int L = min_level; L <= max_level; ++L) chosen[L - min_level] = s.sorScheduleLevel[2 * L + (precision == 4)];
+  HG_CATCH
+}
+
 int hg_primitive_vertices(const hg_storage* h, int kind, int prim, int ids[4], double coords[3], int* flag) {
   HG_TRY
   const auto& t = S(h).disc.topo();

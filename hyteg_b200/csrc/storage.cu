@@ -950,6 +950,48 @@ void Storage::stokesApply(int opId, const int u[3], int p, const int v[3], int q
     stokesCoupling<float>(*this, o, u, p, v, q, L, maskV, maskP);
 }
 
+void Storage::autotuneSor(int minL, int maxL, int prec, int reps, double* ms) {
+  argCheck(minL >= 0 && maxL <= maxLevel() && minL <= maxL, "autotune: invalid level range");
+  argCheck(prec == 8 || prec == 4, "autotune: precision must be 8 or 4");
+  argCheck(reps >= 1 && reps <= 100, "autotune: repetitions in [1, 100]");
+  if ((int)sorScheduleLevel.size() < 2 * (maxLevel() + 1)) sorScheduleLevel.assign(2 * (maxLevel() + 1), -1);
+  const int pi = prec == 4 ? 1 : 0;
+  const int op = createOperator(FORM_LAPLACE, minL, maxL);
+  cudaEvent_t e0, e1;
+  cudaCheck(cudaEventCreate(&e0), "event");
+  cudaCheck(cudaEventCreate(&e1), "event");
+  for (int L = minL; L <= maxL; ++L) {
+    const int x = createFunction(L, L, prec), b = createFunction(L, L, prec);
+    fillRandom(x, L, HG_ALL, 1, -1.0, 1.0);
+    fillRandom(b, L, HG_ALL, 2, -1.0, 1.0);
+    double best = 0;
+    int pick = 0;
+    for (int sch = 0; sch < 2; ++sch) {
+      sorScheduleLevel[2 * L + pi] = sch;
+      smoothSor(op, x, b, 1.0, L, HG_INNER | HG_NEUMANN, false);  // warm-up (allocates the spare)
+      cudaCheck(cudaEventRecord(e0, stream), "event");
+      for (int r = 0; r < reps; ++r) smoothSor(op, x, b, 1.0, L, HG_INNER | HG_NEUMANN, false);
+      cudaCheck(cudaEventRecord(e1, stream), "event");
+      cudaCheck(cudaEventSynchronize(e1), "event");
+      float t = 0;
+      cudaCheck(cudaEventElapsedTime(&t, e0, e1), "event");
+      const double per = t / reps;
+      if (ms) ms[2 * (L - minL) + sch] = per;
+      if (sch == 0 || per < best) {
+        best = per;
+        pick = sch;
+      }
+    }
+    sorScheduleLevel[2 * L + pi] = pick;
+    fns.erase(x);
+    fns.erase(b);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ops.erase(op);
+  ++generation;
+}
+
 void Storage::reassembleOperator(int id) {
   Operator& o = op(id);
   for (int L = o.minL; L <= o.maxL; ++L) {
@@ -1089,7 +1131,10 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
   // budget), so the re-reads of the later colours hit L2
   auto cellPhase = [&](bool rev) {
     if (!lv.nCellBlocks || !(kinds & (1 << KC))) return;
-    if (sorSchedule == 0 && ld.nWaveTiles) {
+    const int tuned = 2 * L + (sizeof(T) == 4 ? 1 : 0);
+    const int schedule = (int)sorScheduleLevel.size() > tuned && sorScheduleLevel[tuned] >= 0 ? sorScheduleLevel[tuned]
+                                                                                                  : sorSchedule;
+    if (schedule == 0 && ld.nWaveTiles) {
       // one pass into the spare buffer of this level, which then becomes the function's buffer
       Function& fd = fn(dstId);
       std::unique_ptr<DevBuf>& cur = fd.levels[L - fd.minL];

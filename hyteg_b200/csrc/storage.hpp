@@ -109,6 +109,10 @@ struct Storage {
   // Cell-phase schedule of the multicolour SOR: 0 = one wavefront pass that writes a second
   // buffer which then replaces the level buffer, 1 = four in-place colour passes.
   int sorSchedule = 0;
+  std::vector<int> sorScheduleLevel;  // [2 L + (FP32 ? 1 : 0)]: schedule chosen by autotuneSor (-1: sorSchedule)
+  // Times both schedules of one SOR sweep on levels [minL, maxL] in the given precision and keeps
+  // the faster per level; ms[2 * (L - minL) + s] receives the measured times (nullable).
+  void autotuneSor(int minL, int maxL, int prec, int reps, double* ms);
   unsigned long long generation = 0;  // bumped when level tables or schedules change (captured graphs)
   std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> spare;  // (level, precision) -> buffer
   dev::Geometry geom{};              // macro-vertex coordinates and primitive vertex lists (device)

@@ -99,6 +99,13 @@ int hg_storage_set_cell_coefficients(hg_storage* s, const double* k, int ncells)
  * the four colours, written to a second buffer of the level that then replaces the smoothed
  * function's buffer), 1 = four in-place colour passes. Both give the same multicolour sweep. */
 int hg_storage_set_sor_schedule(hg_storage* s, int schedule);
+/* Autotuner (no counterpart in the reference): times one multicolour SOR sweep under both
+ * schedules on every level in [min_level, max_level] (precision 8 or 4, `reps` timed sweeps after
+ * one warm-up, CUDA events on the storage's stream) and keeps the faster schedule per level,
+ * and precision, overriding hg_storage_set_sor_schedule there. ms (nullable): 2 * (levels) times in ms, schedule
+ * 0 then 1 per level; chosen (nullable): the schedule kept per level. */
+int hg_storage_autotune_sor(hg_storage* s, int min_level, int max_level, int precision, int reps, double* ms,
+                            int* chosen);
 /* Topology export: for kind HG_VERTEX ids[0..2]=unused, coords[3]; HG_EDGE ids[2]; HG_FACE ids[3];
  * HG_CELL ids[4]; flag = mesh boundary flag. */
 int hg_primitive_vertices(const hg_storage* s, int kind, int prim, int ids[4], double coords[3], int* flag);

@@ -70,3 +70,26 @@ def test_device_coarse_cg_against_oracle_on_3x3x3_cube(gpu):
     got = H.gather_owned(x.to_numpy(L), node, owned, n)
     inner = ~orc.dirichlet(L)
     assert np.abs(got - ref)[inner].max() / np.abs(ref[inner]).max() < 1e-12
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_autotuned_schedules_give_the_same_cycles(gpu, dtype):
+    L = 5
+    st = hg.PrimitiveStorage.cuboid((0, 0, 0), (1, 1, 1), 2, 2, 2, L)
+    A = hg.P1ConstantLaplaceOperator(st, 0, L)
+    res = []
+    for tune in (False, True):
+        if tune:
+            picks = st.autotune_sor(2, L, dtype=dtype, reps=2)
+            assert set(picks) == set(range(2, L + 1))
+            assert all(c in (0, 1) and t0 > 0 and t1 > 0 for c, t0, t1 in picks.values())
+        x, b = hg.P1Function("x", st, 0, L, dtype=dtype), hg.P1Function("b", st, 0, L, dtype=dtype)
+        b.fill_random(8, L, hg.Inner)
+        gmg = hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 100, 1e-16),
+                                          hg.P1toP1LinearRestriction(), hg.P1toP1LinearProlongation(), 0, L, 3, 3,
+                                          dtype=dtype)
+        for _ in range(3):
+            gmg.solve(A, x, b, L)
+        res.append(x.to_numpy(L).astype(np.float64))
+    tol = 1e-12 if dtype == np.float64 else 1e-5
+    assert np.abs(res[0] - res[1]).max() / np.abs(res[0]).max() < tol
