@@ -411,6 +411,11 @@ class P1ConstantMassOperator(_P1ConstantOperator):
     FORM = 1
 
 
+class P1PSPGOperator(_P1ConstantOperator):
+    """-tau grad p . grad q with tau = |T|^(2/3) / 12 per micro-cell (pressure stabilisation)."""
+    FORM = 2
+
+
 class P1toP1LinearRestriction:
     def restrict(self, function, sourceLevel, flag):
         call("hg_restrict", function.storage.handle, function.id, sourceLevel, flag)
@@ -592,7 +597,8 @@ class P2toP2QuadraticRestriction:
 
 class P2GeometricMultigridSolver:
     """GeometricMultigridSolver for P2ConstantLaplaceOperator: multicolour P2 SOR, quadratic
-    transfers, CG on the coarsest level (FP64)."""
+    transfers, an exact solve on the coarsest level (CG when it has more than 1024 unknowns);
+    FP64. Cycles are replayed from captured CUDA graphs unless set_graphs(False)."""
 
     def __init__(self, storage, A, minLevel, maxLevel, preSmoothSteps=3, postSmoothSteps=3, relax=1.0,
                  coarseMaxIter=1000, coarseTolerance=1e-16):
@@ -604,6 +610,9 @@ class P2GeometricMultigridSolver:
 
     def solve(self, x, b, level):
         call("hg_p2_gmg_solve", self.storage.handle, self.id, x.id, b.id, level)
+
+    def set_graphs(self, enable):
+        call("hg_p2_gmg_set_graphs", self.storage.handle, self.id, 1 if enable else 0)
 
     def solve_to(self, x, b, level, tol, max_iter=100):
         it = ctypes.c_int()
@@ -659,6 +668,77 @@ class P2P1TaylorHoodStokesOperator:
                 _capi.lib.hg_p2_operator_destroy(st.handle, self.id)
         except (AttributeError, TypeError):  # interpreter shutdown
             pass
+
+
+class UzawaSmoother:
+    """UzawaSmoother for P2P1TaylorHoodStokesOperator (block-Laplace variant without stabilisation):
+    r_u = f - D^T p; numGSIterationsVelocity forward P2 SOR sweeps (omega 1) per velocity
+    component; p += relaxParam (g - D u) / diag(PSPG). Velocity DoFs flagged Inner | Neumann are
+    unknowns, every pressure DoF is one. solve(u, p, f, g, level) is one smoothing step."""
+
+    def __init__(self, storage, S, minLevel, maxLevel, relaxParam, numGSIterationsVelocity=2):
+        self.storage, self.S = storage, S
+        self.minLevel, self.maxLevel = minLevel, maxLevel
+        self.relax, self.sweeps = float(relaxParam), int(numGSIterationsVelocity)
+        self._native = _StokesUzawaGmg(storage, S, minLevel, maxLevel, 0, 0, self.relax, self.sweeps)
+
+    def solve(self, u, p, f, g, level):
+        ui = (ctypes.c_int * 3)(*[x.id for x in u])
+        fi = (ctypes.c_int * 3)(*[x.id for x in f])
+        call("hg_p2p1_stokes_uzawa_smooth", self.storage.handle, self._native.id, ui, p.id, fi, g.id, level)
+
+
+def estimateUzawaRelaxationParameter(storage, S, level, numPowerIterations=20, numGSIterationsVelocity=2, seed=42):
+    """estimateUzawaRelaxationParameter: the spectral radius of M_lumped^-1 D S D^T (S: the Uzawa
+    smoother's velocity sweeps from zero) by power iterations from seeded uniform [0, 1) values."""
+    native = _StokesUzawaGmg(storage, S, level, level, 0, 0, 1.0, numGSIterationsVelocity)
+    w = ctypes.c_double()
+    call("hg_p2p1_stokes_uzawa_estimate_omega", storage.handle, native.id, level, int(numPowerIterations),
+         ctypes.c_uint64(seed), ctypes.byref(w))
+    return w.value
+
+
+class _StokesUzawaGmg:
+    def __init__(self, storage, S, minLevel, maxLevel, pre, post, relax, sweeps):
+        self.storage = storage
+        h = ctypes.c_int()
+        call("hg_p2p1_stokes_uzawa_gmg_create", storage.handle, S.id, minLevel, maxLevel, int(pre), int(post),
+             float(relax), int(sweeps), ctypes.byref(h))
+        self.id = h.value
+
+    def __del__(self):
+        try:
+            st = getattr(self, "storage", None)
+            if st is not None and st.handle:
+                _capi.lib.hg_p2p1_stokes_uzawa_gmg_destroy(st.handle, self.id)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+
+
+class StokesGeometricMultigridSolver:
+    """GeometricMultigridSolver for P2P1TaylorHoodStokesOperator with an UzawaSmoother and the
+    P2P1StokesToP2P1Stokes restriction / prolongation (quadratic velocity, linear pressure); the
+    coarsest level is solved by the pseudo-inverse of the operator on its unknowns."""
+
+    def __init__(self, storage, S, smoother, minLevel, maxLevel, preSmoothSteps=2, postSmoothSteps=2):
+        self.storage = storage
+        self._native = _StokesUzawaGmg(storage, S, minLevel, maxLevel, preSmoothSteps, postSmoothSteps,
+                                       smoother.relax, smoother.sweeps)
+
+    def solve(self, u, p, f, g, level):
+        ui = (ctypes.c_int * 3)(*[x.id for x in u])
+        fi = (ctypes.c_int * 3)(*[x.id for x in f])
+        call("hg_p2p1_stokes_uzawa_gmg_solve", self.storage.handle, self._native.id, ui, p.id, fi, g.id, level)
+
+    def solve_to(self, u, p, f, g, level, tol, max_iter=100):
+        ui = (ctypes.c_int * 3)(*[x.id for x in u])
+        fi = (ctypes.c_int * 3)(*[x.id for x in f])
+        it = ctypes.c_int()
+        rel = ctypes.c_double()
+        hist = np.zeros(max_iter)
+        call("hg_p2p1_stokes_uzawa_gmg_solve_to", self.storage.handle, self._native.id, ui, p.id, fi, g.id, level,
+             float(tol), int(max_iter), ctypes.byref(it), ctypes.byref(rel), dptr(hist), int(max_iter))
+        return it.value, rel.value, hist[: it.value].copy()
 
 
 class SolveServer:

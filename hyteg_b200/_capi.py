@@ -99,6 +99,15 @@ _SIGS = {
     "hg_p2_gmg_create": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, c_int, c_double, P(c_int)]),
     "hg_p2_gmg_destroy": (c_int, [c_void_p, c_int]),
     "hg_p2_gmg_solve": (c_int, [c_void_p, c_int, c_int, c_int, c_int]),
+    "hg_p2_gmg_set_graphs": (c_int, [c_void_p, c_int, c_int]),
+    "hg_p2p1_stokes_uzawa_gmg_create": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_double, c_int,
+                                                 P(c_int)]),
+    "hg_p2p1_stokes_uzawa_gmg_destroy": (c_int, [c_void_p, c_int]),
+    "hg_p2p1_stokes_uzawa_smooth": (c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), c_int, c_int]),
+    "hg_p2p1_stokes_uzawa_estimate_omega": (c_int, [c_void_p, c_int, c_int, c_int, ctypes.c_uint64, P(c_double)]),
+    "hg_p2p1_stokes_uzawa_gmg_solve": (c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), c_int, c_int]),
+    "hg_p2p1_stokes_uzawa_gmg_solve_to": (c_int, [c_void_p, c_int, P(c_int), c_int, P(c_int), c_int, c_int, c_double,
+                                                   c_int, P(c_int), P(c_double), P(c_double), c_int]),
     "hg_p2_gmg_solve_to": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_int, P(c_int), P(c_double),
                                    P(c_double), c_int]),
     "hg_p2p1_stokes_create": (c_int, [c_void_p, c_int, c_int, P(c_int)]),

@@ -764,7 +764,7 @@ int hg_p2_gmg_solve(hg_storage* h, int gmg, int x, int b, int level) {
   HG_TRY
   hg::P2Gmg& g = P2G(h, gmg);
   hg::argCheck(level >= g.minL && level <= g.maxL, "level outside the solver's range");
-  g.solveRecursively(x, b, level);
+  g.runCycle(x, b, level);
   HG_CATCH
 }
 
@@ -798,6 +798,65 @@ int hg_p2p1_stokes_minres(hg_storage* h, int op, const int u[3], int p, const in
   HG_TRY
   hg::argCheck(u && f && tol > 0.0 && max_iter >= 0 && nu >= 0, "invalid arguments");
   const int n = hg::stokesMinres(S(h), op, u, p, f, g, level, nu, max_iter, tol, rel_residual, history, history_cap);
+  if (iterations) *iterations = n;
+  HG_CATCH
+}
+
+int hg_p2p1_stokes_uzawa_gmg_create(hg_storage* h, int op, int min_level, int max_level, int pre_smooth,
+                                    int post_smooth, double omega, int velocity_sweeps, int* gmg) {
+  HG_TRY
+  hg::argCheck(gmg != nullptr, "invalid arguments");
+  hg::Storage& s = S(h);
+  const int id = s.nextId++;
+  s.stokesGmgs[id].reset(
+      new hg::StokesGmg(s, op, min_level, max_level, pre_smooth, post_smooth, omega, velocity_sweeps));
+  *gmg = id;
+  HG_CATCH
+}
+
+int hg_p2p1_stokes_uzawa_gmg_destroy(hg_storage* h, int gmg) {
+  HG_TRY
+  S(h).stokesGmgs.erase(gmg);
+  HG_CATCH
+}
+
+static hg::StokesGmg& SG(hg_storage* h, int gmg) {
+  auto& m = S(h).stokesGmgs;
+  auto it = m.find(gmg);
+  hg::argCheck(it != m.end(), "unknown Stokes multigrid handle");
+  return *it->second;
+}
+
+int hg_p2p1_stokes_uzawa_smooth(hg_storage* h, int gmg, const int u[3], int p, const int f[3], int g, int level) {
+  HG_TRY
+  hg::StokesGmg& m = SG(h, gmg);
+  hg::argCheck(u && f && level >= m.minL && level <= m.maxL, "invalid arguments");
+  m.smooth(u, p, f, g, level);
+  HG_CATCH
+}
+
+int hg_p2p1_stokes_uzawa_estimate_omega(hg_storage* h, int gmg, int level, int power_iterations, uint64_t seed,
+                                        double* omega) {
+  HG_TRY
+  hg::argCheck(omega != nullptr, "invalid arguments");
+  *omega = SG(h, gmg).estimateOmega(level, power_iterations, seed);
+  HG_CATCH
+}
+
+int hg_p2p1_stokes_uzawa_gmg_solve(hg_storage* h, int gmg, const int u[3], int p, const int f[3], int g, int level) {
+  HG_TRY
+  hg::StokesGmg& m = SG(h, gmg);
+  hg::argCheck(u && f && level >= m.minL && level <= m.maxL, "invalid arguments");
+  m.solveRecursively(u, p, f, g, level);
+  HG_CATCH
+}
+
+int hg_p2p1_stokes_uzawa_gmg_solve_to(hg_storage* h, int gmg, const int u[3], int p, const int f[3], int g, int level,
+                                      double tol, int max_iter, int* iterations, double* rel_residual, double* history,
+                                      int history_cap) {
+  HG_TRY
+  hg::argCheck(u && f && tol > 0.0 && max_iter >= 0, "invalid arguments");
+  const int n = SG(h, gmg).solveTo(u, p, f, g, level, tol, max_iter, rel_residual, history, history_cap);
   if (iterations) *iterations = n;
   HG_CATCH
 }
@@ -905,6 +964,14 @@ int hg_function_fill_random(hg_storage* h, int fn, int level, unsigned flag, uin
   HG_TRY
   hg::argCheck(lo <= hi, "lo must not exceed hi");
   S(h).fillRandom(fn, level, flag, seed, lo, hi);
+  HG_CATCH
+}
+
+int hg_p2_gmg_set_graphs(hg_storage* h, int gmg, int enable) {
+  HG_TRY
+  hg::P2Gmg& g = P2G(h, gmg);
+  g.graphs = enable != 0;
+  if (!g.graphs) g.cache.clear();
   HG_CATCH
 }
 

@@ -538,6 +538,17 @@ static void cellRow(const Topology& topo, int c, int64_t N, const int64_t p[3], 
       if (form == FORM_LAPLACE) {
         elementLaplace(P, K);
         for (double& k : K) k *= ce.k;
+      } else if (form == FORM_PSPG) {
+        elementLaplace(P, K);
+        double a[3][3];
+        for (int i = 0; i < 3; ++i)
+          for (int dd = 0; dd < 3; ++dd) a[i][dd] = P[i + 1][dd] - P[0][dd];
+        const double vol = std::fabs(a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) -
+                                     a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                                     a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0])) /
+                           6.0;
+        const double tau = std::pow(vol, 2.0 / 3.0) / 12.0;
+        for (double& k : K) k *= -tau;
       } else {
         elementMass(P, K);
       }

@@ -97,7 +97,10 @@ class Discretization {
 // rows of the owned DoFs (P1Elements.hpp:430-496, P1ConstantOperator.cpp:543-595); entries
 // are kept for every structural neighbour, also when their weight is zero.
 // ---------------------------------------------------------------------------------------
-enum FormKind { FORM_LAPLACE = 0, FORM_MASS = 1 };
+// FORM_PSPG: the pressure stabilisation form -tau grad p . grad q with tau = |T|^(2/3) / 12 of
+// each micro-cell T (P1PSPGOperator; its inverse diagonal scales the pressure update of the
+// Uzawa smoother). Cell coefficients do not enter it.
+enum FormKind { FORM_LAPLACE = 0, FORM_MASS = 1, FORM_PSPG = 2 };
 
 // The fifteen cell-stencil offsets in the fixed order used by the device kernels:
 // C, E, W, N, S, NW, SE, TC, TW, TS, TSE, BC, BE, BN, BNW

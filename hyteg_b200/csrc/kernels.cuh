@@ -13,6 +13,9 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <utility>
+
+#include "p2_stencil.h"
 
 namespace hg {
 namespace dev {
@@ -856,6 +859,33 @@ struct P2Tables {
 };
 
 constexpr int MODE_DIAG = 3;  // P2: sum of the element diagonals (the matrix diagonal)
+constexpr int MODE_SOR = 4;   // P2 interior: x += omega (b - A x) / a_ii in place, one colour
+
+// Row j of A at node (X, Y, Z) of a macro-cell restricted to that cell: the sum over the level-L
+// micro-cells inside the cell holding the node as local node j (DIAG: of their diagonals only).
+// u is the cell's array, pbz the first index of the planes Z-2 .. Z+2.
+template <class T, bool DIAG>
+__device__ __forceinline__ T p2GatherNode(const P2Tables& tb, const T* Kc, const T* __restrict__ u, const int (&pbz)[5],
+                                          int w, int N, int X, int Y, int Z) {
+  const int pc = (X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2);
+  T s = T(0);
+  for (int k = 0; k < tb.nCand[pc]; ++k) {
+    const int t = tb.cand[pc][k][0], j = tb.cand[pc][k][1];
+    const int ax = (X - tb.off[t][j][0]) >> 1, ay = (Y - tb.off[t][j][1]) >> 1, az = (Z - tb.off[t][j][2]) >> 1;
+    if (ax < 0 || ay < 0 || az < 0 || ax + ay + az >= N - tb.widthRed[t]) continue;
+    const T* Kr = Kc + t * 100 + j * 10;
+    if (DIAG) {
+      s += Kr[j];
+      continue;
+    }
+#pragma unroll
+    for (int m = 0; m < 10; ++m) {
+      const int qx = 2 * ax + tb.off[t][m][0], qy = 2 * ay + tb.off[t][m][1], qz = 2 * az + tb.off[t][m][2];
+      s += Kr[m] * __ldg(u + pbz[qz - Z + 2] + rowStart(w - qz, qy) + qx);
+    }
+  }
+  return s;
+}
 
 // colour, sel: when sel >= 0 only nodes whose colour (low 7 bits of the per-slot colour byte)
 // is sel are computed (one pass of the multicolour SOR); bit 7 of the byte marks owned slots.
@@ -883,26 +913,165 @@ __global__ void __launch_bounds__(kBlock) p2CellKernel(LevelDev lv, P2Tables tb,
     for (int X = lane; X <= M - Z - Y; X += 32) {
       const int64_t i = base + r0 + X;
       if (sel >= 0 && (colour[i] & 0x7f) != sel) continue;
-      const int pc = (X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2);
-      T s = T(0);
-      for (int k = 0; k < tb.nCand[pc]; ++k) {
-        const int t = tb.cand[pc][k][0], j = tb.cand[pc][k][1];
-        const int ax = (X - tb.off[t][j][0]) >> 1, ay = (Y - tb.off[t][j][1]) >> 1, az = (Z - tb.off[t][j][2]) >> 1;
-        if (ax < 0 || ay < 0 || az < 0 || ax + ay + az >= N - tb.widthRed[t]) continue;
-        const T* Kr = Kc + t * 100 + j * 10;
-        if (MODE == MODE_DIAG) {
-          s += Kr[j];
-          continue;
-        }
-#pragma unroll
-        for (int m = 0; m < 10; ++m) {
-          const int qx = 2 * ax + tb.off[t][m][0], qy = 2 * ay + tb.off[t][m][1], qz = 2 * az + tb.off[t][m][2];
-          s += Kr[m] * __ldg(src + base + pbz[qz - Z + 2] + rowStart(w - qz, qy) + qx);
-        }
-      }
+      const T s = p2GatherNode<T, MODE == MODE_DIAG>(tb, Kc, src + base, pbz, w, N, X, Y, Z);
       const bool interior = X >= 1 && Y >= 1 && Z >= 1 && X + Y + Z <= M - 1;
       if (!interior) dst[i] = s;
       else if (cellOn) dst[i] = MODE == MODE_RESIDUAL ? rhs[i] - s : s;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// P2 interior nodes by constant stencils. An interior node of a macro-cell (X, Y, Z >= 1,
+// X + Y + Z <= M - 1 on lattice M = 2^(L+1)) couples only to nodes of the micro-cells inside the
+// cell, in the same pattern for every node of its parity class, so its row of A is a constant
+// stencil per (cell, class): the offsets are compile-time lists (p2_stencil.h), the weights a
+// per-cell table W[cell][p2s::kTotal] assembled on the host from the element matrices. A block
+// works on one (cell, plane Z); each warp takes whole rows, its lanes every second node of the
+// row, so all lanes of a warp run the same class.
+// ---------------------------------------------------------------------------------------
+template <int DY, int DZ>
+__device__ __forceinline__ int p2RowBase(const int (&pbz)[5], int w, int Y, int Z) {
+  return pbz[DZ + 2] + rowStart(w - Z - DZ, Y + DY);
+}
+
+// The loads go through the read-only path also in the in-place SOR pass: no thread reads a value
+// that another thread writes during the launch (a colour class couples to no node of its own
+// colour), and each thread reads its own node before writing it.
+template <class T, int... DX, int... DY, int... DZ, int... I>
+__device__ __forceinline__ T p2StencilDot(p2s::List<p2s::O<DX, DY, DZ>...>, std::integer_sequence<int, I...>,
+                                          const T* u, const T* wt, const int (&pbz)[5], int w, int X, int Y, int Z) {
+  T s = T(0);
+  ((s += wt[I] * __ldg(u + p2RowBase<DY, DZ>(pbz, w, Y, Z) + X + DX)), ...);
+  return s;
+}
+
+// One row (Y, Z) of class PC: MODE_REPLACE dst = A src, MODE_RESIDUAL dst = rhs - A src,
+// MODE_SOR dst (== src) += omega (rhs - A dst) / a_ii. With sel >= 0 only the nodes of colour sel
+// are computed: the vertex class is split into four colours, read from the colour bytes; a whole
+// edge class is one colour in a cell's frame.
+template <class T, int MODE, int PC>
+__device__ __forceinline__ void p2StencilRow(const T* wts, T* dst, const T* src, const T* rhs, int64_t base,
+                                             const int (&pbz)[5], int w, int M, int Y, int Z, int lane,
+                                             const unsigned char* __restrict__ colour, int sel, T omega) {
+  using S = typename p2s::Class<PC>::type;
+  constexpr int kFirst = p2s::kFirst[PC], kCentre = p2s::kCentre[PC], kLen = p2s::kLen[PC];
+  const T* wt = wts + kFirst;
+  const int r0 = pbz[2] + rowStart(w - Z, Y);
+#pragma unroll 1
+  for (int X = ((PC & 1) ? 1 : 2) + 2 * lane; X <= M - 1 - Y - Z; X += 64) {
+    const int64_t i = base + r0 + X;
+    if (PC == 0 && sel >= 0 && (colour[i] & 0x7f) != sel) continue;
+    const T s = p2StencilDot<T>(S{}, std::make_integer_sequence<int, kLen>{}, src + base, wt, pbz, w, X, Y, Z);
+    if (MODE == MODE_REPLACE)
+      dst[i] = s;
+    else if (MODE == MODE_RESIDUAL)
+      dst[i] = rhs[i] - s;
+    else
+      dst[i] += omega * (rhs[i] - s) / wt[kCentre];
+  }
+}
+
+template <class T, int MODE>
+__device__ __forceinline__ void p2StencilRowAny(int pc, const T* wts, T* dst, const T* src, const T* rhs, int64_t base,
+                                                const int (&pbz)[5], int w, int M, int Y, int Z, int lane,
+                                                const unsigned char* __restrict__ colour, int sel, T omega) {
+  switch (pc) {
+    case 0: p2StencilRow<T, MODE, 0>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
+    case 1: p2StencilRow<T, MODE, 1>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
+    case 2: p2StencilRow<T, MODE, 2>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
+    case 3: p2StencilRow<T, MODE, 3>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
+    case 4: p2StencilRow<T, MODE, 4>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
+    case 5: p2StencilRow<T, MODE, 5>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
+    case 6: p2StencilRow<T, MODE, 6>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
+    default: p2StencilRow<T, MODE, 7>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
+  }
+}
+
+// Grid: nCells * (M - 3) blocks, block b on cell b / (M - 3), plane Z = 1 + b % (M - 3) (the
+// planes holding interior nodes; needs M >= 4). Only cells of a flagged DoF type are written.
+// sel >= 0 (one colour pass of the SOR, MODE_SOR or MODE_REPLACE): classOfColour[cell * 11 + sel]
+// is the class of colour sel in the cell's frame (0 for the four vertex colours, -1 when no
+// interior node has the colour). MODE_SOR updates in place: dst == src, rhs = b.
+template <class T, int MODE>
+__global__ void __launch_bounds__(kBlock) p2StencilKernel(LevelDev lv, const T* __restrict__ W, T* dst, const T* src,
+                                                          const T* __restrict__ rhs, unsigned mask,
+                                                          const unsigned char* __restrict__ colour,
+                                                          const signed char* __restrict__ classOfColour, int sel,
+                                                          T omega) {
+  const int M = lv.N, w = lv.w, nPl = M - 3;
+  const int c = blockIdx.x / nPl, Z = 1 + blockIdx.x % nPl;
+  if (!(lv.cellType[c] & mask)) return;
+  int pcSel = 0;
+  if (sel >= 0) {
+    pcSel = classOfColour[c * 11 + sel];
+    if (pcSel < 0 || ((pcSel >> 2) & 1) != (Z & 1)) return;
+  }
+  __shared__ T wts[p2s::kTotal];
+  for (int k = threadIdx.x; k < p2s::kTotal; k += blockDim.x) wts[k] = W[(int64_t)c * p2s::kTotal + k];
+  __syncthreads();
+  int pbz[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    const int z = Z - 2 + d;
+    pbz[d] = (z >= 0 && z <= M) ? int(tetSize(w) - tetSize(w - z)) : 0;
+  }
+  const int64_t base = lv.cellOff[c];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (sel >= 0) {
+#pragma unroll 1
+    for (int Y = (((pcSel >> 1) & 1) ? 1 : 2) + 2 * warp; Y <= M - 2 - Z; Y += 2 * (kBlock / 32))
+      p2StencilRowAny<T, MODE>(pcSel, wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega);
+  } else {
+#pragma unroll 1
+    for (int Y = 1 + warp; Y <= M - 2 - Z; Y += kBlock / 32) {
+#pragma unroll 1
+      for (int px = 0; px < 2; ++px)
+        p2StencilRowAny<T, MODE>(px | ((Y & 1) << 1) | ((Z & 1) << 2), wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane,
+                                 colour, sel, omega);
+    }
+  }
+}
+
+// The closure nodes of every macro-cell (its faces, edges and vertices): this cell's share of
+// row j of A, by the element gather, written into the cell's closure slot (p2AddKernel sums the
+// shares into the owner). Grid: nCells * (M + kP2FaceChunks(M)) blocks. Per cell, M blocks take
+// the boundary rings of the planes Z = 1 .. M (3 (M - Z) nodes, 1 at the top), and
+// kP2FaceChunks(M) blocks take the face Z = 0 in chunks of eight rows (a warp per row).
+__host__ __device__ __forceinline__ int p2FaceChunks(int M) { return (M + 1 + 7) / 8; }
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2ClosureKernel(LevelDev lv, P2Tables tb, const T* __restrict__ K,
+                                                          T* __restrict__ dst, const T* __restrict__ src,
+                                                          const unsigned char* __restrict__ colour, int sel) {
+  const int M = lv.N, N = M / 2, w = lv.w, perCell = M + p2FaceChunks(M);
+  const int c = blockIdx.x / perCell, q = blockIdx.x % perCell;
+  const int Z = q < M ? q + 1 : 0;
+  const int64_t base = lv.cellOff[c];
+  const T* Kc = K + (int64_t)c * 600;
+  int pbz[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    const int z = Z - 2 + d;
+    pbz[d] = (z >= 0 && z <= M) ? int(tetSize(w) - tetSize(w - z)) : 0;
+  }
+  auto node = [&](int X, int Y) {
+    const int64_t i = base + pbz[2] + rowStart(w - Z, Y) + X;
+    if (sel < 0 || (colour[i] & 0x7f) == sel) dst[i] = p2GatherNode<T, false>(tb, Kc, src + base, pbz, w, N, X, Y, Z);
+  };
+  const int n = M - Z;
+  if (Z == 0) {
+    const int Y = (q - M) * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (Y <= n)
+      for (int X = lane; X <= n - Y; X += 32) node(X, Y);
+  } else {
+    for (int r = threadIdx.x; r < (n == 0 ? 1 : 3 * n); r += blockDim.x) {
+      if (r <= n)
+        node(r, 0);
+      else if (r <= 2 * n)
+        node(0, r - n);
+      else
+        node(n - (r - 2 * n), r - 2 * n);
     }
   }
 }
@@ -1291,6 +1460,50 @@ __global__ void __launch_bounds__(kBlock) castKernel(const Chunk* __restrict__ c
     if (add) dst[j] += TD(src[j]);
     else dst[j] = TD(src[j]);
   }
+}
+
+// x[idx[i]] += sum_k Ainv(i, k) r[idx[k]] for the n unknowns of a coarse level (the exact coarse
+// solve; Ainv column-major, n * 8 bytes of dynamic shared memory): every block stages r at the
+// unknowns in shared memory, each thread computes one row.
+static __global__ void __launch_bounds__(kBlock) denseCorrectKernel(const int64_t* __restrict__ idx, int n,
+                                                                    const double* __restrict__ Ainv,
+                                                                    const double* __restrict__ r, double* x) {
+  extern __shared__ double rs[];
+  for (int k = threadIdx.x; k < n; k += blockDim.x) rs[k] = r[idx[k]];
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double t = 0.0;
+  for (int k = 0; k < n; ++k) t += Ainv[(int64_t)k * n + i] * rs[k];
+  x[idx[i]] += t;
+}
+
+// dst = vals[chunk] at every slot of every chunk (a constant per primitive array).
+static __global__ void __launch_bounds__(kBlock) fillChunksKernel(const Chunk* __restrict__ chunks,
+                                                                  const double* __restrict__ vals, double* dst) {
+  const Chunk ch = chunks[blockIdx.x];
+  const double v = vals[blockIdx.x];
+  for (int i = threadIdx.x; i < ch.len; i += blockDim.x) dst[ch.start + i] = v;
+}
+
+// The exact coarse solve of a block system over up to four functions: unknown i is slot idx[i]
+// of function comp[i]; x_comp[i][idx[i]] += sum_k Kinv(i, k) r_comp[k][idx[k]] (Kinv column-major,
+// n * 8 bytes of dynamic shared memory).
+struct BlockPtrs {
+  const double* r[4];
+  double* x[4];
+};
+static __global__ void __launch_bounds__(kBlock) blockDenseCorrectKernel(const int64_t* __restrict__ idx,
+                                                                         const unsigned char* __restrict__ comp, int n,
+                                                                         const double* __restrict__ Kinv, BlockPtrs bp) {
+  extern __shared__ double rs[];
+  for (int k = threadIdx.x; k < n; k += blockDim.x) rs[k] = bp.r[comp[k]][idx[k]];
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double t = 0.0;
+  for (int k = 0; k < n; ++k) t += Kinv[(int64_t)k * n + i] * rs[k];
+  bp.x[comp[i]][idx[i]] += t;
 }
 
 // One colour pass of the P2 multicolour SOR on the owned DoFs of the flagged primitives:

@@ -72,8 +72,7 @@ Gmg::Gmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int post_, double
 }
 
 Gmg::~Gmg() {
-  setGraphs(graphs);
-  for (auto& c : captured) cudaGraphExecDestroy(c.exec);
+  cache.clear();
   for (int id : {tmp, cp, cz, cap, cr, cx64, cb64, x32, b32, r64})
     if (id >= 0) s.fns.erase(id);
 }
@@ -85,10 +84,61 @@ bool Gmg::deviceCoarse() const {
 
 void Gmg::setGraphs(bool on) {
   graphs = on;
-  if (!on) {
-    for (auto& c : captured) cudaGraphExecDestroy(c.exec);
-    captured.clear();
-    warm.clear();
+  if (!on) cache.clear();
+}
+
+void GraphCache::clear() {
+  for (auto& c : captured) cudaGraphExecDestroy(c.exec);
+  captured.clear();
+  warm.clear();
+}
+
+void GraphCache::run(Storage& s, const std::function<std::vector<uintptr_t>()>& signature,
+                     const std::function<void()>& cycle) {
+  const std::vector<uintptr_t> sig = signature();
+  for (auto& c : captured)
+    if (c.sig == sig) {
+      cudaCheck(cudaGraphLaunch(c.exec, s.stream), "graph launch");
+      s.launches += c.launches;
+      return;
+    }
+  bool seen = false;
+  for (auto& w : warm) seen = seen || w == sig;
+  if (!seen) {  // first cycle under this signature runs eagerly (allocates buffers, tables)
+    cycle();
+    if (signature() == sig) warm.push_back(sig);
+    if (warm.size() > 8) warm.erase(warm.begin());
+    return;
+  }
+  const unsigned long long l0 = s.launches;
+  cudaCheck(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+  cudaGraph_t g = nullptr;
+  try {
+    cycle();
+  } catch (...) {
+    cudaStreamEndCapture(s.stream, &g);
+    if (g) cudaGraphDestroy(g);
+    s.launches = l0;
+    throw;
+  }
+  cudaCheck(cudaStreamEndCapture(s.stream, &g), "end capture");
+  Captured c;
+  c.sig = sig;
+  c.launches = s.launches - l0;
+  s.launches = l0;
+  cudaError_t e = cudaGraphInstantiate(&c.exec, g, 0);
+  cudaGraphDestroy(g);
+  cudaCheck(e, "graph instantiate");
+  if (signature() != sig) {  // the host-side buffer state did not return: no replay
+    cudaGraphExecDestroy(c.exec);
+    throw Error(HG_ERR_INTERNAL, "captured cycle changed the buffer state");
+  }
+  cudaCheck(cudaGraphLaunch(c.exec, s.stream), "graph launch");
+  s.launches += c.launches;
+  captured.push_back(c);
+  if (captured.size() > 4) {
+    cudaGraphExecDestroy(captured.front().exec);
+    captured.erase(captured.begin());
   }
 }
 
@@ -143,51 +193,7 @@ void Gmg::runCycle(int x, int b, int L) {
     solveRecursively(x, b, L);
     return;
   }
-  const std::vector<uintptr_t> sig = signature(x, b, L);
-  for (auto& c : captured)
-    if (c.sig == sig) {
-      cudaCheck(cudaGraphLaunch(c.exec, s.stream), "graph launch");
-      s.launches += c.launches;
-      return;
-    }
-  bool seen = false;
-  for (auto& w : warm) seen = seen || w == sig;
-  if (!seen) {  // first cycle under this signature runs eagerly (allocates spare buffers, tables)
-    solveRecursively(x, b, L);
-    if (signature(x, b, L) == sig) warm.push_back(sig);
-    if (warm.size() > 8) warm.erase(warm.begin());
-    return;
-  }
-  const unsigned long long l0 = s.launches;
-  cudaCheck(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-  cudaGraph_t g = nullptr;
-  try {
-    solveRecursively(x, b, L);
-  } catch (...) {
-    cudaStreamEndCapture(s.stream, &g);
-    if (g) cudaGraphDestroy(g);
-    s.launches = l0;
-    throw;
-  }
-  cudaCheck(cudaStreamEndCapture(s.stream, &g), "end capture");
-  Captured c;
-  c.sig = sig;
-  c.launches = s.launches - l0;
-  s.launches = l0;
-  cudaError_t e = cudaGraphInstantiate(&c.exec, g, 0);
-  cudaGraphDestroy(g);
-  cudaCheck(e, "graph instantiate");
-  if (signature(x, b, L) != sig) {  // the host-side buffer state did not return: no replay
-    cudaGraphExecDestroy(c.exec);
-    throw Error(HG_ERR_INTERNAL, "captured cycle changed the buffer state");
-  }
-  cudaCheck(cudaGraphLaunch(c.exec, s.stream), "graph launch");
-  s.launches += c.launches;
-  captured.push_back(c);
-  if (captured.size() > 4) {
-    cudaGraphExecDestroy(captured.front().exec);
-    captured.erase(captured.begin());
-  }
+  cache.run(s, [&] { return signature(x, b, L); }, [&] { solveRecursively(x, b, L); });
 }
 
 // GeometricMultigridSolver::solveRecursively (src/hyteg/solvers/GeometricMultigridSolver.hpp:136-235)
@@ -266,8 +272,119 @@ P2Gmg::P2Gmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int post_, do
 }
 
 P2Gmg::~P2Gmg() {
+  cache.clear();
   for (int id : {tmp, cp, cz, cap, cr, cx64, cb64})
     if (id >= 0) s.fns.erase(id);
+}
+
+// The operator restricted to the unknowns of the coarsest level, column by column (the operator
+// applied to unit vectors), inverted on the host by Gauss-Jordan elimination with partial pivoting.
+bool P2Gmg::buildCoarseDirect() {
+  if (coarseN >= 0) return coarseN > 0;
+  coarseN = 0;
+  const unsigned flag = HG_INNER | HG_NEUMANN | HG_FREESLIP;
+  const int Lf = minL + 1;
+  P2Additive& ad = s.p2Additive(Lf);
+  std::vector<int64_t> idx;
+  for (size_t i = 0; i < ad.hostOwner.size(); ++i)
+    if (ad.hostOwnerType[i] & flag) idx.push_back(ad.hostOwner[i]);
+  const int n = (int)idx.size();
+  if (ad.hostOwner.empty() || n == 0 || n > kCoarseDirectMax) return false;
+  const int64_t total = s.disc.level(Lf).total;
+  const int e = s.createFunction(Lf, Lf, 8), y = s.createFunction(Lf, Lf, 8);
+  std::vector<double> he((size_t)total, 0.0), hy((size_t)total), a((size_t)n * n), inv((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    he[(size_t)idx[j]] = 1.0;
+    cudaCheck(cudaMemcpyAsync(s.data(e, Lf), he.data(), (size_t)total * 8, cudaMemcpyHostToDevice, s.stream), "coarse");
+    cudaCheck(cudaStreamSynchronize(s.stream), "coarse");
+    he[(size_t)idx[j]] = 0.0;
+    s.p2Apply(op, e, y, -1, minL, flag, 0);
+    cudaCheck(cudaMemcpyAsync(hy.data(), s.data(y, Lf), (size_t)total * 8, cudaMemcpyDeviceToHost, s.stream), "coarse");
+    cudaCheck(cudaStreamSynchronize(s.stream), "coarse");
+    for (int i = 0; i < n; ++i) a[(size_t)i * n + j] = hy[(size_t)idx[i]];  // row-major A(i, j)
+  }
+  s.fns.erase(e);
+  s.fns.erase(y);
+  for (int i = 0; i < n; ++i) inv[(size_t)i * n + i] = 1.0;
+  for (int c = 0; c < n; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < n; ++r)
+      if (std::fabs(a[(size_t)r * n + c]) > std::fabs(a[(size_t)piv * n + c])) piv = r;
+    argCheck(a[(size_t)piv * n + c] != 0.0, "P2 multigrid: singular coarse-level operator");
+    if (piv != c)
+      for (int k = 0; k < n; ++k) {
+        std::swap(a[(size_t)piv * n + k], a[(size_t)c * n + k]);
+        std::swap(inv[(size_t)piv * n + k], inv[(size_t)c * n + k]);
+      }
+    const double d = 1.0 / a[(size_t)c * n + c];
+    for (int k = 0; k < n; ++k) {
+      a[(size_t)c * n + k] *= d;
+      inv[(size_t)c * n + k] *= d;
+    }
+    for (int r = 0; r < n; ++r) {
+      const double f = a[(size_t)r * n + c];
+      if (r == c || f == 0.0) continue;
+      for (int k = 0; k < n; ++k) {
+        a[(size_t)r * n + k] -= f * a[(size_t)c * n + k];
+        inv[(size_t)r * n + k] -= f * inv[(size_t)c * n + k];
+      }
+    }
+  }
+  std::vector<double> colMajor((size_t)n * n);
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < n; ++k) colMajor[(size_t)k * n + i] = inv[(size_t)i * n + k];
+  coarseIdx.reset(new DevBuf());
+  coarseIdx->alloc((size_t)n * sizeof(int64_t));
+  coarseInv.reset(new DevBuf());
+  coarseInv->alloc((size_t)n * n * sizeof(double));
+  cudaCheck(cudaMemcpyAsync(coarseIdx->p, idx.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s.stream), "coarse");
+  cudaCheck(cudaMemcpyAsync(coarseInv->p, colMajor.data(), colMajor.size() * 8, cudaMemcpyHostToDevice, s.stream),
+            "coarse");
+  cudaCheck(cudaStreamSynchronize(s.stream), "coarse");
+  coarseN = n;
+  return true;
+}
+
+// Coarsest level: x += A^-1 (b - A x) on the unknowns (one residual, one dense product, one halo
+// refresh, all on the device), or CG when the coarse level has too many unknowns.
+void P2Gmg::coarseSolve(int x, int b, int L) {
+  if (!buildCoarseDirect()) {
+    coarseCg(x, b, L);
+    return;
+  }
+  const unsigned flag = HG_INNER | HG_NEUMANN | HG_FREESLIP;
+  s.p2Apply(op, x, cr, b, L, flag, 2);
+  dev::denseCorrectKernel<<<(coarseN + dev::kBlock - 1) / dev::kBlock, dev::kBlock, (size_t)coarseN * 8, s.stream>>>(
+      (const int64_t*)coarseIdx->p, coarseN, (const double*)coarseInv->p, (const double*)s.data(cr, L + 1),
+      (double*)s.data(x, L + 1));
+  ++s.launches;
+  cudaCheck(cudaGetLastError(), "coarse solve");
+  s.communicate(x, L + 1, (1 << G_COUNT) - 1);
+}
+
+std::vector<uintptr_t> P2Gmg::signature(int x, int b, int L) {
+  std::vector<uintptr_t> sig = {(uintptr_t)L, (uintptr_t)x, (uintptr_t)b, (uintptr_t)op, (uintptr_t)s.generation,
+                                (uintptr_t)symmetric, (uintptr_t)coarseN};
+  P2Operator& o = s.p2op(op);
+  for (int l = minL; l <= L; ++l) {
+    for (int id : {x, b, tmp}) sig.push_back((uintptr_t)s.data(id, l + 1));
+    auto sc = s.p2scratch.find({l + 1, prec});
+    sig.push_back(sc != s.p2scratch.end() ? (uintptr_t)s.data(sc->second, l + 1) : 0);
+    auto dg = o.diag.find({l, prec});
+    sig.push_back(dg != o.diag.end() ? (uintptr_t)s.data(dg->second, l + 1) : 0);
+  }
+  for (int id : {cr, cx64, cb64})
+    if (id >= 0) sig.push_back((uintptr_t)s.data(id, minL + 1));
+  sig.push_back(coarseInv ? (uintptr_t)coarseInv->p : 0);
+  return sig;
+}
+
+void P2Gmg::runCycle(int x, int b, int L) {
+  if (!graphs || !buildCoarseDirect()) {
+    solveRecursively(x, b, L);
+    return;
+  }
+  cache.run(s, [&] { return signature(x, b, L); }, [&] { solveRecursively(x, b, L); });
 }
 
 // CGSolver (CGSolver.hpp:69-150, identity preconditioner) with the P2 operator of level L.
@@ -303,11 +420,11 @@ void P2Gmg::solveRecursively(int x, int b, int L) {
   const unsigned flag = HG_INNER | HG_NEUMANN;
   if (L == minL) {
     if (prec == 8) {
-      coarseCg(x, b, L);
+      coarseSolve(x, b, L);
     } else {  // FP32 cycle: the coarse problem in FP64, rounded back
       s.copyCast(cb64, b, L + 1, HG_ALL, false);
       s.copyCast(cx64, x, L + 1, HG_ALL, false);
-      coarseCg(cx64, cb64, L);
+      coarseSolve(cx64, cb64, L);
       s.copyCast(x, cx64, L + 1, HG_ALL, false);
     }
     return;
@@ -321,6 +438,295 @@ void P2Gmg::solveRecursively(int x, int b, int L) {
   solveRecursively(x, b, L - 1);
   s.p2Prolongate(x, L - 1, flag, true);
   for (int i = 0; i < post; ++i) s.p2Sor(op, x, b, omega, L, flag, symmetric);
+}
+
+// Moore-Penrose inverse of a symmetric n x n matrix (row-major, overwritten) by cyclic Jacobi
+// rotations (Golub and Van Loan, Matrix Computations, section 8.5): eigenvalues below
+// 1e-10 * max |eigenvalue| count as zero. Returns the pseudo-inverse column-major (= row-major).
+static std::vector<double> symmetricPinv(std::vector<double>& A, int n) {
+  std::vector<double> V((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
+  double total = 0.0;
+  for (double v : A) total += v * v;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) off += A[(size_t)p * n + q] * A[(size_t)p * n + q];
+    if (off <= 1e-32 * total) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = A[(size_t)p * n + q];
+        if (apq == 0.0) continue;
+        const double theta = (A[(size_t)q * n + q] - A[(size_t)p * n + p]) / (2.0 * apq);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < n; ++k) {  // columns p, q
+          const double akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+          A[(size_t)k * n + p] = c * akp - sn * akq;
+          A[(size_t)k * n + q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {  // rows p, q
+          const double apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+          A[(size_t)p * n + k] = c * apk - sn * aqk;
+          A[(size_t)q * n + k] = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = V[(size_t)k * n + p], vkq = V[(size_t)k * n + q];
+          V[(size_t)k * n + p] = c * vkp - sn * vkq;
+          V[(size_t)k * n + q] = sn * vkp + c * vkq;
+        }
+      }
+  }
+  double lmax = 0.0;
+  for (int i = 0; i < n; ++i) lmax = std::max(lmax, std::fabs(A[(size_t)i * n + i]));
+  std::vector<double> P((size_t)n * n, 0.0);
+  for (int m = 0; m < n; ++m) {
+    const double l = A[(size_t)m * n + m];
+    if (std::fabs(l) <= 1e-10 * lmax) continue;
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < n; ++k) P[(size_t)i * n + k] += V[(size_t)i * n + m] * V[(size_t)k * n + m] / l;
+  }
+  return P;
+}
+
+StokesGmg::StokesGmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int post_, double omega_, int sweeps)
+    : s(st), op(op_), minL(minL_), maxL(maxL_), pre(pre_), post(post_), omega(omega_), velocitySweeps(sweeps) {
+  P2Operator& o = s.p2op(op);
+  argCheck(!o.dd.empty(), "Stokes multigrid: not a Stokes operator");
+  argCheck(minL >= o.minL && maxL <= o.maxL && minL <= maxL, "Stokes multigrid: levels outside the operator's range");
+  argCheck(pre >= 0 && post >= 0 && sweeps >= 1, "Stokes multigrid: invalid smoothing steps");
+  for (int k = 0; k < 3; ++k) {
+    ru[k] = s.createFunction(minL + 1, maxL + 1, 8);
+    tu[k] = s.createFunction(minL + 1, maxL + 1, 8);
+  }
+  rp = s.createFunction(minL, maxL, 8);
+  tp = s.createFunction(minL, maxL, 8);
+  pspg = s.createOperator(FORM_PSPG, minL, maxL);
+  for (int L = minL; L <= maxL; ++L) invDiag.push_back(s.p1Diagonal(pspg, L));
+}
+
+StokesGmg::~StokesGmg() {
+  for (int k = 0; k < 3; ++k) {
+    s.fns.erase(ru[k]);
+    s.fns.erase(tu[k]);
+  }
+  s.fns.erase(rp);
+  s.fns.erase(tp);
+  for (int d : invDiag) s.fns.erase(d);
+  s.ops.erase(pspg);
+}
+
+// UzawaSmoother::uzawaSmooth, block-Laplace variant without stabilisation (UzawaSmoother.hpp:287-423);
+// invDiag holds the PSPG diagonal itself: r_p / diag == pspg_inv_diag applied to r_p.
+void StokesGmg::smooth(const int u[3], int p, const int f[3], int g, int L) {
+  const unsigned fv = HG_INNER | HG_NEUMANN, fp = HG_ALL;
+  const int Lv = L + 1;
+  const double a[2] = {1.0, -1.0};
+  s.stokesDivT(op, p, ru, L, fv, false);
+  for (int k = 0; k < 3; ++k) {
+    const int src[2] = {f[k], ru[k]};
+    s.lincomb(ru[k], Lv, fv, 2, a, src, false, 0.0);
+  }
+  for (int i = 0; i < velocitySweeps; ++i)
+    for (int k = 0; k < 3; ++k) s.p2Sor(op, u[k], ru[k], 1.0, L, fv, false);
+  s.stokesDiv(op, u, rp, L, fp);
+  const int src[2] = {g, rp};
+  s.lincomb(rp, L, fp, 2, a, src, false, 0.0);
+  s.divideBy(rp, rp, invDiag[L - minL], L, fp);
+  s.lincomb(p, L, fp, 1, &omega, &rp, true, 0.0);
+  s.communicate(p, L, (1 << G_COUNT) - 1);
+}
+
+// tu = f - (A u + D^T p), tp = g - D u on the unknowns
+static void stokesResidual(Storage& s, int op, const int u[3], int p, const int f[3], int g, const int tu[3], int tp,
+                           int L) {
+  const unsigned fv = HG_INNER | HG_NEUMANN, fp = HG_ALL;
+  const double a[2] = {1.0, -1.0};
+  s.stokesApply(op, u, p, tu, tp, L, fv, fp);
+  for (int k = 0; k < 3; ++k) {
+    const int src[2] = {f[k], tu[k]};
+    s.lincomb(tu[k], L + 1, fv, 2, a, src, false, 0.0);
+  }
+  const int src[2] = {g, tp};
+  s.lincomb(tp, L, fp, 2, a, src, false, 0.0);
+}
+
+double StokesGmg::residualNorm(const int u[3], int p, const int f[3], int g, int L) {
+  stokesResidual(s, op, u, p, f, g, tu, tp, L);
+  double t = s.dot(tp, tp, L, HG_ALL);
+  for (int k = 0; k < 3; ++k) t += s.dot(tu[k], tu[k], L + 1, HG_INNER | HG_NEUMANN);
+  return std::sqrt(t);
+}
+
+double StokesGmg::estimateOmega(int L, int iters, uint64_t seed) {
+  argCheck(L >= minL && L <= maxL && iters >= 1, "Uzawa estimate: invalid level or iterations");
+  const unsigned all = HG_ALL, fv = HG_INNER | HG_NEUMANN;
+  const int Lv = L + 1;
+  const int mass = s.createOperator(FORM_MASS, L, L);
+  const int ones = s.createFunction(L, L, 8), lumped = s.createFunction(L, L, 8);
+  const int itv = s.createFunction(L, L, 8), aux = s.createFunction(L, L, 8);
+  s.lincomb(ones, L, all, 0, nullptr, nullptr, false, 1.0);
+  s.apply(mass, ones, lumped, L, all, 0);
+  s.fillRandom(itv, L, all, seed, 0.0, 1.0);
+  auto E = [&](int src, int dst) {
+    for (int k = 0; k < 3; ++k) s.lincomb(ru[k], Lv, all, 0, nullptr, nullptr, false, 0.0);
+    s.stokesDivT(op, src, tu, L, all, false);
+    for (int i = 0; i < velocitySweeps; ++i)
+      for (int k = 0; k < 3; ++k) s.p2Sor(op, ru[k], tu[k], 1.0, L, fv, false);
+    s.stokesDiv(op, ru, dst, L, all);
+    s.divideBy(dst, dst, lumped, L, all);
+  };
+  auto scaleInto = [&](int dst, int src) {
+    const double inv = 1.0 / std::sqrt(s.dot(src, src, L, all));
+    s.lincomb(dst, L, all, 1, &inv, &src, false, 0.0);
+  };
+  scaleInto(itv, itv);
+  E(itv, aux);
+  double radius = 0.0;
+  for (int i = 0; i < iters; ++i) {
+    scaleInto(itv, aux);
+    E(itv, aux);
+    radius = s.dot(itv, aux, L, all);
+  }
+  for (int id : {ones, lumped, itv, aux}) s.fns.erase(id);
+  s.ops.erase(mass);
+  return radius;
+}
+
+// The block operator on the coarse unknowns, probed column by column with unit vectors,
+// symmetrised, and its pseudo-inverse uploaded.
+void StokesGmg::buildCoarse() {
+  if (coarseN >= 0) return;
+  const unsigned fv = HG_INNER | HG_NEUMANN | HG_FREESLIP;
+  const int Lv = minL + 1, Lp = minL;
+  P2Additive& av = s.p2Additive(Lv);
+  P2Additive& ap = s.p2Additive(Lp);
+  argCheck(!av.hostOwner.empty() && !ap.hostOwner.empty(), "Stokes multigrid: coarse level too large");
+  std::vector<int64_t> idx;
+  std::vector<unsigned char> comp;
+  for (int k = 0; k < 3; ++k)
+    for (size_t i = 0; i < av.hostOwner.size(); ++i)
+      if (av.hostOwnerType[i] & fv) {
+        idx.push_back(av.hostOwner[i]);
+        comp.push_back((unsigned char)k);
+      }
+  for (size_t i = 0; i < ap.hostOwner.size(); ++i) {
+    idx.push_back(ap.hostOwner[i]);
+    comp.push_back(3);
+  }
+  const int n = (int)idx.size();
+  argCheck(n <= kCoarseMax, "Stokes multigrid: more than 1024 coarse unknowns");
+  const int64_t nv = s.disc.level(Lv).total, np = s.disc.level(Lp).total;
+  int e[4], y[4];
+  for (int k = 0; k < 4; ++k) {
+    e[k] = s.createFunction(k < 3 ? Lv : Lp, k < 3 ? Lv : Lp, 8);
+    y[k] = s.createFunction(k < 3 ? Lv : Lp, k < 3 ? Lv : Lp, 8);
+  }
+  auto lvl = [&](int k) { return k < 3 ? Lv : Lp; };
+  auto len = [&](int k) { return k < 3 ? nv : np; };
+  std::vector<std::vector<double>> he(4), hy(4);
+  for (int k = 0; k < 4; ++k) {
+    he[k].assign((size_t)len(k), 0.0);
+    hy[k].assign((size_t)len(k), 0.0);
+  }
+  std::vector<double> K((size_t)n * n);
+  for (int j = 0; j < n; ++j) {
+    he[comp[j]][(size_t)idx[j]] = 1.0;
+    for (int k = 0; k < 4; ++k)
+      cudaCheck(cudaMemcpyAsync(s.data(e[k], lvl(k)), he[k].data(), (size_t)len(k) * 8, cudaMemcpyHostToDevice, s.stream),
+                "coarse");
+    cudaCheck(cudaStreamSynchronize(s.stream), "coarse");
+    he[comp[j]][(size_t)idx[j]] = 0.0;
+    s.stokesApply(op, e, e[3], y, y[3], minL, HG_INNER | HG_NEUMANN, HG_ALL);
+    for (int k = 0; k < 4; ++k)
+      cudaCheck(cudaMemcpyAsync(hy[k].data(), s.data(y[k], lvl(k)), (size_t)len(k) * 8, cudaMemcpyDeviceToHost, s.stream),
+                "coarse");
+    cudaCheck(cudaStreamSynchronize(s.stream), "coarse");
+    for (int i = 0; i < n; ++i) K[(size_t)i * n + j] = hy[comp[i]][(size_t)idx[i]];
+  }
+  for (int k = 0; k < 4; ++k) {
+    s.fns.erase(e[k]);
+    s.fns.erase(y[k]);
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) {
+      const double m = 0.5 * (K[(size_t)i * n + j] + K[(size_t)j * n + i]);
+      K[(size_t)i * n + j] = K[(size_t)j * n + i] = m;
+    }
+  const std::vector<double> P = symmetricPinv(K, n);
+  coarseIdx.reset(new DevBuf());
+  coarseIdx->alloc((size_t)std::max(n, 1) * sizeof(int64_t));
+  coarseComp.reset(new DevBuf());
+  coarseComp->alloc((size_t)std::max(n, 1));
+  coarseInv.reset(new DevBuf());
+  coarseInv->alloc((size_t)std::max(n, 1) * std::max(n, 1) * sizeof(double));
+  if (n) {
+    cudaCheck(cudaMemcpyAsync(coarseIdx->p, idx.data(), (size_t)n * 8, cudaMemcpyHostToDevice, s.stream), "coarse");
+    cudaCheck(cudaMemcpyAsync(coarseComp->p, comp.data(), (size_t)n, cudaMemcpyHostToDevice, s.stream), "coarse");
+    cudaCheck(cudaMemcpyAsync(coarseInv->p, P.data(), P.size() * 8, cudaMemcpyHostToDevice, s.stream), "coarse");
+    cudaCheck(cudaStreamSynchronize(s.stream), "coarse");
+  }
+  coarseN = n;
+}
+
+// x += K^+ (b - K x) on the coarse unknowns
+void StokesGmg::coarseSolve(const int u[3], int p, const int f[3], int g) {
+  buildCoarse();
+  if (coarseN == 0) return;
+  stokesResidual(s, op, u, p, f, g, tu, tp, minL);
+  dev::BlockPtrs bp;
+  for (int k = 0; k < 3; ++k) {
+    bp.r[k] = (const double*)s.data(tu[k], minL + 1);
+    bp.x[k] = (double*)s.data(u[k], minL + 1);
+  }
+  bp.r[3] = (const double*)s.data(tp, minL);
+  bp.x[3] = (double*)s.data(p, minL);
+  dev::blockDenseCorrectKernel<<<(coarseN + dev::kBlock - 1) / dev::kBlock, dev::kBlock, (size_t)coarseN * 8,
+                                  s.stream>>>((const int64_t*)coarseIdx->p, (const unsigned char*)coarseComp->p, coarseN,
+                                              (const double*)coarseInv->p, bp);
+  ++s.launches;
+  cudaCheck(cudaGetLastError(), "Stokes coarse solve");
+  for (int k = 0; k < 3; ++k) s.communicate(u[k], minL + 1, (1 << G_COUNT) - 1);
+  s.communicate(p, minL, (1 << G_COUNT) - 1);
+}
+
+void StokesGmg::solveRecursively(const int u[3], int p, const int f[3], int g, int L) {
+  const unsigned fv = HG_INNER | HG_NEUMANN, fp = HG_ALL;
+  if (L == minL) {
+    coarseSolve(u, p, f, g);
+    return;
+  }
+  for (int i = 0; i < pre; ++i) smooth(u, p, f, g, L);
+  stokesResidual(s, op, u, p, f, g, tu, tp, L);
+  const double one = 1.0;
+  for (int k = 0; k < 3; ++k) {
+    s.p2Restrict(tu[k], L, fv);
+    s.lincomb(f[k], L, fv, 1, &one, &tu[k], false, 0.0);  // lattice level L = P2 level L - 1
+    s.lincomb(u[k], L, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+  }
+  s.restrictFn(tp, L, fp);
+  s.lincomb(g, L - 1, fp, 1, &one, &tp, false, 0.0);
+  s.lincomb(p, L - 1, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+  solveRecursively(u, p, f, g, L - 1);
+  for (int k = 0; k < 3; ++k) s.p2Prolongate(u[k], L - 1, fv, true);
+  s.prolongate(p, L - 1, fp, true);
+  for (int i = 0; i < post; ++i) smooth(u, p, f, g, L);
+}
+
+int StokesGmg::solveTo(const int u[3], int p, const int f[3], int g, int L, double tol, int maxIter, double* relRes,
+                       double* history, int historyCap) {
+  argCheck(L >= minL && L <= maxL, "Stokes multigrid: level outside the solver's range");
+  const double r0 = residualNorm(u, p, f, g, L);
+  double rel = 1.0;
+  int it = 0;
+  while (it < maxIter && rel > tol && r0 > 0.0) {
+    solveRecursively(u, p, f, g, L);
+    ++it;
+    rel = residualNorm(u, p, f, g, L) / r0;
+    if (history && it <= historyCap) history[it - 1] = rel;
+  }
+  if (relRes) *relRes = r0 > 0.0 ? rel : 0.0;
+  return it;
 }
 
 int stokesMinres(Storage& s, int op, const int u[3], int p, const int f[3], int g, int L, int nu, int maxIter,
@@ -385,7 +791,7 @@ int stokesMinres(Storage& s, int op, const int u[3], int p, const int f[3], int 
     for (int k = 0; k < 3; ++k) {
       s.copyCast(pb, src.u[k], Lv, fv, false);
       for (int l = 1; l <= Lv; ++l) s.lincomb(px, l, HG_ALL, 0, nullptr, nullptr, false, 0.0);
-      mg.solveRecursively(px, pb, L);
+      mg.runCycle(px, pb, L);
       s.copyCast(dst.u[k], px, Lv, fv, false);
     }
     (void)one;
@@ -473,7 +879,7 @@ int P2Gmg::solveTo(int x, int b, int L, double tol, int maxIter, double* relRes,
   double rel = 1.0;
   int it = 0;
   while (it < maxIter && rel > tol && r0 > 0.0) {
-    solveRecursively(x, b, L);
+    runCycle(x, b, L);
     ++it;
     s.p2Apply(op, x, tmp, b, L, flag, 2);
     rel = std::sqrt(s.dot(tmp, tmp, Lf, flag)) / r0;

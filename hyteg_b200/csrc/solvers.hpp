@@ -4,11 +4,32 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
+#include <memory>
 #include <vector>
 
 namespace hg {
 
 struct Storage;
+struct DevBuf;
+
+// Captured CUDA graphs of one solver's cycle, keyed by a signature: every device address the
+// cycle reads or writes plus what fixes its kernel arguments. run() replays a graph captured
+// under the same signature. A new signature runs eagerly (which builds lazily allocated tables
+// and buffers); once a signature has run eagerly and come back unchanged, its next cycle is
+// captured and replayed from then on. At most four graphs are kept.
+struct GraphCache {
+  struct Captured {
+    std::vector<uintptr_t> sig;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches = 0;
+  };
+  std::vector<Captured> captured;
+  std::vector<std::vector<uintptr_t>> warm;  // signatures that ran eagerly once
+  ~GraphCache() { clear(); }
+  void clear();
+  void run(Storage& s, const std::function<std::vector<uintptr_t>()>& signature, const std::function<void()>& cycle);
+};
 
 // Returns the number of iterations taken; workspace functions must cover level L.
 int cgSolve(Storage& s, int op, int x, int b, int L, int maxIter, double tol, int p, int z, int ap, int r,
@@ -30,14 +51,8 @@ struct Gmg {
   void setGraphs(bool on);
   bool deviceCoarse() const;  // the coarse level has vertex and edge DoFs only
 
-  struct Captured {
-    std::vector<uintptr_t> sig;
-    cudaGraphExec_t exec = nullptr;
-    unsigned long long launches = 0;
-  };
   bool graphs = true;
-  std::vector<Captured> captured;
-  std::vector<std::vector<uintptr_t>> warm;  // signatures that ran eagerly once
+  GraphCache cache;
   std::vector<uintptr_t> signature(int x, int b, int L);
 
   Storage& s;
@@ -52,14 +67,25 @@ struct Gmg {
 };
 
 // P2 geometric multigrid on P2 levels [minL, maxL] (the P2 DoFs of level L are the vertex DoFs
-// of level L + 1): multicolour P2 SOR, quadratic transfers, CG on the coarsest level; FP64.
+// of level L + 1): multicolour P2 SOR, quadratic transfers, an exact solve on the coarsest level
+// (the inverse of A on its unknowns, up to kCoarseDirectMax of them; CG beyond), in FP64.
 struct P2Gmg {
+  static constexpr int kCoarseDirectMax = 1024;
   P2Gmg(Storage& s, int op, int minL, int maxL, int pre, int post, double omega, int coarseMaxIter,
         double coarseTol, int prec = 8);
   ~P2Gmg();
   void solveRecursively(int x, int b, int L);
+  // One cycle, replayed from a captured CUDA graph when the coarse solve runs on the device.
+  void runCycle(int x, int b, int L);
   int solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap);
   int coarseCg(int x, int b, int L);
+  void coarseSolve(int x, int b, int L);  // FP64 x, b on the coarsest level
+  bool buildCoarseDirect();               // false when the coarse level has too many unknowns
+  std::vector<uintptr_t> signature(int x, int b, int L);
+  int coarseN = -1;  // unknowns of the exact coarse solve (0: CG; -1: not yet built)
+  std::unique_ptr<DevBuf> coarseIdx, coarseInv;
+  bool graphs = true;
+  GraphCache cache;
 
   Storage& s;
   int op, minL, maxL, pre, post;
@@ -70,6 +96,45 @@ struct P2Gmg {
   int prec = 8;                      // precision of the cycle (4: FP32 hierarchy, coarse CG in FP64)
   int cx64 = -1, cb64 = -1;          // FP64 coarse-level copies for an FP32 cycle
   bool symmetric = false;  // post-smoothing with backward sweeps (a symmetric cycle)
+};
+
+// Geometric multigrid on the whole P2-P1 Taylor-Hood system (GeometricMultigridSolver with
+// P2P1TaylorHoodStokesOperator, GeometricMultigridSolver.hpp:136-235) with the Uzawa smoother
+// (UzawaSmoother.hpp:338-423, block-Laplace variant without stabilisation):
+//   r_u = f - D^T p;  velocitySweeps times: one forward P2 SOR sweep (omega 1) per component on
+//   A u_k = r_u,k;  r_p = g - D u;  p += omega r_p / diag(PSPG)
+// and the composite transfers (P2P1StokesToP2P1StokesRestriction / Prolongation: quadratic on the
+// velocity, linear on the pressure). Velocity DoFs flagged Inner | Neumann are unknowns; the
+// pressure is all-inner (every DoF an unknown, P2P1TaylorHoodFunction.hpp:61). The coarsest level
+// is solved by the pseudo-inverse of the operator on its unknowns (the constant pressure and the
+// pressure DoFs coupled to no free velocity DoF span its null space), built once. FP64.
+struct StokesGmg {
+  static constexpr int kCoarseMax = 1024;
+  StokesGmg(Storage& s, int op, int minL, int maxL, int pre, int post, double omega, int velocitySweeps);
+  ~StokesGmg();
+  void smooth(const int u[3], int p, const int f[3], int g, int L);
+  void solveRecursively(const int u[3], int p, const int f[3], int g, int L);
+  // V-cycles until ||b - K x|| <= tol ||b - K x0|| (unknowns only) or maxIter; returns the cycles.
+  int solveTo(const int u[3], int p, const int f[3], int g, int L, double tol, int maxIter, double* relRes,
+              double* history, int historyCap);
+  double residualNorm(const int u[3], int p, const int f[3], int g, int L);
+  // estimateUzawaRelaxationParameter (UzawaSmoother.hpp:52-68): iters power iterations
+  // (SpectrumEstimation.hpp:57-81) on E = M_lumped^-1 D S D^T, S = velocitySweeps forward P2 SOR
+  // sweeps per component from zero, started from seeded uniform [0, 1) values.
+  double estimateOmega(int L, int iters, uint64_t seed);
+  void coarseSolve(const int u[3], int p, const int f[3], int g);
+  void buildCoarse();
+
+  Storage& s;
+  int op, minL, maxL, pre, post;
+  double omega;
+  int velocitySweeps;
+  int pspg = -1;               // P1 PSPG operator on [minL, maxL]
+  int ru[3], rp;               // Uzawa residuals
+  int tu[3], tp;               // Stokes residual / restricted right-hand sides
+  std::vector<int> invDiag;    // per pressure level minL..maxL: 1 / diag(PSPG)
+  int coarseN = -1;
+  std::unique_ptr<DevBuf> coarseIdx, coarseComp, coarseInv;
 };
 
 // MinResSolver (solvers/MinresSolver.hpp:63-125) for the P2-P1 Taylor-Hood Stokes system on

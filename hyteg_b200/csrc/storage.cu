@@ -166,6 +166,7 @@ void Storage::buildLevel(int L) {
     for (int64_t s = 0; s < size; s += 8192) chunks.push_back({off + s, (int)std::min<int64_t>(8192, size - s), type});
   };
   for (int c = 0; c < lv.nCells; ++c) addChunks(lay.off[KC][c], lay.size[KC][c], cellType[c]);
+  ld.nCellChunks = (int)chunks.size();
   for (int f = 0; f < lv.nFaces; ++f) addChunks(lay.off[KF][f], lay.size[KF][f], faceType[f]);
   for (int e = 0; e < lv.nEdges; ++e) addChunks(lay.off[KE][e], lay.size[KE][e], lowType[e]);
   for (size_t v = 0; v < topo.verts.size(); ++v) addChunks(lay.off[KV][v], lay.size[KV][v], lowType[lv.nEdges + v]);
@@ -513,6 +514,8 @@ static void refillStencil(const dev::StencilDev<T>& d, const LevelStencils& st, 
   cudaCheck(cudaStreamSynchronize(stream), "stencil refill");
 }
 
+static std::vector<double> p2Stencils(const std::vector<double>& K, int nCells);
+
 int Storage::createP2Operator(int form, int minL, int maxL) {
   argCheck(form == FORM_LAPLACE, "P2 operators: only the Laplace form is available");
   argCheck(minL >= 0 && maxL + 1 <= maxLevel() && minL <= maxL,
@@ -531,6 +534,16 @@ int Storage::createP2Operator(int form, int minL, int maxL) {
     o->kf.emplace_back(new DevBuf());
     o->kf.back()->alloc(Kf.size() * sizeof(float));
     cudaCheck(cudaMemcpyAsync(o->kf.back()->p, Kf.data(), Kf.size() * sizeof(float), cudaMemcpyHostToDevice, stream),
+              "P2 upload");
+    const std::vector<double> S = p2Stencils(K, (int)disc.topo().cells.size());
+    std::vector<float> Sf(S.begin(), S.end());
+    o->sd.emplace_back(new DevBuf());
+    o->sd.back()->alloc(S.size() * sizeof(double));
+    cudaCheck(cudaMemcpyAsync(o->sd.back()->p, S.data(), S.size() * sizeof(double), cudaMemcpyHostToDevice, stream),
+              "P2 upload");
+    o->sf.emplace_back(new DevBuf());
+    o->sf.back()->alloc(Sf.size() * sizeof(float));
+    cudaCheck(cudaMemcpyAsync(o->sf.back()->p, Sf.data(), Sf.size() * sizeof(float), cudaMemcpyHostToDevice, stream),
               "P2 upload");
     cudaCheck(cudaStreamSynchronize(stream), "P2 upload");
   }
@@ -602,6 +615,7 @@ P2Additive& Storage::p2Additive(int Lf) {
   // p = (b1 & 1) | (b2 & 1) << 1 | (b3 & 1) << 2; p = 0 (micro-vertices of the coarse level) is
   // split into ((b1 >> 1) + 2 (b2 >> 1) + 3 (b3 >> 1)) mod 4, the others are colours 3 + p
   std::vector<unsigned char> col((size_t)ld.lay->total, 0x7f);
+  const bool keepOwners = ld.lay->total <= (int64_t(1) << 20);  // small (coarse) levels only
   for (int k = 0; k < 4; ++k)
     for (size_t pr = 0; pr < ld.lay->off[k].size(); ++pr)
       for (int64_t loc = 0; loc < ld.lay->size[k][pr]; ++loc) {
@@ -611,11 +625,42 @@ P2Additive& Storage::p2Additive(int Lf) {
         const int par = int(w[1] & 1) | (int(w[2] & 1) << 1) | (int(w[3] & 1) << 2);
         int c = par ? 3 + par : int(((w[1] >> 1) + 2 * (w[2] >> 1) + 3 * (w[3] >> 1)) % 4);
         const Slot o = disc.owner(Lf, b);
-        if (o.kind == k && o.prim == (int)pr && o.local == loc) c |= 0x80;
+        if (o.kind == k && o.prim == (int)pr && o.local == loc) {
+          c |= 0x80;
+          if (!keepOwners) {
+            col[(size_t)(ld.lay->off[k][pr] + loc)] = (unsigned char)c;
+            continue;
+          }
+          ad.hostOwner.push_back(ld.lay->off[k][pr] + loc);
+          ad.hostOwnerType.push_back(k == KC   ? ld.hostCellType[pr]
+                                     : k == KF ? ld.hostFaceType[pr]
+                                     : k == KE ? ld.hostLowType[pr]
+                                               : ld.hostLowType[ld.lv.nEdges + pr]);
+        }
         col[(size_t)(ld.lay->off[k][pr] + loc)] = (unsigned char)c;
       }
   ad.colour.alloc(col.size());
   cudaCheck(cudaMemcpyAsync(ad.colour.p, col.data(), col.size(), cudaMemcpyHostToDevice, stream), "p2 colour");
+  // the parity class of each colour's interior nodes per cell: an edge class is one colour in a
+  // cell's frame (read at its interior node nearest the origin), the vertex class holds colours 0-3
+  {
+    const int64_t M = ld.lv.N, w = M + 1;
+    auto tet = [](int64_t n) { return n * (n + 1) * (n + 2) / 6; };
+    std::vector<signed char> cls((size_t)ld.lv.nCells * 11, -1);
+    for (int c = 0; c < ld.lv.nCells; ++c) {
+      for (int k = 0; k < 4 && M >= 8; ++k) cls[(size_t)c * 11 + k] = 0;
+      for (int pc = 1; pc < 8; ++pc) {
+        const int64_t X = (pc & 1) ? 1 : 2, Y = (pc & 2) ? 1 : 2, Z = (pc & 4) ? 1 : 2;
+        if (X + Y + Z > M - 1) continue;
+        const int64_t loc = tet(w) - tet(w - Z) + Y * (w - Z + 1) - Y * (Y + 1) / 2 + X;
+        const int colr = col[(size_t)(ld.lay->off[KC][c] + loc)] & 0x7f;
+        argCheck(colr >= 4 && colr < 11 && cls[(size_t)c * 11 + colr] < 0, "P2 colour classes are inconsistent");
+        cls[(size_t)c * 11 + colr] = (signed char)pc;
+      }
+    }
+    ad.classOfColour.alloc(cls.size());
+    cudaCheck(cudaMemcpyAsync(ad.classOfColour.p, cls.data(), cls.size(), cudaMemcpyHostToDevice, stream), "p2 colour");
+  }
   std::vector<unsigned char> mult((size_t)ld.lay->total, 1);
   for (size_t i = 0; i + 1 < ptr.size(); ++i)
     for (int k = ptr[i]; k < ptr[i + 1]; ++k) mult[(size_t)cp[k]] = (unsigned char)(ptr[i + 1] - ptr[i]);
@@ -631,6 +676,31 @@ static const dev::P2Tables& p2TablesOnce() {
   return tb;
 }
 
+// Interior stencil weights of every cell: for each parity class, the sum over the class's
+// candidate micro-cells (type t, local node j) of row j of their element matrices, scattered
+// to the lattice offsets of the ten nodes in the order of p2s::kOff.
+static std::vector<double> p2Stencils(const std::vector<double>& K, int nCells) {
+  const dev::P2Tables& tb = p2TablesOnce();
+  std::vector<double> S((size_t)nCells * p2s::kTotal, 0.0);
+  for (int c = 0; c < nCells; ++c)
+    for (int pc = 0; pc < 8; ++pc) {
+      double* sc = S.data() + (size_t)c * p2s::kTotal + p2s::kFirst[pc];
+      for (int k = 0; k < tb.nCand[pc]; ++k) {
+        const int t = tb.cand[pc][k][0], j = tb.cand[pc][k][1];
+        for (int m = 0; m < 10; ++m) {
+          int e = 0;
+          while (e < p2s::kLen[pc] && !(p2s::kOff[pc][e][0] == tb.off[t][m][0] - tb.off[t][j][0] &&
+                                        p2s::kOff[pc][e][1] == tb.off[t][m][1] - tb.off[t][j][1] &&
+                                        p2s::kOff[pc][e][2] == tb.off[t][m][2] - tb.off[t][j][2]))
+            ++e;
+          if (e == p2s::kLen[pc]) throw Error(HG_ERR_INTERNAL, "P2 stencil offset table does not match the micro-cells");
+          sc[e] += K[(size_t)c * 600 + t * 100 + j * 10 + m];
+        }
+      }
+    }
+  return S;
+}
+
 // Cell gather + additive owner sums for one P2 level: dst = A src, rhs - A src or diag(A), on the
 // flagged DoFs of colour `sel` (all when sel < 0). The copies of dst are not refreshed here.
 template <class T, int MODE>
@@ -641,8 +711,20 @@ void Storage::p2Launch(P2Operator& o, int L, T* dst, const T* src, const T* rhs,
   const T* K = (const T*)(sizeof(T) == 8 ? o.kd[L - o.minL]->p : o.kf[L - o.minL]->p);
   const int nb = ld.lv.nCells * (ld.lv.N + 1);
   const unsigned char* col = (const unsigned char*)ad.colour.p;
-  dev::p2CellKernel<T, MODE><<<nb, dev::kBlock, 0, stream>>>(ld.lv, p2TablesOnce(), K, dst, src, rhs, mask, col, sel);
-  ++launches;
+  if constexpr (MODE == dev::MODE_DIAG) {
+    dev::p2CellKernel<T, MODE><<<nb, dev::kBlock, 0, stream>>>(ld.lv, p2TablesOnce(), K, dst, src, rhs, mask, col, sel);
+    ++launches;
+  } else {
+    // interior nodes by their constant stencils, closure nodes by the element gather
+    if (ld.lv.N >= 4) {
+      const T* W = (const T*)(sizeof(T) == 8 ? o.sd[L - o.minL]->p : o.sf[L - o.minL]->p);
+      dev::p2StencilKernel<T, MODE><<<ld.lv.nCells * (ld.lv.N - 3), dev::kBlock, 0, stream>>>(
+          ld.lv, W, dst, src, rhs, mask, col, (const signed char*)ad.classOfColour.p, sel, T(0));
+      ++launches;
+    }
+    dev::p2ClosureKernel<T><<<ld.lv.nCells * (ld.lv.N + dev::p2FaceChunks(ld.lv.N)), dev::kBlock, 0, stream>>>(ld.lv, p2TablesOnce(), K, dst, src, col, sel);
+    ++launches;
+  }
   if (ad.n) {
     constexpr int AM = MODE == dev::MODE_RESIDUAL ? dev::MODE_RESIDUAL : dev::MODE_REPLACE;
     dev::p2AddKernel<T, AM><<<(ad.n + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, stream>>>(
@@ -710,14 +792,51 @@ void Storage::p2SorT(P2Operator& o, int opId, int x, int b, int L, unsigned mask
   const int ax = p2scratch[key];
   const LevelData& ld = levels[Lf];
   P2Additive& ad = p2Additive(Lf);
+  const T* K = (const T*)(sizeof(T) == 8 ? o.kd[L - o.minL]->p : o.kf[L - o.minL]->p);
+  const T* W = (const T*)(sizeof(T) == 8 ? o.sd[L - o.minL]->p : o.sf[L - o.minL]->p);
+  const unsigned char* col = (const unsigned char*)ad.colour.p;
   for (int k = 0; k < 11; ++k) {
     const int c = backwards ? 10 - k : k;
     communicate(x, Lf, 1 << G_CELL);
-    p2Launch<T, dev::MODE_REPLACE>(o, L, (T*)data(ax, Lf), (const T*)data(x, Lf), nullptr, mask, c);
-    dev::p2SorUpdateKernel<T><<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (const unsigned char*)ad.colour.p, c,
-                                                                     (T*)data(x, Lf), (const T*)data(b, Lf),
-                                                                     (const T*)data(ax, Lf), (const T*)data(dg, Lf), omega);
+    T* xd = (T*)data(x, Lf);
+    const T* bd = (const T*)data(b, Lf);
+    T* axd = (T*)data(ax, Lf);
+    // face, edge and vertex DoFs of colour c: each cell's share of A x from the pass's start values
+    // (the colours of DoFs on different primitives are defined in different vertex frames, so a
+    // closure DoF may couple to an interior DoF of the same colour: its share is taken first)
+    dev::p2ClosureKernel<T><<<ld.lv.nCells * (ld.lv.N + dev::p2FaceChunks(ld.lv.N)), dev::kBlock, 0, stream>>>(ld.lv, p2TablesOnce(), K, axd, xd, col, c);
     ++launches;
+    // interior nodes of colour c. An edge colour is one parity class in a cell's frame and couples
+    // to no other node of its class, so those are updated in place (the closure copies keep their
+    // start values until the next refresh). The four vertex colours ((b1 + 2 b2 + 3 b3) / 2 mod 4
+    // in ascending vertex-ID order) separate the micro-edges along the macro-edges but not every
+    // diagonal micro-edge (barycentric step (1, -1, 1, -1)), so a vertex colour takes A x into the
+    // scratch first and is updated with the other owners.
+    const bool vertexColour = c < 4;
+    if (ld.lv.N >= 4) {
+      const signed char* cls = (const signed char*)ad.classOfColour.p;
+      if (vertexColour)
+        dev::p2StencilKernel<T, dev::MODE_REPLACE><<<ld.lv.nCells * (ld.lv.N - 3), dev::kBlock, 0, stream>>>(
+            ld.lv, W, axd, xd, nullptr, mask, col, cls, c, T(0));
+      else
+        dev::p2StencilKernel<T, dev::MODE_SOR><<<ld.lv.nCells * (ld.lv.N - 3), dev::kBlock, 0, stream>>>(
+            ld.lv, W, xd, xd, bd, mask, col, cls, c, omega);
+      ++launches;
+    }
+    // owner sums of the shares and the update of the face, edge and vertex DoFs (of the cell
+    // interiors too for a vertex colour)
+    if (ad.n) {
+      dev::p2AddKernel<T, dev::MODE_REPLACE><<<(ad.n + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, stream>>>(
+          (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
+          ad.n, axd, nullptr, mask, col, c);
+      ++launches;
+    }
+    const int first = vertexColour ? 0 : ld.nCellChunks;
+    if (ld.nChunks > first) {
+      dev::p2SorUpdateKernel<T><<<ld.nChunks - first, dev::kBlock, 0, stream>>>(ld.chunks + first, mask, col, c, xd, bd,
+                                                                               axd, (const T*)data(dg, Lf), omega);
+      ++launches;
+    }
   }
   cudaCheck(cudaGetLastError(), "P2 SOR");
   communicate(x, Lf, kAllGroups);
@@ -887,15 +1006,15 @@ int Storage::createStokesOperator(int minL, int maxL) {
   return id;
 }
 
+// v_k = D_k^T p (or += with add) at the velocity DoFs flagged by maskV: shares into three scratch
+// functions, owner sums, then written where flagged.
 template <class T>
-static void stokesCoupling(Storage& st, P2Operator& o, const int u[3], int p, const int v[3], int q, int L,
-                           unsigned maskV, unsigned maskP) {
+static void stokesDivTImpl(Storage& st, P2Operator& o, int p, const int v[3], int L, unsigned maskV, bool add) {
   const int Lv = L + 1, Lp = L;
   const LevelData& lvv = st.levels[Lv];
   const LevelData& lvp = st.levels[Lp];
   const T* D = (const T*)(sizeof(T) == 8 ? o.dd[L - o.minL]->p : o.df[L - o.minL]->p);
   const int prec = (int)sizeof(T);
-  // v_k += D_k^T p: shares into three scratch functions, owner sums, then added where flagged
   int sc[3];
   for (int k = 0; k < 3; ++k) {
     auto key = std::make_pair(Lv, 16 + 8 * k + prec);  // three distinct scratch buffers per level
@@ -914,11 +1033,20 @@ static void stokesCoupling(Storage& st, P2Operator& o, const int u[3], int p, co
           (const int64_t*)adv.owner.p, (const int*)adv.ptr.p, (const int64_t*)adv.copies.p,
           (const unsigned char*)adv.type.p, adv.n, (T*)st.data(sc[k], Lv), nullptr, maskV, nullptr, -1);
     const double one = 1.0;
-    st.lincomb(v[k], Lv, maskV, 1, &one, &sc[k], true, 0.0);
+    st.lincomb(v[k], Lv, maskV, 1, &one, &sc[k], add, 0.0);
     st.communicate(v[k], Lv, (1 << G_COUNT) - 1);
     st.launches += adv.n ? 1 : 0;
   }
-  // q = sum_k D_k u_k
+  cudaCheck(cudaGetLastError(), "Stokes divT");
+}
+
+// q = sum_k D_k u_k at the pressure DoFs flagged by maskP.
+template <class T>
+static void stokesDivImpl(Storage& st, P2Operator& o, const int u[3], int q, int L, unsigned maskP) {
+  const int Lv = L + 1, Lp = L;
+  const LevelData& lvv = st.levels[Lv];
+  const LevelData& lvp = st.levels[Lp];
+  const T* D = (const T*)(sizeof(T) == 8 ? o.dd[L - o.minL]->p : o.df[L - o.minL]->p);
   for (int k = 0; k < 3; ++k) st.communicate(u[k], Lv, 1 << G_CELL);
   P2Additive& adp = st.p2Additive(Lp);
   dev::p2DivKernel<T><<<lvp.lv.nCells * (lvp.lv.N + 1), dev::kBlock, 0, st.stream>>>(
@@ -931,8 +1059,56 @@ static void stokesCoupling(Storage& st, P2Operator& o, const int u[3], int p, co
         (const unsigned char*)adp.type.p, adp.n, (T*)st.data(q, Lp), nullptr, maskP, nullptr, -1);
     ++st.launches;
   }
-  cudaCheck(cudaGetLastError(), "Stokes coupling");
+  cudaCheck(cudaGetLastError(), "Stokes div");
   st.communicate(q, Lp, (1 << G_COUNT) - 1);
+}
+
+int Storage::p1Diagonal(int opId, int L) {
+  Operator& o = op(opId);
+  argCheck(L >= o.minL && L <= o.maxL, "level outside the operator's level range");
+  const LevelStencils& h = o.host[L - o.minL];
+  const LevelData& ld = levels[L];
+  const LevelLayout& lay = *ld.lay;
+  std::vector<double> vals;  // one value per chunk, in the chunk order of the level
+  auto add = [&](int64_t size, double v) {
+    for (int64_t s = 0; s < size; s += 8192) vals.push_back(v);
+  };
+  for (size_t c = 0; c < lay.size[KC].size(); ++c) add(lay.size[KC][c], h.cell[c][0]);
+  for (size_t f = 0; f < lay.size[KF].size(); ++f) add(lay.size[KF][f], h.face[f].empty() ? 0.0 : h.face[f][0].w);
+  for (size_t e = 0; e < lay.size[KE].size(); ++e) add(lay.size[KE][e], h.edge[e].empty() ? 0.0 : h.edge[e][0].w);
+  for (size_t v = 0; v < lay.size[KV].size(); ++v) add(lay.size[KV][v], h.vert[v].empty() ? 0.0 : h.vert[v][0].w);
+  argCheck((int)vals.size() == ld.nChunks, "diagonal: chunk table mismatch");
+  const int d = createFunction(L, L, 8);
+  if (ld.nChunks) {
+    DevBuf dv;
+    dv.alloc(vals.size() * sizeof(double));
+    cudaCheck(cudaMemcpyAsync(dv.p, vals.data(), vals.size() * sizeof(double), cudaMemcpyHostToDevice, stream), "diag");
+    dev::fillChunksKernel<<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, (const double*)dv.p, (double*)data(d, L));
+    ++launches;
+    cudaCheck(cudaStreamSynchronize(stream), "diag");
+  }
+  communicate(d, L, kAllGroups);
+  return d;
+}
+
+void Storage::stokesDivT(int opId, int p, const int v[3], int L, unsigned maskV, bool add) {
+  P2Operator& o = p2op(opId);
+  argCheck(!o.dd.empty(), "not a Stokes operator");
+  argCheck(L >= o.minL && L <= o.maxL, "level outside the Stokes operator's level range");
+  if (fn(p).prec == 8)
+    stokesDivTImpl<double>(*this, o, p, v, L, maskV, add);
+  else
+    stokesDivTImpl<float>(*this, o, p, v, L, maskV, add);
+}
+
+void Storage::stokesDiv(int opId, const int u[3], int q, int L, unsigned maskP) {
+  P2Operator& o = p2op(opId);
+  argCheck(!o.dd.empty(), "not a Stokes operator");
+  argCheck(L >= o.minL && L <= o.maxL, "level outside the Stokes operator's level range");
+  if (fn(q).prec == 8)
+    stokesDivImpl<double>(*this, o, u, q, L, maskP);
+  else
+    stokesDivImpl<float>(*this, o, u, q, L, maskP);
 }
 
 void Storage::stokesApply(int opId, const int u[3], int p, const int v[3], int q, int L, unsigned maskV,
@@ -944,10 +1120,8 @@ void Storage::stokesApply(int opId, const int u[3], int p, const int v[3], int q
   for (int k = 0; k < 3; ++k) argCheck(fn(u[k]).prec == prec && fn(v[k]).prec == prec, "Stokes: precision mismatch");
   argCheck(fn(q).prec == prec, "Stokes: precision mismatch");
   for (int k = 0; k < 3; ++k) p2Apply(opId, u[k], v[k], -1, L, maskV, 0);
-  if (prec == 8)
-    stokesCoupling<double>(*this, o, u, p, v, q, L, maskV, maskP);
-  else
-    stokesCoupling<float>(*this, o, u, p, v, q, L, maskV, maskP);
+  stokesDivT(opId, p, v, L, maskV, true);
+  stokesDiv(opId, u, q, L, maskP);
 }
 
 void Storage::autotuneSor(int minL, int maxL, int prec, int reps, double* ms) {
@@ -1003,7 +1177,7 @@ void Storage::reassembleOperator(int id) {
 }
 
 int Storage::createOperator(int form, int minL, int maxL) {
-  argCheck(form == FORM_LAPLACE || form == FORM_MASS, "unknown form");
+  argCheck(form == FORM_LAPLACE || form == FORM_MASS || form == FORM_PSPG, "unknown form");
   argCheck(minL >= 0 && maxL <= maxLevel() && minL <= maxL, "invalid level range");
   std::unique_ptr<Operator> op(new Operator());
   op->form = form;

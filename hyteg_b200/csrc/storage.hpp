@@ -32,6 +32,7 @@ struct LevelData {
   int64_t commBegin[G_COUNT] = {0, 0, 0, 0, 0}, commCount[G_COUNT] = {0, 0, 0, 0, 0};
   dev::Chunk* chunks = nullptr;
   int nChunks = 0;
+  int nCellChunks = 0;  // the chunks of the cell arrays come first
   // register-blocked cell sweep: work items grouped by macro-cell groups small enough to stay in L2
   dev::StripItem* tiles = nullptr;
   int nTiles = 0;
@@ -66,6 +67,7 @@ struct P2Operator {
   std::vector<std::unique_ptr<DevBuf>> kd, kf;  // per level: [cell][type][10][10] in FP64 / FP32
   std::map<std::pair<int, int>, int> diag;      // (level, precision) -> diagonal function
   std::vector<std::unique_ptr<DevBuf>> dd, df;  // Taylor-Hood divergence per level: [cell][type][3][4][10]
+  std::vector<std::unique_ptr<DevBuf>> sd, sf;  // interior stencils per level: [cell][p2s::kTotal]
 };
 
 // Cell-closure copies of every DoF owned by a face, edge or vertex of one lattice level.
@@ -75,6 +77,9 @@ struct P2Additive {
   DevBuf owner, ptr, copies, type;
   DevBuf colour;  // per slot: SOR colour of the DoF (0..10), bit 7 on its owner slot
   DevBuf mult;    // per slot: number of macro-cells holding the DoF (1 for cell-owned)
+  DevBuf classOfColour;  // per cell and colour 0..10: parity class of the colour's interior nodes, or -1
+  std::vector<int64_t> hostOwner;           // the owner slot of every DoF (levels up to 2^20 slots)
+  std::vector<unsigned char> hostOwnerType;  // and its DoF type
 };
 
 // Candidate micro-cells and coarse P2 basis values for the fine nodes of the 64 residue classes.
@@ -85,6 +90,7 @@ struct P2Transfer {
 
 struct Gmg;
 struct P2Gmg;
+struct StokesGmg;
 
 struct Storage {
   Storage(const Topology& topo, int maxLevel);
@@ -100,6 +106,7 @@ struct Storage {
   std::map<int, std::unique_ptr<Gmg>> gmgs;
   std::map<int, std::unique_ptr<P2Operator>> p2ops;
   std::map<int, std::unique_ptr<P2Gmg>> p2gmgs;
+  std::map<int, std::unique_ptr<StokesGmg>> stokesGmgs;
   std::deque<P2Additive> p2add;  // per lattice level
   int nextId = 1;
   int structureOp = -1;
@@ -158,6 +165,12 @@ struct Storage {
   //   q   = sum_k D_k u_k     (pressure DoFs flagged by maskP)
   int createStokesOperator(int minL, int maxL);
   void stokesApply(int op, const int u[3], int p, const int v[3], int q, int L, unsigned maskV, unsigned maskP);
+  // the coupling blocks alone: v_k = D_k^T p (v_k += with add), q = sum_k D_k u_k
+  void stokesDivT(int op, int p, const int v[3], int L, unsigned maskV, bool add);
+  void stokesDiv(int op, const int u[3], int q, int L, unsigned maskP);
+  // Diagonal of a P1 operator on level L (the stencil centre of each primitive's DoFs) as a new
+  // FP64 function of that level, owned by the caller.
+  int p1Diagonal(int op, int L);
   int p2Scratch(int Lf, int prec);
   template <class T, int MODE>
   void p2Launch(P2Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask, int sel);

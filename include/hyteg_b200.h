@@ -227,15 +227,46 @@ int hg_p2p1_stokes_minres(hg_storage* s, int op, const int u[3], int p, const in
 int hg_p2p1_stokes_minres_mixed(hg_storage* s, int op, const int u[3], int p, const int f[3], int g, int level, int nu,
                                 int max_iter, double tol, int precondition_precision, int* iterations,
                                 double* rel_residual, double* history, int history_cap);
+/* Geometric multigrid on the whole Taylor-Hood system (GeometricMultigridSolver with
+ * P2P1TaylorHoodStokesOperator, GeometricMultigridSolver.hpp:136-235) with the Uzawa smoother
+ * (UzawaSmoother.hpp:287-423, block-Laplace variant without stabilisation: r_u = f - D^T p;
+ * velocity_sweeps forward P2 SOR sweeps per component; p += omega (g - D u) / diag(PSPG)) and the
+ * composite transfers (P2P1StokesToP2P1StokesRestriction / Prolongation.hpp: quadratic on the
+ * velocity, linear on the pressure). Velocity DoFs flagged Inner | Neumann are unknowns, every
+ * pressure DoF is one (all-inner, P2P1TaylorHoodFunction.hpp:61). The coarsest level is solved by
+ * the pseudo-inverse of the operator on its unknowns (at most 1024). u, f: velocity P2 functions,
+ * p, g: pressure P1 functions, covering [min_level, max_level].
+ *   smooth:   one UzawaSmoother::solve step on level
+ *   solve:    one V(pre, post) cycle
+ *   solve_to: cycles to the relative residual tol (over the unknowns) */
+int hg_p2p1_stokes_uzawa_gmg_create(hg_storage* s, int op, int min_level, int max_level, int pre_smooth,
+                                    int post_smooth, double omega, int velocity_sweeps, int* gmg);
+int hg_p2p1_stokes_uzawa_gmg_destroy(hg_storage* s, int gmg);
+int hg_p2p1_stokes_uzawa_smooth(hg_storage* s, int gmg, const int u[3], int p, const int f[3], int g, int level);
+/* estimateUzawaRelaxationParameter (UzawaSmoother.hpp:52-68): the spectral radius of
+ * M_lumped^-1 D S D^T (S: the smoother's velocity sweeps from zero) by power_iterations power
+ * iterations (SpectrumEstimation.hpp:57-81) from seeded uniform [0, 1) values. */
+int hg_p2p1_stokes_uzawa_estimate_omega(hg_storage* s, int gmg, int level, int power_iterations, uint64_t seed,
+                                        double* omega);
+int hg_p2p1_stokes_uzawa_gmg_solve(hg_storage* s, int gmg, const int u[3], int p, const int f[3], int g, int level);
+int hg_p2p1_stokes_uzawa_gmg_solve_to(hg_storage* s, int gmg, const int u[3], int p, const int f[3], int g, int level,
+                                      double tol, int max_iter, int* iterations, double* rel_residual, double* history,
+                                      int history_cap);
+
 /* P2 geometric multigrid (GeometricMultigridSolver with P2ConstantLaplaceOperator, the P2 SOR
- * above, the quadratic transfers and CG on min_level), FP64. x, b: P2 functions covering
- * [min_level, max_level]. solve: one cycle; solve_to: cycles to the relative residual tol. */
+ * above and the quadratic transfers; GeometricMultigridSolver.hpp:136-235), FP64. x, b: P2
+ * functions covering [min_level, max_level]. solve: one cycle; solve_to: cycles to the relative
+ * residual tol. The coarsest level is solved exactly when it has at most 1024 unknowns (the
+ * inverse of the operator on them, built once), else by CG with coarse_max_iter / coarse_tol.
+ * With the exact coarse solve, cycles are captured as CUDA graphs and replayed (default on;
+ * the first cycle with a given set of buffers runs eagerly). set_graphs(0) turns that off. */
 int hg_p2_gmg_create(hg_storage* s, int op, int min_level, int max_level, int pre_smooth, int post_smooth,
                      double omega, int coarse_max_iter, double coarse_tol, int* gmg);
 int hg_p2_gmg_destroy(hg_storage* s, int gmg);
 int hg_p2_gmg_solve(hg_storage* s, int gmg, int x, int b, int level);
 int hg_p2_gmg_solve_to(hg_storage* s, int gmg, int x, int b, int level, double tol, int max_iter, int* iterations,
                        double* rel_residual, double* history, int history_cap);
+int hg_p2_gmg_set_graphs(hg_storage* s, int gmg, int enable);
 
 /* ---------------------------------------------------------------------------------------
  * Solve server (continuous batching). No counterpart in the reference, which solves one
@@ -270,7 +301,9 @@ int hg_server_stats(hg_server* srv, int64_t stats[6]);
  * values depend only on (seed, slot), so equal topologies give equal vectors. */
 int hg_function_fill_random(hg_storage* s, int fn, int level, unsigned flag, uint64_t seed, double lo, double hi);
 
-/* form: 0 = diffusion (Laplace, scaled by the per-cell coefficient), 1 = mass */
+/* form: 0 = diffusion (Laplace, scaled by the per-cell coefficient), 1 = mass, 2 = PSPG
+ * stabilisation -tau grad p . grad q with tau = |T|^(2/3) / 12 per micro-cell (P1PSPGOperator,
+ * p1functionspace/P1ConstantOperator.hpp:201-208; forms/form_fenics_generated/p1_tet_pspg_tet.h) */
 int hg_operator_create(hg_storage* s, int form, int min_level, int max_level, int* op);
 int hg_operator_destroy(hg_storage* s, int op);
 /* update: 0 = Replace, 1 = Add */

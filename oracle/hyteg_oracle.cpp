@@ -76,6 +76,15 @@ void laplaceElement(const double p[4][3], double K[4][4]) {
     for (int j = 0; j < 4; ++j) K[i][j] = vol * (g[i][0] * g[j][0] + g[i][1] * g[j][1] + g[i][2] * g[j][2]);
 }
 
+double tetVolume(const double p[4][3]) {
+  double a[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int d = 0; d < 3; ++d) a[i][d] = p[i + 1][d] - p[0][d];
+  const double det = a[0][0] * (a[1][1] * a[2][2] - a[1][2] * a[2][1]) - a[0][1] * (a[1][0] * a[2][2] - a[1][2] * a[2][0]) +
+                     a[0][2] * (a[1][0] * a[2][1] - a[1][1] * a[2][0]);
+  return std::fabs(det) / 6.0;
+}
+
 void massElement(const double p[4][3], double K[4][4]) {
   double a[3][3];
   for (int i = 0; i < 3; ++i)
@@ -206,8 +215,8 @@ struct LevelData {
   bool haveP2prol = false;
   std::vector<Node> nodes;
   std::unordered_map<Key, int64_t, KeyHash> index;
-  Csr A[2];                  // 0: diffusion (per-cell coefficient), 1: mass
-  bool haveA[2] = {false, false};
+  Csr A[3];                  // 0: diffusion (per-cell coefficient), 1: mass, 2: PSPG
+  bool haveA[3] = {false, false, false};
   // prolongation from the next coarser level: per node up to two coarse nodes
   std::vector<std::array<int64_t, 2>> pc;
   std::vector<std::array<double, 2>> pw;
@@ -393,6 +402,12 @@ void buildMatrix(Oracle& o, int L, int form) {
               laplaceElement(p, K);
               for (auto& r : K)
                 for (double& v : r) v *= o.k[ci];
+            } else if (form == 2) {
+              // PSPG (data/operators/form_pspg_tet.ufl): -tau grad p . grad q, tau = |T|^(2/3) / 12
+              laplaceElement(p, K);
+              const double tau = std::pow(tetVolume(p), 2.0 / 3.0) / 12.0;
+              for (auto& r : K)
+                for (double& v : r) v *= -tau;
             } else {
               massElement(p, K);
             }
@@ -605,6 +620,29 @@ void orc_prolongate(void* h, int Lc, const double* coarse, double* fine, int add
   const LevelData& f = o.lv[Lc + 1];
   for (size_t i = 0; i < f.nodes.size(); ++i) {
     if (f.nodes[i].dirichlet) continue;
+    double v = 0.0;
+    for (int k = 0; k < 2; ++k)
+      if (f.pc[i][k] >= 0) v += f.pw[i][k] * coarse[f.pc[i][k]];
+    fine[i] = add ? fine[i] + v : v;
+  }
+}
+
+// The same transfers on every node (a function whose DoFs are all unknowns, like the
+// Taylor-Hood pressure): coarse = P^T fine, fine (+)= P coarse.
+void orc_restrict_all(void* h, int Lf, const double* fine, double* coarse) {
+  Oracle& o = *(Oracle*)h;
+  const LevelData& f = o.lv[Lf];
+  const LevelData& c = o.lv[Lf - 1];
+  for (size_t j = 0; j < c.nodes.size(); ++j) coarse[j] = 0.0;
+  for (size_t i = 0; i < f.nodes.size(); ++i)
+    for (int k = 0; k < 2; ++k)
+      if (f.pc[i][k] >= 0) coarse[f.pc[i][k]] += f.pw[i][k] * fine[i];
+}
+
+void orc_prolongate_all(void* h, int Lc, const double* coarse, double* fine, int add) {
+  Oracle& o = *(Oracle*)h;
+  const LevelData& f = o.lv[Lc + 1];
+  for (size_t i = 0; i < f.nodes.size(); ++i) {
     double v = 0.0;
     for (int k = 0; k < 2; ++k)
       if (f.pc[i][k] >= 0) v += f.pw[i][k] * coarse[f.pc[i][k]];
@@ -831,6 +869,38 @@ void orc_stokes_apply(void* h, int L, const double* u0, const double* u1, const 
         q[i] += D.val[m] * u[k][D.col[m]];
         v[k][D.col[m]] += D.val[m] * p[i];
       }
+  }
+}
+
+// P1 PSPG element matrix -tau K_laplace, tau = |T|^(2/3) / 12
+void orc_element_pspg(const double* coords12, double* K16) {
+  double p[4][3], K[4][4];
+  for (int m = 0; m < 4; ++m)
+    for (int d = 0; d < 3; ++d) p[m][d] = coords12[3 * m + d];
+  laplaceElement(p, K);
+  const double tau = std::pow(tetVolume(p), 2.0 / 3.0) / 12.0;
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) K16[4 * a + b] = -tau * K[a][b];
+}
+
+// Row sums of the assembled mass matrix of level L (the lumped mass, every node)
+void orc_lumped_mass(void* h, int L, double* d) {
+  Oracle& o = *(Oracle*)h;
+  const Csr& A = matrix(o, L, 1);
+  for (size_t i = 0; i + 1 < A.ptr.size(); ++i) {
+    d[i] = 0.0;
+    for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k) d[i] += A.val[k];
+  }
+}
+
+// Diagonal of the assembled PSPG matrix of level L (every node)
+void orc_pspg_diag(void* h, int L, double* d) {
+  Oracle& o = *(Oracle*)h;
+  const Csr& A = matrix(o, L, 2);
+  for (size_t i = 0; i + 1 < A.ptr.size(); ++i) {
+    d[i] = 0.0;
+    for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+      if (A.col[k] == (int64_t)i) d[i] += A.val[k];
   }
 }
 

@@ -49,6 +49,11 @@ def _load_oracle():
         "orc_p2_cg": (c_int, [c_void_p, c_int, P(c_double), P(c_double), c_int, c_double]),
         "orc_stokes_apply": (None, [c_void_p, c_int] + [P(c_double)] * 8),
         "orc_p2p1_div_element": (None, [P(c_double), P(c_double)]),
+        "orc_element_pspg": (None, [P(c_double), P(c_double)]),
+        "orc_pspg_diag": (None, [c_void_p, c_int, P(c_double)]),
+        "orc_lumped_mass": (None, [c_void_p, c_int, P(c_double)]),
+        "orc_restrict_all": (None, [c_void_p, c_int, P(c_double), P(c_double)]),
+        "orc_prolongate_all": (None, [c_void_p, c_int, P(c_double), P(c_double), c_int]),
         "orc_cell_local_stencil": (None, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, P(c_double)]),
     }
     for name, (res, args) in sig.items():
@@ -82,11 +87,12 @@ def ref_lib():
     r.ref_p1_tet_diffusion.argtypes = [d, d]
     r.ref_p1_tet_mass.argtypes = [d, d]
     r.ref_p2_tet_diffusion.argtypes = [d, d]
+    r.ref_p1_tet_pspg.argtypes = [d, d]
     r.ref_p2_to_p1_div.argtypes = [d, c_int, d]
     r.ref_p1_to_p2_divt.argtypes = [d, c_int, d]
     for f in (r.ref_apply_cell, r.ref_sor_cell, r.ref_apply_face, r.ref_restrict_cell, r.ref_prolongate_cell,
               r.ref_p1_tet_diffusion, r.ref_p1_tet_mass, r.ref_p2_tet_diffusion, r.ref_p2_to_p1_div,
-              r.ref_p1_to_p2_divt):
+              r.ref_p1_to_p2_divt, r.ref_p1_tet_pspg):
         f.restype = None
     return r
 
@@ -220,6 +226,118 @@ class Oracle:
         q = np.zeros(self.n(L))
         lib().orc_stokes_apply(self.h, L, dp(u[0]), dp(u[1]), dp(u[2]), dp(p), dp(v[0]), dp(v[1]), dp(v[2]), dp(q))
         return v, q
+
+    def restrict_all(self, Lf, fine):
+        """P1 linear restriction P^T on every node (all-inner functions such as the pressure)."""
+        fine = np.ascontiguousarray(fine, dtype=np.float64)
+        coarse = np.zeros(self.n(Lf - 1))
+        lib().orc_restrict_all(self.h, Lf, dp(fine), dp(coarse))
+        return coarse
+
+    def prolongate_all(self, Lc, coarse, fine=None, add=False):
+        coarse = np.ascontiguousarray(coarse, dtype=np.float64)
+        fine = np.zeros(self.n(Lc + 1)) if fine is None else np.ascontiguousarray(fine, dtype=np.float64).copy()
+        lib().orc_prolongate_all(self.h, Lc, dp(coarse), dp(fine), 1 if add else 0)
+        return fine
+
+    def pspg_diag(self, L):
+        """Diagonal of the assembled P1 PSPG matrix (-tau grad.grad, tau = |T|^(2/3) / 12)."""
+        d = np.zeros(self.n(L))
+        lib().orc_pspg_diag(self.h, L, dp(d))
+        return d
+
+    def uzawa_smooth(self, L, u, p, f, g, omega, velocity_sweeps=2):
+        """UzawaSmoother::uzawaSmooth (solvers/UzawaSmoother.hpp:287-423, block-Laplace variant
+        without stabilisation) on P2 level L: r_u = f - D^T p; velocity_sweeps times one forward
+        multicolour P2 SOR sweep (omega 1) per component; r_p = g - D u; p += omega r_p / diag(PSPG).
+        Velocity Dirichlet values are kept; every pressure node is an unknown."""
+        nv, npr = self.n(L + 1), self.n(L)
+        u = [np.array(x, dtype=np.float64) for x in u]
+        p = np.array(p, dtype=np.float64)
+        dt, _ = self.stokes_apply(L, [np.zeros(nv)] * 3, p)
+        r = [f[k] - dt[k] for k in range(3)]
+        for _ in range(velocity_sweeps):
+            for k in range(3):
+                u[k] = self.p2_sor(L, u[k], r[k], 1.0)
+        _, q = self.stokes_apply(L, u, np.zeros(npr))
+        p = p + omega * (g - q) / self.pspg_diag(L)
+        return u, p
+
+    def uzawa_estimate(self, L, start, iterations, velocity_sweeps=2):
+        """estimateUzawaRelaxationParameter (solvers/UzawaSmoother.hpp:52-68): power iterations
+        (numerictools/SpectrumEstimation.hpp:57-81) on E = M_lumped^-1 D S D^T from `start`, S the
+        velocity sweeps of the Uzawa smoother from zero; 2-norms over every pressure node."""
+        nv, npr = self.n(L + 1), self.n(L)
+        lumped = np.zeros(npr)
+        lib().orc_lumped_mass(self.h, L, dp(lumped))
+
+        def E(v):
+            dt, _ = self.stokes_apply(L, [np.zeros(nv)] * 3, v)
+            u = [np.zeros(nv) for _ in range(3)]
+            for _ in range(velocity_sweeps):
+                for k in range(3):
+                    u[k] = self.p2_sor(L, u[k], dt[k], 1.0)
+            _, q = self.stokes_apply(L, u, np.zeros(npr))
+            return q / lumped
+
+        it = np.asarray(start, dtype=np.float64) / np.linalg.norm(start)
+        aux = E(it)
+        radius = 0.0
+        for _ in range(iterations):
+            it = aux / np.linalg.norm(aux)
+            aux = E(it)
+            radius = float(it @ aux)
+        return radius
+
+    def stokes_residual(self, L, u, p, f, g):
+        v, q = self.stokes_apply(L, u, p)
+        dv = self.dirichlet(L + 1)
+        return [np.where(dv, 0.0, f[k] - v[k]) for k in range(3)], g - q
+
+    def stokes_coarse_solve(self, L, u, p, f, g):
+        """u, p += K^+ (b - K x) on the unknowns of level L (inner velocity DoFs, every pressure
+        DoF); K^+ the pseudo-inverse of the assembled block operator (numpy)."""
+        dv = self.dirichlet(L + 1)
+        free = np.where(~dv)[0]
+        nf, npr = len(free), self.n(L)
+        n = 3 * nf + npr
+        K = np.zeros((n, n))
+        for c in range(n):
+            e = np.zeros(n)
+            e[c] = 1.0
+            uu = [np.zeros(self.n(L + 1)) for _ in range(3)]
+            for k in range(3):
+                uu[k][free] = e[k * nf:(k + 1) * nf]
+            v, q = self.stokes_apply(L, uu, e[3 * nf:])
+            K[:, c] = np.concatenate([v[0][free], v[1][free], v[2][free], q])
+        K = 0.5 * (K + K.T)
+        ru, rp = self.stokes_residual(L, u, p, f, g)
+        x = np.linalg.pinv(K, rcond=1e-10, hermitian=True) @ np.concatenate([ru[0][free], ru[1][free], ru[2][free], rp])
+        u = [np.array(x_, dtype=np.float64) for x_ in u]
+        for k in range(3):
+            u[k][free] += x[k * nf:(k + 1) * nf]
+        return u, p + x[3 * nf:]
+
+    def stokes_uzawa_cycle(self, L, minL, u, p, f, g, pre, post, omega, velocity_sweeps=2):
+        """One V-cycle of GeometricMultigridSolver (GeometricMultigridSolver.hpp:136-235) on the
+        Taylor-Hood system with the Uzawa smoother and the composite transfers (quadratic on the
+        velocity, linear on the pressure), the pseudo-inverse on level minL."""
+        if L == minL:
+            return self.stokes_coarse_solve(L, u, p, f, g)
+        for _ in range(pre):
+            u, p = self.uzawa_smooth(L, u, p, f, g, omega, velocity_sweeps)
+        ru, rp = self.stokes_residual(L, u, p, f, g)
+        dc = self.dirichlet(L)
+        fc = [np.where(dc, 0.0, self.p2_restrict(L, ru[k])) for k in range(3)]
+        gc = self.restrict_all(L, rp)
+        uc, pc = self.stokes_uzawa_cycle(L - 1, minL, [np.zeros(self.n(L))] * 3, np.zeros(self.n(L - 1)), fc, gc, pre,
+                                         post, omega, velocity_sweeps)
+        dv = self.dirichlet(L + 1)
+        u = [np.where(dv, u[k], self.p2_prolongate(L - 1, uc[k], u[k], add=True)) for k in range(3)]
+        p = self.prolongate_all(L - 1, pc, p, add=True)
+        for _ in range(post):
+            u, p = self.uzawa_smooth(L, u, p, f, g, omega, velocity_sweeps)
+        return u, p
 
     def cell_local_stencil(self, L, cell, x, y, z, form=0):
         out = np.zeros(15)

@@ -8,6 +8,7 @@
 #include "hyteg/fenics/ufc.h"
 #include "hyteg/forms/form_fenics_generated/p1_tet_diffusion.h"
 #include "hyteg/forms/form_fenics_generated/p1_tet_mass.h"
+#include "hyteg/forms/form_fenics_generated/p1_tet_pspg_tet.h"
 #include "hyteg/forms/form_fenics_generated/p2_tet_diffusion.h"
 #include "hyteg/forms/form_fenics_generated/p2_to_p1_tet_div_tet.h"
 #include "hyteg/forms/form_fenics_generated/p1_to_p2_tet_divt_tet.h"
@@ -87,6 +88,13 @@ void ref_p1_tet_diffusion(const double* coords12, double* K16) {
 
 void ref_p1_tet_mass(const double* coords12, double* K16) {
   p1_tet_mass_cell_integral_0_otherwise f;
+  f.tabulate_tensor(K16, nullptr, coords12, 0);
+}
+
+// PSPG stabilisation form -tau grad p . grad q, tau = |T|^(2/3) / 12 (P1PSPGOperator; its
+// inverse diagonal is the pressure scaling of the Uzawa smoother).
+void ref_p1_tet_pspg(const double* coords12, double* K16) {
+  p1_tet_pspg_tet_cell_integral_0_otherwise f;
   f.tabulate_tensor(K16, nullptr, coords12, 0);
 }
 

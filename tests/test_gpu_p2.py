@@ -1,6 +1,8 @@
 """P2 Laplace apply and residual on the device against the oracle's globally assembled P2
-matrix (48-tet cube, P2 levels 0-3 = vertex lattices 1-4; 3x3x3 cube for coarse levels with
-inner DoFs on every primitive kind).
+matrix (48-tet cube, P2 levels 0-4 = vertex lattices 1-5; 3x3x3 cube for coarse levels with
+inner DoFs on every primitive kind). From lattice 8 per macro-cell on, every parity class has
+interior nodes, which take the constant-stencil kernels; the closure nodes take the element
+gather.
 
 Tolerances: 1e-13 relative in FP64 and 2e-5 in FP32 (max-norm over inner DoFs); Dirichlet DoFs
 are not written."""
@@ -181,3 +183,89 @@ def test_p2_multigrid_solves_to_oracle_solution(cube2):
     ref = orc.p2_cg(L, np.zeros(n), bg, 20000, 1e-14)
     got = H.gather_owned(x.to_numpy(L), node, owned, n)
     assert rel(got, ref, inner) < 1e-8
+
+
+@pytest.fixture(scope="module")
+def cube2l4():
+    return setup(2, 4)
+
+
+@pytest.mark.parametrize("residual", [False, True])
+def test_p2_apply_interior_stencils_level4(cube2l4, residual):
+    # lattice 32 per macro-cell: most DoFs are interior and take the constant-stencil kernel
+    got, ref, inner, d0 = run_apply(cube2l4, 4, np.float64, residual, 90 + residual)
+    assert rel(got, ref, inner) < 1e-13
+    assert np.array_equal(got[~inner], d0[~inner])
+
+
+@pytest.mark.parametrize("backwards", [False, True])
+def test_p2_multicolour_sor_level4(cube2l4, backwards):
+    st, orc, maps = cube2l4
+    L = 4
+    node, owned = maps[L]
+    n = orc.n(L + 1)
+    rng = np.random.default_rng(300 + backwards)
+    u0, f0 = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    A = hg.P2ConstantLaplaceOperator(st, 0, L)
+    x, b = hg.P2Function("x", st, 0, L), hg.P2Function("b", st, 0, L)
+    x.from_numpy(L, H.scatter(node, u0))
+    b.from_numpy(L, H.scatter(node, f0))
+    for _ in range(2):
+        (A.smooth_sor_backwards if backwards else A.smooth_sor)(x, b, 0.9, L)
+    got = H.gather_owned(x.to_numpy(L), node, owned, n)
+    ref = orc.p2_sor(L, u0, f0, 0.9, sweeps=2, backwards=backwards)
+    inner = ~orc.dirichlet(L + 1)
+    assert rel(got, ref, inner) < 1e-13
+    # copies of every DoF agree with its owner after the sweeps
+    full = x.to_numpy(L)
+    used = owned >= 0
+    assert np.array_equal(full[used], got[node[used]])
+
+
+def test_p2_graph_cycles_match_eager_cycles(cube2):
+    # replayed CUDA graphs launch the same kernels; the restriction's atomic sums make the
+    # agreement one of rounding, not of bits
+    st, orc, maps = cube2
+    L = 3
+    node, owned = maps[L]
+    bg = np.random.default_rng(7).uniform(-1, 1, orc.n(L + 1))
+    bg[orc.dirichlet(L + 1)] = 0.0
+    out = []
+    for graphs in (False, True):
+        A = hg.P2ConstantLaplaceOperator(st, 0, 3)
+        x, b = hg.P2Function("x", st, 0, 3), hg.P2Function("b", st, 0, 3)
+        b.from_numpy(L, H.scatter(node, bg))
+        gmg = hg.P2GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0)
+        gmg.set_graphs(graphs)
+        launches = []
+        for _ in range(5):
+            l0 = st.launch_count()
+            gmg.solve(x, b, L)
+            launches.append(st.launch_count() - l0)
+        out.append((x.to_numpy(L), launches))
+    (xe, le), (xg, lg) = out
+    assert le == lg
+    assert np.abs(xe - xg).max() / np.abs(xe).max() < 1e-13
+
+
+def test_p2_multigrid_exact_coarse_solve_on_3x3x3_cube(cube3):
+    # 125 unknowns on the coarsest P2 level: solved exactly through the inverse on the device
+    st, orc, maps = cube3
+    L = 1
+    node, owned = maps[L]
+    n = orc.n(L + 1)
+    inner = ~orc.dirichlet(L + 1)
+    assert (~orc.dirichlet(1)).sum() == 125
+    bg = np.random.default_rng(11).uniform(-1, 1, n)
+    bg[~inner] = 0.0
+    A = hg.P2ConstantLaplaceOperator(st, 0, 1)
+    x, b = hg.P2Function("x", st, 0, 1), hg.P2Function("b", st, 0, 1)
+    b.from_numpy(L, H.scatter(node, bg))
+    gmg = hg.P2GeometricMultigridSolver(st, A, 0, L, 2, 2, 1.0)
+    it, relres, hist = gmg.solve_to(x, b, L, 1e-11, 40)
+    assert relres <= 1e-11
+    ref = orc.p2_cg(L, np.zeros(n), bg, 20000, 1e-14)
+    got = H.gather_owned(x.to_numpy(L), node, owned, n)
+    assert rel(got, ref, inner) < 1e-8
+    # a two-level cycle whose coarse level is exact contracts strongly
+    assert (hist[1:] / hist[:-1]).max() < 0.4

@@ -287,3 +287,29 @@ def test_p2p1_divergence_element_matches_reference_forms(ref, oracle_mod):
             B = B.reshape(10, 4)[perm, :]
             assert np.abs(D[k] - A).max() <= 1e-13 * np.abs(A).max()
             assert np.abs(D[k].T - B).max() <= 1e-13 * np.abs(B).max()
+
+
+def test_pspg_element_matches_reference_form(ref, oracle_mod):
+    # p1_tet_pspg_tet: -tau grad p . grad q, tau = |T|^(2/3) / 12 (the Uzawa smoother's pressure scaling)
+    rng = np.random.default_rng(17)
+    for _ in range(10):
+        c = np.ascontiguousarray(rng.uniform(-1, 1, (4, 3)).reshape(12))
+        K = np.zeros(16)
+        ref.ref_p1_tet_pspg(oracle_mod.dp(c), oracle_mod.dp(K))
+        mine = np.zeros(16)
+        oracle_mod.lib().orc_element_pspg(oracle_mod.dp(c), oracle_mod.dp(mine))
+        assert np.abs(mine - K).max() <= 1e-13 * np.abs(K).max()
+
+
+def test_pspg_diagonal_is_the_element_sum(oracle_mod):
+    # the diagonal of the assembled PSPG matrix: on the uniformly refined unit cube every micro-cell
+    # of level L has volume 1 / (48 8^L) and tau = vol^(2/3) / 12, so diag = -tau * Laplace diagonal
+    coords, tets = oracle_mod.cuboid_mesh((0, 0, 0), (1, 1, 1), 2, 2, 2)
+    o = oracle_mod.Oracle(coords, tets, 2)
+    for L in (1, 2):
+        vol = 1.0 / (48 * 8 ** L)
+        tau = vol ** (2.0 / 3.0) / 12.0
+        n = o.n(L)
+        lap = np.array([o.apply(L, np.eye(1, n, i)[0])[i] for i in range(n)])
+        inner = ~o.dirichlet(L)
+        assert np.allclose(o.pspg_diag(L)[inner], -tau * lap[inner], rtol=1e-12)
