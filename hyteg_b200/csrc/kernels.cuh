@@ -1034,45 +1034,119 @@ __global__ void __launch_bounds__(kBlock) p2StencilKernel(LevelDev lv, const T* 
 }
 
 // The closure nodes of every macro-cell (its faces, edges and vertices): this cell's share of
-// row j of A, by the element gather, written into the cell's closure slot (p2AddKernel sums the
-// shares into the owner). Grid: nCells * (M + kP2FaceChunks(M)) blocks. Per cell, M blocks take
-// the boundary rings of the planes Z = 1 .. M (3 (M - Z) nodes, 1 at the top), and
-// kP2FaceChunks(M) blocks take the face Z = 0 in chunks of eight rows (a warp per row).
+// row j of A, written into the cell's closure slot (p2AddKernel sums the shares into the owner).
+// A node inside one face of the cell sees the same micro-cells at every node of its (face, class):
+// its share is a constant stencil (p2s::FaceList, weights FW[cell][p2s::kFaceTotal]). Nodes on the
+// cell's edges and vertices take the element gather. Grid: nCells * (M + p2FaceChunks(M)) blocks.
+// Per cell, M blocks take the planes Z = 1 .. M: on each, warps 0-5 walk the lines of faces
+// Y = 0, X = 0 and X + Y + Z = M (one warp per line and parity, so a warp runs one class), warp 6
+// the three edge nodes of the plane. p2FaceChunks(M) blocks take the face Z = 0 in chunks of eight
+// rows (a warp per row).
 __host__ __device__ __forceinline__ int p2FaceChunks(int M) { return (M + 1 + 7) / 8; }
+
+template <class T, int K>
+__device__ __forceinline__ T p2FaceDot(const T* u, const T* fw, const int (&pbz)[5], int w, int X, int Y, int Z) {
+  using S = typename p2s::FaceList<K>::type;
+  constexpr int kFirst = p2s::kFaceFirst[K], kLen = p2s::kFaceLen[K];
+  return p2StencilDot<T>(S{}, std::make_integer_sequence<int, kLen>{}, u, fw + kFirst, pbz, w, X, Y, Z);
+}
+
+template <class T>
+__device__ __forceinline__ T p2FaceDotAny(int k, const T* u, const T* fw, const int (&pbz)[5], int w, int X, int Y,
+                                          int Z) {
+  switch (k) {
+    case 0: return p2FaceDot<T, 0>(u, fw, pbz, w, X, Y, Z);
+    case 1: return p2FaceDot<T, 1>(u, fw, pbz, w, X, Y, Z);
+    case 2: return p2FaceDot<T, 2>(u, fw, pbz, w, X, Y, Z);
+    case 3: return p2FaceDot<T, 3>(u, fw, pbz, w, X, Y, Z);
+    case 4: return p2FaceDot<T, 4>(u, fw, pbz, w, X, Y, Z);
+    case 5: return p2FaceDot<T, 5>(u, fw, pbz, w, X, Y, Z);
+    case 6: return p2FaceDot<T, 6>(u, fw, pbz, w, X, Y, Z);
+    case 7: return p2FaceDot<T, 7>(u, fw, pbz, w, X, Y, Z);
+    case 8: return p2FaceDot<T, 8>(u, fw, pbz, w, X, Y, Z);
+    case 9: return p2FaceDot<T, 9>(u, fw, pbz, w, X, Y, Z);
+    case 10: return p2FaceDot<T, 10>(u, fw, pbz, w, X, Y, Z);
+    case 11: return p2FaceDot<T, 11>(u, fw, pbz, w, X, Y, Z);
+    case 12: return p2FaceDot<T, 12>(u, fw, pbz, w, X, Y, Z);
+    case 13: return p2FaceDot<T, 13>(u, fw, pbz, w, X, Y, Z);
+    case 14: return p2FaceDot<T, 14>(u, fw, pbz, w, X, Y, Z);
+    default: return p2FaceDot<T, 15>(u, fw, pbz, w, X, Y, Z);
+  }
+}
+
+// Entry of (face f, class pc) in the face tables; the classes of a face are listed ascending:
+// Z = 0: {0, 1, 2, 3}; Y = 0: {0, 1, 4, 5}; X = 0: {0, 2, 4, 6}; X + Y + Z = M: {0, 3, 5, 6}.
+__device__ __forceinline__ int p2FaceEntry(int f, int pc) {
+  switch (f) {
+    case 0: return pc;
+    case 1: return 4 + ((pc & 1) | ((pc >> 1) & 2));
+    case 2: return 8 + (((pc >> 1) & 1) | ((pc >> 1) & 2));
+    default: return 12 + (pc == 0 ? 0 : pc == 3 ? 1 : pc == 5 ? 2 : 3);
+  }
+}
 
 template <class T>
 __global__ void __launch_bounds__(kBlock) p2ClosureKernel(LevelDev lv, P2Tables tb, const T* __restrict__ K,
-                                                          T* __restrict__ dst, const T* __restrict__ src,
+                                                          const T* __restrict__ FW, T* __restrict__ dst,
+                                                          const T* __restrict__ src,
                                                           const unsigned char* __restrict__ colour, int sel) {
   const int M = lv.N, N = M / 2, w = lv.w, perCell = M + p2FaceChunks(M);
   const int c = blockIdx.x / perCell, q = blockIdx.x % perCell;
   const int Z = q < M ? q + 1 : 0;
   const int64_t base = lv.cellOff[c];
   const T* Kc = K + (int64_t)c * 600;
+  __shared__ T fw[p2s::kFaceTotal];
+  for (int k = threadIdx.x; k < p2s::kFaceTotal; k += blockDim.x) fw[k] = FW[(int64_t)c * p2s::kFaceTotal + k];
+  __syncthreads();
   int pbz[5];
 #pragma unroll
   for (int d = 0; d < 5; ++d) {
     const int z = Z - 2 + d;
     pbz[d] = (z >= 0 && z <= M) ? int(tetSize(w) - tetSize(w - z)) : 0;
   }
-  auto node = [&](int X, int Y) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  auto gatherNode = [&](int X, int Y) {
     const int64_t i = base + pbz[2] + rowStart(w - Z, Y) + X;
     if (sel < 0 || (colour[i] & 0x7f) == sel) dst[i] = p2GatherNode<T, false>(tb, Kc, src + base, pbz, w, N, X, Y, Z);
   };
+  auto faceNode = [&](int k, int X, int Y) {
+    const int64_t i = base + pbz[2] + rowStart(w - Z, Y) + X;
+    if (sel < 0 || (colour[i] & 0x7f) == sel) dst[i] = p2FaceDotAny<T>(k, src + base, fw, pbz, w, X, Y, Z);
+  };
   const int n = M - Z;
   if (Z == 0) {
-    const int Y = (q - M) * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (Y <= n)
-      for (int X = lane; X <= n - Y; X += 32) node(X, Y);
-  } else {
-    for (int r = threadIdx.x; r < (n == 0 ? 1 : 3 * n); r += blockDim.x) {
-      if (r <= n)
-        node(r, 0);
-      else if (r <= 2 * n)
-        node(0, r - n);
-      else
-        node(n - (r - 2 * n), r - 2 * n);
+    const int Y = (q - M) * 8 + warp;
+    if (Y > n) return;
+    if (Y == 0) {
+      for (int X = lane; X <= n; X += 32) gatherNode(X, 0);
+      return;
     }
+    if (lane == 0) gatherNode(0, Y);
+    if (lane == 1 && n - Y > 0) gatherNode(n - Y, Y);
+#pragma unroll 1
+    for (int px = 0; px < 2; ++px) {
+      const int k = p2FaceEntry(0, px | ((Y & 1) << 1));
+      for (int X = (px ? 1 : 2) + 2 * lane; X <= n - 1 - Y; X += 64) faceNode(k, X, Y);
+    }
+  } else if (n == 0) {
+    if (threadIdx.x == 0) gatherNode(0, 0);
+  } else if (warp < 6) {
+    const int line = warp >> 1, par = warp & 1, zb = (Z & 1) << 2;
+    for (int t = (par ? 1 : 2) + 2 * lane; t <= n - 1; t += 64) {
+      if (line == 0)  // face Y = 0: X = t
+        faceNode(p2FaceEntry(1, par | zb), t, 0);
+      else if (line == 1)  // face X = 0: Y = t
+        faceNode(p2FaceEntry(2, (par << 1) | zb), 0, t);
+      else  // face X + Y + Z = M: Y = t, X = n - t
+        faceNode(p2FaceEntry(3, ((n - t) & 1) | (par << 1) | zb), n - t, t);
+    }
+  } else if (warp == 6 && lane < 3) {
+    if (lane == 0)
+      gatherNode(0, 0);
+    else if (lane == 1)
+      gatherNode(n, 0);
+    else
+      gatherNode(0, n);
   }
 }
 

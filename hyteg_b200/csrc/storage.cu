@@ -515,6 +515,7 @@ static void refillStencil(const dev::StencilDev<T>& d, const LevelStencils& st, 
 }
 
 static std::vector<double> p2Stencils(const std::vector<double>& K, int nCells);
+static std::vector<double> p2FaceStencils(const std::vector<double>& K, int nCells);
 
 int Storage::createP2Operator(int form, int minL, int maxL) {
   argCheck(form == FORM_LAPLACE, "P2 operators: only the Laplace form is available");
@@ -544,6 +545,16 @@ int Storage::createP2Operator(int form, int minL, int maxL) {
     o->sf.emplace_back(new DevBuf());
     o->sf.back()->alloc(Sf.size() * sizeof(float));
     cudaCheck(cudaMemcpyAsync(o->sf.back()->p, Sf.data(), Sf.size() * sizeof(float), cudaMemcpyHostToDevice, stream),
+              "P2 upload");
+    const std::vector<double> F = p2FaceStencils(K, (int)disc.topo().cells.size());
+    std::vector<float> Ff(F.begin(), F.end());
+    o->fd.emplace_back(new DevBuf());
+    o->fd.back()->alloc(F.size() * sizeof(double));
+    cudaCheck(cudaMemcpyAsync(o->fd.back()->p, F.data(), F.size() * sizeof(double), cudaMemcpyHostToDevice, stream),
+              "P2 upload");
+    o->ff.emplace_back(new DevBuf());
+    o->ff.back()->alloc(Ff.size() * sizeof(float));
+    cudaCheck(cudaMemcpyAsync(o->ff.back()->p, Ff.data(), Ff.size() * sizeof(float), cudaMemcpyHostToDevice, stream),
               "P2 upload");
     cudaCheck(cudaStreamSynchronize(stream), "P2 upload");
   }
@@ -701,6 +712,30 @@ static std::vector<double> p2Stencils(const std::vector<double>& K, int nCells) 
   return S;
 }
 
+// Face-interior stencil weights of every cell: per (face, class) entry k, the sum over its
+// micro-cells p2s::kFaceCand[k] of their element rows, scattered to the offsets p2s::kFaceOff[k].
+static std::vector<double> p2FaceStencils(const std::vector<double>& K, int nCells) {
+  const dev::P2Tables& tb = p2TablesOnce();
+  std::vector<double> S((size_t)nCells * p2s::kFaceTotal, 0.0);
+  for (int c = 0; c < nCells; ++c)
+    for (int k = 0; k < p2s::kFaceStencils; ++k) {
+      double* sc = S.data() + (size_t)c * p2s::kFaceTotal + p2s::kFaceFirst[k];
+      for (int q = 0; q < p2s::kFaceNCand[k]; ++q) {
+        const int t = p2s::kFaceCand[k][q][0], j = p2s::kFaceCand[k][q][1];
+        for (int m = 0; m < 10; ++m) {
+          int e = 0;
+          while (e < p2s::kFaceLen[k] && !(p2s::kFaceOff[k][e][0] == tb.off[t][m][0] - tb.off[t][j][0] &&
+                                           p2s::kFaceOff[k][e][1] == tb.off[t][m][1] - tb.off[t][j][1] &&
+                                           p2s::kFaceOff[k][e][2] == tb.off[t][m][2] - tb.off[t][j][2]))
+            ++e;
+          if (e == p2s::kFaceLen[k]) throw Error(HG_ERR_INTERNAL, "P2 face stencil table does not match the micro-cells");
+          sc[e] += K[(size_t)c * 600 + t * 100 + j * 10 + m];
+        }
+      }
+    }
+  return S;
+}
+
 // Cell gather + additive owner sums for one P2 level: dst = A src, rhs - A src or diag(A), on the
 // flagged DoFs of colour `sel` (all when sel < 0). The copies of dst are not refreshed here.
 template <class T, int MODE>
@@ -722,7 +757,9 @@ void Storage::p2Launch(P2Operator& o, int L, T* dst, const T* src, const T* rhs,
           ld.lv, W, dst, src, rhs, mask, col, (const signed char*)ad.classOfColour.p, sel, T(0));
       ++launches;
     }
-    dev::p2ClosureKernel<T><<<ld.lv.nCells * (ld.lv.N + dev::p2FaceChunks(ld.lv.N)), dev::kBlock, 0, stream>>>(ld.lv, p2TablesOnce(), K, dst, src, col, sel);
+    const T* FW = (const T*)(sizeof(T) == 8 ? o.fd[L - o.minL]->p : o.ff[L - o.minL]->p);
+    dev::p2ClosureKernel<T><<<ld.lv.nCells * (ld.lv.N + dev::p2FaceChunks(ld.lv.N)), dev::kBlock, 0, stream>>>(
+        ld.lv, p2TablesOnce(), K, FW, dst, src, col, sel);
     ++launches;
   }
   if (ad.n) {
@@ -794,6 +831,7 @@ void Storage::p2SorT(P2Operator& o, int opId, int x, int b, int L, unsigned mask
   P2Additive& ad = p2Additive(Lf);
   const T* K = (const T*)(sizeof(T) == 8 ? o.kd[L - o.minL]->p : o.kf[L - o.minL]->p);
   const T* W = (const T*)(sizeof(T) == 8 ? o.sd[L - o.minL]->p : o.sf[L - o.minL]->p);
+  const T* FW = (const T*)(sizeof(T) == 8 ? o.fd[L - o.minL]->p : o.ff[L - o.minL]->p);
   const unsigned char* col = (const unsigned char*)ad.colour.p;
   for (int k = 0; k < 11; ++k) {
     const int c = backwards ? 10 - k : k;
@@ -804,7 +842,8 @@ void Storage::p2SorT(P2Operator& o, int opId, int x, int b, int L, unsigned mask
     // face, edge and vertex DoFs of colour c: each cell's share of A x from the pass's start values
     // (the colours of DoFs on different primitives are defined in different vertex frames, so a
     // closure DoF may couple to an interior DoF of the same colour: its share is taken first)
-    dev::p2ClosureKernel<T><<<ld.lv.nCells * (ld.lv.N + dev::p2FaceChunks(ld.lv.N)), dev::kBlock, 0, stream>>>(ld.lv, p2TablesOnce(), K, axd, xd, col, c);
+    dev::p2ClosureKernel<T><<<ld.lv.nCells * (ld.lv.N + dev::p2FaceChunks(ld.lv.N)), dev::kBlock, 0, stream>>>(
+        ld.lv, p2TablesOnce(), K, FW, axd, xd, col, c);
     ++launches;
     // interior nodes of colour c. An edge colour is one parity class in a cell's frame and couples
     // to no other node of its class, so those are updated in place (the closure copies keep their

@@ -68,6 +68,7 @@ struct P2Operator {
   std::map<std::pair<int, int>, int> diag;      // (level, precision) -> diagonal function
   std::vector<std::unique_ptr<DevBuf>> dd, df;  // Taylor-Hood divergence per level: [cell][type][3][4][10]
   std::vector<std::unique_ptr<DevBuf>> sd, sf;  // interior stencils per level: [cell][p2s::kTotal]
+  std::vector<std::unique_ptr<DevBuf>> fd, ff;  // face-interior stencils per level: [cell][p2s::kFaceTotal]
 };
 
 // Cell-closure copies of every DoF owned by a face, edge or vertex of one lattice level.
