@@ -204,31 +204,51 @@ __global__ void __launch_bounds__(kBlock, 4) cellSorKernel(LevelDev lv, const T*
 // result equals four separate colour sweeps over the whole cell, and the four stages of a step
 // touch disjoint data (they write the planes s, s-2, s-4, s-6 and read only those and the odd
 // planes between them) and need no barrier between them.
-// A block owns a 32 x 28 (x, y) tile of one macro-cell for all planes. It recomputes a shrinking
+// A block owns a 32 x TY (x, y) tile of one macro-cell for all planes (WaveCfg). It recomputes a shrinking
 // halo (stage k on the tile widened by 3 - k) from the start-of-sweep values, which makes the
 // tiles independent: they read uOld and write uNew, and the caller swaps the two buffers.
-// Planes s-7 .. s+1 of the tile widened by 4 (40 x 36 points) live in a 9-slot shared-memory
+// Planes s-7 .. s+1 of the tile widened by 4 (40 x (TY + 8) points) live in a 9-slot shared-memory
 // ring; plane s+2 is loaded into registers during step s and stored into the slot that plane
 // s-7 frees. Point (rx, ry) of the region sits at
 //   ry * 42 + ((rx mod 4 + 2 ry) mod 4) * 10 + rx / 4,
 // i.e. each row is split by x mod 4 and the split is rotated by 2y. The points of one colour then
 // occupy the same sub-row of every row, and with the row stride 42 (= 10 mod 16) the 16 lanes
-// of a half-warp never share a bank pair. Thread t < 360 owns the four columns 4(t mod 10) .. +3
+// of a half-warp never share a bank pair. Thread t < 10 (TY + 8) owns the columns 4(t mod 10) .. +3
 // of region row t / 10: it loads and stores them and, in every stage, updates the one of them
 // that carries the stage's colour.
 // ---------------------------------------------------------------------------------------
 constexpr int kWaveTX = 32;                         // tile extent in x (multiple of 4)
-constexpr int kWaveTY = 28;                         // tile extent in y (even)
 constexpr int kWaveH = 4;                           // halo loaded around the tile
 constexpr int kWaveRX = kWaveTX + 2 * kWaveH;       // region extent in x (40)
-constexpr int kWaveRY = kWaveTY + 2 * kWaveH;       // region extent in y (36)
 constexpr int kWaveQ = kWaveRX / 4;                 // column groups per region row (10)
 constexpr int kWaveS = 42;                          // shared-memory row stride (10 mod 16)
-constexpr int kWavePlane = kWaveRY * kWaveS;        // elements per plane slot
 constexpr int kWaveSlots = 9;
-constexpr int kWaveGroups = kWaveRY * kWaveQ;       // 360 column groups, one per thread
-constexpr int kWaveThreads = 384;
 constexpr int kWaveMaxN = 4096;                     // largest level size the shared-memory limit is set for
+
+// Tile height, block size and blocks per SM per precision. 32 x 28 tiles (region 40 x 36, 360
+// column groups): FP64 109 KB of ring, two blocks per SM; FP32 55 KB, three blocks per SM (a
+// register budget of 56 per thread). Measured per level-8 sweep, FP64: 2.34 ms (32 x 28, two
+// blocks per SM), 2.35 ms (32 x 16, three), 2.78 ms (32 x 60, one); FP32: 1.41 ms (32 x 28,
+// three), 1.67 ms (32 x 28, four at 40 registers), 1.83 ms (32 x 60, two).
+template <class T>
+struct WaveCfg;
+template <>
+struct WaveCfg<double> {
+  static constexpr int TY = 28, THREADS = 384, MIN_BLOCKS = 2;
+};
+template <>
+struct WaveCfg<float> {
+  static constexpr int TY = 28, THREADS = 384, MIN_BLOCKS = 3;
+};
+template <class T>
+struct WaveGeom {
+  static constexpr int TY = WaveCfg<T>::TY;        // tile extent in y (even)
+  static constexpr int RY = TY + 2 * kWaveH;       // region extent in y
+  static constexpr int PLANE = RY * kWaveS;        // elements per plane slot
+  static constexpr int GROUPS = RY * kWaveQ;       // column groups, one per thread
+  static constexpr int THREADS = WaveCfg<T>::THREADS;
+  static_assert(THREADS >= GROUPS && THREADS % 32 == 0 && TY % 2 == 0, "wave tile configuration");
+};
 
 struct WaveTile {
   int cell, x0, y0, pEnd;  // tile origin; pEnd = N - x0 - y0, its last plane
@@ -237,17 +257,19 @@ struct WaveTile {
 // Dynamic shared memory of the kernel for level size N.
 template <class T>
 inline size_t waveSmemBytes(int N) {
-  return size_t(kWaveSlots) * kWavePlane * sizeof(T) + size_t(N + 2) * sizeof(int);
+  return size_t(kWaveSlots) * WaveGeom<T>::PLANE * sizeof(T) + size_t(N + 2) * sizeof(int);
 }
 
 template <class T>
-__global__ void __launch_bounds__(kWaveThreads, sizeof(T) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(WaveCfg<T>::THREADS, WaveCfg<T>::MIN_BLOCKS)
     cellSorWaveKernel(LevelDev lv, const WaveTile* __restrict__ tiles, const T* __restrict__ cellW,
                       const T* __restrict__ uOld, T* __restrict__ uNew, const T* __restrict__ rhs, unsigned mask,
                       T omega, int backwards) {
+  constexpr int kTY = WaveGeom<T>::TY, kRY = WaveGeom<T>::RY, kPlane = WaveGeom<T>::PLANE;
+  constexpr int kGroups = WaveGeom<T>::GROUPS, kThreads = WaveGeom<T>::THREADS;
   extern __shared__ __align__(16) unsigned char waveSmem[];
   T* sm = reinterpret_cast<T*>(waveSmem);
-  int* pbTab = reinterpret_cast<int*>(sm + kWaveSlots * kWavePlane);  // first index of plane p
+  int* pbTab = reinterpret_cast<int*>(sm + kWaveSlots * kPlane);  // first index of plane p
   const WaveTile tl = tiles[blockIdx.x];
   const int N = lv.N, w = lv.w, tid = threadIdx.x;
   const int64_t base = lv.cellOff[tl.cell];
@@ -255,15 +277,15 @@ __global__ void __launch_bounds__(kWaveThreads, sizeof(T) == 4 ? 3 : 2)
   T* __restrict__ un = uNew + base;
   const T* __restrict__ f = rhs + base;
   const int xb = tl.x0 - kWaveH, yb = tl.y0 - kWaveH;  // region origin in cell coordinates
-  for (int p = tid; p <= N; p += kWaveThreads) pbTab[p] = int(tetSize(w) - tetSize(w - p));
+  for (int p = tid; p <= N; p += kThreads) pbTab[p] = int(tetSize(w) - tetSize(w - p));
   // the thread's column group: region row gy, region columns 4 gx .. 4 gx + 3
-  const bool owner = tid < kWaveGroups;
+  const bool owner = tid < kGroups;
   const int gy = tid / kWaveQ, gx = tid - (tid / kWaveQ) * kWaveQ;
   const int y = yb + gy, x4 = xb + 4 * gx;
   const int Ay = y * (w + 1) - (y * (y + 1)) / 2;  // rowStart(w - p, y) = Ay - y p
   const int rot = (2 * gy) & 3;                     // sub-row of column j: (j + rot) mod 4
   const int so = gy * kWaveS + gx;
-  const bool storer = owner && gy >= kWaveH && gy < kWaveH + kWaveTY && gx >= 1 && gx < kWaveQ - 1;
+  const bool storer = owner && gy >= kWaveH && gy < kWaveH + kTY && gx >= 1 && gx < kWaveQ - 1;
   __syncthreads();
 
   if (!(lv.cellType[tl.cell] & mask)) {  // not smoothed: the tile is copied
@@ -284,7 +306,7 @@ __global__ void __launch_bounds__(kWaveThreads, sizeof(T) == 4 ? 3 : 2)
   unsigned rowBits = 0;  // bit k: row gy lies in the region of stage k and y >= 1
 #pragma unroll
   for (int k = 0; k < 4; ++k)
-    if (owner && gy >= k + 1 && gy < kWaveRY - 1 - k && y >= 1) rowBits |= 1u << k;
+    if (owner && gy >= k + 1 && gy < kRY - 1 - k && y >= 1) rowBits |= 1u << k;
 
   T stg[4];
   auto loadRegs = [&](int p) {  // plane p of the thread's columns (points of the closed cell)
@@ -297,7 +319,7 @@ __global__ void __launch_bounds__(kWaveThreads, sizeof(T) == 4 ? 3 : 2)
   };
   auto storeRegs = [&](int p, int slot) {
     if (owner && p <= N && y >= 0 && y <= N - p) {
-      T* s = sm + slot * kWavePlane + so;
+      T* s = sm + slot * kPlane + so;
 #pragma unroll
       for (int j = 0; j < 4; ++j)
         if (x4 + j >= 0 && x4 + j + y <= N - p) s[((j + rot) & 3) * kWaveQ] = stg[j];
@@ -318,9 +340,9 @@ __global__ void __launch_bounds__(kWaveThreads, sizeof(T) == 4 ? 3 : 2)
     const int dE = e1 + qe, dW = w1 - qw, dN = kWaveS + n2, dS = n2 - kWaveS;
     const int dNW = kWaveS + e1 - qw, dSE = w1 - kWaveS + qe;
     const int o = so + sg * kWaveQ;
-    T* sP = sm + sp * kWavePlane + o;
-    const T* sT = sm + st * kWavePlane + o;
-    const T* sB = sm + sb * kWavePlane + o;
+    T* sP = sm + sp * kPlane + o;
+    const T* sT = sm + st * kPlane + o;
+    const T* sB = sm + sb * kPlane + o;
     const T rh = f[pbTab[p] + Ay - y * p + x];
     // three independent partial sums (this plane, the plane above, the plane below)
     T a = wt[1] * sP[dE];
@@ -341,7 +363,7 @@ __global__ void __launch_bounds__(kWaveThreads, sizeof(T) == 4 ? 3 : 2)
   };
   auto store = [&](int p, int slot) {  // the tile's points of plane p (interior and boundary) to uNew
     if (!storer || y > N - p) return;
-    const T* s = sm + slot * kWavePlane + so;
+    const T* s = sm + slot * kPlane + so;
     const int g = pbTab[p] + Ay - y * p + x4;
 #pragma unroll
     for (int j = 0; j < 4; ++j)

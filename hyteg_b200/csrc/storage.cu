@@ -196,16 +196,20 @@ void Storage::buildLevel(int L) {
   ld.comm = (uint2*)upload(keep, comm, stream);
   ld.chunks = (dev::Chunk*)upload(keep, chunks, stream);
   buildTiles(L);
-  // single-pass SOR tiles: every (x, y) of the cell is in exactly one tile, tallest tiles first
+  // single-pass SOR tiles: every (x, y) of the cell is in exactly one tile, tallest tiles first;
+  // one list per precision (the tile heights differ)
   {
-    std::vector<dev::WaveTile> wt;
-    if (N >= 4)
-      for (int c = 0; c < lv.nCells; ++c)
-        for (int y0 = 0; y0 <= N; y0 += dev::kWaveTY)
-          for (int x0 = 0; x0 + y0 <= N; x0 += dev::kWaveTX) wt.push_back({c, x0, y0, (int)N - x0 - y0});
-    std::stable_sort(wt.begin(), wt.end(), [](const dev::WaveTile& a, const dev::WaveTile& b) { return a.pEnd > b.pEnd; });
-    ld.waveTiles = (dev::WaveTile*)upload(keep, wt, stream);
-    ld.nWaveTiles = (int)wt.size();
+    for (int pi = 0; pi < 2; ++pi) {
+      const int ty = pi == 0 ? dev::WaveGeom<double>::TY : dev::WaveGeom<float>::TY;
+      std::vector<dev::WaveTile> wt;
+      if (N >= 4)
+        for (int c = 0; c < lv.nCells; ++c)
+          for (int y0 = 0; y0 <= N; y0 += ty)
+            for (int x0 = 0; x0 + y0 <= N; x0 += dev::kWaveTX) wt.push_back({c, x0, y0, (int)N - x0 - y0});
+      std::stable_sort(wt.begin(), wt.end(), [](const dev::WaveTile& a, const dev::WaveTile& b) { return a.pEnd > b.pEnd; });
+      ld.waveTiles[pi] = (dev::WaveTile*)upload(keep, wt, stream);
+      ld.nWaveTiles[pi] = (int)wt.size();
+    }
     int64_t first = lay.total;
     for (int k : {KV, KE, KF})
       for (int64_t o : lay.off[k]) first = std::min(first, o);
@@ -1347,7 +1351,8 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
     const int tuned = 2 * L + (sizeof(T) == 4 ? 1 : 0);
     const int schedule = (int)sorScheduleLevel.size() > tuned && sorScheduleLevel[tuned] >= 0 ? sorScheduleLevel[tuned]
                                                                                                   : sorSchedule;
-    if (schedule == 0 && ld.nWaveTiles) {
+    const int pi = sizeof(T) == 4 ? 1 : 0;
+    if (schedule == 0 && ld.nWaveTiles[pi]) {
       // one pass into the spare buffer of this level, which then becomes the function's buffer
       Function& fd = fn(dstId);
       std::unique_ptr<DevBuf>& cur = fd.levels[L - fd.minL];
@@ -1359,8 +1364,8 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
       }
       T* out = (T*)sp->p;
       const size_t smem = dev::waveSmemBytes<T>(lv.N);
-      dev::cellSorWaveKernel<T><<<ld.nWaveTiles, dev::kWaveThreads, smem, stream>>>(lv, ld.waveTiles, st.cellW, u, out,
-                                                                                  rhs, mask, omega, rev ? 1 : 0);
+      dev::cellSorWaveKernel<T><<<ld.nWaveTiles[pi], dev::WaveGeom<T>::THREADS, smem, stream>>>(
+          lv, ld.waveTiles[pi], st.cellW, u, out, rhs, mask, omega, rev ? 1 : 0);
       ++launches;
       const int64_t tail = ld.lay->total - ld.nonCellBegin;
       if (tail > 0)

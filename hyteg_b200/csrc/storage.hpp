@@ -41,8 +41,8 @@ struct LevelData {
   std::unique_ptr<DevBuf> tileBuf;
   DevBuf partial;
   // single-pass SOR: one 32 x 32 (x, y) tile of a macro-cell per block, the tallest first
-  dev::WaveTile* waveTiles = nullptr;
-  int nWaveTiles = 0;
+  dev::WaveTile* waveTiles[2] = {nullptr, nullptr};  // single-pass SOR tiles: [0] FP64, [1] FP32 geometry
+  int nWaveTiles[2] = {0, 0};
   int64_t nonCellBegin = 0;  // first slot after the cell arrays (faces, edges, vertices follow)
   std::vector<unsigned char> hostCellType, hostFaceType, hostLowType;
   std::vector<std::unique_ptr<DevBuf>> keep;
