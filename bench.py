@@ -606,15 +606,37 @@ def run_ours(args):
     value = world * N_in * args.steps / t_max / 1e9
 
     # --- end to end through the public API with host buffers --------------------------------
+    # Every step uploads its right-hand side from pinned host memory and reads its residual norm
+    # back. The upload of step k + 1 runs on a copy stream into the second of two right-hand-side
+    # hierarchies while step k solves (double buffering); the first upload is not overlapped.
+    b2 = hg.P1Function("b2", st, 0, L)
+    bufs = (b, b2)
+    copy_stream = torch.cuda.Stream()
+    host_np = host_b.numpy()
+    b2.from_numpy(L, host_np)
+    for _ in range(3):  # the cycles on the second buffer run eagerly, then from their own graph
+        gmg.solve(A, x, b2, L)
     torch.cuda.synchronize()
     barrier(pg)
+    copied = [ev(), ev()]
+    released = [ev(), ev()]
     e0, e1 = ev(), ev()
     e0.record(stream)
-    for _ in range(args.steps):
-        b.from_numpy(L, host_b.numpy())        # H2D of the step's input from pinned memory
-        gmg.solve(A, x, b, L)
-        A.residual(x, b, r, L, Inner)
+    copy_stream.wait_stream(stream)
+    bufs[0].upload_async(L, host_np, copy_stream.cuda_stream)
+    copied[0].record(copy_stream)
+    for k in range(args.steps):
+        cur = k % 2
+        if k + 1 < args.steps:  # the next step's input, behind the step that last used its buffer
+            if k >= 1:
+                copy_stream.wait_event(released[1 - cur])
+            bufs[1 - cur].upload_async(L, host_np, copy_stream.cuda_stream)
+            copied[1 - cur].record(copy_stream)
+        stream.wait_event(copied[cur])
+        gmg.solve(A, x, bufs[cur], L)
+        A.residual(x, bufs[cur], r, L, Inner)
         _ = r.dotGlobal(r, L, Inner)           # D2H of the step's result (residual norm)
+        released[cur].record(stream)
     e1.record(stream)
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) * 1e-3, pg)
@@ -633,7 +655,9 @@ def run_ours(args):
                      "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": BYTES["sor_sweep"] * Nc},
         "e2e": {"value": world * N_in * args.steps / t_e2e / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": n * 8,
-                "d2h_bytes_per_step": 8},
+                "d2h_bytes_per_step": 8,
+                "pipelining": "two right-hand-side buffers: the pinned-host upload of step k+1 (copy stream) "
+                              "overlaps the cycle of step k; the first upload is not overlapped"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "kernels": kernels,

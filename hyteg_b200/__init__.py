@@ -284,6 +284,14 @@ class P1Function:
         a = np.ascontiguousarray(a, dtype=self.dtype)
         call("hg_function_upload", self.storage.handle, self.id, level, a.ctypes.data_as(ctypes.c_void_p), a.size)
 
+    def upload_async(self, level, a, stream):
+        """Enqueue the upload of the contiguous host array `a` (pinned memory for an asynchronous
+        copy; kept alive by the caller) on the CUDA stream handle `stream`, without waiting."""
+        if a.dtype != self.dtype or not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("upload_async: a contiguous array of the function's precision is required")
+        call("hg_function_upload_async", self.storage.handle, self.id, level, a.ctypes.data_as(ctypes.c_void_p), a.size,
+             ctypes.c_void_p(stream))
+
     def communicate(self, level):
         call("hg_communicate", self.storage.handle, self.id, level)
 

@@ -274,6 +274,16 @@ int hg_function_upload(hg_storage* h, int fn, int level, const void* host, int64
   HG_CATCH
 }
 
+int hg_function_upload_async(hg_storage* h, int fn, int level, const void* host, int64_t n, void* stream) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  hg::Function& f = s.fn(fn);
+  hg::argCheck(n == s.disc.level(level).total, "upload size must equal the level buffer size");
+  hg::cudaCheck(cudaMemcpyAsync(s.data(fn, level), host, (size_t)n * f.prec, cudaMemcpyHostToDevice, (cudaStream_t)stream),
+                "upload");
+  HG_CATCH
+}
+
 int hg_function_download(hg_storage* h, int fn, int level, void* host, int64_t n) {
   HG_TRY
   hg::Storage& s = S(h);

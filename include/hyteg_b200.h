@@ -153,6 +153,11 @@ int hg_function_device_ptr(hg_storage* s, int fn, int level, void** ptr);
 /* Host <-> device copies of one level buffer (n elements of the function's precision). */
 int hg_function_upload(hg_storage* s, int fn, int level, const void* host, int64_t n);
 int hg_function_download(hg_storage* s, int fn, int level, void* host, int64_t n);
+/* The upload enqueued on the caller's CUDA stream (a cudaStream_t), without waiting: the caller
+ * orders it against the storage's stream with events and keeps the host buffer (pinned, for an
+ * asynchronous copy) alive until it completes. For pipelining the next input's copy with the
+ * current solve. */
+int hg_function_upload_async(hg_storage* s, int fn, int level, const void* host, int64_t n, void* stream);
 int hg_communicate(hg_storage* s, int fn, int level);
 int hg_interpolate_const(hg_storage* s, int fn, double value, int level, unsigned flag);
 /* Built-in expressions at the flagged DoFs (then the halo is refreshed): expr 0 =

@@ -1,0 +1,82 @@
+"""Host-facing entry points: the asynchronous upload on a caller's stream gives the same level
+buffer as the synchronous one, and a double-buffered pipeline (upload of the next right-hand
+side overlapping the current cycle) gives the same iterates as the plain loop."""
+import numpy as np
+import pytest
+
+import hyteg_b200 as hg
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    if hg.device_count() == 0:
+        pytest.skip("no CUDA device")
+    import torch
+    L = 4
+    st = hg.PrimitiveStorage.cuboid((0, 0, 0), (1, 1, 1), 2, 2, 2, L)
+    stream = torch.cuda.Stream()
+    st.set_stream(stream.cuda_stream)
+    return st, L, stream
+
+
+def test_upload_async_matches_upload(env):
+    import torch
+    st, L, stream = env
+    n = st.level_size(L)
+    host = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    host.numpy()[:] = np.random.default_rng(1).uniform(-1, 1, n)
+    a, b = hg.P1Function("a", st, L, L), hg.P1Function("b", st, L, L)
+    a.from_numpy(L, host.numpy())
+    cs = torch.cuda.Stream()
+    b.upload_async(L, host.numpy(), cs.cuda_stream)
+    cs.synchronize()
+    assert np.array_equal(a.to_numpy(L), b.to_numpy(L))
+    with pytest.raises(ValueError):
+        b.upload_async(L, host.numpy().astype(np.float32), cs.cuda_stream)
+
+
+def test_double_buffered_pipeline_gives_the_same_iterates(env):
+    import torch
+    st, L, stream = env
+    n = st.level_size(L)
+    A = hg.P1ConstantLaplaceOperator(st, 0, L)
+    rhs = []
+    for k in range(4):
+        h = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        h.numpy()[:] = np.random.default_rng(10 + k).uniform(-1, 1, n)
+        rhs.append(h)
+
+    def solver():
+        return hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 50, 1e-16),
+                                           hg.P1toP1LinearRestriction(), hg.P1toP1LinearProlongation(), 0, L, 3, 3)
+
+    # plain loop
+    x, b = hg.P1Function("x", st, 0, L), hg.P1Function("b", st, 0, L)
+    g = solver()
+    for h in rhs:
+        b.from_numpy(L, h.numpy())
+        g.solve(A, x, b, L)
+    plain = x.to_numpy(L)
+    # pipelined loop: two buffers, uploads on a copy stream ordered by events
+    y = hg.P1Function("y", st, 0, L)
+    bufs = (hg.P1Function("b0", st, 0, L), hg.P1Function("b1", st, 0, L))
+    g2 = solver()
+    cs = torch.cuda.Stream()
+    copied = [torch.cuda.Event(), torch.cuda.Event()]
+    released = [torch.cuda.Event(), torch.cuda.Event()]
+    bufs[0].upload_async(L, rhs[0].numpy(), cs.cuda_stream)
+    copied[0].record(cs)
+    for k in range(len(rhs)):
+        cur = k % 2
+        if k + 1 < len(rhs):
+            if k >= 1:
+                cs.wait_event(released[1 - cur])
+            bufs[1 - cur].upload_async(L, rhs[k + 1].numpy(), cs.cuda_stream)
+            copied[1 - cur].record(cs)
+        stream.wait_event(copied[cur])
+        g2.solve(A, y, bufs[cur], L)
+        released[cur].record(stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(plain, y.to_numpy(L))
