@@ -975,13 +975,31 @@ __device__ __forceinline__ T p2StencilDot(p2s::List<p2s::O<DX, DY, DZ>...>, std:
 template <class T, int MODE, int PC>
 __device__ __forceinline__ void p2StencilRow(const T* wts, T* dst, const T* src, const T* rhs, int64_t base,
                                              const int (&pbz)[5], int w, int M, int Y, int Z, int lane,
-                                             const unsigned char* __restrict__ colour, int sel, T omega) {
+                                             const unsigned char* __restrict__ colour, int sel, T omega, int vstep) {
   using S = typename p2s::Class<PC>::type;
   constexpr int kFirst = p2s::kFirst[PC], kCentre = p2s::kCentre[PC], kLen = p2s::kLen[PC];
   const T* wt = wts + kFirst;
   const int r0 = pbz[2] + rowStart(w - Z, Y);
+  int X0 = ((PC & 1) ? 1 : 2) + 2 * lane, dX = 64;
+  if (PC == 0 && sel >= 0) {
+    // vertex colour sel along the row: the colour of the vertex node 2 + 2t is c(2) + vstep t mod 4,
+    // so the lanes take every fourth (vstep odd) or every second (vstep 2) vertex node from the first
+    if (M - 1 - Y - Z < 2) return;
+    const int diff = (sel - (colour[base + r0 + 2] & 0x7f)) & 3;
+    int t0, ts;
+    if (vstep & 1) {
+      t0 = (diff * vstep) & 3;
+      ts = 4;
+    } else {
+      if (diff & 1) return;
+      t0 = (diff >> 1) & 1;
+      ts = 2;
+    }
+    X0 = 2 + 2 * t0 + 2 * ts * lane;
+    dX = 64 * ts;
+  }
 #pragma unroll 1
-  for (int X = ((PC & 1) ? 1 : 2) + 2 * lane; X <= M - 1 - Y - Z; X += 64) {
+  for (int X = X0; X <= M - 1 - Y - Z; X += dX) {
     const int64_t i = base + r0 + X;
     if (PC == 0 && sel >= 0 && (colour[i] & 0x7f) != sel) continue;
     const T s = p2StencilDot<T>(S{}, std::make_integer_sequence<int, kLen>{}, src + base, wt, pbz, w, X, Y, Z);
@@ -997,24 +1015,27 @@ __device__ __forceinline__ void p2StencilRow(const T* wts, T* dst, const T* src,
 template <class T, int MODE>
 __device__ __forceinline__ void p2StencilRowAny(int pc, const T* wts, T* dst, const T* src, const T* rhs, int64_t base,
                                                 const int (&pbz)[5], int w, int M, int Y, int Z, int lane,
-                                                const unsigned char* __restrict__ colour, int sel, T omega) {
+                                                const unsigned char* __restrict__ colour, int sel, T omega,
+                                                int vstep) {
   switch (pc) {
-    case 0: p2StencilRow<T, MODE, 0>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
-    case 1: p2StencilRow<T, MODE, 1>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
-    case 2: p2StencilRow<T, MODE, 2>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
-    case 3: p2StencilRow<T, MODE, 3>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
-    case 4: p2StencilRow<T, MODE, 4>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
-    case 5: p2StencilRow<T, MODE, 5>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
-    case 6: p2StencilRow<T, MODE, 6>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
-    default: p2StencilRow<T, MODE, 7>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega); break;
+    case 0: p2StencilRow<T, MODE, 0>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega, vstep); break;
+    case 1: p2StencilRow<T, MODE, 1>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega, vstep); break;
+    case 2: p2StencilRow<T, MODE, 2>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega, vstep); break;
+    case 3: p2StencilRow<T, MODE, 3>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega, vstep); break;
+    case 4: p2StencilRow<T, MODE, 4>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega, vstep); break;
+    case 5: p2StencilRow<T, MODE, 5>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega, vstep); break;
+    case 6: p2StencilRow<T, MODE, 6>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega, vstep); break;
+    default: p2StencilRow<T, MODE, 7>(wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega, vstep); break;
   }
 }
 
 // Grid: nCells * (M - 3) blocks, block b on cell b / (M - 3), plane Z = 1 + b % (M - 3) (the
 // planes holding interior nodes; needs M >= 4). Only cells of a flagged DoF type are written.
-// sel >= 0 (one colour pass of the SOR, MODE_SOR or MODE_REPLACE): classOfColour[cell * 11 + sel]
+// sel >= 0 (one colour pass of the SOR, MODE_SOR or MODE_REPLACE): classOfColour[cell * 12 + sel]
 // is the class of colour sel in the cell's frame (0 for the four vertex colours, -1 when no
-// interior node has the colour). MODE_SOR updates in place: dst == src, rhs = b.
+// interior node has the colour), classOfColour[cell * 12 + 11] the change of the vertex colour
+// from one vertex node of a row to the next (1, 2 or 3). MODE_SOR updates in place: dst == src,
+// rhs = b.
 template <class T, int MODE>
 __global__ void __launch_bounds__(kBlock) p2StencilKernel(LevelDev lv, const T* __restrict__ W, T* dst, const T* src,
                                                           const T* __restrict__ rhs, unsigned mask,
@@ -1024,9 +1045,10 @@ __global__ void __launch_bounds__(kBlock) p2StencilKernel(LevelDev lv, const T* 
   const int M = lv.N, w = lv.w, nPl = M - 3;
   const int c = blockIdx.x / nPl, Z = 1 + blockIdx.x % nPl;
   if (!(lv.cellType[c] & mask)) return;
-  int pcSel = 0;
+  int pcSel = 0, vstep = 1;
   if (sel >= 0) {
-    pcSel = classOfColour[c * 11 + sel];
+    pcSel = classOfColour[c * 12 + sel];
+    vstep = classOfColour[c * 12 + 11];
     if (pcSel < 0 || ((pcSel >> 2) & 1) != (Z & 1)) return;
   }
   __shared__ T wts[p2s::kTotal];
@@ -1043,14 +1065,14 @@ __global__ void __launch_bounds__(kBlock) p2StencilKernel(LevelDev lv, const T* 
   if (sel >= 0) {
 #pragma unroll 1
     for (int Y = (((pcSel >> 1) & 1) ? 1 : 2) + 2 * warp; Y <= M - 2 - Z; Y += 2 * (kBlock / 32))
-      p2StencilRowAny<T, MODE>(pcSel, wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega);
+      p2StencilRowAny<T, MODE>(pcSel, wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane, colour, sel, omega, vstep);
   } else {
 #pragma unroll 1
     for (int Y = 1 + warp; Y <= M - 2 - Z; Y += kBlock / 32) {
 #pragma unroll 1
       for (int px = 0; px < 2; ++px)
         p2StencilRowAny<T, MODE>(px | ((Y & 1) << 1) | ((Z & 1) << 2), wts, dst, src, rhs, base, pbz, w, M, Y, Z, lane,
-                                 colour, sel, omega);
+                                 colour, sel, omega, vstep);
     }
   }
 }
@@ -1170,6 +1192,37 @@ __global__ void __launch_bounds__(kBlock) p2ClosureKernel(LevelDev lv, P2Tables 
     else
       gatherNode(0, n);
   }
+}
+
+// The closure nodes of one SOR colour from a per-colour list (one thread per node): the same
+// shares as p2ClosureKernel, without visiting the nodes of the other colours. k = face-stencil
+// entry of a face-interior node, -1 for a node on a cell edge or vertex (element gather).
+struct P2ClosureNode {
+  int cell;
+  unsigned short x, y, z;
+  signed char k;
+  unsigned char pad;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2ClosureListKernel(LevelDev lv, P2Tables tb, const T* __restrict__ K,
+                                                              const T* __restrict__ FW, T* __restrict__ dst,
+                                                              const T* __restrict__ src,
+                                                              const P2ClosureNode* __restrict__ list, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const P2ClosureNode nd = list[i];
+  const int M = lv.N, N = M / 2, w = lv.w, X = nd.x, Y = nd.y, Z = nd.z;
+  int pbz[5];
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    const int z = Z - 2 + d;
+    pbz[d] = (z >= 0 && z <= M) ? int(tetSize(w) - tetSize(w - z)) : 0;
+  }
+  const int64_t base = lv.cellOff[nd.cell];
+  const T s = nd.k >= 0 ? p2FaceDotAny<T>(nd.k, src + base, FW + (int64_t)nd.cell * p2s::kFaceTotal, pbz, w, X, Y, Z)
+                        : p2GatherNode<T, false>(tb, K + (int64_t)nd.cell * 600, src + base, pbz, w, N, X, Y, Z);
+  dst[base + pbz[2] + rowStart(w - Z, Y) + X] = s;
 }
 
 // ---------------------------------------------------------------------------------------

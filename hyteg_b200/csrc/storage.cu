@@ -661,20 +661,68 @@ P2Additive& Storage::p2Additive(int Lf) {
   {
     const int64_t M = ld.lv.N, w = M + 1;
     auto tet = [](int64_t n) { return n * (n + 1) * (n + 2) / 6; };
-    std::vector<signed char> cls((size_t)ld.lv.nCells * 11, -1);
+    std::vector<signed char> cls((size_t)ld.lv.nCells * 12, -1);
+    auto colourAt = [&](int c, int64_t X, int64_t Y, int64_t Z) {
+      const int64_t loc = tet(w) - tet(w - Z) + Y * (w - Z + 1) - Y * (Y + 1) / 2 + X;
+      return col[(size_t)(ld.lay->off[KC][c] + loc)] & 0x7f;
+    };
     for (int c = 0; c < ld.lv.nCells; ++c) {
-      for (int k = 0; k < 4 && M >= 8; ++k) cls[(size_t)c * 11 + k] = 0;
+      for (int k = 0; k < 4 && M >= 8; ++k) cls[(size_t)c * 12 + k] = 0;
+      // step of the vertex colour along a row (1 when a row holds at most one interior vertex node)
+      cls[(size_t)c * 12 + 11] = (signed char)(M >= 16 ? (colourAt(c, 4, 2, 2) - colourAt(c, 2, 2, 2)) & 3 : 1);
+      argCheck(cls[(size_t)c * 12 + 11] != 0, "P2 vertex colours do not change along a row");
       for (int pc = 1; pc < 8; ++pc) {
         const int64_t X = (pc & 1) ? 1 : 2, Y = (pc & 2) ? 1 : 2, Z = (pc & 4) ? 1 : 2;
         if (X + Y + Z > M - 1) continue;
-        const int64_t loc = tet(w) - tet(w - Z) + Y * (w - Z + 1) - Y * (Y + 1) / 2 + X;
-        const int colr = col[(size_t)(ld.lay->off[KC][c] + loc)] & 0x7f;
-        argCheck(colr >= 4 && colr < 11 && cls[(size_t)c * 11 + colr] < 0, "P2 colour classes are inconsistent");
-        cls[(size_t)c * 11 + colr] = (signed char)pc;
+        const int colr = colourAt(c, X, Y, Z);
+        argCheck(colr >= 4 && colr < 11 && cls[(size_t)c * 12 + colr] < 0, "P2 colour classes are inconsistent");
+        cls[(size_t)c * 12 + colr] = (signed char)pc;
       }
     }
     ad.classOfColour.alloc(cls.size());
     cudaCheck(cudaMemcpyAsync(ad.classOfColour.p, cls.data(), cls.size(), cudaMemcpyHostToDevice, stream), "p2 colour");
+    // closure nodes of every cell grouped by colour (then by face-stencil entry, so that the warps
+    // of the list kernel mostly run one stencil)
+    auto faceEntry = [](int f, int pc) {
+      switch (f) {
+        case 0: return pc;
+        case 1: return 4 + ((pc & 1) | ((pc >> 1) & 2));
+        case 2: return 8 + (((pc >> 1) & 1) | ((pc >> 1) & 2));
+        default: return 12 + (pc == 0 ? 0 : pc == 3 ? 1 : pc == 5 ? 2 : 3);
+      }
+    };
+    std::vector<std::pair<int, dev::P2ClosureNode>> nodes;
+    for (int c = 0; c < ld.lv.nCells; ++c)
+      for (int64_t Z = 0; Z <= M; ++Z)
+        for (int64_t Y = 0; Y <= M - Z; ++Y)
+          for (int64_t X = 0; X <= M - Z - Y; ++X) {
+            const bool on[4] = {Z == 0, Y == 0, X == 0, X + Y + Z == M};
+            const int nOn = on[0] + on[1] + on[2] + on[3];
+            if (nOn == 0) continue;
+            int k = -1;
+            if (nOn == 1) {
+              const int f = on[0] ? 0 : on[1] ? 1 : on[2] ? 2 : 3;
+              k = faceEntry(f, int((X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2)));
+            }
+            dev::P2ClosureNode nd{c, (unsigned short)X, (unsigned short)Y, (unsigned short)Z, (signed char)k, 0};
+            nodes.push_back({colourAt(c, X, Y, Z) * 32 + (k + 1), nd});
+          }
+    std::stable_sort(nodes.begin(), nodes.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    std::vector<dev::P2ClosureNode> list(nodes.size());
+    for (int k = 0; k < 12; ++k) ad.closureBegin[k] = 0;
+    int cur = 0;
+    for (size_t i = 0; i < nodes.size(); ++i) {
+      list[i] = nodes[i].second;
+      const int colr = nodes[i].first / 32;
+      argCheck(colr < 11, "closure node without an SOR colour");
+      while (cur < colr) ad.closureBegin[++cur] = (int)i;
+    }
+    while (cur < 11) ad.closureBegin[++cur] = (int)nodes.size();
+    ad.closureList.alloc(std::max<size_t>(1, list.size()) * sizeof(dev::P2ClosureNode));
+    if (!list.empty())
+      cudaCheck(cudaMemcpyAsync(ad.closureList.p, list.data(), list.size() * sizeof(dev::P2ClosureNode),
+                                cudaMemcpyHostToDevice, stream),
+                "p2 closure list");
   }
   std::vector<unsigned char> mult((size_t)ld.lay->total, 1);
   for (size_t i = 0; i + 1 < ptr.size(); ++i)
@@ -846,9 +894,13 @@ void Storage::p2SorT(P2Operator& o, int opId, int x, int b, int L, unsigned mask
     // face, edge and vertex DoFs of colour c: each cell's share of A x from the pass's start values
     // (the colours of DoFs on different primitives are defined in different vertex frames, so a
     // closure DoF may couple to an interior DoF of the same colour: its share is taken first)
-    dev::p2ClosureKernel<T><<<ld.lv.nCells * (ld.lv.N + dev::p2FaceChunks(ld.lv.N)), dev::kBlock, 0, stream>>>(
-        ld.lv, p2TablesOnce(), K, FW, axd, xd, col, c);
-    ++launches;
+    const int nList = ad.closureBegin[c + 1] - ad.closureBegin[c];
+    if (nList > 0) {
+      dev::p2ClosureListKernel<T><<<(nList + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, stream>>>(
+          ld.lv, p2TablesOnce(), K, FW, axd, xd, (const dev::P2ClosureNode*)ad.closureList.p + ad.closureBegin[c],
+          nList);
+      ++launches;
+    }
     // interior nodes of colour c. An edge colour is one parity class in a cell's frame and couples
     // to no other node of its class, so those are updated in place (the closure copies keep their
     // start values until the next refresh). The four vertex colours ((b1 + 2 b2 + 3 b3) / 2 mod 4
