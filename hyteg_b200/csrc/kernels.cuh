@@ -1655,18 +1655,33 @@ static __global__ void __launch_bounds__(kBlock) blockDenseCorrectKernel(const i
   bp.x[comp[i]][idx[i]] += t;
 }
 
-// One colour pass of the P2 multicolour SOR on the owned DoFs of the flagged primitives:
-// x += omega (b - Ax) / diag, with Ax (in ax) computed for this colour from the pass's start values.
+// The owner update of one P2 SOR colour from per-colour lists: entries t < nAdd are indices into
+// the owner table (a face, edge or vertex DoF: its cells' shares are summed here), the others are
+// interior slots whose A x is in ax (the vertex colours). x += omega (b - A x) / diag.
 template <class T>
-__global__ void __launch_bounds__(kBlock) p2SorUpdateKernel(const Chunk* __restrict__ chunks, unsigned mask,
-                                                            const unsigned char* __restrict__ colour, int sel, T* x,
-                                                            const T* __restrict__ b, const T* __restrict__ ax,
-                                                            const T* __restrict__ diag, T omega) {
-  const Chunk ch = chunks[blockIdx.x];
-  if (!(ch.type & mask)) return;
-  for (int i = threadIdx.x; i < ch.len; i += blockDim.x) {
-    const int64_t j = ch.start + i;
-    if (colour[j] == (0x80 | sel)) x[j] += omega * (b[j] - ax[j]) / diag[j];
+__global__ void __launch_bounds__(kBlock) p2SorOwnersKernel(const int64_t* __restrict__ owner,
+                                                            const int* __restrict__ ptr,
+                                                            const int64_t* __restrict__ copies,
+                                                            const unsigned char* __restrict__ type,
+                                                            const int* __restrict__ addIdx, int nAdd,
+                                                            const int64_t* __restrict__ inner,
+                                                            const unsigned char* __restrict__ innerType, int nInner,
+                                                            unsigned mask, T* x, const T* __restrict__ b,
+                                                            const T* __restrict__ ax, const T* __restrict__ diag,
+                                                            T omega) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nAdd) {
+    const int j = addIdx[t];
+    if (!(type[j] & mask)) return;
+    T s = T(0);
+    for (int k = ptr[j]; k < ptr[j + 1]; ++k) s += ax[copies[k]];
+    const int64_t o = owner[j];
+    x[o] += omega * (b[o] - s) / diag[o];
+  } else if (t < nAdd + nInner) {
+    const int q = t - nAdd;
+    if (!(innerType[q] & mask)) return;
+    const int64_t o = inner[q];
+    x[o] += omega * (b[o] - ax[o]) / diag[o];
   }
 }
 

@@ -718,6 +718,48 @@ P2Additive& Storage::p2Additive(int Lf) {
       while (cur < colr) ad.closureBegin[++cur] = (int)i;
     }
     while (cur < 11) ad.closureBegin[++cur] = (int)nodes.size();
+    // the owner updates by colour: face, edge and vertex owners (indices into the owner table)
+    // and, for the vertex colours, the interior vertex nodes of the cells
+    std::vector<std::vector<int>> addBy(11);
+    for (size_t i = 0; i < own.size(); ++i) addBy[col[(size_t)own[i]] & 0x7f].push_back((int)i);
+    std::vector<std::vector<int64_t>> innerBy(4);
+    std::vector<std::vector<unsigned char>> innerTy(4);
+    for (int c = 0; c < ld.lv.nCells; ++c)
+      for (int64_t Z = 2; Z <= M - 1; Z += 2)
+        for (int64_t Y = 2; Y + Z <= M - 1; Y += 2)
+          for (int64_t X = 2; X + Y + Z <= M - 1; X += 2) {
+            const int colr = colourAt(c, X, Y, Z);
+            const int64_t loc = tet(w) - tet(w - Z) + Y * (w - Z + 1) - Y * (Y + 1) / 2 + X;
+            innerBy[colr].push_back(ld.lay->off[KC][c] + loc);
+            innerTy[colr].push_back(ld.hostCellType[c]);
+          }
+    std::vector<int> addFlat;
+    std::vector<int64_t> innerFlat;
+    std::vector<unsigned char> innerTyFlat;
+    for (int k = 0; k < 11; ++k) {
+      ad.updAddBegin[k] = (int)addFlat.size();
+      addFlat.insert(addFlat.end(), addBy[k].begin(), addBy[k].end());
+      ad.updInnerBegin[k] = (int)innerFlat.size();
+      if (k < 4) {
+        innerFlat.insert(innerFlat.end(), innerBy[k].begin(), innerBy[k].end());
+        innerTyFlat.insert(innerTyFlat.end(), innerTy[k].begin(), innerTy[k].end());
+      }
+    }
+    ad.updAddBegin[11] = (int)addFlat.size();
+    ad.updInnerBegin[11] = (int)innerFlat.size();
+    ad.updAdd.alloc(std::max<size_t>(1, addFlat.size()) * sizeof(int));
+    ad.updInner.alloc(std::max<size_t>(1, innerFlat.size()) * sizeof(int64_t));
+    ad.updInnerType.alloc(std::max<size_t>(1, innerTyFlat.size()));
+    if (!addFlat.empty())
+      cudaCheck(cudaMemcpyAsync(ad.updAdd.p, addFlat.data(), addFlat.size() * sizeof(int), cudaMemcpyHostToDevice, stream),
+                "p2 update lists");
+    if (!innerFlat.empty()) {
+      cudaCheck(cudaMemcpyAsync(ad.updInner.p, innerFlat.data(), innerFlat.size() * sizeof(int64_t),
+                                cudaMemcpyHostToDevice, stream),
+                "p2 update lists");
+      cudaCheck(cudaMemcpyAsync(ad.updInnerType.p, innerTyFlat.data(), innerTyFlat.size(), cudaMemcpyHostToDevice, stream),
+                "p2 update lists");
+    }
     ad.closureList.alloc(std::max<size_t>(1, list.size()) * sizeof(dev::P2ClosureNode));
     if (!list.empty())
       cudaCheck(cudaMemcpyAsync(ad.closureList.p, list.data(), list.size() * sizeof(dev::P2ClosureNode),
@@ -920,16 +962,14 @@ void Storage::p2SorT(P2Operator& o, int opId, int x, int b, int L, unsigned mask
     }
     // owner sums of the shares and the update of the face, edge and vertex DoFs (of the cell
     // interiors too for a vertex colour)
-    if (ad.n) {
-      dev::p2AddKernel<T, dev::MODE_REPLACE><<<(ad.n + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, stream>>>(
+    const int nAdd = ad.updAddBegin[c + 1] - ad.updAddBegin[c];
+    const int nInner = ad.updInnerBegin[c + 1] - ad.updInnerBegin[c];
+    if (nAdd + nInner > 0) {
+      dev::p2SorOwnersKernel<T><<<(nAdd + nInner + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, stream>>>(
           (const int64_t*)ad.owner.p, (const int*)ad.ptr.p, (const int64_t*)ad.copies.p, (const unsigned char*)ad.type.p,
-          ad.n, axd, nullptr, mask, col, c);
-      ++launches;
-    }
-    const int first = vertexColour ? 0 : ld.nCellChunks;
-    if (ld.nChunks > first) {
-      dev::p2SorUpdateKernel<T><<<ld.nChunks - first, dev::kBlock, 0, stream>>>(ld.chunks + first, mask, col, c, xd, bd,
-                                                                               axd, (const T*)data(dg, Lf), omega);
+          (const int*)ad.updAdd.p + ad.updAddBegin[c], nAdd, (const int64_t*)ad.updInner.p + ad.updInnerBegin[c],
+          (const unsigned char*)ad.updInnerType.p + ad.updInnerBegin[c], nInner, mask, xd, bd, axd,
+          (const T*)data(dg, Lf), omega);
       ++launches;
     }
   }

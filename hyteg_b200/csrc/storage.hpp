@@ -79,6 +79,10 @@ struct P2Additive {
   DevBuf colour;  // per slot: SOR colour of the DoF (0..10), bit 7 on its owner slot
   DevBuf mult;    // per slot: number of macro-cells holding the DoF (1 for cell-owned)
   DevBuf classOfColour;  // per cell: [0..10] parity class of colour k's interior nodes (or -1), [11] vertex colour step
+  DevBuf updAdd;                            // owner-table indices of the face/edge/vertex DoFs by colour
+  int updAddBegin[12] = {0};
+  DevBuf updInner, updInnerType;            // interior vertex slots (and their cell's type) by colour
+  int updInnerBegin[12] = {0};
   DevBuf closureList;                       // closure nodes of the cells (dev::P2ClosureNode) by colour
   int closureBegin[12] = {0};               // first entry of colour k; closureBegin[11] = total
   std::vector<int64_t> hostOwner;           // the owner slot of every DoF (levels up to 2^20 slots)
