@@ -101,6 +101,27 @@ def face_stencils(M=16):
     return out
 
 
+def divt_stencils():
+    """Per velocity class: the pressure-lattice offsets (relative to (X >> 1, Y >> 1, Z >> 1)) of
+    the vertices of the micro-cells around an interior velocity node, with the (type, local node j,
+    vertex i) triples that contribute to each."""
+    off = node_offsets()
+    out = []
+    for pc in range(8):
+        par = (pc & 1, (pc >> 1) & 1, (pc >> 2) & 1)
+        contrib = {}
+        for t in range(6):
+            for j in range(10):
+                if tuple(c & 1 for c in off[t][j]) != par:
+                    continue
+                for i in range(4):
+                    e = tuple((off[t][i][d] - off[t][j][d] + par[d]) // 2 for d in range(3))
+                    contrib.setdefault(e, []).append((t, j, i))
+        keys = sorted(contrib, key=lambda o: (o[2], o[1], o[0]))
+        out.append(keys)
+    return out
+
+
 def render():
     st = stencils()
     n = max(len(s) for s in st)
@@ -163,6 +184,26 @@ def render():
     for k, f in enumerate(fs):
         lines.append("using F%d = List<%s>;  // face %d (%s), class %d" % (k, ", ".join("O<%d, %d, %d>" % o for o in f[3]),
                                                                         f[0], FACES[f[0]], f[1]))
+    dt = divt_stencils()
+    lines += [
+        "",
+        "// Taylor-Hood coupling at interior velocity nodes (divT): per velocity class, the offsets",
+        "// (ex, ey, ez) of the pressure nodes on the pressure lattice, relative to (X >> 1, Y >> 1, Z >> 1).",
+        "// The divergence at an interior pressure node (x, y, z) reads the velocity nodes (2x, 2y, 2z) + S0.",
+        "constexpr int kDivTMaxLen = %d;" % max(len(d) for d in dt),
+        "constexpr int kDivTLen[8] = {%s};" % ", ".join(str(len(d)) for d in dt),
+        "constexpr int kDivTTotal = %d;" % sum(len(d) for d in dt),
+        "constexpr int kDivTFirst[8] = {%s};" % ", ".join(str(sum(len(x) for x in dt[:k])) for k in range(8)),
+        "constexpr signed char kDivTOff[8][kDivTMaxLen][3] = {",
+    ]
+    for d in dt:
+        lines.append("    {" + ", ".join("{%d, %d, %d}" % o for o in d) + "},")
+    lines.append("};")
+    for pc, d in enumerate(dt):
+        lines.append("using T%d = List<%s>;" % (pc, ", ".join("O<%d, %d, %d>" % o for o in d)))
+    lines += ["", "template <int PC>", "struct DivTList;"]
+    for pc in range(8):
+        lines += ["template <>", "struct DivTList<%d> {" % pc, "  using type = T%d;" % pc, "};"]
     lines += ["", "template <int PC>", "struct Class;"]
     for pc in range(8):
         lines.append("template <>")

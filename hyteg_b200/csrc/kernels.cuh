@@ -1344,7 +1344,7 @@ template <class T>
 __global__ void __launch_bounds__(kBlock) p2DivKernel(LevelDev lvp, LevelDev lvv, P2Tables tb, const T* __restrict__ D,
                                                       T* __restrict__ q, const T* __restrict__ u0,
                                                       const T* __restrict__ u1, const T* __restrict__ u2,
-                                                      unsigned mask) {
+                                                      unsigned mask, bool closureOnly) {
   const int N = lvp.N, nPl = N + 1, wp = lvp.w, wv = lvv.w;
   const int c = blockIdx.x / nPl, z = blockIdx.x % nPl;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1355,6 +1355,7 @@ __global__ void __launch_bounds__(kBlock) p2DivKernel(LevelDev lvp, LevelDev lvv
   const int pb = int(tetSize(wp) - tetSize(wp - z));
   for (int y = warp; y <= N - z; y += kBlock / 32)
     for (int x = lane; x <= N - z - y; x += 32) {
+      if (closureOnly && x >= 1 && y >= 1 && z >= 1 && x + y + z <= N - 1) continue;
       T s = T(0);
       for (int t = 0; t < 6; ++t)
         for (int i = 0; i < 4; ++i) {
@@ -1376,7 +1377,7 @@ __global__ void __launch_bounds__(kBlock) p2DivKernel(LevelDev lvp, LevelDev lvv
 template <class T>
 __global__ void __launch_bounds__(kBlock) p2DivTKernel(LevelDev lvv, LevelDev lvp, P2Tables tb, const T* __restrict__ D,
                                                        T* __restrict__ v0, T* __restrict__ v1, T* __restrict__ v2,
-                                                       const T* __restrict__ p, unsigned mask) {
+                                                       const T* __restrict__ p, unsigned mask, bool closureOnly) {
   const int M = lvv.N, N = M / 2, nPl = M + 1, wv = lvv.w, wp = lvp.w;
   const int c = blockIdx.x / nPl, Z = blockIdx.x % nPl;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1387,6 +1388,7 @@ __global__ void __launch_bounds__(kBlock) p2DivTKernel(LevelDev lvv, LevelDev lv
   const int pb = int(tetSize(wv) - tetSize(wv - Z));
   for (int Y = warp; Y <= M - Z; Y += kBlock / 32)
     for (int X = lane; X <= M - Z - Y; X += 32) {
+      if (closureOnly && X >= 1 && Y >= 1 && Z >= 1 && X + Y + Z <= M - 1) continue;
       const int pc = (X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2);
       T s0 = T(0), s1 = T(0), s2 = T(0);
       for (int k = 0; k < tb.nCand[pc]; ++k) {
@@ -1410,6 +1412,189 @@ __global__ void __launch_bounds__(kBlock) p2DivTKernel(LevelDev lvv, LevelDev lv
         v2[o] = s2;
       }
     }
+}
+
+// Interior nodes of the coupling blocks by constant stencils (the micro-cells around an interior
+// node form the same pattern at every node of its class). Weights per cell: [component][65].
+//   p2DivStencilKernel: q at an interior pressure node (x, y, z) = sum_k sum_e WD_k[e] u_k at the
+//   velocity nodes (2x, 2y, 2z) + p2s::S0[e]. Grid nCells * (Np - 3), one block per (cell, plane).
+//   p2DivTStencilKernel: v_k at an interior velocity node of class pc = sum_e WT_k[e] p at the
+//   pressure nodes (X >> 1, Y >> 1, Z >> 1) + p2s::DivTList<pc>[e]. Grid nCells * (M - 3).
+template <class T>
+__device__ __forceinline__ void p2Acc3(T& s0, T& s1, T& s2, const T* w, int I, const T* u0, const T* u1,
+                                       const T* u2, int o) {
+  s0 += w[I] * __ldg(u0 + o);
+  s1 += w[65 + I] * __ldg(u1 + o);
+  s2 += w[130 + I] * __ldg(u2 + o);
+}
+
+template <class T>
+__device__ __forceinline__ void p2Acc3T(T& s0, T& s1, T& s2, const T* w, int I, T pv) {
+  s0 += w[I] * pv;
+  s1 += w[65 + I] * pv;
+  s2 += w[130 + I] * pv;
+}
+
+template <class T, int... DX, int... DY, int... DZ, int... I>
+__device__ __forceinline__ T p2DivDot(p2s::List<p2s::O<DX, DY, DZ>...>, std::integer_sequence<int, I...>, const T* u0,
+                                      const T* u1, const T* u2, const T* w, const int (&pbz)[5], int wv, int X, int Y,
+                                      int Z) {
+  T s0 = T(0), s1 = T(0), s2 = T(0);
+  (p2Acc3<T>(s0, s1, s2, w, I, u0, u1, u2, p2RowBase<DY, DZ>(pbz, wv, Y, Z) + X + DX), ...);
+  return s0 + (s1 + s2);
+}
+
+template <class T, int... DX, int... DY, int... DZ, int... I>
+__device__ __forceinline__ void p2DivTDot(p2s::List<p2s::O<DX, DY, DZ>...>, std::integer_sequence<int, I...>,
+                                          const T* p, const T* w, const int (&pbz)[5], int wp, int x, int y, int z,
+                                          T& s0, T& s1, T& s2) {
+  (p2Acc3T<T>(s0, s1, s2, w, I, __ldg(p + p2RowBase<DY, DZ>(pbz, wp, y, z) + x + DX)), ...);
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2DivStencilKernel(LevelDev lvp, LevelDev lvv, const T* __restrict__ WD,
+                                                             T* __restrict__ q, const T* __restrict__ u0,
+                                                             const T* __restrict__ u1, const T* __restrict__ u2,
+                                                             unsigned mask) {
+  const int N = lvp.N, nPl = N - 3, wp = lvp.w, wv = lvv.w, M = lvv.N;
+  const int c = blockIdx.x / nPl, z = 1 + blockIdx.x % nPl;
+  if (!(lvp.cellType[c] & mask)) return;
+  __shared__ T wts[195];
+  for (int k = threadIdx.x; k < 195; k += blockDim.x) wts[k] = WD[(int64_t)c * 195 + k];
+  __syncthreads();
+  int pbz[5];  // velocity planes 2z - 2 .. 2z + 2
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    const int zz = 2 * z - 2 + d;
+    pbz[d] = (zz >= 0 && zz <= M) ? int(tetSize(wv) - tetSize(wv - zz)) : 0;
+  }
+  const int64_t vb = lvv.cellOff[c];
+  const int pb = int(tetSize(wp) - tetSize(wp - z));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  using S = p2s::S0;
+  for (int y = 1 + warp; y <= N - 2 - z; y += kBlock / 32)
+    for (int x = 1 + lane; x <= N - 1 - y - z; x += 32)
+      q[lvp.cellOff[c] + pb + rowStart(wp - z, y) + x] =
+          p2DivDot<T>(S{}, std::make_integer_sequence<int, p2s::kLen[0]>{}, u0 + vb, u1 + vb, u2 + vb, wts, pbz, wv,
+                      2 * x, 2 * y, 2 * z);
+}
+
+template <class T, int PC>
+__device__ __forceinline__ void p2DivTRow(const T* wts, T* v0, T* v1, T* v2, const T* p, int64_t vrow,
+                                          const int (&pbzP)[5], int wp, int M, int Y, int Z, int lane) {
+  using S = typename p2s::DivTList<PC>::type;
+  constexpr int kFirst = p2s::kDivTFirst[PC], kLen = p2s::kDivTLen[PC];
+#pragma unroll 1
+  for (int X = ((PC & 1) ? 1 : 2) + 2 * lane; X <= M - 1 - Y - Z; X += 64) {
+    T s0 = T(0), s1 = T(0), s2 = T(0);
+    p2DivTDot<T>(S{}, std::make_integer_sequence<int, kLen>{}, p, wts + kFirst, pbzP, wp, X >> 1, Y >> 1, Z >> 1, s0,
+                 s1, s2);
+    v0[vrow + X] = s0;
+    v1[vrow + X] = s1;
+    v2[vrow + X] = s2;
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2DivTStencilKernel(LevelDev lvv, LevelDev lvp, const T* __restrict__ WT,
+                                                              T* __restrict__ v0, T* __restrict__ v1,
+                                                              T* __restrict__ v2, const T* __restrict__ p,
+                                                              unsigned mask) {
+  const int M = lvv.N, nPl = M - 3, wv = lvv.w, wp = lvp.w, Np = lvp.N;
+  const int c = blockIdx.x / nPl, Z = 1 + blockIdx.x % nPl;
+  if (!(lvv.cellType[c] & mask)) return;
+  __shared__ T wts[195];
+  for (int k = threadIdx.x; k < 195; k += blockDim.x) wts[k] = WT[(int64_t)c * 195 + k];
+  __syncthreads();
+  int pbzP[5];  // pressure planes (Z >> 1) - 2 .. (Z >> 1) + 2
+#pragma unroll
+  for (int d = 0; d < 5; ++d) {
+    const int zz = (Z >> 1) - 2 + d;
+    pbzP[d] = (zz >= 0 && zz <= Np) ? int(tetSize(wp) - tetSize(wp - zz)) : 0;
+  }
+  const T* pc0 = p + lvp.cellOff[c];
+  const int64_t vb = lvv.cellOff[c] + int(tetSize(wv) - tetSize(wv - Z));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int Y = 1 + warp; Y <= M - 2 - Z; Y += kBlock / 32) {
+    const int64_t vrow = vb + rowStart(wv - Z, Y);
+#pragma unroll 1
+    for (int px = 0; px < 2; ++px) {
+      switch (px | ((Y & 1) << 1) | ((Z & 1) << 2)) {
+        case 0: p2DivTRow<T, 0>(wts, v0, v1, v2, pc0, vrow, pbzP, wp, M, Y, Z, lane); break;
+        case 1: p2DivTRow<T, 1>(wts, v0, v1, v2, pc0, vrow, pbzP, wp, M, Y, Z, lane); break;
+        case 2: p2DivTRow<T, 2>(wts, v0, v1, v2, pc0, vrow, pbzP, wp, M, Y, Z, lane); break;
+        case 3: p2DivTRow<T, 3>(wts, v0, v1, v2, pc0, vrow, pbzP, wp, M, Y, Z, lane); break;
+        case 4: p2DivTRow<T, 4>(wts, v0, v1, v2, pc0, vrow, pbzP, wp, M, Y, Z, lane); break;
+        case 5: p2DivTRow<T, 5>(wts, v0, v1, v2, pc0, vrow, pbzP, wp, M, Y, Z, lane); break;
+        case 6: p2DivTRow<T, 6>(wts, v0, v1, v2, pc0, vrow, pbzP, wp, M, Y, Z, lane); break;
+        default: p2DivTRow<T, 7>(wts, v0, v1, v2, pc0, vrow, pbzP, wp, M, Y, Z, lane); break;
+      }
+    }
+  }
+}
+
+// The closure nodes of the coupling blocks from the closure lists (one thread per node, the
+// element gather of p2DivKernel / p2DivTKernel): shares into the cells' closure slots.
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2DivClosureListKernel(LevelDev lvp, LevelDev lvv, P2Tables tb,
+                                                                 const T* __restrict__ D, T* __restrict__ q,
+                                                                 const T* __restrict__ u0, const T* __restrict__ u1,
+                                                                 const T* __restrict__ u2,
+                                                                 const P2ClosureNode* __restrict__ list, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const P2ClosureNode nd = list[idx];
+  const int N = lvp.N, wp = lvp.w, wv = lvv.w, x = nd.x, y = nd.y, z = nd.z;
+  const int64_t vb = lvv.cellOff[nd.cell];
+  const T* Dc = D + (int64_t)nd.cell * 720;
+  auto vidx = [wv](int xx, int yy, int zz) { return int(tetSize(wv) - tetSize(wv - zz)) + rowStart(wv - zz, yy) + xx; };
+  T s = T(0);
+  for (int t = 0; t < 6; ++t)
+    for (int i = 0; i < 4; ++i) {
+      const int ax = x - (tb.off[t][i][0] >> 1), ay = y - (tb.off[t][i][1] >> 1), az = z - (tb.off[t][i][2] >> 1);
+      if (ax < 0 || ay < 0 || az < 0 || ax + ay + az >= N - tb.widthRed[t]) continue;
+      const T* Dr = Dc + t * 120 + i * 10;
+#pragma unroll
+      for (int j = 0; j < 10; ++j) {
+        const int64_t g = vb + vidx(2 * ax + tb.off[t][j][0], 2 * ay + tb.off[t][j][1], 2 * az + tb.off[t][j][2]);
+        s += Dr[j] * __ldg(u0 + g) + Dr[40 + j] * __ldg(u1 + g) + Dr[80 + j] * __ldg(u2 + g);
+      }
+    }
+  q[lvp.cellOff[nd.cell] + int(tetSize(wp) - tetSize(wp - z)) + rowStart(wp - z, y) + x] = s;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) p2DivTClosureListKernel(LevelDev lvv, LevelDev lvp, P2Tables tb,
+                                                                  const T* __restrict__ D, T* __restrict__ v0,
+                                                                  T* __restrict__ v1, T* __restrict__ v2,
+                                                                  const T* __restrict__ p,
+                                                                  const P2ClosureNode* __restrict__ list, int n) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  const P2ClosureNode nd = list[idx];
+  const int M = lvv.N, N = M / 2, wv = lvv.w, wp = lvp.w, X = nd.x, Y = nd.y, Z = nd.z;
+  const int64_t pbase = lvp.cellOff[nd.cell];
+  const T* Dc = D + (int64_t)nd.cell * 720;
+  auto pidx = [wp](int x, int y, int z) { return int(tetSize(wp) - tetSize(wp - z)) + rowStart(wp - z, y) + x; };
+  const int pc = (X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2);
+  T s0 = T(0), s1 = T(0), s2 = T(0);
+  for (int k = 0; k < tb.nCand[pc]; ++k) {
+    const int t = tb.cand[pc][k][0], j = tb.cand[pc][k][1];
+    const int ax = (X - tb.off[t][j][0]) >> 1, ay = (Y - tb.off[t][j][1]) >> 1, az = (Z - tb.off[t][j][2]) >> 1;
+    if (ax < 0 || ay < 0 || az < 0 || ax + ay + az >= N - tb.widthRed[t]) continue;
+    const T* Dt = Dc + t * 120;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const T pv = __ldg(p + pbase + pidx(ax + (tb.off[t][i][0] >> 1), ay + (tb.off[t][i][1] >> 1), az + (tb.off[t][i][2] >> 1)));
+      s0 += Dt[i * 10 + j] * pv;
+      s1 += Dt[40 + i * 10 + j] * pv;
+      s2 += Dt[80 + i * 10 + j] * pv;
+    }
+  }
+  const int64_t o = lvv.cellOff[nd.cell] + int(tetSize(wv) - tetSize(wv - Z)) + rowStart(wv - Z, Y) + X;
+  v0[o] = s0;
+  v1[o] = s1;
+  v2[o] = s2;
 }
 
 // Sums the cells' shares of every DoF owned by a face, edge or vertex (the copies of that DoF in

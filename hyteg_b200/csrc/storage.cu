@@ -1122,11 +1122,71 @@ void Storage::p2Restrict(int id, int Lf, unsigned mask) {
   communicate(id, Lcf, kAllGroups);
 }
 
+// Interior coupling stencils of every cell from the divergence elements D[cell][t][k][i][j]:
+// div weights on p2s::kOff[0] (a pressure vertex i of micro-cell t sees node j at off_j - off_i),
+// divT weights on p2s::kDivTOff (velocity node j of class pc sees vertex i at (off_i - off_j + pc)/2).
+static void p2DivStencils(const std::vector<double>& D, int nCells, std::vector<double>& WD, std::vector<double>& WT) {
+  const dev::P2Tables& tb = p2TablesOnce();
+  WD.assign((size_t)nCells * 195, 0.0);
+  WT.assign((size_t)nCells * 195, 0.0);
+  auto find = [](const signed char (*tab)[3], int len, int dx, int dy, int dz) {
+    for (int e = 0; e < len; ++e)
+      if (tab[e][0] == dx && tab[e][1] == dy && tab[e][2] == dz) return e;
+    throw Error(HG_ERR_INTERNAL, "Taylor-Hood stencil table does not match the micro-cells");
+  };
+  for (int c = 0; c < nCells; ++c) {
+    const double* Dc = D.data() + (size_t)c * 720;
+    for (int t = 0; t < 6; ++t)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 10; ++j) {
+          const int e = find(p2s::kOff[0], p2s::kLen[0], tb.off[t][j][0] - tb.off[t][i][0],
+                             tb.off[t][j][1] - tb.off[t][i][1], tb.off[t][j][2] - tb.off[t][i][2]);
+          for (int k = 0; k < 3; ++k) WD[(size_t)c * 195 + k * 65 + e] += Dc[t * 120 + k * 40 + i * 10 + j];
+        }
+    for (int pc = 0; pc < 8; ++pc) {
+      const int par[3] = {pc & 1, (pc >> 1) & 1, (pc >> 2) & 1};
+      for (int q = 0; q < tb.nCand[pc]; ++q) {
+        const int t = tb.cand[pc][q][0], j = tb.cand[pc][q][1];
+        for (int i = 0; i < 4; ++i) {
+          const int e = find(p2s::kDivTOff[pc], p2s::kDivTLen[pc], (tb.off[t][i][0] - tb.off[t][j][0] + par[0]) / 2,
+                             (tb.off[t][i][1] - tb.off[t][j][1] + par[1]) / 2,
+                             (tb.off[t][i][2] - tb.off[t][j][2] + par[2]) / 2);
+          for (int k = 0; k < 3; ++k)
+            WT[(size_t)c * 195 + k * 65 + p2s::kDivTFirst[pc] + e] += Dc[t * 120 + k * 40 + i * 10 + j];
+        }
+      }
+    }
+  }
+}
+
 int Storage::createStokesOperator(int minL, int maxL) {
   const int id = createP2Operator(FORM_LAPLACE, minL, maxL);
   P2Operator& o = p2op(id);
   for (int L = minL; L <= maxL; ++L) {
     const std::vector<double> D = p2p1CellDiv(disc.topo(), L);
+    {
+      std::vector<double> WD, WT;
+      p2DivStencils(D, (int)disc.topo().cells.size(), WD, WT);
+      auto up = [&](std::vector<std::unique_ptr<DevBuf>>& dst, const std::vector<double>& v, bool fp32) {
+        dst.emplace_back(new DevBuf());
+        if (fp32) {
+          std::vector<float> f(v.begin(), v.end());
+          dst.back()->alloc(f.size() * sizeof(float));
+          cudaCheck(cudaMemcpyAsync(dst.back()->p, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice, stream),
+                    "div stencils");
+          cudaCheck(cudaStreamSynchronize(stream), "div stencils");
+        } else {
+          dst.back()->alloc(v.size() * sizeof(double));
+          cudaCheck(cudaMemcpyAsync(dst.back()->p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, stream),
+                    "div stencils");
+          cudaCheck(cudaStreamSynchronize(stream), "div stencils");
+        }
+      };
+      up(o.wdivd, WD, false);
+      up(o.wdivf, WD, true);
+      up(o.wdivtd, WT, false);
+      up(o.wdivtf, WT, true);
+    }
     std::vector<float> Df(D.begin(), D.end());
     o.dd.emplace_back(new DevBuf());
     o.dd.back()->alloc(D.size() * sizeof(double));
@@ -1158,9 +1218,24 @@ static void stokesDivTImpl(Storage& st, P2Operator& o, int p, const int v[3], in
   }
   st.communicate(p, Lp, 1 << G_CELL);
   P2Additive& adv = st.p2Additive(Lv);
-  dev::p2DivTKernel<T><<<lvv.lv.nCells * (lvv.lv.N + 1), dev::kBlock, 0, st.stream>>>(
-      lvv.lv, lvp.lv, p2TablesOnce(), D, (T*)st.data(sc[0], Lv), (T*)st.data(sc[1], Lv), (T*)st.data(sc[2], Lv),
-      (const T*)st.data(p, Lp), maskV);
+  const bool interior = lvv.lv.N >= 4;
+  if (interior) {
+    const T* WT = (const T*)(sizeof(T) == 8 ? o.wdivtd[L - o.minL]->p : o.wdivtf[L - o.minL]->p);
+    dev::p2DivTStencilKernel<T><<<lvv.lv.nCells * (lvv.lv.N - 3), dev::kBlock, 0, st.stream>>>(
+        lvv.lv, lvp.lv, WT, (T*)st.data(sc[0], Lv), (T*)st.data(sc[1], Lv), (T*)st.data(sc[2], Lv),
+        (const T*)st.data(p, Lp), maskV);
+    ++st.launches;
+  }
+  const int nClosure = adv.closureBegin[11];
+  if (interior && nClosure > 0) {  // the closure nodes from the list, one thread each
+    dev::p2DivTClosureListKernel<T><<<(nClosure + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, st.stream>>>(
+        lvv.lv, lvp.lv, p2TablesOnce(), D, (T*)st.data(sc[0], Lv), (T*)st.data(sc[1], Lv), (T*)st.data(sc[2], Lv),
+        (const T*)st.data(p, Lp), (const dev::P2ClosureNode*)adv.closureList.p, nClosure);
+  } else {
+    dev::p2DivTKernel<T><<<lvv.lv.nCells * (lvv.lv.N + 1), dev::kBlock, 0, st.stream>>>(
+        lvv.lv, lvp.lv, p2TablesOnce(), D, (T*)st.data(sc[0], Lv), (T*)st.data(sc[1], Lv), (T*)st.data(sc[2], Lv),
+        (const T*)st.data(p, Lp), maskV, interior);
+  }
   ++st.launches;
   for (int k = 0; k < 3; ++k) {
     if (adv.n)
@@ -1184,9 +1259,24 @@ static void stokesDivImpl(Storage& st, P2Operator& o, const int u[3], int q, int
   const T* D = (const T*)(sizeof(T) == 8 ? o.dd[L - o.minL]->p : o.df[L - o.minL]->p);
   for (int k = 0; k < 3; ++k) st.communicate(u[k], Lv, 1 << G_CELL);
   P2Additive& adp = st.p2Additive(Lp);
-  dev::p2DivKernel<T><<<lvp.lv.nCells * (lvp.lv.N + 1), dev::kBlock, 0, st.stream>>>(
-      lvp.lv, lvv.lv, p2TablesOnce(), D, (T*)st.data(q, Lp), (const T*)st.data(u[0], Lv), (const T*)st.data(u[1], Lv),
-      (const T*)st.data(u[2], Lv), maskP);
+  const bool interior = lvp.lv.N >= 4;
+  if (interior) {
+    const T* WD = (const T*)(sizeof(T) == 8 ? o.wdivd[L - o.minL]->p : o.wdivf[L - o.minL]->p);
+    dev::p2DivStencilKernel<T><<<lvp.lv.nCells * (lvp.lv.N - 3), dev::kBlock, 0, st.stream>>>(
+        lvp.lv, lvv.lv, WD, (T*)st.data(q, Lp), (const T*)st.data(u[0], Lv), (const T*)st.data(u[1], Lv),
+        (const T*)st.data(u[2], Lv), maskP);
+    ++st.launches;
+  }
+  const int nClosure = adp.closureBegin[11];
+  if (interior && nClosure > 0) {
+    dev::p2DivClosureListKernel<T><<<(nClosure + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, st.stream>>>(
+        lvp.lv, lvv.lv, p2TablesOnce(), D, (T*)st.data(q, Lp), (const T*)st.data(u[0], Lv), (const T*)st.data(u[1], Lv),
+        (const T*)st.data(u[2], Lv), (const dev::P2ClosureNode*)adp.closureList.p, nClosure);
+  } else {
+    dev::p2DivKernel<T><<<lvp.lv.nCells * (lvp.lv.N + 1), dev::kBlock, 0, st.stream>>>(
+        lvp.lv, lvv.lv, p2TablesOnce(), D, (T*)st.data(q, Lp), (const T*)st.data(u[0], Lv), (const T*)st.data(u[1], Lv),
+        (const T*)st.data(u[2], Lv), maskP, interior);
+  }
   ++st.launches;
   if (adp.n) {
     dev::p2AddKernel<T, dev::MODE_REPLACE><<<(adp.n + dev::kBlock - 1) / dev::kBlock, dev::kBlock, 0, st.stream>>>(

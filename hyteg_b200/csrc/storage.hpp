@@ -69,6 +69,9 @@ struct P2Operator {
   std::vector<std::unique_ptr<DevBuf>> dd, df;  // Taylor-Hood divergence per level: [cell][type][3][4][10]
   std::vector<std::unique_ptr<DevBuf>> sd, sf;  // interior stencils per level: [cell][p2s::kTotal]
   std::vector<std::unique_ptr<DevBuf>> fd, ff;  // face-interior stencils per level: [cell][p2s::kFaceTotal]
+  // Taylor-Hood coupling at interior nodes per level, [cell][component][65]: div (offsets p2s::S0 on
+  // the velocity lattice) and divT (offsets p2s::DivTList per velocity class on the pressure lattice)
+  std::vector<std::unique_ptr<DevBuf>> wdivd, wdivf, wdivtd, wdivtf;
 };
 
 // Cell-closure copies of every DoF owned by a face, edge or vertex of one lattice level.
