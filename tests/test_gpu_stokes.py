@@ -157,3 +157,43 @@ def test_minres_with_fp32_preconditioner_matches_fp64(env):
         assert np.abs(u32[k][m] - u64[k][m]).max() < 1e-8
     mp = maps[L][1] == 1
     assert np.abs(p32[mp] - p64[mp]).max() / np.abs(p64[mp]).max() < 1e-7
+
+
+@pytest.fixture(scope="module")
+def env3():
+    if hg.device_count() == 0:
+        pytest.skip("no CUDA device")
+    coords, tets, mesh, orc = H.cube(4)
+    st = hg.PrimitiveStorage.cuboid((0, 0, 0), (1, 1, 1), 2, 2, 2, 4)
+    maps = {}
+    for L in (3, 4):
+        xyz, owned = mesh.slot_info(L)
+        maps[L] = (H.match_slots(xyz, orc.nodes(L)[0]), owned, xyz)
+    return st, orc, maps
+
+
+def test_stokes_apply_level3_interior_stencils(env3):
+    # pressure lattice 8, velocity lattice 16 per macro-cell: most nodes take the interior
+    # div / divT stencils, the closure nodes the per-node gathers from the closure lists
+    st, orc, maps = env3
+    L = 3
+    S = hg.P2P1TaylorHoodStokesOperator(st, 0, L)
+    nv, np_ = orc.n(L + 1), orc.n(L)
+    rng = np.random.default_rng(313)
+    uu = [rng.uniform(-1, 1, nv) for _ in range(3)]
+    pp = rng.uniform(-1, 1, np_)
+    u = [hg.P2Function("u%d" % k, st, 0, L) for k in range(3)]
+    v = [hg.P2Function("v%d" % k, st, 0, L) for k in range(3)]
+    p, q = hg.P1Function("p", st, 0, L), hg.P1Function("q", st, 0, L)
+    for k in range(3):
+        u[k].from_numpy(L, H.scatter(maps[L + 1][0], uu[k]))
+        v[k].from_numpy(L, np.zeros(st.level_size(L + 1)))
+    p.from_numpy(L, H.scatter(maps[L][0], pp))
+    S.apply(u, p, v, q, L)
+    vr, qr = orc.stokes_apply(L, uu, pp)
+    inner = ~orc.dirichlet(L + 1)
+    for k in range(3):
+        got = H.gather_owned(v[k].to_numpy(L), maps[L + 1][0], maps[L + 1][1], nv)
+        assert rel(got, vr[k], inner) < 1e-13
+    gq = H.gather_owned(q.to_numpy(L), maps[L][0], maps[L][1], np_)
+    assert rel(gq, qr, np.ones(np_, dtype=bool)) < 1e-13
