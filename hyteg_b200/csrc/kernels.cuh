@@ -207,9 +207,9 @@ __global__ void __launch_bounds__(kBlock, 4) cellSorKernel(LevelDev lv, const T*
 // A block owns a 32 x TY (x, y) tile of one macro-cell for all planes (WaveCfg). It recomputes a shrinking
 // halo (stage k on the tile widened by 3 - k) from the start-of-sweep values, which makes the
 // tiles independent: they read uOld and write uNew, and the caller swaps the two buffers.
-// Planes s-7 .. s+1 of the tile widened by 4 (40 x (TY + 8) points) live in a 9-slot shared-memory
-// ring; plane s+2 is loaded into registers during step s and stored into the slot that plane
-// s-7 frees. Point (rx, ry) of the region sits at
+// Planes s-7 .. s+1 (and s-8 with a 10-plane ring) of the tile widened by 4 (40 x (TY + 8) points)
+// live in a shared-memory ring; plane s+2 is loaded into registers during step s and stored into
+// the slot of the oldest plane. Point (rx, ry) of the region sits at
 //   ry * 42 + ((rx mod 4 + 2 ry) mod 4) * 10 + rx / 4,
 // i.e. each row is split by x mod 4 and the split is rotated by 2y. The points of one colour then
 // occupy the same sub-row of every row, and with the row stride 42 (= 10 mod 16) the 16 lanes
@@ -222,23 +222,25 @@ constexpr int kWaveH = 4;                           // halo loaded around the ti
 constexpr int kWaveRX = kWaveTX + 2 * kWaveH;       // region extent in x (40)
 constexpr int kWaveQ = kWaveRX / 4;                 // column groups per region row (10)
 constexpr int kWaveS = 42;                          // shared-memory row stride (10 mod 16)
-constexpr int kWaveSlots = 9;
 constexpr int kWaveMaxN = 4096;                     // largest level size the shared-memory limit is set for
 
-// Tile height, block size and blocks per SM per precision. 32 x 28 tiles (region 40 x 36, 360
-// column groups): FP64 109 KB of ring, two blocks per SM; FP32 55 KB, three blocks per SM (a
-// register budget of 56 per thread). Measured per level-8 sweep, FP64: 2.34 ms (32 x 28, two
-// blocks per SM), 2.35 ms (32 x 16, three), 2.78 ms (32 x 60, one); FP32: 1.41 ms (32 x 28,
-// three), 1.67 ms (32 x 28, four at 40 registers), 1.83 ms (32 x 60, two).
+// Tile height, block size, blocks per SM and ring planes per precision. A 10-plane ring needs one
+// barrier per step instead of two. FP64: 32 x 24 tiles (region 40 x 32, 320 column groups),
+// 108 KB of ring, two blocks per SM; FP32: 32 x 28 tiles (region 40 x 36, 360 groups), 61 KB,
+// three blocks per SM (a register budget of 56 per thread). Measured per level-8 sweep, FP64:
+// 2.21 ms (32 x 24, 10 planes), 2.34 ms (32 x 28, 9 planes, two barriers), 2.35 ms (32 x 16, 9,
+// three blocks per SM), 2.78 ms (32 x 60, 9, one block per SM); FP32: 1.36 ms (32 x 28, 10
+// planes), 1.41 ms (32 x 28, 9 planes), 1.67 ms (four blocks per SM at 40 registers), 1.83 ms
+// (32 x 60, two blocks per SM).
 template <class T>
 struct WaveCfg;
 template <>
 struct WaveCfg<double> {
-  static constexpr int TY = 28, THREADS = 384, MIN_BLOCKS = 2;
+  static constexpr int TY = 24, THREADS = 320, MIN_BLOCKS = 2, SLOTS = 10;
 };
 template <>
 struct WaveCfg<float> {
-  static constexpr int TY = 28, THREADS = 384, MIN_BLOCKS = 3;
+  static constexpr int TY = 28, THREADS = 384, MIN_BLOCKS = 3, SLOTS = 10;
 };
 template <class T>
 struct WaveGeom {
@@ -247,7 +249,9 @@ struct WaveGeom {
   static constexpr int PLANE = RY * kWaveS;        // elements per plane slot
   static constexpr int GROUPS = RY * kWaveQ;       // column groups, one per thread
   static constexpr int THREADS = WaveCfg<T>::THREADS;
+  static constexpr int SLOTS = WaveCfg<T>::SLOTS;  // ring planes: 9 (s-7 .. s+1), or 10 to drop a barrier
   static_assert(THREADS >= GROUPS && THREADS % 32 == 0 && TY % 2 == 0, "wave tile configuration");
+  static_assert(SLOTS == 9 || SLOTS == 10, "wave ring size");
 };
 
 struct WaveTile {
@@ -257,7 +261,7 @@ struct WaveTile {
 // Dynamic shared memory of the kernel for level size N.
 template <class T>
 inline size_t waveSmemBytes(int N) {
-  return size_t(kWaveSlots) * WaveGeom<T>::PLANE * sizeof(T) + size_t(N + 2) * sizeof(int);
+  return size_t(WaveGeom<T>::SLOTS) * WaveGeom<T>::PLANE * sizeof(T) + size_t(N + 2) * sizeof(int);
 }
 
 template <class T>
@@ -266,10 +270,10 @@ __global__ void __launch_bounds__(WaveCfg<T>::THREADS, WaveCfg<T>::MIN_BLOCKS)
                       const T* __restrict__ uOld, T* __restrict__ uNew, const T* __restrict__ rhs, unsigned mask,
                       T omega, int backwards) {
   constexpr int kTY = WaveGeom<T>::TY, kRY = WaveGeom<T>::RY, kPlane = WaveGeom<T>::PLANE;
-  constexpr int kGroups = WaveGeom<T>::GROUPS, kThreads = WaveGeom<T>::THREADS;
+  constexpr int kGroups = WaveGeom<T>::GROUPS, kThreads = WaveGeom<T>::THREADS, kSlots = WaveGeom<T>::SLOTS;
   extern __shared__ __align__(16) unsigned char waveSmem[];
   T* sm = reinterpret_cast<T*>(waveSmem);
-  int* pbTab = reinterpret_cast<int*>(sm + kWaveSlots * kPlane);  // first index of plane p
+  int* pbTab = reinterpret_cast<int*>(sm + kSlots * kPlane);  // first index of plane p
   const WaveTile tl = tiles[blockIdx.x];
   const int N = lv.N, w = lv.w, tid = threadIdx.x;
   const int64_t base = lv.cellOff[tl.cell];
@@ -369,26 +373,31 @@ __global__ void __launch_bounds__(WaveCfg<T>::THREADS, WaveCfg<T>::MIN_BLOCKS)
     for (int j = 0; j < 4; ++j)
       if (x4 + j + y <= N - p) un[g + j] = s[((j + rot) & 3) * kWaveQ];
   };
-  auto wrap = [](int v) { return v >= kWaveSlots ? v - kWaveSlots : v; };  // v in [0, 2 * slots)
+  auto wrap = [](int v) { return v >= kSlots ? v - kSlots : v; };  // v in [0, 2 * slots)
 
   loadRegs(0);
   storeRegs(0, 0);
   loadRegs(1);
   storeRegs(1, 1);
   const int sEnd = tl.pEnd + 6;
-  int ss = 0;  // s mod 9
+  // Plane p lives in ring slot p mod kSlots. With 9 slots, plane s+2 takes the slot of plane s-7,
+  // which stage 3 of the same step still reads: a second barrier separates them. With 10 slots it
+  // takes the slot of plane s-8, last read in step s-1 (stage 3 on plane s-7) and so already
+  // behind the first barrier of step s. The store of plane s-6 reads only the thread's own
+  // columns, whose final values the thread itself wrote in stage 3 of this step.
+  int ss = 0;  // s mod kSlots
   for (int s = 0; s <= sEnd; ++s) {
     loadRegs(s + 2);
     __syncthreads();  // the previous step's stores into the ring are visible
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int p = s - 2 * k;
-      const int sp = wrap(ss + kWaveSlots - 2 * k);  // slot of plane p
-      if (p >= 1 && p <= N - 3) stage(k, p, sp, wrap(sp + 1), wrap(sp + kWaveSlots - 1));
+      const int sp = wrap(ss + kSlots - 2 * k);  // slot of plane p
+      if (p >= 1 && p <= N - 3) stage(k, p, sp, wrap(sp + 1), wrap(sp + kSlots - 1));
     }
-    __syncthreads();  // plane s-7 is no longer read; plane s-6 is final
+    if (kSlots == 9) __syncthreads();  // plane s-7 is no longer read
     storeRegs(s + 2, wrap(ss + 2));
-    if (s >= 6 && s - 6 <= tl.pEnd) store(s - 6, wrap(ss + 3));  // (s - 6) mod 9 = (s + 3) mod 9
+    if (s >= 6 && s - 6 <= tl.pEnd) store(s - 6, wrap(ss + kSlots - 6));
     ss = wrap(ss + 1);
   }
 }
