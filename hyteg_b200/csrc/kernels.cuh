@@ -232,24 +232,34 @@ constexpr int kWaveMaxN = 4096;                     // largest level size the sh
 // three blocks per SM), 2.78 ms (32 x 60, 9, one block per SM); FP32: 1.36 ms (32 x 28, 10
 // planes), 1.41 ms (32 x 28, 9 planes), 1.67 ms (four blocks per SM at 40 registers), 1.83 ms
 // (32 x 60, two blocks per SM).
-template <class T>
+// V = 1 is a second, shorter tile (32 x 12) for the autotuner: more blocks per SM and more tiles
+// per level, for levels whose 32 x 24 (28) tiles fill the GPU in few waves.
+template <class T, int V = 0>
 struct WaveCfg;
 template <>
-struct WaveCfg<double> {
+struct WaveCfg<double, 0> {
   static constexpr int TY = 24, THREADS = 320, MIN_BLOCKS = 2, SLOTS = 10;
 };
 template <>
-struct WaveCfg<float> {
+struct WaveCfg<float, 0> {
   static constexpr int TY = 28, THREADS = 384, MIN_BLOCKS = 3, SLOTS = 10;
 };
-template <class T>
+template <>
+struct WaveCfg<double, 1> {
+  static constexpr int TY = 12, THREADS = 224, MIN_BLOCKS = 3, SLOTS = 10;
+};
+template <>
+struct WaveCfg<float, 1> {
+  static constexpr int TY = 12, THREADS = 224, MIN_BLOCKS = 4, SLOTS = 10;
+};
+template <class T, int V = 0>
 struct WaveGeom {
-  static constexpr int TY = WaveCfg<T>::TY;        // tile extent in y (even)
-  static constexpr int RY = TY + 2 * kWaveH;       // region extent in y
-  static constexpr int PLANE = RY * kWaveS;        // elements per plane slot
-  static constexpr int GROUPS = RY * kWaveQ;       // column groups, one per thread
-  static constexpr int THREADS = WaveCfg<T>::THREADS;
-  static constexpr int SLOTS = WaveCfg<T>::SLOTS;  // ring planes: 9 (s-7 .. s+1), or 10 to drop a barrier
+  static constexpr int TY = WaveCfg<T, V>::TY;        // tile extent in y (even)
+  static constexpr int RY = TY + 2 * kWaveH;          // region extent in y
+  static constexpr int PLANE = RY * kWaveS;           // elements per plane slot
+  static constexpr int GROUPS = RY * kWaveQ;          // column groups, one per thread
+  static constexpr int THREADS = WaveCfg<T, V>::THREADS;
+  static constexpr int SLOTS = WaveCfg<T, V>::SLOTS;  // ring planes: 9 (s-7 .. s+1), or 10 to drop a barrier
   static_assert(THREADS >= GROUPS && THREADS % 32 == 0 && TY % 2 == 0, "wave tile configuration");
   static_assert(SLOTS == 9 || SLOTS == 10, "wave ring size");
 };
@@ -259,18 +269,18 @@ struct WaveTile {
 };
 
 // Dynamic shared memory of the kernel for level size N.
-template <class T>
+template <class T, int V = 0>
 inline size_t waveSmemBytes(int N) {
-  return size_t(WaveGeom<T>::SLOTS) * WaveGeom<T>::PLANE * sizeof(T) + size_t(N + 2) * sizeof(int);
+  return size_t(WaveGeom<T, V>::SLOTS) * WaveGeom<T, V>::PLANE * sizeof(T) + size_t(N + 2) * sizeof(int);
 }
 
-template <class T>
-__global__ void __launch_bounds__(WaveCfg<T>::THREADS, WaveCfg<T>::MIN_BLOCKS)
+template <class T, int V>
+__global__ void __launch_bounds__(WaveCfg<T, V>::THREADS, WaveCfg<T, V>::MIN_BLOCKS)
     cellSorWaveKernel(LevelDev lv, const WaveTile* __restrict__ tiles, const T* __restrict__ cellW,
                       const T* __restrict__ uOld, T* __restrict__ uNew, const T* __restrict__ rhs, unsigned mask,
                       T omega, int backwards) {
-  constexpr int kTY = WaveGeom<T>::TY, kRY = WaveGeom<T>::RY, kPlane = WaveGeom<T>::PLANE;
-  constexpr int kGroups = WaveGeom<T>::GROUPS, kThreads = WaveGeom<T>::THREADS, kSlots = WaveGeom<T>::SLOTS;
+  constexpr int kTY = WaveGeom<T, V>::TY, kRY = WaveGeom<T, V>::RY, kPlane = WaveGeom<T, V>::PLANE;
+  constexpr int kGroups = WaveGeom<T, V>::GROUPS, kThreads = WaveGeom<T, V>::THREADS, kSlots = WaveGeom<T, V>::SLOTS;
   extern __shared__ __align__(16) unsigned char waveSmem[];
   T* sm = reinterpret_cast<T*>(waveSmem);
   int* pbTab = reinterpret_cast<int*>(sm + kSlots * kPlane);  // first index of plane p

@@ -66,11 +66,17 @@ static unsigned char dofType(int meshFlag) {
 
 Storage::Storage(const Topology& topo, int maxLevel) : disc(topo, maxLevel) {
   cudaCheck(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "cudaStreamCreate");
-  cudaCheck(cudaFuncSetAttribute(dev::cellSorWaveKernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)dev::waveSmemBytes<double>(dev::kWaveMaxN)),
+  cudaCheck(cudaFuncSetAttribute(dev::cellSorWaveKernel<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dev::waveSmemBytes<double, 0>(dev::kWaveMaxN)),
             "wave kernel shared memory");
-  cudaCheck(cudaFuncSetAttribute(dev::cellSorWaveKernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)dev::waveSmemBytes<float>(dev::kWaveMaxN)),
+  cudaCheck(cudaFuncSetAttribute(dev::cellSorWaveKernel<float, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dev::waveSmemBytes<float, 0>(dev::kWaveMaxN)),
+            "wave kernel shared memory");
+  cudaCheck(cudaFuncSetAttribute(dev::cellSorWaveKernel<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dev::waveSmemBytes<double, 1>(dev::kWaveMaxN)),
+            "wave kernel shared memory");
+  cudaCheck(cudaFuncSetAttribute(dev::cellSorWaveKernel<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)dev::waveSmemBytes<float, 1>(dev::kWaveMaxN)),
             "wave kernel shared memory");
   stream = ownStream;
   levels.resize(maxLevel + 1);
@@ -199,17 +205,21 @@ void Storage::buildLevel(int L) {
   // single-pass SOR tiles: every (x, y) of the cell is in exactly one tile, tallest tiles first;
   // one list per precision (the tile heights differ)
   {
-    for (int pi = 0; pi < 2; ++pi) {
-      const int ty = pi == 0 ? dev::WaveGeom<double>::TY : dev::WaveGeom<float>::TY;
-      std::vector<dev::WaveTile> wt;
-      if (N >= 4)
-        for (int c = 0; c < lv.nCells; ++c)
-          for (int y0 = 0; y0 <= N; y0 += ty)
-            for (int x0 = 0; x0 + y0 <= N; x0 += dev::kWaveTX) wt.push_back({c, x0, y0, (int)N - x0 - y0});
-      std::stable_sort(wt.begin(), wt.end(), [](const dev::WaveTile& a, const dev::WaveTile& b) { return a.pEnd > b.pEnd; });
-      ld.waveTiles[pi] = (dev::WaveTile*)upload(keep, wt, stream);
-      ld.nWaveTiles[pi] = (int)wt.size();
-    }
+    const int tys[2][2] = {{dev::WaveGeom<double, 0>::TY, dev::WaveGeom<double, 1>::TY},
+                           {dev::WaveGeom<float, 0>::TY, dev::WaveGeom<float, 1>::TY}};
+    for (int pi = 0; pi < 2; ++pi)
+      for (int gv = 0; gv < 2; ++gv) {
+        const int ty = tys[pi][gv];
+        std::vector<dev::WaveTile> wt;
+        if (N >= 4)
+          for (int c = 0; c < lv.nCells; ++c)
+            for (int y0 = 0; y0 <= N; y0 += ty)
+              for (int x0 = 0; x0 + y0 <= N; x0 += dev::kWaveTX) wt.push_back({c, x0, y0, (int)N - x0 - y0});
+        std::stable_sort(wt.begin(), wt.end(),
+                         [](const dev::WaveTile& a, const dev::WaveTile& b) { return a.pEnd > b.pEnd; });
+        ld.waveTiles[pi][gv] = (dev::WaveTile*)upload(keep, wt, stream);
+        ld.nWaveTiles[pi][gv] = (int)wt.size();
+      }
     int64_t first = lay.total;
     for (int k : {KV, KE, KF})
       for (int64_t o : lay.off[k]) first = std::min(first, o);
@@ -1365,7 +1375,7 @@ void Storage::autotuneSor(int minL, int maxL, int prec, int reps, double* ms) {
     fillRandom(b, L, HG_ALL, 2, -1.0, 1.0);
     double best = 0;
     int pick = 0;
-    for (int sch = 0; sch < 2; ++sch) {
+    for (int sch = 0; sch < 3; ++sch) {
       sorScheduleLevel[2 * L + pi] = sch;
       smoothSor(op, x, b, 1.0, L, HG_INNER | HG_NEUMANN, false);  // warm-up (allocates the spare)
       cudaCheck(cudaEventRecord(e0, stream), "event");
@@ -1375,7 +1385,7 @@ void Storage::autotuneSor(int minL, int maxL, int prec, int reps, double* ms) {
       float t = 0;
       cudaCheck(cudaEventElapsedTime(&t, e0, e1), "event");
       const double per = t / reps;
-      if (ms) ms[2 * (L - minL) + sch] = per;
+      if (ms) ms[3 * (L - minL) + sch] = per;
       if (sch == 0 || per < best) {
         best = per;
         pick = sch;
@@ -1533,8 +1543,8 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
     const int tuned = 2 * L + (sizeof(T) == 4 ? 1 : 0);
     const int schedule = (int)sorScheduleLevel.size() > tuned && sorScheduleLevel[tuned] >= 0 ? sorScheduleLevel[tuned]
                                                                                                   : sorSchedule;
-    const int pi = sizeof(T) == 4 ? 1 : 0;
-    if (schedule == 0 && ld.nWaveTiles[pi]) {
+    const int pi = sizeof(T) == 4 ? 1 : 0, gv = schedule == 2 ? 1 : 0;
+    if (schedule != 1 && ld.nWaveTiles[pi][gv]) {
       // one pass into the spare buffer of this level, which then becomes the function's buffer
       Function& fd = fn(dstId);
       std::unique_ptr<DevBuf>& cur = fd.levels[L - fd.minL];
@@ -1545,9 +1555,14 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
         cudaCheck(cudaMemsetAsync(sp->p, 0, sp->bytes, stream), "spare memset");  // alignment padding stays zero
       }
       T* out = (T*)sp->p;
-      const size_t smem = dev::waveSmemBytes<T>(lv.N);
-      dev::cellSorWaveKernel<T><<<ld.nWaveTiles[pi], dev::WaveGeom<T>::THREADS, smem, stream>>>(
-          lv, ld.waveTiles[pi], st.cellW, u, out, rhs, mask, omega, rev ? 1 : 0);
+      if (gv == 0)
+        dev::cellSorWaveKernel<T, 0><<<ld.nWaveTiles[pi][0], dev::WaveGeom<T, 0>::THREADS,
+                                       dev::waveSmemBytes<T, 0>(lv.N), stream>>>(lv, ld.waveTiles[pi][0], st.cellW, u,
+                                                                                  out, rhs, mask, omega, rev ? 1 : 0);
+      else
+        dev::cellSorWaveKernel<T, 1><<<ld.nWaveTiles[pi][1], dev::WaveGeom<T, 1>::THREADS,
+                                       dev::waveSmemBytes<T, 1>(lv.N), stream>>>(lv, ld.waveTiles[pi][1], st.cellW, u,
+                                                                                  out, rhs, mask, omega, rev ? 1 : 0);
       ++launches;
       const int64_t tail = ld.lay->total - ld.nonCellBegin;
       if (tail > 0)

@@ -41,8 +41,9 @@ struct LevelData {
   std::unique_ptr<DevBuf> tileBuf;
   DevBuf partial;
   // single-pass SOR: one 32 x 32 (x, y) tile of a macro-cell per block, the tallest first
-  dev::WaveTile* waveTiles[2] = {nullptr, nullptr};  // single-pass SOR tiles: [0] FP64, [1] FP32 geometry
-  int nWaveTiles[2] = {0, 0};
+  // single-pass SOR tiles per [precision: 0 FP64, 1 FP32][tile geometry: 0, 1]
+  dev::WaveTile* waveTiles[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int nWaveTiles[2][2] = {{0, 0}, {0, 0}};
   int64_t nonCellBegin = 0;  // first slot after the cell arrays (faces, edges, vertices follow)
   std::vector<unsigned char> hostCellType, hostFaceType, hostLowType;
   std::vector<std::unique_ptr<DevBuf>> keep;
@@ -124,11 +125,12 @@ struct Storage {
   int64_t l2Budget = int64_t(1) << 62;  // bytes of L2 one SOR cell group may occupy (default: one group)
   unsigned long long launches = 0;  // kernels launched by this storage
   // Cell-phase schedule of the multicolour SOR: 0 = one wavefront pass that writes a second
-  // buffer which then replaces the level buffer, 1 = four in-place colour passes.
+  // buffer which then replaces the level buffer, 1 = four in-place colour passes, 2 = the
+  // wavefront pass with the shorter tile geometry.
   int sorSchedule = 0;
   std::vector<int> sorScheduleLevel;  // [2 L + (FP32 ? 1 : 0)]: schedule chosen by autotuneSor (-1: sorSchedule)
-  // Times both schedules of one SOR sweep on levels [minL, maxL] in the given precision and keeps
-  // the faster per level; ms[2 * (L - minL) + s] receives the measured times (nullable).
+  // Times the three schedules of one SOR sweep on levels [minL, maxL] in the given precision and
+  // keeps the fastest per level; ms[3 * (L - minL) + s] receives the measured times (nullable).
   void autotuneSor(int minL, int maxL, int prec, int reps, double* ms);
   unsigned long long generation = 0;  // bumped when level tables or schedules change (captured graphs)
   std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> spare;  // (level, precision) -> buffer

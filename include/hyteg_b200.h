@@ -97,13 +97,14 @@ int hg_storage_launch_count(const hg_storage* s, unsigned long long* count);
 int hg_storage_set_cell_coefficients(hg_storage* s, const double* k, int ncells);
 /* Cell-phase schedule of the multicolour SOR: 0 (default) = one pass per sweep (z-wavefront over
  * the four colours, written to a second buffer of the level that then replaces the smoothed
- * function's buffer), 1 = four in-place colour passes. Both give the same multicolour sweep. */
+ * function's buffer), 1 = four in-place colour passes, 2 = the single pass with shorter tiles
+ * (32 x 12 instead of 32 x 24 / 28). All give the same multicolour sweep. */
 int hg_storage_set_sor_schedule(hg_storage* s, int schedule);
-/* Autotuner (no counterpart in the reference): times one multicolour SOR sweep under both
+/* Autotuner (no counterpart in the reference): times one multicolour SOR sweep under the three
  * schedules on every level in [min_level, max_level] (precision 8 or 4, `reps` timed sweeps after
- * one warm-up, CUDA events on the storage's stream) and keeps the faster schedule per level,
- * and precision, overriding hg_storage_set_sor_schedule there. ms (nullable): 2 * (levels) times in ms, schedule
- * 0 then 1 per level; chosen (nullable): the schedule kept per level. */
+ * one warm-up, CUDA events on the storage's stream) and keeps the fastest schedule per level and
+ * precision, overriding hg_storage_set_sor_schedule there. ms (nullable): 3 * (levels) times in
+ * ms, schedules 0, 1, 2 per level; chosen (nullable): the schedule kept per level. */
 int hg_storage_autotune_sor(hg_storage* s, int min_level, int max_level, int precision, int reps, double* ms,
                             int* chosen);
 /* Topology export: for kind HG_VERTEX ids[0..2]=unused, coords[3]; HG_EDGE ids[2]; HG_FACE ids[3];

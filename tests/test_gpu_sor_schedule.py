@@ -1,6 +1,6 @@
 """The single-pass (z-wavefront, double-buffered) multicolour SOR against the four in-place
-colour passes and against the oracle, at levels where a macro-cell spans several 32 x 32 tiles
-(level 5: 3 tiles per cell, level 6: 10).
+colour passes and against the oracle, at levels where a macro-cell spans several tiles (32 x 24 or
+32 x 28, and the shorter 32 x 12 tiles of schedule 2).
 
 Tolerances: FP64 1e-13 relative (max-norm over inner DoFs); FP32 1e-5 relative (the two
 schedules round the relaxation differently)."""
@@ -42,14 +42,16 @@ def cube6():
 @pytest.mark.parametrize("L", [5, 6])
 @pytest.mark.parametrize("backwards", [False, True])
 @pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-13), (np.float32, 1e-5)])
-def test_single_pass_equals_colour_passes(cube6, L, backwards, dtype, tol):
+@pytest.mark.parametrize("schedule", [0, 2])
+def test_single_pass_equals_colour_passes(cube6, L, backwards, dtype, tol, schedule):
+    # schedule 0: 32 x 24 (FP64) / 32 x 28 (FP32) tiles; schedule 2: 32 x 12 tiles
     st, mesh = cube6
     n = st.level_size(L)
     _, owned = mesh.slot_info(L)
     rng = np.random.default_rng(L + 10 * backwards)
     x0 = rng.uniform(-1, 1, n).astype(dtype)
     b0 = rng.uniform(-1, 1, n).astype(dtype)
-    got = run_sor(st, L, x0, b0, dtype, 0, 2, backwards)
+    got = run_sor(st, L, x0, b0, dtype, schedule, 2, backwards)
     ref = run_sor(st, L, x0, b0, dtype, 1, 2, backwards)
     m = owned == 1
     assert np.abs(got[m] - ref[m]).max() / np.abs(ref[m]).max() < tol
