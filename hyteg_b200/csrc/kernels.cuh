@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(kBlock, 4) cellSorKernel(LevelDev lv, const T*
   const int64_t base = lv.cellOff[c];
   T* uc = u + base;
   const T* __restrict__ f = rhs + base;
-  const T om = omega, om1 = T(1) - omega, dinv = omega / wt[0];
+  const T om = omega, om1 = T(1) - omega;
   const int W = lv.w - z;
   auto ld = [uc](int i) { return uc[i]; };
   for (int y = 1 + (int)(threadIdx.x >> 5); y <= W - 3; y += kBlock / 32) {
@@ -192,7 +192,6 @@ __global__ void __launch_bounds__(kBlock, 4) cellSorKernel(LevelDev lv, const T*
       if (two) uc[r.r0 + x2] = om1 * uc[r.r0 + x2] + (s2 * om) / wt[0];
     }
   }
-  (void)dinv;
 }
 
 // ---------------------------------------------------------------------------------------

@@ -794,7 +794,6 @@ int stokesMinres(Storage& s, int op, const int u[3], int p, const int f[3], int 
       mg.runCycle(px, pb, L);
       s.copyCast(dst.u[k], px, Lv, fv, false);
     }
-    (void)one;
     s.divideBy(dst.p, src.p, lumped, Lp, fp);
     const double mean = s.dot(dst.p, ones, Lp, fp) / nP;
     s.lincomb(dst.p, Lp, fp, 1, &one, &dst.p, false, -mean);

@@ -464,7 +464,7 @@ double Storage::dot(int a, int b, int L, unsigned mask) {
 // operators
 // ------------------------------------------------------------------------------------------
 template <class T>
-static dev::StencilDev<T> packStencil(std::vector<std::unique_ptr<DevBuf>>& keep, const LevelStencils& st, int nEdges,
+static dev::StencilDev<T> packStencil(std::vector<std::unique_ptr<DevBuf>>& keep, const LevelStencils& st,
                                       cudaStream_t stream) {
   std::vector<T> cellW;
   for (auto& c : st.cell)
@@ -489,7 +489,6 @@ static dev::StencilDev<T> packStencil(std::vector<std::unique_ptr<DevBuf>>& keep
   };
   for (auto& e : st.edge) addLow(e);
   for (auto& v : st.vert) addLow(v);
-  (void)nEdges;
   dev::StencilDev<T> d;
   d.cellW = (const T*)upload(keep, cellW, stream);
   d.faceEnt = (const dev::FaceEnt<T>*)upload(keep, fe, stream);
@@ -1420,8 +1419,8 @@ int Storage::createOperator(int form, int minL, int maxL) {
   op->maxL = maxL;
   for (int L = minL; L <= maxL; ++L) {
     op->host.push_back(assembleStencils(disc, L, (FormKind)form));
-    op->d.push_back(packStencil<double>(op->keep, op->host.back(), (int)disc.topo().edges.size(), stream));
-    op->f.push_back(packStencil<float>(op->keep, op->host.back(), (int)disc.topo().edges.size(), stream));
+    op->d.push_back(packStencil<double>(op->keep, op->host.back(), stream));
+    op->f.push_back(packStencil<float>(op->keep, op->host.back(), stream));
   }
   cudaCheck(cudaStreamSynchronize(stream), "operator upload");
   const int id = nextId++;
