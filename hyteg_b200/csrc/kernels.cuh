@@ -978,12 +978,13 @@ __device__ __forceinline__ int p2RowBase(const int (&pbz)[5], int w, int Y, int 
 // The loads go through the read-only path also in the in-place SOR pass: no thread reads a value
 // that another thread writes during the launch (a colour class couples to no node of its own
 // colour), and each thread reads its own node before writing it.
+// Four partial sums (entry I into sum I mod 4) keep the FMA dependency chains short.
 template <class T, int... DX, int... DY, int... DZ, int... I>
 __device__ __forceinline__ T p2StencilDot(p2s::List<p2s::O<DX, DY, DZ>...>, std::integer_sequence<int, I...>,
                                           const T* u, const T* wt, const int (&pbz)[5], int w, int X, int Y, int Z) {
-  T s = T(0);
-  ((s += wt[I] * __ldg(u + p2RowBase<DY, DZ>(pbz, w, Y, Z) + X + DX)), ...);
-  return s;
+  T s[4] = {T(0), T(0), T(0), T(0)};
+  ((s[I & 3] += wt[I] * __ldg(u + p2RowBase<DY, DZ>(pbz, w, Y, Z) + X + DX)), ...);
+  return (s[0] + s[1]) + (s[2] + s[3]);
 }
 
 // One row (Y, Z) of class PC: MODE_REPLACE dst = A src, MODE_RESIDUAL dst = rhs - A src,
@@ -1055,7 +1056,7 @@ __device__ __forceinline__ void p2StencilRowAny(int pc, const T* wts, T* dst, co
 // from one vertex node of a row to the next (1, 2 or 3). MODE_SOR updates in place: dst == src,
 // rhs = b.
 template <class T, int MODE>
-__global__ void __launch_bounds__(kBlock) p2StencilKernel(LevelDev lv, const T* __restrict__ W, T* dst, const T* src,
+__global__ void __launch_bounds__(kBlock, 2) p2StencilKernel(LevelDev lv, const T* __restrict__ W, T* dst, const T* src,
                                                           const T* __restrict__ rhs, unsigned mask,
                                                           const unsigned char* __restrict__ colour,
                                                           const signed char* __restrict__ classOfColour, int sel,
@@ -1439,11 +1440,11 @@ __global__ void __launch_bounds__(kBlock) p2DivTKernel(LevelDev lvv, LevelDev lv
 //   p2DivTStencilKernel: v_k at an interior velocity node of class pc = sum_e WT_k[e] p at the
 //   pressure nodes (X >> 1, Y >> 1, Z >> 1) + p2s::DivTList<pc>[e]. Grid nCells * (M - 3).
 template <class T>
-__device__ __forceinline__ void p2Acc3(T& s0, T& s1, T& s2, const T* w, int I, const T* u0, const T* u1,
-                                       const T* u2, int o) {
-  s0 += w[I] * __ldg(u0 + o);
-  s1 += w[65 + I] * __ldg(u1 + o);
-  s2 += w[130 + I] * __ldg(u2 + o);
+__device__ __forceinline__ void p2Acc3(T (&s)[6], const T* w, int I, const T* u0, const T* u1, const T* u2, int o) {
+  const int h = I & 1;  // two partial sums per component
+  s[h] += w[I] * __ldg(u0 + o);
+  s[2 + h] += w[65 + I] * __ldg(u1 + o);
+  s[4 + h] += w[130 + I] * __ldg(u2 + o);
 }
 
 template <class T>
@@ -1457,9 +1458,9 @@ template <class T, int... DX, int... DY, int... DZ, int... I>
 __device__ __forceinline__ T p2DivDot(p2s::List<p2s::O<DX, DY, DZ>...>, std::integer_sequence<int, I...>, const T* u0,
                                       const T* u1, const T* u2, const T* w, const int (&pbz)[5], int wv, int X, int Y,
                                       int Z) {
-  T s0 = T(0), s1 = T(0), s2 = T(0);
-  (p2Acc3<T>(s0, s1, s2, w, I, u0, u1, u2, p2RowBase<DY, DZ>(pbz, wv, Y, Z) + X + DX), ...);
-  return s0 + (s1 + s2);
+  T s[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+  (p2Acc3<T>(s, w, I, u0, u1, u2, p2RowBase<DY, DZ>(pbz, wv, Y, Z) + X + DX), ...);
+  return (s[0] + s[1]) + ((s[2] + s[3]) + (s[4] + s[5]));
 }
 
 template <class T, int... DX, int... DY, int... DZ, int... I>
