@@ -577,8 +577,8 @@ def run_ours(args):
     for name, dt in (("fp64", np.float64), ("fp32", np.float32)):
         picks = st.autotune_sor(2, L, dtype=dt, reps=3)
         autotune[name] = {str(lv): {"schedule": c, "ms_single_pass": t0, "ms_colour_passes": t1,
-                                    "ms_single_pass_short_tiles": t2}
-                          for lv, (c, t0, t1, t2) in picks.items()}
+                                    "ms_single_pass_short_tiles": t2, "ms_colour_split": t3}
+                          for lv, (c, t0, t1, t2, t3) in picks.items()}
 
     # --- time to solution: FP64 GMG vs mixed precision (FP32 cycles inside FP64 defect correction)
     solve = None if args.cycle_only else time_to_solution(hg, st, A, L, N_in, Inner)

@@ -209,19 +209,19 @@ class PrimitiveStorage:
 
     def set_sor_schedule(self, schedule):
         """0: single-pass wavefront SOR (level buffers double-buffered), 1: in-place colour passes,
-        2: the single pass with shorter tiles."""
+        2: the single pass with shorter tiles, 3: colour passes on colour-split copies of the cell
+        arrays (converted once per group of sweeps)."""
         call("hg_storage_set_sor_schedule", self._h, int(schedule))
 
     def autotune_sor(self, minLevel, maxLevel, dtype=np.float64, reps=3):
-        """Times the three SOR schedules per level and keeps the fastest; returns
-        {level: (chosen schedule, ms of schedule 0, ms of schedule 1, ms of schedule 2)}."""
+        """Times the four SOR schedules per level (groups of three sweeps) and keeps the fastest;
+        returns {level: (chosen schedule, ms per sweep of schedules 0, 1, 2, 3)}."""
         n = maxLevel - minLevel + 1
-        ms = np.zeros(3 * n)
+        ms = np.zeros(4 * n)
         ch = np.zeros(n, dtype=np.int32)
         prec = {np.dtype(np.float64): 8, np.dtype(np.float32): 4}[np.dtype(dtype)]
         call("hg_storage_autotune_sor", self._h, minLevel, maxLevel, prec, int(reps), dptr(ms), iptr(ch))
-        return {minLevel + i: (int(ch[i]), float(ms[3 * i]), float(ms[3 * i + 1]), float(ms[3 * i + 2]))
-                for i in range(n)}
+        return {minLevel + i: (int(ch[i]),) + tuple(float(ms[4 * i + k]) for k in range(4)) for i in range(n)}
 
     def set_stream(self, stream_ptr):
         call("hg_storage_set_stream", self._h, ctypes.c_void_p(stream_ptr))

@@ -154,8 +154,9 @@ int hg_storage_set_cell_coefficients(hg_storage* h, const double* k, int ncells)
 
 int hg_storage_set_sor_schedule(hg_storage* h, int schedule) {
   HG_TRY
-  hg::argCheck(schedule >= 0 && schedule <= 2,
-               "SOR schedule must be 0 (single pass), 1 (colour passes) or 2 (single pass, short tiles)");
+  hg::argCheck(schedule >= 0 && schedule <= 3,
+               "SOR schedule must be 0 (single pass), 1 (colour passes), 2 (single pass, short tiles) or 3 "
+               "(colour passes in the colour-split order)");
   S(h).sorSchedule = schedule;
   ++S(h).generation;
   HG_CATCH

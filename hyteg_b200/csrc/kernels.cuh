@@ -412,6 +412,109 @@ __global__ void __launch_bounds__(WaveCfg<T, V>::THREADS, WaveCfg<T, V>::MIN_BLO
 }
 
 // ---------------------------------------------------------------------------------------
+// Colour-split order of the closed macro-cells (SOR schedule 3). Every row (y, z) keeps its
+// slots, and inside a row of m points the points are ordered by x mod 4, then by x: sub-row q
+// holds x = q, q + 4, ... and starts at slot q * (m / 4) + min(q, m mod 4) of the row. The
+// points of one colour ((x + 2y + 3z) mod 4) then fill one sub-row of every row, and a colour
+// pass reads and writes whole runs of consecutive slots instead of every fourth one. The SOR
+// converts a level into this order before its sweeps and back after them.
+// ---------------------------------------------------------------------------------------
+__host__ __device__ __forceinline__ int splitSub(int m, int q) { return q * (m >> 2) + (q < (m & 3) ? q : (m & 3)); }
+
+// Position in the colour-split order of point p of a triangle plane with W points per edge
+// (p = rowStart(W, y) + x). The row comes from the root of rowStart(W, y) = y (2W + 1 - y) / 2
+// and is corrected by whole rows.
+__device__ __forceinline__ int splitOfPlanePoint(int W, int p) {
+  const float b = float(2 * W + 1);
+  int y = int((b - sqrtf(fmaxf(b * b - 8.0f * float(p), 0.0f))) * 0.5f);
+  y = max(0, min(y, W - 1));
+  while (y > 0 && rowStart(W, y) > p) --y;
+  while (y < W - 1 && rowStart(W, y + 1) <= p) ++y;
+  const int r0 = rowStart(W, y), x = p - r0;
+  return r0 + splitSub(W - y, x & 3) + (x >> 2);
+}
+
+// dst = src with the cell arrays converted into (TO_SPLIT) or out of the colour-split order;
+// one block per (macro-cell, plane), the threads walk the plane's points (kSplitUnroll each per
+// round, loads before stores).
+constexpr int kSplitUnroll = 4;
+template <class T, bool TO_SPLIT>
+__global__ void __launch_bounds__(kBlock) cellSplitKernel(LevelDev lv, T* __restrict__ dst, const T* __restrict__ src) {
+  const int nPl = lv.N + 1;
+  const int c = blockIdx.x / nPl, z = blockIdx.x - (blockIdx.x / nPl) * nPl;
+  const int W = lv.w - z;  // points on an edge of plane z
+  const int64_t base = lv.cellOff[c] + (tetSize(lv.w) - tetSize(W));
+  const int n = triSize(W);
+  for (int p0 = threadIdx.x; p0 < n; p0 += kBlock * kSplitUnroll) {
+    T v[kSplitUnroll];
+    int to[kSplitUnroll];
+#pragma unroll
+    for (int k = 0; k < kSplitUnroll; ++k) {
+      const int p = p0 + k * kBlock;
+      if (p < n) {
+        const int s = splitOfPlanePoint(W, p);
+        v[k] = TO_SPLIT ? src[base + p] : src[base + s];
+        to[k] = TO_SPLIT ? s : p;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kSplitUnroll; ++k)
+      if (p0 + k * kBlock < n) dst[base + to[k]] = v[k];
+  }
+}
+
+// One colour pass of the multicolour SOR on cell interiors held in the colour-split order
+// (the same update as cellSorKernel). The points of the colour in row (y, z) are x = q + 4j, and
+// each of the 14 neighbours of such a point lies in sub-row (q + dx) mod 4 of its row at position
+// j + floor((q + dx) / 4): all 15 slots a point touches are a per-row constant plus j. The rows
+// of one colour (the same in every macro-cell of a level) are listed once with these 15 constants
+// (SplitRow), and every point of the colour once as (row << 10 | j), so one thread updates one
+// point and consecutive threads read runs of consecutive slots, whatever the row lengths. A
+// colour never neighbours itself: the neighbours are constant during the pass and are read
+// through the read-only path.
+struct SplitRow {
+  int i[16];  // slots (cell-relative, at j = 0) of C E W N S NW SE TC TW TS TSE BC BE BN BNW; pad
+};
+constexpr int kSplitJBits = 10;
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) cellSorSplitKernel(LevelDev lv, const T* __restrict__ cellW, T* u,
+                                                             const T* __restrict__ rhs, unsigned mask,
+                                                             const SplitRow* __restrict__ rows,
+                                                             const unsigned* __restrict__ points, int nPoints,
+                                                             int blocksPerCell, T omega) {
+  const int c = blockIdx.x / blocksPerCell;
+  if (!(lv.cellType[c] & mask)) return;
+  __shared__ T wt[16];
+  if (threadIdx.x < 15) wt[threadIdx.x] = cellW[16 * c + threadIdx.x];
+  __syncthreads();
+  const int t = (blockIdx.x - c * blocksPerCell) * kBlock + threadIdx.x;
+  if (t >= nPoints) return;
+  const unsigned e = __ldg(points + t);
+  const int4* rp = reinterpret_cast<const int4*>(rows + (e >> kSplitJBits));
+  const int4 r0 = __ldg(rp), r1 = __ldg(rp + 1), r2 = __ldg(rp + 2), r3 = __ldg(rp + 3);
+  const int64_t base = lv.cellOff[c] + (int64_t)(e & ((1u << kSplitJBits) - 1));
+  T* uc = u + base;
+  // sum_{k >= 1} w_k u(x + d_k) in the order E W N S NW SE TC TW TS TSE BC BE BN BNW
+  T s = wt[1] * __ldg(uc + r0.y);
+  s += wt[2] * __ldg(uc + r0.z);
+  s += wt[3] * __ldg(uc + r0.w);
+  s += wt[4] * __ldg(uc + r1.x);
+  s += wt[5] * __ldg(uc + r1.y);
+  s += wt[6] * __ldg(uc + r1.z);
+  s += wt[7] * __ldg(uc + r1.w);
+  s += wt[8] * __ldg(uc + r2.x);
+  s += wt[9] * __ldg(uc + r2.y);
+  s += wt[10] * __ldg(uc + r2.z);
+  s += wt[11] * __ldg(uc + r2.w);
+  s += wt[12] * __ldg(uc + r3.x);
+  s += wt[13] * __ldg(uc + r3.y);
+  s += wt[14] * __ldg(uc + r3.z);
+  const T om1 = T(1) - omega, dinv = omega / wt[0];
+  uc[r0.x] = om1 * uc[r0.x] + (__ldg(rhs + base + r0.x) - s) * dinv;
+}
+
+// ---------------------------------------------------------------------------------------
 // Register-blocked 2.5-D cell sweep (the kernel behind apply and residual on cell interiors).
 // A warp owns a strip of 30 x-columns (lanes 1..30; lanes 0 and 31 only carry the x-halo) by
 // kStripR rows and marches up z through a range of planes. Each lane keeps the rows
@@ -1763,6 +1866,19 @@ __global__ void commGatherKernel(T* buf, const uint2* __restrict__ table, int64_
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const uint2 t = table[i];
     buf[t.x] = buf[t.y];
+  }
+}
+
+// The same refresh while the cell arrays of the level live in a second buffer in the
+// colour-split order: slots below cellEnd (the table holds their split positions) are in
+// cells, the others in buf.
+template <class T>
+__global__ void commGatherSplitKernel(T* buf, T* cells, const uint2* __restrict__ table, int64_t n, int64_t cellEnd) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint2 t = table[i];
+    const T v = t.y < cellEnd ? cells[t.y] : buf[t.y];
+    if (t.x < cellEnd) cells[t.x] = v;
+    else buf[t.x] = v;
   }
 }
 

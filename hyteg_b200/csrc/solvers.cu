@@ -181,6 +181,9 @@ std::vector<uintptr_t> Gmg::signature(int x, int b, int L) {
     sig.push_back((uintptr_t)s.data(tmp, l));
     auto it = s.spare.find({l, prec});
     sig.push_back(it != s.spare.end() && it->second ? (uintptr_t)it->second->p : 0);
+    auto is = s.splitRhs.find({l, prec});
+    sig.push_back(is != s.splitRhs.end() && is->second ? (uintptr_t)is->second->p : 0);
+    sig.push_back((uintptr_t)s.levels[l].commSplit);
     sig.push_back((uintptr_t)o.d[l - o.minL].cellW);
   }
   for (int id : {cp, cz, cap, cr, cx64, cb64})
@@ -203,7 +206,7 @@ void Gmg::solveRecursively(int x, int b, int L) {
     coarseSolve(x, b, L);
     return;
   }
-  for (int i = 0; i < pre; ++i) s.smoothSor(op, x, b, omega, L, flag, false);
+  s.smoothSorSweeps(op, x, b, omega, L, flag, pre, false, false);
   s.residual(op, x, b, tmp, L, flag);
   s.restrictFn(tmp, L, flag);
   const double one = 1.0;
@@ -212,7 +215,8 @@ void Gmg::solveRecursively(int x, int b, int L) {
   solveRecursively(x, b, L - 1);
   if (cycle == 1) solveRecursively(x, b, L - 1);
   s.prolongate(x, L - 1, flag, true);
-  for (int i = 0; i < post; ++i) s.smoothSor(op, x, b, omega, L, flag, false);
+  // b is unchanged on this level since the pre-smoothing, which left its colour-split copy
+  s.smoothSorSweeps(op, x, b, omega, L, flag, post, false, pre > 0);
 }
 
 int Gmg::solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap) {

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -332,6 +333,122 @@ void Storage::communicate(int id, int L, int groupMask) {
   cudaCheck(cudaGetLastError(), "communicate");
 }
 
+template <class T>
+void Storage::communicateSplit(T* buf, T* cells, int L, int groupMask) {
+  buildSplit(L);
+  const LevelData& ld = levels[L];
+  const uint2* table = ld.commSplit;
+  int k = 0;
+  while (k < G_COUNT) {
+    if (!(groupMask & (1 << k))) {
+      ++k;
+      continue;
+    }
+    const int64_t begin = ld.commBegin[k];
+    int64_t n = 0;
+    while (k < G_COUNT && (groupMask & (1 << k))) n += ld.commCount[k++];
+    if (n == 0) continue;
+    dev::commGatherSplitKernel<T><<<grid1d(n), 256, 0, stream>>>(buf, cells, table + begin, n, ld.nonCellBegin);
+    ++launches;
+  }
+  cudaCheck(cudaGetLastError(), "communicate (split)");
+}
+
+// Schedule-3 tables of level L: the halo table with every slot of a cell array replaced by its
+// position in the colour-split order (a permutation inside each row of the cell's array), and
+// per colour the interior rows (their 15 slots at j = 0) and points (row << 10 | j) that
+// cellSorSplitKernel walks; the same for every macro-cell of the level.
+void Storage::buildSplit(int L) {
+  LevelData& ld = levels[L];
+  if (ld.commSplit) return;
+  const LevelLayout& lay = *ld.lay;
+  const int64_t w = lay.w, N = w - 1;
+  argCheck(N <= 4096, "colour-split SOR: level too large");
+  auto tet = [](int64_t a) { return a * (a + 1) * (a + 2) / 6; };
+  auto tri = [](int64_t a) { return a * (a + 1) / 2; };
+  auto rowStart = [&](int64_t z, int64_t y) {
+    const int64_t W = w - z;
+    return tet(w) - tet(W) + y * (W + 1) - y * (y + 1) / 2;
+  };
+  std::vector<int> perm((size_t)tet(w));
+  for (int64_t z = 0; z < w; ++z)
+    for (int64_t y = 0; y < w - z; ++y) {
+      const int64_t r0 = rowStart(z, y);
+      const int m = (int)(w - z - y);
+      for (int x = 0; x < m; ++x) perm[(size_t)(r0 + x)] = (int)(r0 + dev::splitSub(m, x & 3) + (x >> 2));
+    }
+  std::vector<std::pair<int64_t, int64_t>> cells;  // (offset, size), ascending
+  for (size_t c = 0; c < lay.off[KC].size(); ++c) cells.push_back({lay.off[KC][c], lay.size[KC][c]});
+  std::sort(cells.begin(), cells.end());
+  auto map = [&](int64_t slot) -> unsigned {
+    if (slot < ld.nonCellBegin && !cells.empty()) {
+      auto it = std::upper_bound(cells.begin(), cells.end(), std::make_pair(slot, INT64_MAX));
+      if (it != cells.begin()) {
+        --it;
+        const int64_t local = slot - it->first;
+        if (local < it->second && local < (int64_t)perm.size()) return (unsigned)(it->first + perm[(size_t)local]);
+      }
+    }
+    return (unsigned)slot;
+  };
+  std::vector<uint2> comm;
+  for (int k = 0; k < G_COUNT; ++k)
+    for (size_t i = 0; i < lay.commDst[k].size(); ++i)
+      comm.push_back(make_uint2(map(lay.commDst[k][i]), map(lay.commSrc[k][i])));
+  const uint2* commSplit = comm.empty() ? ld.comm : (const uint2*)upload(ld.keep, comm, stream);
+  // rows and points per colour (interior: x, y, z >= 1, x + y + z <= N - 1)
+  for (int col = 0; col < 4; ++col) {
+    std::vector<dev::SplitRow> rows;
+    std::vector<unsigned> points;
+    for (int64_t z = 1; z <= N - 3; ++z) {
+      const int64_t W = w - z;
+      for (int64_t y = 1; y <= W - 3; ++y) {
+        const int m = (int)(W - y);
+        const int q = (int)((((col - 2 * y - 3 * z) % 4) + 4) % 4);
+        const int j0 = q == 0 ? 1 : 0, jEnd = m - 2 - q >= 0 ? (m - 2 - q) / 4 : -1;
+        if (jEnd < j0) continue;
+        const int qE = (q + 1) & 3, qW = (q + 3) & 3, jE = q == 3 ? 1 : 0, jW = q == 0 ? -1 : 0;
+        const int64_t r0 = rowStart(z, y), rN = r0 + m, rS = r0 - (m + 1);
+        const int64_t rT = r0 + tri(W) - y, rTS = rT - m, rB = r0 - tri(W + 1) + y, rBN = rB + (m + 1);
+        auto sub = [](int mm, int qq) { return (int64_t)dev::splitSub(mm, qq); };
+        dev::SplitRow r;
+        const int64_t v[16] = {r0 + sub(m, q),          r0 + sub(m, qE) + jE,      r0 + sub(m, qW) + jW,
+                               rN + sub(m - 1, q),      rS + sub(m + 1, q),        rN + sub(m - 1, qW) + jW,
+                               rS + sub(m + 1, qE) + jE, rT + sub(m - 1, q),       rT + sub(m - 1, qW) + jW,
+                               rTS + sub(m, q),         rTS + sub(m, qE) + jE,     rB + sub(m + 1, q),
+                               rB + sub(m + 1, qE) + jE, rBN + sub(m, q),          rBN + sub(m, qW) + jW,
+                               0};
+        for (int k = 0; k < 16; ++k) r.i[k] = (int)v[k];
+        argCheck(rows.size() < (size_t(1) << (32 - dev::kSplitJBits)), "colour-split SOR: too many rows");
+        const unsigned id = (unsigned)rows.size();
+        rows.push_back(r);
+        for (int j = j0; j <= jEnd; ++j) points.push_back(id << dev::kSplitJBits | (unsigned)j);
+      }
+    }
+    ld.splitRows[col] = (const dev::SplitRow*)upload(ld.keep, rows, stream);
+    ld.splitPoints[col] = (const unsigned*)upload(ld.keep, points, stream);
+    ld.nSplitPoints[col] = (int)points.size();
+  }
+  cudaCheck(cudaStreamSynchronize(stream), "colour-split tables");  // the host vectors go out of scope
+  ld.commSplit = commSplit;
+}
+
+DevBuf& Storage::spareBuf(std::map<std::pair<int, int>, std::unique_ptr<DevBuf>>& pool, int L, int prec) {
+  std::unique_ptr<DevBuf>& sp = pool[{L, prec}];
+  const size_t bytes = (size_t)levels[L].lay->total * prec;
+  if (!sp || sp->bytes != bytes) {
+    sp.reset(new DevBuf());
+    sp->alloc(bytes);
+    cudaCheck(cudaMemsetAsync(sp->p, 0, sp->bytes, stream), "spare memset");  // alignment padding stays zero
+  }
+  return *sp;
+}
+
+int Storage::sorScheduleFor(int L, int prec) const {
+  const int tuned = 2 * L + (prec == 4 ? 1 : 0);
+  return (int)sorScheduleLevel.size() > tuned && sorScheduleLevel[tuned] >= 0 ? sorScheduleLevel[tuned] : sorSchedule;
+}
+
 void Storage::lincomb(int dst, int L, unsigned mask, int n, const double* a, const int* srcs, bool add,
                       double constant) {
   argCheck(n >= 0 && n <= 3, "at most three source functions");
@@ -447,6 +564,8 @@ int64_t Storage::deviceBytes() const {
   for (auto& o : ops)
     for (auto& k : o.second->keep) b += (int64_t)k->bytes;
   for (auto& sp : spare)
+    if (sp.second) b += (int64_t)sp.second->bytes;
+  for (auto& sp : splitRhs)
     if (sp.second) b += (int64_t)sp.second->bytes;
   return b;
 }
@@ -1401,17 +1520,18 @@ void Storage::autotuneSor(int minL, int maxL, int prec, int reps, double* ms) {
     fillRandom(b, L, HG_ALL, 2, -1.0, 1.0);
     double best = 0;
     int pick = 0;
-    for (int sch = 0; sch < 3; ++sch) {
+    for (int sch = 0; sch < 4; ++sch) {
       sorScheduleLevel[2 * L + pi] = sch;
-      smoothSor(op, x, b, 1.0, L, HG_INNER | HG_NEUMANN, false);  // warm-up (allocates the spare)
+      // warm-up (allocates the spare buffers and tables), then groups of three sweeps
+      smoothSorSweeps(op, x, b, 1.0, L, HG_INNER | HG_NEUMANN, 3, false, false);
       cudaCheck(cudaEventRecord(e0, stream), "event");
-      for (int r = 0; r < reps; ++r) smoothSor(op, x, b, 1.0, L, HG_INNER | HG_NEUMANN, false);
+      for (int r = 0; r < reps; ++r) smoothSorSweeps(op, x, b, 1.0, L, HG_INNER | HG_NEUMANN, 3, false, false);
       cudaCheck(cudaEventRecord(e1, stream), "event");
       cudaCheck(cudaEventSynchronize(e1), "event");
       float t = 0;
       cudaCheck(cudaEventElapsedTime(&t, e0, e1), "event");
-      const double per = t / reps;
-      if (ms) ms[3 * (L - minL) + sch] = per;
+      const double per = t / (3.0 * reps);
+      if (ms) ms[4 * (L - minL) + sch] = per;
       if (sch == 0 || per < best) {
         best = per;
         pick = sch;
@@ -1536,13 +1656,15 @@ void Storage::residual(int opId, int x, int b, int r, int L, unsigned mask) {
 
 template <class T>
 void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned mask, T omega, bool backwards,
-                   int kinds, bool refresh) {
+                   int kinds, bool refresh, T* cellU, const T* cellF) {
   const LevelData& ld = levels[L];
   const dev::StencilDev<T>& st = stencilOf<T>(o, L);
   const dev::LevelDev& lv = ld.lv;
   const int nVertBlocks = lv.nLowBlocks - lv.nLowEdgeBlocks;
   auto comm = [&](int groups) {
-    if (refresh) communicate(dstId, L, groups);
+    if (!refresh) return;
+    if (cellU) communicateSplit<T>(u, cellU, L, groups);
+    else communicate(dstId, L, groups);
   };
   auto verts = [&]() {
     if (nVertBlocks && (kinds & (1 << KV))) {
@@ -1566,20 +1688,25 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
   // budget), so the re-reads of the later colours hit L2
   auto cellPhase = [&](bool rev) {
     if (!lv.nCellBlocks || !(kinds & (1 << KC))) return;
-    const int tuned = 2 * L + (sizeof(T) == 4 ? 1 : 0);
-    const int schedule = (int)sorScheduleLevel.size() > tuned && sorScheduleLevel[tuned] >= 0 ? sorScheduleLevel[tuned]
-                                                                                                  : sorSchedule;
+    if (cellU) {  // colour-split copy: four in-place passes, one launch each over all cells
+      for (int k = 0; k < 4; ++k) {
+        const int c = rev ? 3 - k : k, n = ld.nSplitPoints[c];
+        if (n == 0) continue;
+        const int bpc = (n + dev::kBlock - 1) / dev::kBlock;
+        dev::cellSorSplitKernel<T><<<(unsigned)(bpc * lv.nCells), dev::kBlock, 0, stream>>>(
+            lv, st.cellW, cellU, cellF, mask, ld.splitRows[c], ld.splitPoints[c], n, bpc, omega);
+        ++launches;
+      }
+      return;
+    }
+    const int schedule = sorScheduleFor(L, (int)sizeof(T));
     const int pi = sizeof(T) == 4 ? 1 : 0, gv = schedule == 2 ? 1 : 0;
-    if (schedule != 1 && ld.nWaveTiles[pi][gv]) {
+    if ((schedule == 0 || schedule == 2) && ld.nWaveTiles[pi][gv]) {
       // one pass into the spare buffer of this level, which then becomes the function's buffer
       Function& fd = fn(dstId);
       std::unique_ptr<DevBuf>& cur = fd.levels[L - fd.minL];
+      spareBuf(spare, L, (int)sizeof(T));
       std::unique_ptr<DevBuf>& sp = spare[{L, (int)sizeof(T)}];
-      if (!sp || sp->bytes != cur->bytes) {
-        sp.reset(new DevBuf());
-        sp->alloc(cur->bytes);
-        cudaCheck(cudaMemsetAsync(sp->p, 0, sp->bytes, stream), "spare memset");  // alignment padding stays zero
-      }
       T* out = (T*)sp->p;
       if (gv == 0)
         dev::cellSorWaveKernel<T, 0><<<ld.nWaveTiles[pi][0], dev::WaveGeom<T, 0>::THREADS,
@@ -1647,11 +1774,52 @@ void Storage::smoothSor(int opId, int dst, int rhs, double omega, int L, unsigne
   argCheck(fd.prec == fn(rhs).prec, "smooth_sor: precision mismatch");
   for (auto& c : o.host[L - o.minL].cell)
     if (levels[L].lv.nCellBlocks && c[0] == 0.0) throw Error(HG_ERR_NUMERIC, "zero diagonal in cell stencil");
+  if (kinds == 15 && refresh && sorScheduleFor(L, fd.prec) == 3 && levels[L].lv.nCellBlocks) {
+    smoothSorSweeps(opId, dst, rhs, omega, L, mask, 1, backwards, false);
+    return;
+  }
   if (fd.prec == 8)
     sorT<double>(o, dst, L, (double*)data(dst, L), (const double*)data(rhs, L), mask, omega, backwards, kinds, refresh);
   else
     sorT<float>(o, dst, L, (float*)data(dst, L), (const float*)data(rhs, L), mask, (float)omega, backwards, kinds,
                 refresh);
+}
+
+void Storage::smoothSorSweeps(int opId, int dst, int rhs, double omega, int L, unsigned mask, int sweeps,
+                              bool backwards, bool rhsReady) {
+  Function& fd = fn(dst);
+  if (sorScheduleFor(L, fd.prec) != 3 || !levels[L].lv.nCellBlocks || sweeps <= 0) {
+    for (int i = 0; i < sweeps; ++i) smoothSor(opId, dst, rhs, omega, L, mask, backwards);
+    return;
+  }
+  Operator& o = op(opId);
+  argCheck(L >= o.minL && L <= o.maxL, "level outside the operator's level range");
+  argCheck(dst != rhs, "smooth_sor: dst and rhs must differ");
+  argCheck(fd.prec == fn(rhs).prec, "smooth_sor: precision mismatch");
+  for (auto& c : o.host[L - o.minL].cell)
+    if (c[0] == 0.0) throw Error(HG_ERR_NUMERIC, "zero diagonal in cell stencil");
+  const LevelData& ld = levels[L];
+  const unsigned nb = (unsigned)(ld.lv.nCells * (ld.lv.N + 1));
+  auto run = [&](auto zero) {
+    using T = decltype(zero);
+    T* u = (T*)data(dst, L);
+    const T* b = (const T*)data(rhs, L);
+    buildSplit(L);
+    T* cu = (T*)spareBuf(spare, L, (int)sizeof(T)).p;
+    T* cf = (T*)spareBuf(splitRhs, L, (int)sizeof(T)).p;
+    dev::cellSplitKernel<T, true><<<nb, dev::kBlock, 0, stream>>>(ld.lv, cu, u);
+    ++launches;
+    if (!rhsReady) {
+      dev::cellSplitKernel<T, true><<<nb, dev::kBlock, 0, stream>>>(ld.lv, cf, b);
+      ++launches;
+    }
+    for (int i = 0; i < sweeps; ++i) sorT<T>(o, dst, L, u, b, mask, (T)omega, backwards, 15, true, cu, cf);
+    dev::cellSplitKernel<T, false><<<nb, dev::kBlock, 0, stream>>>(ld.lv, u, cu);
+    ++launches;
+    cudaCheck(cudaGetLastError(), "sor (colour-split)");
+  };
+  if (fd.prec == 8) run(0.0);
+  else run(0.0f);
 }
 
 // The fine-level face/edge/vertex stencil structure drives the restriction; it is taken from

@@ -45,6 +45,12 @@ struct LevelData {
   dev::WaveTile* waveTiles[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   int nWaveTiles[2][2] = {{0, 0}, {0, 0}};
   int64_t nonCellBegin = 0;  // first slot after the cell arrays (faces, edges, vertices follow)
+  // SOR schedule 3 (built on first use): the halo table with every cell slot at its colour-split
+  // position (same groups as comm), and per colour the rows and points of the cell interiors
+  const uint2* commSplit = nullptr;
+  const dev::SplitRow* splitRows[4] = {nullptr, nullptr, nullptr, nullptr};
+  const unsigned* splitPoints[4] = {nullptr, nullptr, nullptr, nullptr};
+  int nSplitPoints[4] = {0, 0, 0, 0};
   std::vector<unsigned char> hostCellType, hostFaceType, hostLowType;
   std::vector<std::unique_ptr<DevBuf>> keep;
 };
@@ -128,14 +134,20 @@ struct Storage {
   unsigned long long launches = 0;  // kernels launched by this storage
   // Cell-phase schedule of the multicolour SOR: 0 = one wavefront pass that writes a second
   // buffer which then replaces the level buffer, 1 = four in-place colour passes, 2 = the
-  // wavefront pass with the shorter tile geometry.
+  // wavefront pass with the shorter tile geometry, 3 = four colour passes on a copy of the
+  // cell arrays in the colour-split order (converted once per group of sweeps).
   int sorSchedule = 0;
   std::vector<int> sorScheduleLevel;  // [2 L + (FP32 ? 1 : 0)]: schedule chosen by autotuneSor (-1: sorSchedule)
-  // Times the three schedules of one SOR sweep on levels [minL, maxL] in the given precision and
-  // keeps the fastest per level; ms[3 * (L - minL) + s] receives the measured times (nullable).
+  int sorScheduleFor(int L, int prec) const;
+  // Times the four schedules of the SOR on levels [minL, maxL] in the given precision, in groups
+  // of three sweeps (the smoothing of a V(3,3) cycle), and keeps the fastest per level;
+  // ms[4 * (L - minL) + s] receives the time per sweep (nullable).
   void autotuneSor(int minL, int maxL, int prec, int reps, double* ms);
   unsigned long long generation = 0;  // bumped when level tables or schedules change (captured graphs)
   std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> spare;  // (level, precision) -> buffer
+  std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> splitRhs;  // (level, precision) -> split rhs copy
+  DevBuf& spareBuf(std::map<std::pair<int, int>, std::unique_ptr<DevBuf>>& pool, int L, int prec);
+  void buildSplit(int L);  // the schedule-3 tables of level L (no-op once built)
   dev::Geometry geom{};              // macro-vertex coordinates and primitive vertex lists (device)
   std::vector<std::unique_ptr<DevBuf>> geomKeep;
 
@@ -197,15 +209,23 @@ struct Storage {
   void residual(int op, int x, int b, int r, int L, unsigned mask);
   void smoothSor(int op, int dst, int rhs, double omega, int L, unsigned mask, bool backwards, int kinds = 15,
                  bool refresh = true);
+  // `sweeps` SOR sweeps in a row. Under schedule 3 the cell arrays of dst (and of rhs, unless
+  // rhsReady: rhs is unchanged since the last group of sweeps on this level and precision) are
+  // converted into the colour-split order once, and dst is converted back after the last sweep.
+  void smoothSorSweeps(int op, int dst, int rhs, double omega, int L, unsigned mask, int sweeps, bool backwards,
+                       bool rhsReady);
   void restrictFn(int id, int Lf, unsigned mask);
   void prolongate(int id, int Lc, unsigned mask, bool add);
   const Operator& structure();
 
   template <class T, int MODE>
   void stencilOp(Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask, int kinds = 15);
+  // cellU / cellF (nullable): the level's cell arrays of u and rhs in the colour-split order
   template <class T>
   void sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned mask, T omega, bool backwards, int kinds,
-            bool refresh);
+            bool refresh, T* cellU = nullptr, const T* cellF = nullptr);
+  template <class T>
+  void communicateSplit(T* buf, T* cells, int L, int groupMask);
   template <class T>
   void restrictT(int id, int Lf, unsigned mask);
   template <class T>

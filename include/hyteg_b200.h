@@ -98,13 +98,17 @@ int hg_storage_set_cell_coefficients(hg_storage* s, const double* k, int ncells)
 /* Cell-phase schedule of the multicolour SOR: 0 (default) = one pass per sweep (z-wavefront over
  * the four colours, written to a second buffer of the level that then replaces the smoothed
  * function's buffer), 1 = four in-place colour passes, 2 = the single pass with shorter tiles
- * (32 x 12 instead of 32 x 24 / 28). All give the same multicolour sweep. */
+ * (32 x 12 instead of 32 x 24 / 28), 3 = four colour passes on copies of the cell arrays in the
+ * colour-split order (each row ordered by x mod 4; the copies are made once per group of sweeps
+ * of a multigrid smoothing step and the result is copied back). All give the same multicolour
+ * sweep. */
 int hg_storage_set_sor_schedule(hg_storage* s, int schedule);
-/* Autotuner (no counterpart in the reference): times one multicolour SOR sweep under the three
- * schedules on every level in [min_level, max_level] (precision 8 or 4, `reps` timed sweeps after
- * one warm-up, CUDA events on the storage's stream) and keeps the fastest schedule per level and
- * precision, overriding hg_storage_set_sor_schedule there. ms (nullable): 3 * (levels) times in
- * ms, schedules 0, 1, 2 per level; chosen (nullable): the schedule kept per level. */
+/* Autotuner (no counterpart in the reference): times the multicolour SOR under the four
+ * schedules on every level in [min_level, max_level] (precision 8 or 4; `reps` timed groups of
+ * three sweeps, the smoothing step of a V(3,3) cycle, after one warm-up group; CUDA events on the
+ * storage's stream) and keeps the fastest schedule per level and precision, overriding
+ * hg_storage_set_sor_schedule there. ms (nullable): 4 * (levels) times per sweep in ms, schedules
+ * 0, 1, 2, 3 per level; chosen (nullable): the schedule kept per level. */
 int hg_storage_autotune_sor(hg_storage* s, int min_level, int max_level, int precision, int reps, double* ms,
                             int* chosen);
 /* Topology export: for kind HG_VERTEX ids[0..2]=unused, coords[3]; HG_EDGE ids[2]; HG_FACE ids[3];

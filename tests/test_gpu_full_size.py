@@ -4,7 +4,8 @@
 - The constant stencils annihilate constants and linear functions at inner DoFs (the property
   the reference's P1LaplaceOperator3DTest checks).
 - An exact solution is a fixed point of the SOR sweep: with b = A x, one sweep (single-pass
-  wavefront and four colour passes, FP64 and FP32) leaves x unchanged to rounding.
+  wavefront, four colour passes, and colour passes on colour-split copies; FP64 and FP32) leaves
+  x unchanged to rounding.
 - Restriction is the transpose of prolongation on inner DoFs: <R r, c> = <r, P c>.
 - apply is linear: A (2 x + 3 y) = 2 A x + 3 A y.
 
@@ -46,7 +47,7 @@ def test_stencils_annihilate_constants_and_linears(l8):
         assert inner_max(y, L) < 1e-12 * scale
 
 
-@pytest.mark.parametrize("schedule", [0, 1])
+@pytest.mark.parametrize("schedule", [0, 1, 3])
 @pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 1e-5)])
 def test_exact_solution_is_a_fixed_point_of_sor(l8, schedule, dtype, tol):
     st, A = l8

@@ -82,7 +82,7 @@ def test_autotuned_schedules_give_the_same_cycles(gpu, dtype):
         if tune:
             picks = st.autotune_sor(2, L, dtype=dtype, reps=2)
             assert set(picks) == set(range(2, L + 1))
-            assert all(c in (0, 1, 2) and t0 > 0 and t1 > 0 and t2 > 0 for c, t0, t1, t2 in picks.values())
+            assert all(c in (0, 1, 2, 3) and min(ts) > 0 for c, *ts in picks.values())
         x, b = hg.P1Function("x", st, 0, L, dtype=dtype), hg.P1Function("b", st, 0, L, dtype=dtype)
         b.fill_random(8, L, hg.Inner)
         gmg = hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 100, 1e-16),
