@@ -43,6 +43,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--level", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--sor-schedule", type=int, default=None, choices=[0, 1, 2, 3],
+                   help="force one SOR cell-phase schedule on every level instead of autotuning (profiling runs)")
     p.add_argument("--cycle-only", action="store_true",
                    help="only the kernels, autotuner and timed cycles (profiling runs); implies no serving")
     p.add_argument("--stokes-level", type=int, default=6,
@@ -574,7 +576,12 @@ def run_ours(args):
 
     # --- autotuner: the faster SOR schedule per level and precision, used from here on
     autotune = {}
+    if args.sor_schedule is not None:
+        st.set_sor_schedule(args.sor_schedule)
+        autotune = {"forced_schedule": args.sor_schedule}
     for name, dt in (("fp64", np.float64), ("fp32", np.float32)):
+        if args.sor_schedule is not None:
+            break
         picks = st.autotune_sor(2, L, dtype=dt, reps=3)
         autotune[name] = {str(lv): {"schedule": c, "ms_single_pass": t0, "ms_colour_passes": t1,
                                     "ms_single_pass_short_tiles": t2, "ms_colour_split": t3}
