@@ -16,6 +16,7 @@ behaviour) and forward to the C-ABI of libhyteg_b200.so (include/hyteg_b200.h):
 Every computation runs on the GPU; importing the package without the built library raises.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -62,6 +63,24 @@ class HostMesh:
         t = np.ascontiguousarray(tets, dtype=np.int32)
         call("hg_mesh_create_tets", len(c), dptr(c), len(t), iptr(t), max_level, ctypes.byref(h))
         return cls(h, max_level)
+
+    @classmethod
+    def cubed_domain(cls, cubes, cube_type, max_level):
+        """MeshInfo::meshCubedDomain(cubeCoordinates, cubeType) (MeshGenCubedDomain.cpp:115-383)."""
+        h = ctypes.c_void_p()
+        c = np.ascontiguousarray(cubes, dtype=np.int32).reshape(-1, 3)
+        call("hg_mesh_create_cubed_domain", len(c), iptr(c), int(cube_type), max_level, ctypes.byref(h))
+        return cls(h, max_level)
+
+    @classmethod
+    def from_gmsh(cls, path, max_level, flags_from_file=False):
+        """MeshInfo::fromGmshFile (MeshGenFromGmshFile.cpp:31-206), Gmsh 2.2 ASCII."""
+        h = ctypes.c_void_p()
+        call("hg_mesh_create_gmsh", os.fsencode(path), max_level, 1 if flags_from_file else 0, ctypes.byref(h))
+        return cls(h, max_level)
+
+    def write_gmsh(self, path):
+        call("hg_mesh_write_gmsh", self._h, os.fsencode(path))
 
     def __del__(self):
         try:
@@ -168,6 +187,26 @@ class PrimitiveStorage:
         call("hg_storage_create_tets", len(c), dptr(c), len(t), iptr(t), max_level, ctypes.byref(h))
         return cls(h, max_level, ("tets", (c, t)))
 
+    @classmethod
+    def cubed_domain(cls, cubes, cube_type, max_level):
+        """MeshInfo::meshCubedDomain + SetupPrimitiveStorage + setMeshBoundaryFlagsOnBoundary(1, 0, true)."""
+        h = ctypes.c_void_p()
+        c = np.ascontiguousarray(cubes, dtype=np.int32).reshape(-1, 3)
+        call("hg_storage_create_cubed_domain", len(c), iptr(c), int(cube_type), max_level, ctypes.byref(h))
+        return cls(h, max_level, ("cubed", (c, int(cube_type))))
+
+    @classmethod
+    def from_gmsh(cls, path, max_level, flags_from_file=False):
+        """MeshInfo::fromGmshFile + SetupPrimitiveStorage; boundary flags from the geometry (as
+        setMeshBoundaryFlagsOnBoundary(1, 0, true)) unless flags_from_file."""
+        h = ctypes.c_void_p()
+        call("hg_storage_create_gmsh", os.fsencode(path), max_level, 1 if flags_from_file else 0, ctypes.byref(h))
+        return cls(h, max_level, ("gmsh", (os.fspath(path), bool(flags_from_file))))
+
+    def write_gmsh(self, path):
+        """The macro-mesh as a Gmsh 2.2 file; from_gmsh(path, flags_from_file=True) restores it."""
+        call("hg_storage_write_gmsh", self._h, os.fsencode(path))
+
     def close(self):
         if getattr(self, "_h", None):
             _capi.lib.hg_storage_destroy(self._h)
@@ -189,6 +228,10 @@ class PrimitiveStorage:
             kind, a = self._mesh_args
             if kind == "cuboid":
                 self._host = HostMesh.cuboid(a[0], a[1], a[2], a[3], a[4], self.max_level)
+            elif kind == "cubed":
+                self._host = HostMesh.cubed_domain(a[0], a[1], self.max_level)
+            elif kind == "gmsh":
+                self._host = HostMesh.from_gmsh(a[0], self.max_level, a[1])
             else:
                 self._host = HostMesh.from_tets(a[0], a[1], self.max_level)
             if getattr(self, "_k", None) is not None:

@@ -20,6 +20,7 @@ c_uint = ctypes.c_uint
 c_double = ctypes.c_double
 c_int64 = ctypes.c_int64
 c_void_p = ctypes.c_void_p
+c_char_p = ctypes.c_char_p
 P = ctypes.POINTER
 
 HG_OK, HG_ERR_ARG, HG_ERR_CUDA, HG_ERR_OOM, HG_ERR_STATE, HG_ERR_NUMERIC, HG_ERR_INTERNAL = range(7)
@@ -36,6 +37,9 @@ _SIGS = {
     "hg_device_count": (c_int, []),
     "hg_storage_create_cuboid": (c_int, [P(c_double), P(c_double), c_int, c_int, c_int, c_int, P(c_void_p)]),
     "hg_storage_create_tets": (c_int, [c_int, P(c_double), c_int, P(c_int), c_int, P(c_void_p)]),
+    "hg_storage_create_cubed_domain": (c_int, [c_int, P(c_int), c_int, c_int, P(c_void_p)]),
+    "hg_storage_create_gmsh": (c_int, [c_char_p, c_int, c_int, P(c_void_p)]),
+    "hg_storage_write_gmsh": (c_int, [c_void_p, c_char_p]),
     "hg_storage_destroy": (c_int, [c_void_p]),
     "hg_storage_counts": (c_int, [c_void_p, P(c_int)]),
     "hg_storage_set_stream": (c_int, [c_void_p, c_void_p]),
@@ -49,6 +53,9 @@ _SIGS = {
     "hg_level_size": (c_int, [c_void_p, c_int, P(c_int64)]),
     "hg_mesh_create_cuboid": (c_int, [P(c_double), P(c_double), c_int, c_int, c_int, c_int, P(c_void_p)]),
     "hg_mesh_create_tets": (c_int, [c_int, P(c_double), c_int, P(c_int), c_int, P(c_void_p)]),
+    "hg_mesh_create_cubed_domain": (c_int, [c_int, P(c_int), c_int, c_int, P(c_void_p)]),
+    "hg_mesh_create_gmsh": (c_int, [c_char_p, c_int, c_int, P(c_void_p)]),
+    "hg_mesh_write_gmsh": (c_int, [c_void_p, c_char_p]),
     "hg_mesh_destroy": (c_int, [c_void_p]),
     "hg_mesh_counts": (c_int, [c_void_p, P(c_int)]),
     "hg_mesh_set_cell_coefficients": (c_int, [c_void_p, P(c_double), c_int]),

@@ -52,11 +52,11 @@ int hg_device_count(void) {
   return n;
 }
 
-static int createFrom(const hg::Topology& topo, int maxLevel, hg_storage** out) {
+static int createFrom(const hg::Topology& topo, int maxLevel, hg_storage** out, bool geometryFlags = true) {
   hg::argCheck(out != nullptr, "null output pointer");
   if (hg_device_count() == 0) throw hg::Error(HG_ERR_CUDA, "no CUDA device visible");
   hg::Topology t = topo;
-  t.setBoundaryFlags(1, 0);
+  if (geometryFlags) t.setBoundaryFlags(1, 0);
   hg_storage* h = new hg_storage();
   try {
     h->s = new hg::Storage(t, maxLevel);
@@ -94,6 +94,57 @@ int hg_storage_create_tets(int nverts, const double* coords, int ncells, const i
     }
   }
   return createFrom(hg::Topology::fromTets(c, t), max_level, out);
+  HG_CATCH
+}
+
+static std::vector<std::array<int, 3>> cubeList(int ncubes, const int* cubes) {
+  hg::argCheck(ncubes > 0 && cubes != nullptr, "no cubes");
+  std::vector<std::array<int, 3>> v(ncubes);
+  for (int i = 0; i < ncubes; ++i) {
+    for (int d = 0; d < 3; ++d) {
+      hg::argCheck(cubes[3 * i + d] > -(1 << 20) && cubes[3 * i + d] < (1 << 20), "cube coordinate out of range");
+      v[i][d] = cubes[3 * i + d];
+    }
+  }
+  return v;
+}
+
+static hg::Topology cubedDomain(int ncubes, const int* cubes, int cubeType) {
+  hg::argCheck(cubeType == 0 || cubeType == 1, "cube type must be 0 or 1");
+  return hg::meshCubedDomain(cubeList(ncubes, cubes), cubeType);
+}
+
+static hg::Topology gmshTopology(const char* path, int flagsFromFile) {
+  hg::argCheck(path != nullptr, "null path");
+  try {
+    return hg::readGmsh(path, flagsFromFile != 0);
+  } catch (const std::runtime_error& e) {
+    throw hg::Error(HG_ERR_ARG, e.what());
+  }
+}
+
+int hg_storage_create_cubed_domain(int ncubes, const int* cubes, int cube_type, int max_level, hg_storage** out) {
+  HG_TRY
+  hg::argCheck(max_level >= 0 && max_level <= 10, "max_level out of range [0,10]");
+  return createFrom(cubedDomain(ncubes, cubes, cube_type), max_level, out);
+  HG_CATCH
+}
+
+int hg_storage_create_gmsh(const char* path, int max_level, int flags_from_file, hg_storage** out) {
+  HG_TRY
+  hg::argCheck(max_level >= 0 && max_level <= 10, "max_level out of range [0,10]");
+  return createFrom(gmshTopology(path, flags_from_file), max_level, out, flags_from_file == 0);
+  HG_CATCH
+}
+
+int hg_storage_write_gmsh(const hg_storage* h, const char* path) {
+  HG_TRY
+  hg::argCheck(h != nullptr && path != nullptr, "null argument");
+  try {
+    hg::writeGmsh(h->s->disc.topo(), path);
+  } catch (const std::runtime_error& e) {
+    throw hg::Error(HG_ERR_ARG, e.what());
+  }
   HG_CATCH
 }
 
@@ -476,10 +527,10 @@ static const hg::LevelStencils& meshStencil(const hg_mesh* mc, int level, int fo
   return it->second;
 }
 
-static int meshFrom(const hg::Topology& topo, int maxLevel, hg_mesh** out) {
+static int meshFrom(const hg::Topology& topo, int maxLevel, hg_mesh** out, bool geometryFlags = true) {
   hg::argCheck(out != nullptr, "null output pointer");
   hg::Topology t = topo;
-  t.setBoundaryFlags(1, 0);
+  if (geometryFlags) t.setBoundaryFlags(1, 0);
   hg_mesh* m = new hg_mesh();
   try {
     m->d = new hg::Discretization(t, maxLevel);
@@ -514,6 +565,31 @@ int hg_mesh_create_tets(int nverts, const double* coords, int ncells, const int*
       t[i][k] = tets[4 * i + k];
     }
   return meshFrom(hg::Topology::fromTets(c, t), max_level, out);
+  HG_CATCH
+}
+
+int hg_mesh_create_cubed_domain(int ncubes, const int* cubes, int cube_type, int max_level, hg_mesh** out) {
+  HG_TRY
+  hg::argCheck(max_level >= 0 && max_level <= 10, "max_level out of range [0,10]");
+  return meshFrom(cubedDomain(ncubes, cubes, cube_type), max_level, out);
+  HG_CATCH
+}
+
+int hg_mesh_create_gmsh(const char* path, int max_level, int flags_from_file, hg_mesh** out) {
+  HG_TRY
+  hg::argCheck(max_level >= 0 && max_level <= 10, "max_level out of range [0,10]");
+  return meshFrom(gmshTopology(path, flags_from_file), max_level, out, flags_from_file == 0);
+  HG_CATCH
+}
+
+int hg_mesh_write_gmsh(const hg_mesh* m, const char* path) {
+  HG_TRY
+  hg::argCheck(m != nullptr && path != nullptr, "null argument");
+  try {
+    hg::writeGmsh(m->d->topo(), path);
+  } catch (const std::runtime_error& e) {
+    throw hg::Error(HG_ERR_ARG, e.what());
+  }
   HG_CATCH
 }
 

@@ -66,4 +66,22 @@ struct Topology {
 // MeshInfo::meshCuboid(p0, p1, nx, ny, nz) followed by SetupPrimitiveStorage.
 Topology meshCuboid(const double p0[3], const double p1[3], int nx, int ny, int nz);
 
+// MeshInfo::meshCubedDomain(cubeCoordinates, cubeType) followed by SetupPrimitiveStorage
+// (src/hyteg/mesh/MeshGenCubedDomain.cpp:115-383): unit cubes at the given integer positions,
+// 6 tetrahedra per cube (type 0, the meshCuboid split) or 24 (type 1, with face-centre and cube
+// centre vertices).
+Topology meshCubedDomain(const std::vector<std::array<int, 3>>& cubes, int cubeType);
+
+// MeshInfo::fromGmshFile (src/hyteg/mesh/MeshGenFromGmshFile.cpp:31-206): a Gmsh 2.2 ASCII
+// file with nodes, lines (type 1), triangles (2), tetrahedra (4) and points (15). With
+// fileFlags the first tag of every line and triangle becomes the boundary flag of that edge or
+// face (all other primitives 0), as MeshInfo keeps them; otherwise the flags are left for
+// setBoundaryFlags. Throws std::runtime_error on a malformed file.
+Topology readGmsh(const std::string& path, bool fileFlags);
+// The inverse, as the wire format of a macro-mesh: nodes in vertex order (IDs from 1),
+// flagged edges and faces as lines and triangles (two tags, the flag twice), then the cells in
+// frame order. readGmsh(writeGmsh(t), fileFlags) reproduces t's primitives and their order; with
+// fileFlags the edge and face flags too (vertex flags read as 0: points carry none).
+void writeGmsh(const Topology& t, const std::string& path);
+
 }  // namespace hg

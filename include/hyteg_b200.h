@@ -81,6 +81,23 @@ int hg_storage_create_cuboid(const double lo[3], const double hi[3], int nx, int
 /* Explicit tetrahedral mesh: coords[3*nverts], tets[4*ncells] (vertex IDs in cell-frame order). */
 int hg_storage_create_tets(int nverts, const double* coords, int ncells, const int* tets, int max_level,
                            hg_storage** out);
+/* MeshInfo::meshCubedDomain (src/hyteg/mesh/MeshGenCubedDomain.cpp:115-383) + SetupPrimitiveStorage +
+ * setMeshBoundaryFlagsOnBoundary(1, 0, true): unit cubes at the integer positions cubes[3*ncubes]
+ * (duplicates ignored), split into 6 tetrahedra each (cube_type 0, the meshCuboid split) or 24
+ * (cube_type 1: face-centre and cube-centre vertices). */
+int hg_storage_create_cubed_domain(int ncubes, const int* cubes, int cube_type, int max_level, hg_storage** out);
+/* MeshInfo::fromGmshFile (src/hyteg/mesh/MeshGenFromGmshFile.cpp:31-206) + SetupPrimitiveStorage: a
+ * Gmsh 2.2 ASCII file (nodes; lines, triangles, tetrahedra and points). flags_from_file = 0 sets the
+ * boundary flags from the geometry as setMeshBoundaryFlagsOnBoundary(1, 0, true) does; 1 keeps the
+ * first tag of each line and triangle as the flag of that edge or face (others 0), as MeshInfo
+ * does. A malformed file, a version other than 2.2, an unknown element type or a node outside every
+ * tetrahedron fails with HG_ERR_ARG. */
+int hg_storage_create_gmsh(const char* path, int max_level, int flags_from_file, hg_storage** out);
+/* The storage's macro-mesh as a Gmsh 2.2 file (the wire format of a topology): vertices in ID order,
+ * flagged edges and faces as lines and triangles, cells in frame order. Reading it back reproduces
+ * the storage's primitives and their order; with flags_from_file = 0 the geometric boundary flags,
+ * with 1 the written edge and face flags (vertices 0, as the reference's reader gives them). */
+int hg_storage_write_gmsh(const hg_storage* s, const char* path);
 int hg_storage_destroy(hg_storage* s);
 /* counts[4] = {#vertices, #edges, #faces, #cells} */
 int hg_storage_counts(const hg_storage* s, int counts[4]);
@@ -124,6 +141,9 @@ int hg_level_size(const hg_storage* s, int level, int64_t* n);
  * layout, halo tables and stencil tables, for inspection and CPU-side verification. ---- */
 int hg_mesh_create_cuboid(const double lo[3], const double hi[3], int nx, int ny, int nz, int max_level, hg_mesh** out);
 int hg_mesh_create_tets(int nverts, const double* coords, int ncells, const int* tets, int max_level, hg_mesh** out);
+int hg_mesh_create_cubed_domain(int ncubes, const int* cubes, int cube_type, int max_level, hg_mesh** out);
+int hg_mesh_create_gmsh(const char* path, int max_level, int flags_from_file, hg_mesh** out);
+int hg_mesh_write_gmsh(const hg_mesh* m, const char* path);
 int hg_mesh_destroy(hg_mesh* m);
 int hg_mesh_counts(const hg_mesh* m, int counts[4]);
 int hg_mesh_set_cell_coefficients(hg_mesh* m, const double* k, int ncells);
