@@ -279,6 +279,34 @@ def load_traffic(kernel, L):
         return None
 
 
+def reassembly_bench(hg, k=4, L=6, reps=5):
+    """Stencil re-assembly for new macro-cell coefficients (the setup of a request in the solve
+    server) on the largest serving shape, the k^3 cube of 6 k^3 macro-cells, levels 0..L: on the
+    host (assembly and upload) against the device (one kernel per level from the term lists, built
+    once). Wall clock around each call with the stream synchronised (both are host-issued work)."""
+    st = hg.PrimitiveStorage.cuboid((0, 0, 0), (1, 1, 1), k, k, k, L)
+    A = hg.P1ConstantLaplaceOperator(st, 0, L)
+    rng = np.random.default_rng(3)
+    t0 = time.perf_counter()
+    A.reassemble(on_device=True)  # builds the term lists
+    st.synchronize()
+    t_build = time.perf_counter() - t0
+    res = {}
+    for name, dev in (("host", False), ("device", True)):
+        ts = []
+        for _ in range(reps):
+            st.set_cell_coefficients(np.exp(rng.uniform(-1, 1, 6 * k ** 3)))
+            st.synchronize()
+            t0 = time.perf_counter()
+            A.reassemble(on_device=dev)
+            st.synchronize()
+            ts.append(time.perf_counter() - t0)
+        res[name + "_ms"] = float(np.median(ts)) * 1e3
+    res.update({"mesh": "%d^3 cube, %d macro-cells, levels 0..%d" % (k, 6 * k ** 3, L),
+                "term_lists_build_ms": t_build * 1e3, "speedup": res["host_ms"] / res["device_ms"]})
+    return res
+
+
 def serving_bench(hg, n_requests, seed=2024):
     """Batched serving on a seeded request stream (config 5, bounded sample): k in U{1..4}
     sub-cubes per direction (6..384 tets), level in U{3..6}, coefficient log-uniform in
@@ -573,6 +601,8 @@ def run_ours(args):
     if L >= 3 and not args.cycle_only:
         kernels["p2"] = p2_kernels(hg, st, L - 2, timed)
         kernels["stokes"] = stokes_bench(hg, st, min(L - 2, args.stokes_level))
+    if not args.cycle_only:
+        kernels["reassembly"] = reassembly_bench(hg)
 
     # --- autotuner: the faster SOR schedule per level and precision, used from here on
     autotune = {}

@@ -138,6 +138,12 @@ class HostMesh:
         call("hg_mesh_halo_table", self._h, level, group, i64ptr(dst), i64ptr(src), ctypes.byref(n))
         return dst, src
 
+    def assembly_plan_check(self, level, form):
+        """(targets, terms, mismatches) of the device re-assembly's term lists against the tables."""
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        call("hg_mesh_assembly_plan_check", self._h, level, form, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
     def cell_stencil(self, level, form, cell):
         w = np.zeros(15)
         call("hg_mesh_cell_stencil", self._h, level, form, cell, dptr(w))
@@ -427,6 +433,11 @@ class _P1ConstantOperator:
         if src is dst:
             raise ValueError("apply: src and dst must be different functions")
         call("hg_apply", self.storage.handle, self.id, src.id, dst.id, level, flag, updateType)
+
+    def reassemble(self, on_device=True):
+        """Stencils from the storage's current cell coefficients, on the device (bit-identical to
+        the host assembly) or on the host."""
+        call("hg_operator_reassemble", self.storage.handle, self.id, 1 if on_device else 0)
 
     def apply_primitives(self, src, dst, level, flag, updateType=Replace, kinds=15, refresh=True):
         """Only the kernels of the selected primitive kinds (bit set over VERTEX..CELL)."""

@@ -65,6 +65,7 @@ _SIGS = {
     "hg_mesh_level_size": (c_int, [c_void_p, c_int, P(c_int64)]),
     "hg_mesh_slot_info": (c_int, [c_void_p, c_int, P(c_double), P(ctypes.c_byte), c_int64]),
     "hg_mesh_halo_table": (c_int, [c_void_p, c_int, c_int, P(c_int64), P(c_int64), P(c_int64)]),
+    "hg_mesh_assembly_plan_check": (c_int, [c_void_p, c_int, c_int, P(c_int64), P(c_int64), P(c_int64)]),
     "hg_mesh_cell_stencil": (c_int, [c_void_p, c_int, c_int, c_int, P(c_double)]),
     "hg_mesh_face_stencil": (c_int, [c_void_p, c_int, c_int, c_int, P(c_int), P(c_int), P(c_int), P(c_double), c_int, P(c_int)]),
     "hg_mesh_low_stencil": (c_int, [c_void_p, c_int, c_int, c_int, c_int, P(c_int64), P(c_double), c_int, P(c_int)]),
@@ -85,6 +86,7 @@ _SIGS = {
     "hg_dot": (c_int, [c_void_p, c_int, c_int, c_int, c_uint, P(c_double)]),
     "hg_dot_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_uint, c_void_p]),
     "hg_operator_create": (c_int, [c_void_p, c_int, c_int, c_int, P(c_int)]),
+    "hg_operator_reassemble": (c_int, [c_void_p, c_int, c_int]),
     "hg_operator_destroy": (c_int, [c_void_p, c_int]),
     "hg_apply": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_uint, c_int]),
     "hg_apply_primitives": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_uint, c_int, c_int, c_int]),

@@ -396,6 +396,15 @@ int hg_operator_create(hg_storage* h, int form, int min_level, int max_level, in
   HG_CATCH
 }
 
+int hg_operator_reassemble(hg_storage* h, int op, int on_device) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  s.op(op);
+  hg::argCheck(op != s.structureOp, "internal operator");
+  s.reassembleOperator(op, on_device != 0);
+  HG_CATCH
+}
+
 int hg_operator_destroy(hg_storage* h, int op) {
   HG_TRY
   hg::Storage& s = S(h);
@@ -735,6 +744,34 @@ int hg_mesh_halo_table(const hg_mesh* m, int level, int group, int64_t* dst, int
     std::memcpy(src, lay.commSrc[group].data(), cnt * sizeof(int64_t));
   }
   *n = cnt;
+  HG_CATCH
+}
+
+int hg_mesh_assembly_plan_check(const hg_mesh* m, int level, int form, int64_t* targets, int64_t* terms,
+                                int64_t* mismatches) {
+  HG_TRY
+  hg::argCheck(targets && terms && mismatches, "null output");
+  const auto& st = meshStencil(M(m), level, form);
+  const hg::AssemblyPlan p = hg::buildAssemblyPlan(*M(m)->d, level, (hg::FormKind)form);
+  const hg::Topology& topo = M(m)->d->topo();
+  std::vector<double> ref;  // the assembled values in target order
+  for (auto& c : st.cell)
+    for (int k = 0; k < 16; ++k) ref.push_back(c[k]);
+  for (auto& f : st.face)
+    for (int k = 0; k < 16; ++k) ref.push_back(k < (int)f.size() ? f[k].w : 0.0);
+  for (auto& e : st.edge)
+    for (auto& x : e) ref.push_back(x.w);
+  for (auto& v : st.vert)
+    for (auto& x : v) ref.push_back(x.w);
+  hg::argCheck((int64_t)ref.size() == p.nCell + p.nFace + p.nLow, "plan targets differ from the stencil tables");
+  int64_t bad = 0;
+  for (int64_t t = 0; t < (int64_t)ref.size(); ++t) {
+    const double v = hg::evaluatePlanTarget(p, t, topo);
+    if (std::memcmp(&v, &ref[t], sizeof(double)) != 0) ++bad;
+  }
+  *targets = (int64_t)ref.size();
+  *terms = (int64_t)p.terms.size();
+  *mismatches = bad;
   HG_CATCH
 }
 

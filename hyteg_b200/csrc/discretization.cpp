@@ -517,7 +517,8 @@ void elementMass(const double p[4][3], double K[16]) {
 }
 
 // Row of the assembled operator at micro-vertex P (cell-local index p of cell c): calls
-// add(q, weight) for every vertex q of every micro-cell of c containing p.
+// add(q, raw, scaled) for every vertex q of every micro-cell of c containing p. The weight is
+// raw * k(c) when scaled (the diffusion form), else raw.
 template <class F>
 static void cellRow(const Topology& topo, int c, int64_t N, const int64_t p[3], FormKind form, F&& add) {
   const auto& ce = topo.cells[c];
@@ -528,6 +529,7 @@ static void cellRow(const Topology& topo, int c, int64_t N, const int64_t p[3], 
     const int64_t width = N - kMicroCellWidthReduction[t];
     if (width <= 0) continue;
     double K[16];
+    bool scaled = false;
     {
       double P[4][3];
       for (int m = 0; m < 4; ++m)
@@ -537,7 +539,7 @@ static void cellRow(const Topology& topo, int c, int64_t N, const int64_t p[3], 
                                   (double)N;
       if (form == FORM_LAPLACE) {
         elementLaplace(P, K);
-        for (double& k : K) k *= ce.k;
+        scaled = true;
       } else if (form == FORM_PSPG) {
         elementLaplace(P, K);
         double a[3][3];
@@ -558,7 +560,7 @@ static void cellRow(const Topology& topo, int c, int64_t N, const int64_t p[3], 
       if (i0 < 0 || i1 < 0 || i2 < 0 || i0 + i1 + i2 > width - 1) continue;
       for (int m = 0; m < 4; ++m) {
         const int64_t q[3] = {i0 + kMicroCell[t][m][0], i1 + kMicroCell[t][m][1], i2 + kMicroCell[t][m][2]};
-        add(q, K[4 * k + m]);
+        add(q, K[4 * k + m], scaled);
       }
     }
   }
@@ -570,23 +572,41 @@ static void cellLocal(const MacroCell& c, const Bary& p, int64_t out[3]) {
   out[2] = p.of(c.v[3]);
 }
 
-LevelStencils assembleStencils(const Discretization& d, int L, FormKind form) {
+namespace {
+// Accumulators of one stencil entry: the value (summed in traversal order), or the list of its
+// terms in that order.
+struct NumAcc {
+  double v = 0.0;
+  void add(const Topology& t, int cell, double raw, bool scaled) { v += scaled ? raw * t.cells[cell].k : raw; }
+};
+struct TermAcc {
+  std::vector<PlanTerm> v;
+  void add(const Topology&, int cell, double raw, bool scaled) { v.push_back({cell, scaled ? 1 : 0, raw}); }
+};
+
+template <class Acc>
+struct StencilAcc {
+  std::vector<std::array<Acc, 16>> cell;
+  std::vector<std::vector<std::pair<std::array<int, 3>, Acc>>> face;  // diagonal first
+  std::vector<std::vector<std::pair<int64_t, Acc>>> edge, vert;      // diagonal first
+};
+
+template <class Acc>
+StencilAcc<Acc> assembleAcc(const Discretization& d, int L, FormKind form) {
   const Topology& topo = d.topo();
   const int64_t N = int64_t(1) << L, w = N + 1;
-  LevelStencils st;
-  st.L = L;
+  StencilAcc<Acc> st;
 
   // cells: interior point (1,1,1) exists for N >= 4
   st.cell.resize(topo.cells.size());
   for (size_t c = 0; c < topo.cells.size(); ++c) {
-    st.cell[c].fill(0.0);
     if (N < 4) continue;
     const int64_t p[3] = {1, 1, 1};
-    cellRow(topo, (int)c, N, p, form, [&](const int64_t* q, double wgt) {
+    cellRow(topo, (int)c, N, p, form, [&](const int64_t* q, double raw, bool scaled) {
       const int dx = int(q[0] - p[0]), dy = int(q[1] - p[1]), dz = int(q[2] - p[2]);
       for (int k = 0; k < 15; ++k)
         if (kCellOffsets[k][0] == dx && kCellOffsets[k][1] == dy && kCellOffsets[k][2] == dz) {
-          st.cell[c][k] += wgt;
+          st.cell[c][k].add(topo, (int)c, raw, scaled);
           return;
         }
       throw std::runtime_error("cell stencil offset outside the 15-point pattern");
@@ -598,14 +618,14 @@ LevelStencils assembleStencils(const Discretization& d, int L, FormKind form) {
   for (size_t f = 0; f < topo.faces.size(); ++f) {
     if (N < 3) continue;
     const auto& fa = topo.faces[f];
-    std::map<std::array<int, 3>, double> acc;
-    acc[{0, 0, 0}] = 0.0;
+    std::map<std::array<int, 3>, Acc> acc;
+    acc[{0, 0, 0}];
     int64_t wts[3] = {N - 2, 1, 1};
     const Bary P = makeBary(fa.v, wts, 3);
     for (int cidx : fa.cells) {
       int64_t p[3];
       cellLocal(topo.cells[cidx], P, p);
-      cellRow(topo, cidx, N, p, form, [&](const int64_t* q, double wgt) {
+      cellRow(topo, cidx, N, p, form, [&](const int64_t* q, double raw, bool scaled) {
         int64_t bw[4] = {N - q[0] - q[1] - q[2], q[0], q[1], q[2]};
         const Bary Q = makeBary(topo.cells[cidx].v, bw, 4);
         const int64_t s = d.localSlotOf(L, KF, (int)f, Q);
@@ -621,34 +641,33 @@ LevelStencils assembleStencils(const Discretization& d, int L, FormKind form) {
         int64_t y = 0;
         while (faceIdx(width, 0, y + 1) <= r) ++y;
         const int64_t x = r - faceIdx(width, 0, y);
-        acc[{layer, int(x - 1), int(y - 1)}] += wgt;
+        acc[{layer, int(x - 1), int(y - 1)}].add(topo, cidx, raw, scaled);
       });
     }
-    st.face[f].push_back({acc[{0, 0, 0}], 0, 0, 0});
+    st.face[f].push_back({{0, 0, 0}, acc[{0, 0, 0}]});
     for (auto& kv : acc)
-      if (!(kv.first[0] == 0 && kv.first[1] == 0 && kv.first[2] == 0))
-        st.face[f].push_back({kv.second, kv.first[0], kv.first[1], kv.first[2]});
+      if (!(kv.first[0] == 0 && kv.first[1] == 0 && kv.first[2] == 0)) st.face[f].push_back(kv);
   }
 
   // edges: interior point x = 1 exists for N >= 2
   auto lowRow = [&](int kind, int prim, const Bary& P, int64_t centerSlot, const std::vector<int>& cells) {
-    std::map<int64_t, double> acc;
-    acc[0] = 0.0;
+    std::map<int64_t, Acc> acc;
+    acc[0];
     for (int cidx : cells) {
       int64_t p[3];
       cellLocal(topo.cells[cidx], P, p);
-      cellRow(topo, cidx, N, p, form, [&](const int64_t* q, double wgt) {
+      cellRow(topo, cidx, N, p, form, [&](const int64_t* q, double raw, bool scaled) {
         int64_t bw[4] = {N - q[0] - q[1] - q[2], q[0], q[1], q[2]};
         const Bary Q = makeBary(topo.cells[cidx].v, bw, 4);
         const int64_t s = d.localSlotOf(L, kind, prim, Q);
         if (s < 0) throw std::runtime_error("stencil neighbour not stored in edge/vertex array");
-        acc[s - centerSlot] += wgt;
+        acc[s - centerSlot].add(topo, cidx, raw, scaled);
       });
     }
-    std::vector<LowEntry> out;
-    out.push_back({acc[0], 0});
+    std::vector<std::pair<int64_t, Acc>> out;
+    out.push_back({0, acc[0]});
     for (auto& kv : acc)
-      if (kv.first != 0) out.push_back({kv.second, kv.first});
+      if (kv.first != 0) out.push_back(kv);
     return out;
   };
   st.edge.resize(topo.edges.size());
@@ -664,6 +683,65 @@ LevelStencils assembleStencils(const Discretization& d, int L, FormKind form) {
     st.vert[v] = lowRow(KV, (int)v, makeBary(&self, &N, 1), 0, topo.verts[v].cells);
   }
   return st;
+}
+}  // namespace
+
+LevelStencils assembleStencils(const Discretization& d, int L, FormKind form) {
+  const StencilAcc<NumAcc> a = assembleAcc<NumAcc>(d, L, form);
+  LevelStencils st;
+  st.L = L;
+  st.cell.resize(a.cell.size());
+  for (size_t c = 0; c < a.cell.size(); ++c)
+    for (int k = 0; k < 16; ++k) st.cell[c][k] = a.cell[c][k].v;
+  st.face.resize(a.face.size());
+  for (size_t f = 0; f < a.face.size(); ++f)
+    for (auto& e : a.face[f]) st.face[f].push_back({e.second.v, e.first[0], e.first[1], e.first[2]});
+  st.edge.resize(a.edge.size());
+  for (size_t e = 0; e < a.edge.size(); ++e)
+    for (auto& x : a.edge[e]) st.edge[e].push_back({x.second.v, x.first});
+  st.vert.resize(a.vert.size());
+  for (size_t v = 0; v < a.vert.size(); ++v)
+    for (auto& x : a.vert[v]) st.vert[v].push_back({x.second.v, x.first});
+  return st;
+}
+
+AssemblyPlan buildAssemblyPlan(const Discretization& d, int L, FormKind form) {
+  const StencilAcc<TermAcc> a = assembleAcc<TermAcc>(d, L, form);
+  AssemblyPlan p;
+  p.L = L;
+  p.first.push_back(0);
+  auto target = [&](const std::vector<PlanTerm>* t) {
+    if (t) p.terms.insert(p.terms.end(), t->begin(), t->end());
+    p.first.push_back((int64_t)p.terms.size());
+  };
+  for (auto& c : a.cell)
+    for (int k = 0; k < 16; ++k) target(&c[k].v);
+  p.nCell = (int64_t)a.cell.size() * 16;
+  for (auto& f : a.face)
+    for (int k = 0; k < 16; ++k) target(k < (int)f.size() ? &f[k].second.v : nullptr);
+  p.nFace = (int64_t)a.face.size() * 16;
+  int64_t nLow = 0;
+  for (auto& e : a.edge)
+    for (auto& x : e) {
+      target(&x.second.v);
+      ++nLow;
+    }
+  for (auto& v : a.vert)
+    for (auto& x : v) {
+      target(&x.second.v);
+      ++nLow;
+    }
+  p.nLow = nLow;
+  return p;
+}
+
+double evaluatePlanTarget(const AssemblyPlan& p, int64_t t, const Topology& topo) {
+  double v = 0.0;
+  for (int64_t i = p.first[t]; i < p.first[t + 1]; ++i) {
+    const PlanTerm& x = p.terms[i];
+    v += x.scaled ? x.K * topo.cells[x.cell].k : x.K;
+  }
+  return v;
 }
 
 }  // namespace hg

@@ -129,6 +129,26 @@ void elementMass(const double p[4][3], double K[16]);
 
 LevelStencils assembleStencils(const Discretization& d, int L, FormKind form);
 
+// The same stencils as sums of element-matrix terms, for re-assembly with new cell coefficients
+// on the device: every entry is sum_i (scaled_i ? K_i * k(cell_i) : K_i), summed in the order of
+// the terms, which is the order assembleStencils adds them in (so both give the same bits).
+// Targets follow the device arrays: [cells][16], then [faces][16] (the face entries, zeros
+// beyond them), then the edge entries and the vertex entries, each primitive's diagonal first.
+struct PlanTerm {
+  int cell;
+  int scaled;  // 1: multiplied by the cell's coefficient (diffusion form)
+  double K;
+};
+struct AssemblyPlan {
+  int L = 0;
+  std::vector<int64_t> first;  // [targets + 1]: term range of each target
+  std::vector<PlanTerm> terms;
+  int64_t nCell = 0, nFace = 0, nLow = 0;
+};
+AssemblyPlan buildAssemblyPlan(const Discretization& d, int L, FormKind form);
+// One target of a plan evaluated on the host with the topology's current coefficients.
+double evaluatePlanTarget(const AssemblyPlan& p, int64_t t, const Topology& topo);
+
 // P2 (quadratic) space of level L, stored as the vertex-DoF lattice of level L + 1: the
 // micro-vertices of level L sit at even coordinates, the midpoints of its micro-edges at the
 // seven other parity classes (the reference's X, Y, Z, XY, XZ, YZ, XYZ edge orientations,

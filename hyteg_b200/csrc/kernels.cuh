@@ -1859,6 +1859,44 @@ __global__ void __launch_bounds__(kBlock) interpolateKernel(LevelDev lv, Geometr
 }
 
 // ---------------------------------------------------------------------------------------
+// Stencil re-assembly for new macro-cell coefficients: every stencil entry of one level is the
+// sum of its element-matrix terms K_i (times the coefficient of the term's cell for the
+// diffusion form), added in the order the host assembly adds them, with explicit
+// round-to-nearest products and sums (no contraction), so the device gives the host's bits. The
+// targets are the level's cell weights [cells][16], face entries [faces][16] and edge/vertex
+// entries, in that order; each is written in FP64 and rounded to FP32.
+// ---------------------------------------------------------------------------------------
+struct PlanTermDev {
+  int cell;
+  int scaled;
+  double K;
+};
+
+static __global__ void __launch_bounds__(kBlock)
+    planAssembleKernel(const int64_t* __restrict__ first, const PlanTermDev* __restrict__ terms,
+                       const double* __restrict__ coef, int64_t nCell, int64_t nFace, int64_t nLow, double* cell64,
+                       float* cell32, FaceEnt<double>* face64, FaceEnt<float>* face32, double* low64, float* low32) {
+  const int64_t t = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  if (t >= nCell + nFace + nLow) return;
+  double v = 0.0;
+  for (int64_t i = first[t]; i < first[t + 1]; ++i) {
+    const PlanTermDev x = terms[i];
+    v = __dadd_rn(v, x.scaled ? __dmul_rn(x.K, coef[x.cell]) : x.K);
+  }
+  const float vf = __double2float_rn(v);
+  if (t < nCell) {
+    cell64[t] = v;
+    cell32[t] = vf;
+  } else if (t < nCell + nFace) {
+    face64[t - nCell].w = v;
+    face32[t - nCell].w = vf;
+  } else {
+    low64[t - nCell - nFace] = v;
+    low32[t - nCell - nFace] = vf;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // Halo refresh: copy slots <- owner slots (one gather; every source is an owned slot).
 // ---------------------------------------------------------------------------------------
 template <class T>

@@ -100,6 +100,7 @@ std::unique_ptr<ServerSlot> Server::buildSlot(int k, int level) {
   s->x = st.createFunction(0, level, 8);
   s->b = st.createFunction(0, level, 8);
   s->op = st.createOperator(0, 0, level);
+  st.reassembleOperator(s->op, true);  // builds the term lists now, so requests only run the kernels
   s->gmg = st.nextId++;
   st.gmgs[s->gmg].reset(new Gmg(st, s->op, 0, level, 3, 3, 1.0, 0, 200, 1e-16, precision_));
   // one iteration so that the smoother's spare buffers exist before the footprint is taken
@@ -125,12 +126,13 @@ void Server::prewarm(int k, int level) {
 void Server::run(ServerRequest& r, ServerSlot& s) {
   Storage& st = *s.st;
   const int L = r.level;
-  // constant coefficient: scale every macro-cell and re-assemble the stencils in place (no device
-  // allocation or release, which would synchronise the whole device and stall the other requests)
+  // constant coefficient: scale every macro-cell and re-assemble the stencils in place on the
+  // device (no device allocation or release, which would synchronise the whole device and stall
+  // the other requests; the term lists are built by the slot's first re-assembly)
   auto& cells = const_cast<Topology&>(st.disc.topo()).cells;
   if (cells.empty() || cells[0].k != r.coefficient) {
     for (auto& c : cells) c.k = r.coefficient;
-    st.reassembleOperator(s.op);
+    st.reassembleOperator(s.op, true);
   }
   r.tSolve = now();
   st.fillRandom(s.b, L, HG_INNER, r.seed, -1.0, 1.0);

@@ -1446,6 +1446,10 @@ static void stokesDivImpl(Storage& st, P2Operator& o, const int u[3], int q, int
 int Storage::p1Diagonal(int opId, int L) {
   Operator& o = op(opId);
   argCheck(L >= o.minL && L <= o.maxL, "level outside the operator's level range");
+  if (o.hostStale) {  // re-assembled on the device since: bring the host copy up to date
+    for (int l = o.minL; l <= o.maxL; ++l) o.host[l - o.minL] = assembleStencils(disc, l, (FormKind)o.form);
+    o.hostStale = false;
+  }
   const LevelStencils& h = o.host[L - o.minL];
   const LevelData& ld = levels[L];
   const LevelLayout& lay = *ld.lay;
@@ -1547,14 +1551,58 @@ void Storage::autotuneSor(int minL, int maxL, int prec, int reps, double* ms) {
   ++generation;
 }
 
-void Storage::reassembleOperator(int id) {
+void Storage::reassembleOperator(int id, bool onDevice) {
   Operator& o = op(id);
-  for (int L = o.minL; L <= o.maxL; ++L) {
-    LevelStencils h = assembleStencils(disc, L, (FormKind)o.form);
-    refillStencil<double>(o.d[L - o.minL], h, stream);
-    refillStencil<float>(o.f[L - o.minL], h, stream);
-    o.host[L - o.minL] = std::move(h);
+  if (!onDevice) {
+    for (int L = o.minL; L <= o.maxL; ++L) {
+      LevelStencils h = assembleStencils(disc, L, (FormKind)o.form);
+      refillStencil<double>(o.d[L - o.minL], h, stream);
+      refillStencil<float>(o.f[L - o.minL], h, stream);
+      o.host[L - o.minL] = std::move(h);
+    }
+    o.hostStale = false;
+    return;
   }
+  if (o.form != FORM_LAPLACE) return;  // the mass and PSPG forms do not depend on the coefficients
+  static_assert(sizeof(dev::PlanTermDev) == sizeof(PlanTerm), "plan term layout");
+  const Topology& topo = disc.topo();
+  if (o.plans.empty()) {
+    for (int L = o.minL; L <= o.maxL; ++L) {
+      const AssemblyPlan p = buildAssemblyPlan(disc, L, (FormKind)o.form);
+      const dev::StencilDev<double>& sd = o.d[L - o.minL];
+      argCheck(p.nCell == (int64_t)topo.cells.size() * 16 && p.nFace == (int64_t)topo.faces.size() * 16,
+               "re-assembly: target layout");
+      (void)sd;
+      Operator::DevPlan dp;
+      dp.first = (const int64_t*)upload(o.keep, p.first, stream);
+      dp.terms = (const dev::PlanTermDev*)upload(o.keep, p.terms, stream);
+      dp.nCell = p.nCell;
+      dp.nFace = p.nFace;
+      dp.nLow = p.nLow;
+      cudaCheck(cudaStreamSynchronize(stream), "plan upload");  // the host vectors go out of scope
+      o.plans.push_back(dp);
+    }
+    o.coef.alloc(std::max<size_t>(topo.cells.size(), 1) * sizeof(double));
+  }
+  std::vector<double> k(topo.cells.size());
+  for (size_t c = 0; c < k.size(); ++c) k[c] = topo.cells[c].k;
+  // from pageable memory: returns once the values are staged, so k may go out of scope
+  cudaCheck(cudaMemcpyAsync(o.coef.p, k.data(), k.size() * sizeof(double), cudaMemcpyHostToDevice, stream),
+            "coefficient upload");
+  for (int L = o.minL; L <= o.maxL; ++L) {
+    const Operator::DevPlan& dp = o.plans[L - o.minL];
+    const dev::StencilDev<double>& sd = o.d[L - o.minL];
+    const dev::StencilDev<float>& sf = o.f[L - o.minL];
+    const int64_t n = dp.nCell + dp.nFace + dp.nLow;
+    if (n == 0) continue;
+    dev::planAssembleKernel<<<(unsigned)((n + dev::kBlock - 1) / dev::kBlock), dev::kBlock, 0, stream>>>(
+        dp.first, dp.terms, (const double*)o.coef.p, dp.nCell, dp.nFace, dp.nLow, const_cast<double*>(sd.cellW),
+        const_cast<float*>(sf.cellW), const_cast<dev::FaceEnt<double>*>(sd.faceEnt),
+        const_cast<dev::FaceEnt<float>*>(sf.faceEnt), const_cast<double*>(sd.lowEntW), const_cast<float*>(sf.lowEntW));
+    ++launches;
+  }
+  cudaCheck(cudaGetLastError(), "re-assembly");
+  o.hostStale = true;
 }
 
 int Storage::createOperator(int form, int minL, int maxL) {

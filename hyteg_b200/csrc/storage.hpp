@@ -66,6 +66,18 @@ struct Operator {
   std::vector<dev::StencilDev<double>> d;
   std::vector<dev::StencilDev<float>> f;
   std::vector<std::unique_ptr<DevBuf>> keep;
+  // Device re-assembly (the diffusion form): per level the terms of every stencil entry, built
+  // on first use. After a device re-assembly the host copy holds the previous coefficients'
+  // values (hostStale): its structure and the signs of its diagonals still hold, and
+  // p1Diagonal re-assembles it before reading values.
+  struct DevPlan {
+    const int64_t* first = nullptr;
+    const dev::PlanTermDev* terms = nullptr;
+    int64_t nCell = 0, nFace = 0, nLow = 0;
+  };
+  std::vector<DevPlan> plans;
+  DevBuf coef;  // [cells] coefficients of the last device re-assembly
+  bool hostStale = false;
 };
 
 // P2 operator: element matrices of the six micro-cell types per macro-cell and level.
@@ -202,8 +214,10 @@ struct Storage {
   void p2Launch(P2Operator& o, int L, T* dst, const T* src, const T* rhs, unsigned mask, int sel);
   template <class T>
   void p2SorT(P2Operator& o, int opId, int x, int b, int L, unsigned mask, T omega, bool backwards);
-  // Re-assemble an operator's stencils from the current cell coefficients into its device arrays.
-  void reassembleOperator(int id);
+  // Re-assemble an operator's stencils from the current cell coefficients into its device
+  // arrays: on the host (assembly, upload), or on the device from the per-entry term lists (the
+  // same bits; forms without coefficients are left as they are).
+  void reassembleOperator(int id, bool onDevice = false);
   Operator& op(int id);
   void apply(int op, int src, int dst, int L, unsigned mask, int update, int kinds = 15, bool refresh = true);
   void residual(int op, int x, int b, int r, int L, unsigned mask);

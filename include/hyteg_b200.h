@@ -161,6 +161,11 @@ int hg_mesh_halo_table(const hg_mesh* m, int level, int group, int64_t* dst, int
  * the order C E W N S NW SE TC TW TS TSE BC BE BN BNW. Faces: entries (layer, dx, dy, weight),
  * layer 0 = face, 1 + n = ghost layer of neighbour cell n. Edges / vertices: entries
  * (relative slot, weight). Entry 0 is the diagonal. cap = capacity of the output arrays. */
+/* Verification of the device re-assembly's term lists (hg_operator_reassemble) on the host:
+ * every stencil entry of (level, form) summed from its terms in order, compared bit for bit with
+ * the assembled tables. targets / terms: sizes of the lists; mismatches: entries that differ. */
+int hg_mesh_assembly_plan_check(const hg_mesh* m, int level, int form, int64_t* targets, int64_t* terms,
+                                int64_t* mismatches);
 int hg_mesh_cell_stencil(const hg_mesh* m, int level, int form, int cell, double w[15]);
 int hg_mesh_face_stencil(const hg_mesh* m, int level, int form, int face, int* layer, int* dx, int* dy, double* w,
                          int cap, int* n);
@@ -336,6 +341,13 @@ int hg_function_fill_random(hg_storage* s, int fn, int level, unsigned flag, uin
  * p1functionspace/P1ConstantOperator.hpp:201-208; forms/form_fenics_generated/p1_tet_pspg_tet.h) */
 int hg_operator_create(hg_storage* s, int form, int min_level, int max_level, int* op);
 int hg_operator_destroy(hg_storage* s, int op);
+/* Re-assembles the operator's stencils on all its levels from the storage's current cell
+ * coefficients (hg_storage_set_cell_coefficients). on_device = 0: on the host, then uploaded (as
+ * at creation). on_device = 1: from per-entry lists of element-matrix terms, one kernel per level
+ * on the storage's stream. The first call builds the lists (host work similar to one host
+ * assembly). The results are bit-identical to the host assembly. Only the diffusion form
+ * depends on the coefficients; the other forms are left as they are. */
+int hg_operator_reassemble(hg_storage* s, int op, int on_device);
 /* update: 0 = Replace, 1 = Add */
 int hg_apply(hg_storage* s, int op, int src, int dst, int level, unsigned flag, int update);
 /* The per-primitive-kind kernels of hg_apply without (refresh = 0) or with (1) the preceding
