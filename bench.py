@@ -679,6 +679,18 @@ def run_ours(args):
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) * 1e-3, pg)
 
+    # --- where one cycle's time goes: the solver's timing tree (device events, eager cycle) ----
+    gmg.set_timing(A, True)
+    gmg.solve(A, x, b, L)
+    tree = gmg.timing_tree(A)["Geometric Multigrid Solver"]
+    gmg.set_timing(A, False)
+    cycle_tree = {"total_ms": tree["total"] * 1e3, "levels": {}}
+    for lv in range(L + 1):
+        node = tree.get("Level %d" % lv, {})
+        cycle_tree["levels"][str(lv)] = {k: node[k]["total"] * 1e3 for k in
+                                         ("Smoother", "Restriction", "Prolongation", "Coarse Grid Solver",
+                                          "Remainder") if k in node}
+
     peak, peak_kind = load_peaks()
     achieved = BYTES["sor_sweep"] * Nc / t_sor_cells / 1e9
     traffic = load_traffic("cellSorWaveKernel<double, 0>", L)
@@ -701,6 +713,7 @@ def run_ours(args):
         "kernels": kernels,
         "solve": solve,
         "autotune_sor": autotune,
+        "timing_tree_one_cycle_ms": cycle_tree,
     }
     if world == 1 and args.serving_requests > 0 and not args.cycle_only:
         out["serving"] = serving_bench(hg, args.serving_requests)

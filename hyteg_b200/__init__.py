@@ -553,6 +553,20 @@ class GeometricMultigridSolver:
         """Replay cycles from captured CUDA graphs (default on; identical results)."""
         call("hg_gmg_set_graphs", self.storage.handle, self._handle(A), 1 if enable else 0)
 
+    def set_timing(self, A, enable):
+        """Device-timed phases in a timing tree (the reference's WcTimingTree nodes); cycles run
+        eagerly while on."""
+        call("hg_gmg_set_timing", self.storage.handle, self._handle(A), 1 if enable else 0)
+
+    def timing_tree(self, A):
+        """The timing tree as a dict (waLBerla TimingTree JSON layout, seconds)."""
+        import json
+        n = ctypes.c_int64()
+        call("hg_gmg_timing_json", self.storage.handle, self._handle(A), None, 0, ctypes.byref(n))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        call("hg_gmg_timing_json", self.storage.handle, self._handle(A), buf, n.value + 1, ctypes.byref(n))
+        return json.loads(buf.value.decode())
+
     def solve_to(self, A, x, b, level, tol, max_iter=100):
         """Iterate to a relative residual tol (FP64 x, b). An FP32 solver runs FP64 defect
         correction around FP32 cycles. Returns (iterations, relative residual, history)."""

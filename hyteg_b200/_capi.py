@@ -135,6 +135,8 @@ _SIGS = {
     "hg_server_solution": (c_int, [c_void_p, c_int64, P(c_double), c_int64, P(c_int64)]),
     "hg_server_stats": (c_int, [c_void_p, P(c_int64)]),
     "hg_function_fill_random": (c_int, [c_void_p, c_int, c_int, c_uint, ctypes.c_uint64, c_double, c_double]),
+    "hg_gmg_set_timing": (c_int, [c_void_p, c_int, c_int]),
+    "hg_gmg_timing_json": (c_int, [c_void_p, c_int, c_char_p, c_int64, P(c_int64)]),
     "hg_gmg_set_graphs": (c_int, [c_void_p, c_int, c_int]),
     "hg_gmg_solve_to": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_int, P(c_int), P(c_double), P(c_double),
                                 c_int]),

@@ -1109,6 +1109,32 @@ int hg_gmg_set_graphs(hg_storage* h, int gmg, int enable) {
   HG_CATCH
 }
 
+int hg_gmg_set_timing(hg_storage* h, int gmg, int enable) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  auto it = s.gmgs.find(gmg);
+  hg::argCheck(it != s.gmgs.end(), "unknown multigrid handle");
+  it->second->setTiming(enable != 0);
+  HG_CATCH
+}
+
+int hg_gmg_timing_json(hg_storage* h, int gmg, char* buf, int64_t cap, int64_t* len) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  auto it = s.gmgs.find(gmg);
+  hg::argCheck(it != s.gmgs.end(), "unknown multigrid handle");
+  hg::argCheck(it->second->timing != nullptr, "timing is off for this solver (hg_gmg_set_timing)");
+  hg::argCheck(len != nullptr, "null length");
+  const std::string j = it->second->timing->json();
+  *len = (int64_t)j.size();
+  if (buf && cap > 0) {
+    const int64_t n = std::min<int64_t>(cap - 1, (int64_t)j.size());
+    std::memcpy(buf, j.data(), (size_t)n);
+    buf[n] = 0;
+  }
+  HG_CATCH
+}
+
 int hg_gmg_solve_to(hg_storage* h, int gmg, int x, int b, int level, double tol, int max_iter, int* iterations,
                     double* rel_residual, double* history, int history_cap) {
   HG_TRY

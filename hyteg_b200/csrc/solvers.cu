@@ -1,6 +1,8 @@
 // CG and geometric multigrid drivers on top of the device kernels (host orchestration; all
 // vector work stays on the device, only convergence scalars are read back).
+#include <algorithm>
 #include <cmath>
+#include <cstdio>
 
 #include "../../include/hyteg_b200.h"
 #include "solvers.hpp"
@@ -87,6 +89,144 @@ void Gmg::setGraphs(bool on) {
   if (!on) cache.clear();
 }
 
+void Gmg::setTiming(bool on) {
+  if (on) timing.reset(new TimingTree());
+  else timing.reset();
+}
+
+// ---------------------------------------------------------------------------------------
+// Timing tree
+// ---------------------------------------------------------------------------------------
+TimingTree::Node& TimingTree::Node::child(const std::string& name) {
+  for (auto& c : children)
+    if (c.first == name) return c.second;
+  children.emplace_back(name, Node());
+  return children.back().second;
+}
+
+TimingTree::~TimingTree() {
+  std::vector<Node*> todo{&root};
+  while (!todo.empty()) {
+    Node* n = todo.back();
+    todo.pop_back();
+    for (auto& p : n->pending) {
+      cudaEventDestroy(p.first);
+      cudaEventDestroy(p.second);
+    }
+    if (n->open) cudaEventDestroy(n->open);
+    for (auto& c : n->children) todo.push_back(&c.second);
+  }
+  for (cudaEvent_t e : pool) cudaEventDestroy(e);
+}
+
+void TimingTree::start(cudaStream_t st, const std::string& name) {
+  Node& n = stack.back()->child(name);
+  argCheck(n.open == nullptr, "timing tree: \"" + name + "\" started twice");
+  cudaEvent_t e;
+  if (!pool.empty()) {
+    e = pool.back();
+    pool.pop_back();
+  } else {
+    cudaCheck(cudaEventCreate(&e), "timing event");
+  }
+  cudaCheck(cudaEventRecord(e, st), "timing event");
+  n.open = e;
+  stack.push_back(&n);
+}
+
+void TimingTree::stop(cudaStream_t st, const std::string& name, int applications) {
+  argCheck(stack.size() > 1, "timing tree: stop without start");
+  Node& n = *stack.back();
+  argCheck(stack[stack.size() - 2]->child(name).open == n.open && n.open != nullptr,
+           "timing tree: \"" + name + "\" is not the innermost open timer");
+  cudaEvent_t e;
+  if (!pool.empty()) {
+    e = pool.back();
+    pool.pop_back();
+  } else {
+    cudaCheck(cudaEventCreate(&e), "timing event");
+  }
+  cudaCheck(cudaEventRecord(e, st), "timing event");
+  n.pending.emplace_back(n.open, e);
+  n.pendingCount.push_back(std::max(applications, 1));
+  n.open = nullptr;
+  stack.pop_back();
+}
+
+void TimingTree::resolve() {
+  std::vector<Node*> todo{&root};
+  while (!todo.empty()) {
+    Node* n = todo.back();
+    todo.pop_back();
+    for (size_t i = 0; i < n->pending.size(); ++i) {
+      cudaCheck(cudaEventSynchronize(n->pending[i].second), "timing resolve");
+      float ms = 0;
+      cudaCheck(cudaEventElapsedTime(&ms, n->pending[i].first, n->pending[i].second), "timing resolve");
+      const int a = n->pendingCount[i];
+      const double t = ms * 1e-3 / a;  // each application's share
+      for (int k = 0; k < a; ++k) {
+        n->min = n->count == 0 ? t : std::min(n->min, t);
+        n->max = n->count == 0 ? t : std::max(n->max, t);
+        n->total += t;
+        n->sumSq += t * t;
+        ++n->count;
+      }
+      pool.push_back(n->pending[i].first);
+      pool.push_back(n->pending[i].second);
+    }
+    n->pending.clear();
+    n->pendingCount.clear();
+    for (auto& c : n->children) todo.push_back(&c.second);
+  }
+}
+
+void TimingTree::reset() {
+  resolve();
+  root = Node();
+  stack.assign(1, &root);
+}
+
+static void timerJson(std::string& out, double total, int64_t count, double mn, double mx, double sumSq) {
+  const double avg = count ? total / count : 0.0;
+  const double var = count ? std::max(sumSq / count - avg * avg, 0.0) : 0.0;
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "\"total\": %.9g, \"average\": %.9g, \"count\": %lld, \"min\": %.9g, \"max\": %.9g, "
+                "\"variance\": %.9g", total, avg, (long long)count, mn, mx, var);
+  out += buf;
+}
+
+static void nodeJson(std::string& out, const TimingTree::Node& n) {
+  out += "{";
+  timerJson(out, n.total, n.count, n.min, n.max, n.sumSq);
+  double covered = 0;
+  for (auto& c : n.children) {
+    out += ", \"" + c.first + "\": ";
+    nodeJson(out, c.second);
+    covered += c.second.total;
+  }
+  if (!n.children.empty()) {  // getCopyWithRemainder
+    const double r = std::max(n.total - covered, 0.0);
+    out += ", \"Remainder\": {";
+    timerJson(out, r, 1, r, r, r * r);
+    out += "}";
+  }
+  out += "}";
+}
+
+std::string TimingTree::json() {
+  resolve();
+  std::string out = "{";
+  bool first = true;
+  for (auto& c : root.children) {
+    if (!first) out += ", ";
+    first = false;
+    out += "\"" + c.first + "\": ";
+    nodeJson(out, c.second);
+  }
+  out += "}";
+  return out;
+}
+
 void GraphCache::clear() {
   for (auto& c : captured) cudaGraphExecDestroy(c.exec);
   captured.clear();
@@ -152,6 +292,7 @@ void Gmg::coarseSolve(int x, int b, int L) {
     xs = cx64;
     bs = cb64;
   }
+  if (timing) timing->start(s.stream, "CG Solver");
   if (deviceCoarse()) {
     const LevelData& ld = s.levels[L];
     Operator& o = s.op(op);
@@ -166,6 +307,7 @@ void Gmg::coarseSolve(int x, int b, int L) {
   } else {
     cgSolve(s, op, xs, bs, L, coarseMaxIter, coarseTol, cp, cz, cap, cr, nullptr);
   }
+  if (timing) timing->stop(s.stream, "CG Solver");
   if (prec == 4) s.copyCast(x, cx64, L, HG_ALL, false);
 }
 
@@ -192,6 +334,12 @@ std::vector<uintptr_t> Gmg::signature(int x, int b, int L) {
 }
 
 void Gmg::runCycle(int x, int b, int L) {
+  if (timing) {  // GeometricMultigridSolver::solve (GeometricMultigridSolver.hpp:127-134), eagerly
+    timing->start(s.stream, "Geometric Multigrid Solver");
+    solveRecursively(x, b, L);
+    timing->stop(s.stream, "Geometric Multigrid Solver");
+    return;
+  }
   if (!graphs || (pre + post) % 2 != 0 || !deviceCoarse()) {
     solveRecursively(x, b, L);
     return;
@@ -202,21 +350,49 @@ void Gmg::runCycle(int x, int b, int L) {
 // GeometricMultigridSolver::solveRecursively (src/hyteg/solvers/GeometricMultigridSolver.hpp:136-235)
 void Gmg::solveRecursively(int x, int b, int L) {
   const unsigned flag = HG_INNER | HG_NEUMANN;
+  TimingTree* tt = timing.get();
+  const std::string lvl = tt ? "Level " + std::to_string(L) : std::string();
+  auto start = [&](const std::string& n) {
+    if (tt) tt->start(s.stream, n);
+  };
+  auto stop = [&](const std::string& n, int applications = 1) {
+    if (tt) tt->stop(s.stream, n, applications);
+  };
   if (L == minL) {
+    start(lvl);
+    start("Coarse Grid Solver");
     coarseSolve(x, b, L);
+    stop("Coarse Grid Solver");
+    stop(lvl);
     return;
   }
-  s.smoothSorSweeps(op, x, b, omega, L, flag, pre, false, false);
+  start(lvl);
+  if (pre > 0) {
+    start("Smoother");
+    s.smoothSorSweeps(op, x, b, omega, L, flag, pre, false, false);
+    stop("Smoother", pre);
+  }
   s.residual(op, x, b, tmp, L, flag);
+  start("Restriction");
   s.restrictFn(tmp, L, flag);
+  stop("Restriction");
   const double one = 1.0;
   s.lincomb(b, L - 1, flag, 1, &one, &tmp, false, 0.0);
   s.lincomb(x, L - 1, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+  stop(lvl);
   solveRecursively(x, b, L - 1);
   if (cycle == 1) solveRecursively(x, b, L - 1);
+  start(lvl);
+  start("Prolongation");
   s.prolongate(x, L - 1, flag, true);
+  stop("Prolongation");
   // b is unchanged on this level since the pre-smoothing, which left its colour-split copy
-  s.smoothSorSweeps(op, x, b, omega, L, flag, post, false, pre > 0);
+  if (post > 0) {
+    start("Smoother");
+    s.smoothSorSweeps(op, x, b, omega, L, flag, post, false, pre > 0);
+    stop("Smoother", post);
+  }
+  stop(lvl);
 }
 
 int Gmg::solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap) {

@@ -6,12 +6,45 @@
 #include <cstdint>
 #include <functional>
 #include <memory>
+#include <string>
+#include <utility>
 #include <vector>
 
 namespace hg {
 
 struct Storage;
 struct DevBuf;
+
+// Hierarchical timers of a solver's phases measured on the device (the reference's
+// walberla::WcTimingTree around GeometricMultigridSolver / CGSolver). start/stop record CUDA
+// events on the storage's stream; intervals are resolved when the tree is read. Each node keeps
+// the waLBerla Timer statistics of its intervals: total, count, min, max, average and variance
+// (seconds). json() writes the tree with a "Remainder" child under every node that has
+// children (the time of the node not covered by them), as the reference writes
+// getCopyWithRemainder() with the waLBerla TimingTree JSON layout: a node is an object with
+// "total", "average", "count", "min", "max", "variance" and one member per child.
+struct TimingTree {
+  struct Node {
+    std::vector<std::pair<std::string, Node>> children;  // in order of first start
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    std::vector<int> pendingCount;  // applications each interval stands for
+    double total = 0, min = 0, max = 0, sumSq = 0;
+    int64_t count = 0;
+    cudaEvent_t open = nullptr;
+    Node& child(const std::string& name);
+  };
+  Node root;
+  std::vector<Node*> stack{&root};
+  std::vector<cudaEvent_t> pool;
+  ~TimingTree();
+  void start(cudaStream_t s, const std::string& name);
+  // `applications` > 1: the interval covers that many applications of the phase (a group of
+  // smoother sweeps); they count separately and share the interval's time equally.
+  void stop(cudaStream_t s, const std::string& name, int applications = 1);
+  void resolve();  // waits for the recorded events
+  void reset();
+  std::string json();
+};
 
 // Captured CUDA graphs of one solver's cycle, keyed by a signature: every device address the
 // cycle reads or writes plus what fixes its kernel arguments. run() replays a graph captured
@@ -54,6 +87,9 @@ struct Gmg {
   bool graphs = true;
   GraphCache cache;
   std::vector<uintptr_t> signature(int x, int b, int L);
+  // device-timed phases (set_timing); cycles run eagerly while it is on
+  std::unique_ptr<TimingTree> timing;
+  void setTiming(bool on);
 
   Storage& s;
   int op, minL, maxL, pre, post;

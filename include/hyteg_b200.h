@@ -384,6 +384,15 @@ int hg_gmg_solve(hg_storage* s, int gmg, int x, int b, int level);
  * solver repeats its cycle; an FP32 solver (precision 4) runs FP64 defect correction: r = b - A x
  * in FP64, one FP32 cycle on A e = r from e = 0 (its coarse CG in FP64), x += e in FP64.
  * history (nullable) receives the relative residual after each iteration. */
+/* Device-timed phases of the multigrid (walberla::WcTimingTree around GeometricMultigridSolver,
+ * GeometricMultigridSolver.hpp:127-234, and CGSolver): on = 1 starts an empty tree (cycles then run
+ * eagerly, not from graphs), 0 drops it. Nodes as in the reference: "Geometric Multigrid Solver" >
+ * "Level L" > "Smoother" (count = sweeps), "Restriction", "Prolongation", "Coarse Grid Solver" >
+ * "CG Solver"; intervals are CUDA events on the storage's stream. */
+int hg_gmg_set_timing(hg_storage* s, int gmg, int on);
+/* The tree as JSON (waLBerla TimingTree layout with "Remainder" nodes, seconds): waits for the
+ * recorded events; *len = the full length; buf (nullable) receives up to cap-1 bytes and a 0. */
+int hg_gmg_timing_json(hg_storage* s, int gmg, char* buf, int64_t cap, int64_t* len);
 /* Cycles are captured as CUDA graphs and replayed (default on) when the coarse level has only
  * vertex and edge DoFs (its CG then runs on the device in one block) and pre + post smoothing
  * steps are even. The first cycle with a given set of buffers runs eagerly, the second is
