@@ -43,6 +43,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--level", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--sqlite", default=None,
+                   help="also append the run's figures as one row to this SQLite file (FixedSizeSQLDB rows)")
     p.add_argument("--sor-schedule", type=int, default=None, choices=[0, 1, 2, 3],
                    help="force one SOR cell-phase schedule on every level instead of autotuning (profiling runs)")
     p.add_argument("--cycle-only", action="store_true",
@@ -277,6 +279,24 @@ def load_traffic(kernel, L):
             return json.load(f).get(kernel, {}).get(str(L))
     except (OSError, ValueError, AttributeError):
         return None
+
+
+def write_sql_row(path, out, L):
+    """The run's headline figures as one row of a FixedSizeSQLDB table (the reference's result
+    export, dataexport/SQL.hpp): the configuration as constant entries, the measurements as
+    variable ones."""
+    from hyteg_b200.sqldb import FixedSizeSQLDB
+    db = FixedSizeSQLDB(path)
+    db.setConstantEntry("workload", out["config"]["workload"])
+    db.setConstantEntry("level", int(L))
+    db.setConstantEntry("n_gpus", int(out["n_gpus"]))
+    db.setConstantEntry("steps", int(out["steps"]))
+    db.setVariableEntry("gdofs", float(out["value"]))
+    db.setVariableEntry("ms_per_cycle", float(out["ms_per_step"]))
+    db.setVariableEntry("e2e_gdofs", float(out["e2e"]["value"]))
+    db.setVariableEntry("roofline_frac", float(out["roofline"]["frac"]))
+    db.setVariableEntry("sm_mhz", float(out.get("clocks", {}).get("sm_mhz") or 0.0))
+    db.writeRowOnRoot()
 
 
 def reassembly_bench(hg, k=4, L=6, reps=5):
@@ -725,6 +745,8 @@ def run_ours(args):
                                    "kind": "reference", "sample": reference_sample_text(L)}
     if rank == 0:
         print(json.dumps(out), flush=True)
+        if args.sqlite:
+            write_sql_row(args.sqlite, out, L)
     del gmg
     if pg is not None:
         pg.destroy_process_group()
