@@ -37,6 +37,13 @@ VERTEX, EDGE, FACE, CELL = 0, 1, 2, 3
 VCYCLE, WCYCLE = 0, 1
 
 
+def split_tables_check(level):
+    """(points, mismatches) of the colour-split SOR tables of a level, checked on the host."""
+    a, b = ctypes.c_int64(), ctypes.c_int64()
+    call("hg_split_tables_check", level, ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
+
+
 def device_count():
     return _capi.lib.hg_device_count()
 

@@ -65,6 +65,7 @@ _SIGS = {
     "hg_mesh_level_size": (c_int, [c_void_p, c_int, P(c_int64)]),
     "hg_mesh_slot_info": (c_int, [c_void_p, c_int, P(c_double), P(ctypes.c_byte), c_int64]),
     "hg_mesh_halo_table": (c_int, [c_void_p, c_int, c_int, P(c_int64), P(c_int64), P(c_int64)]),
+    "hg_split_tables_check": (c_int, [c_int, P(c_int64), P(c_int64)]),
     "hg_mesh_assembly_plan_check": (c_int, [c_void_p, c_int, c_int, P(c_int64), P(c_int64), P(c_int64)]),
     "hg_mesh_cell_stencil": (c_int, [c_void_p, c_int, c_int, c_int, P(c_double)]),
     "hg_mesh_face_stencil": (c_int, [c_void_p, c_int, c_int, c_int, P(c_int), P(c_int), P(c_int), P(c_double), c_int, P(c_int)]),

@@ -747,6 +747,53 @@ int hg_mesh_halo_table(const hg_mesh* m, int level, int group, int64_t* dst, int
   HG_CATCH
 }
 
+int hg_split_tables_check(int level, int64_t* points, int64_t* mismatches) {
+  HG_TRY
+  hg::argCheck(level >= 2 && level <= 10 && points && mismatches, "level in [2, 10] and outputs required");
+  const int64_t w = (int64_t(1) << level) + 1, N = w - 1;
+  auto tet = [](int64_t a) { return a * (a + 1) * (a + 2) / 6; };
+  auto natural = [&](int64_t x, int64_t y, int64_t z) {
+    const int64_t W = w - z;
+    return tet(w) - tet(W) + y * (W + 1) - y * (y + 1) / 2 + x;
+  };
+  auto split = [&](int64_t x, int64_t y, int64_t z) {  // the permutation, from the coordinates
+    const int m = (int)(w - z - y);
+    return natural(0, y, z) + hg::dev::splitSub(m, (int)(x & 3)) + (x >> 2);
+  };
+  // record order C E W N S NW SE TC TW TS TSE BC BE BN BNW
+  static const int off[15][3] = {{0, 0, 0},  {1, 0, 0},  {-1, 0, 0}, {0, 1, 0},   {0, -1, 0},
+                                 {-1, 1, 0}, {1, -1, 0}, {0, 0, 1},  {-1, 0, 1},  {0, -1, 1},
+                                 {1, -1, 1}, {0, 0, -1}, {1, 0, -1}, {0, 1, -1},  {-1, 1, -1}};
+  int64_t total = 0, bad = 0;
+  for (int col = 0; col < 4; ++col) {
+    std::vector<hg::dev::SplitRow> rows;
+    std::vector<unsigned> pts;
+    hg::splitTables(w, col, rows, pts);
+    size_t k = 0;
+    for (int64_t z = 1; z <= N - 3; ++z)
+      for (int64_t y = 1; y <= N - 2 - z; ++y)
+        for (int64_t x = 1; x + y + z <= N - 1; ++x) {
+          if (((x + 2 * y + 3 * z) & 3) != col) continue;
+          ++total;
+          if (k >= pts.size()) {
+            ++bad;
+            continue;
+          }
+          const unsigned e = pts[k++];
+          const hg::dev::SplitRow& r = rows[e >> hg::dev::kSplitJBits];
+          const int64_t j = e & ((1u << hg::dev::kSplitJBits) - 1);
+          bool okp = true;
+          for (int t = 0; t < 15; ++t)
+            okp = okp && r.i[t] + j == split(x + off[t][0], y + off[t][1], z + off[t][2]);
+          bad += okp ? 0 : 1;
+        }
+    bad += (int64_t)(pts.size() - std::min(pts.size(), k));  // table entries without a point
+  }
+  *points = total;
+  *mismatches = bad;
+  HG_CATCH
+}
+
 int hg_mesh_assembly_plan_check(const hg_mesh* m, int level, int form, int64_t* targets, int64_t* terms,
                                 int64_t* mismatches) {
   HG_TRY

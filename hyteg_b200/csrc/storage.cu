@@ -354,6 +354,47 @@ void Storage::communicateSplit(T* buf, T* cells, int L, int groupMask) {
   cudaCheck(cudaGetLastError(), "communicate (split)");
 }
 
+// The interior rows of colour col of a closed macro-cell with w points per edge (x, y, z >= 1,
+// x + y + z <= w - 2), each with its 15 slots at j = 0 in the colour-split order, and the
+// colour's points as (row << kSplitJBits | j), in (z, y, j) order.
+void splitTables(int64_t w, int col, std::vector<dev::SplitRow>& rows, std::vector<unsigned>& points) {
+  const int64_t N = w - 1;
+  argCheck(N <= 4096, "colour-split SOR: level too large");
+  auto tet = [](int64_t a) { return a * (a + 1) * (a + 2) / 6; };
+  auto tri = [](int64_t a) { return a * (a + 1) / 2; };
+  auto rowStart = [&](int64_t z, int64_t y) {
+    const int64_t W = w - z;
+    return tet(w) - tet(W) + y * (W + 1) - y * (y + 1) / 2;
+  };
+  rows.clear();
+  points.clear();
+  for (int64_t z = 1; z <= N - 3; ++z) {
+    const int64_t W = w - z;
+    for (int64_t y = 1; y <= W - 3; ++y) {
+      const int m = (int)(W - y);
+      const int q = (int)((((col - 2 * y - 3 * z) % 4) + 4) % 4);
+      const int j0 = q == 0 ? 1 : 0, jEnd = m - 2 - q >= 0 ? (m - 2 - q) / 4 : -1;
+      if (jEnd < j0) continue;
+      const int qE = (q + 1) & 3, qW = (q + 3) & 3, jE = q == 3 ? 1 : 0, jW = q == 0 ? -1 : 0;
+      const int64_t r0 = rowStart(z, y), rN = r0 + m, rS = r0 - (m + 1);
+      const int64_t rT = r0 + tri(W) - y, rTS = rT - m, rB = r0 - tri(W + 1) + y, rBN = rB + (m + 1);
+      auto sub = [](int mm, int qq) { return (int64_t)dev::splitSub(mm, qq); };
+      dev::SplitRow r;
+      const int64_t v[16] = {r0 + sub(m, q),          r0 + sub(m, qE) + jE,      r0 + sub(m, qW) + jW,
+                             rN + sub(m - 1, q),      rS + sub(m + 1, q),        rN + sub(m - 1, qW) + jW,
+                             rS + sub(m + 1, qE) + jE, rT + sub(m - 1, q),       rT + sub(m - 1, qW) + jW,
+                             rTS + sub(m, q),         rTS + sub(m, qE) + jE,     rB + sub(m + 1, q),
+                             rB + sub(m + 1, qE) + jE, rBN + sub(m, q),          rBN + sub(m, qW) + jW,
+                             0};
+      for (int k = 0; k < 16; ++k) r.i[k] = (int)v[k];
+      argCheck(rows.size() < (size_t(1) << (32 - dev::kSplitJBits)), "colour-split SOR: too many rows");
+      const unsigned id = (unsigned)rows.size();
+      rows.push_back(r);
+      for (int j = j0; j <= jEnd; ++j) points.push_back(id << dev::kSplitJBits | (unsigned)j);
+    }
+  }
+}
+
 // Schedule-3 tables of level L: the halo table with every slot of a cell array replaced by its
 // position in the colour-split order (a permutation inside each row of the cell's array), and
 // per colour the interior rows (their 15 slots at j = 0) and points (row << 10 | j) that
@@ -365,7 +406,6 @@ void Storage::buildSplit(int L) {
   const int64_t w = lay.w, N = w - 1;
   argCheck(N <= 4096, "colour-split SOR: level too large");
   auto tet = [](int64_t a) { return a * (a + 1) * (a + 2) / 6; };
-  auto tri = [](int64_t a) { return a * (a + 1) / 2; };
   auto rowStart = [&](int64_t z, int64_t y) {
     const int64_t W = w - z;
     return tet(w) - tet(W) + y * (W + 1) - y * (y + 1) / 2;
@@ -396,35 +436,11 @@ void Storage::buildSplit(int L) {
     for (size_t i = 0; i < lay.commDst[k].size(); ++i)
       comm.push_back(make_uint2(map(lay.commDst[k][i]), map(lay.commSrc[k][i])));
   const uint2* commSplit = comm.empty() ? ld.comm : (const uint2*)upload(ld.keep, comm, stream);
-  // rows and points per colour (interior: x, y, z >= 1, x + y + z <= N - 1)
+  // rows and points per colour
   for (int col = 0; col < 4; ++col) {
     std::vector<dev::SplitRow> rows;
     std::vector<unsigned> points;
-    for (int64_t z = 1; z <= N - 3; ++z) {
-      const int64_t W = w - z;
-      for (int64_t y = 1; y <= W - 3; ++y) {
-        const int m = (int)(W - y);
-        const int q = (int)((((col - 2 * y - 3 * z) % 4) + 4) % 4);
-        const int j0 = q == 0 ? 1 : 0, jEnd = m - 2 - q >= 0 ? (m - 2 - q) / 4 : -1;
-        if (jEnd < j0) continue;
-        const int qE = (q + 1) & 3, qW = (q + 3) & 3, jE = q == 3 ? 1 : 0, jW = q == 0 ? -1 : 0;
-        const int64_t r0 = rowStart(z, y), rN = r0 + m, rS = r0 - (m + 1);
-        const int64_t rT = r0 + tri(W) - y, rTS = rT - m, rB = r0 - tri(W + 1) + y, rBN = rB + (m + 1);
-        auto sub = [](int mm, int qq) { return (int64_t)dev::splitSub(mm, qq); };
-        dev::SplitRow r;
-        const int64_t v[16] = {r0 + sub(m, q),          r0 + sub(m, qE) + jE,      r0 + sub(m, qW) + jW,
-                               rN + sub(m - 1, q),      rS + sub(m + 1, q),        rN + sub(m - 1, qW) + jW,
-                               rS + sub(m + 1, qE) + jE, rT + sub(m - 1, q),       rT + sub(m - 1, qW) + jW,
-                               rTS + sub(m, q),         rTS + sub(m, qE) + jE,     rB + sub(m + 1, q),
-                               rB + sub(m + 1, qE) + jE, rBN + sub(m, q),          rBN + sub(m, qW) + jW,
-                               0};
-        for (int k = 0; k < 16; ++k) r.i[k] = (int)v[k];
-        argCheck(rows.size() < (size_t(1) << (32 - dev::kSplitJBits)), "colour-split SOR: too many rows");
-        const unsigned id = (unsigned)rows.size();
-        rows.push_back(r);
-        for (int j = j0; j <= jEnd; ++j) points.push_back(id << dev::kSplitJBits | (unsigned)j);
-      }
-    }
+    splitTables(w, col, rows, points);
     ld.splitRows[col] = (const dev::SplitRow*)upload(ld.keep, rows, stream);
     ld.splitPoints[col] = (const unsigned*)upload(ld.keep, points, stream);
     ld.nSplitPoints[col] = (int)points.size();

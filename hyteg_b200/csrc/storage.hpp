@@ -252,6 +252,10 @@ struct Storage {
   void buildTiles(int L);
 };
 
+// Schedule-3 interior rows and points of colour col of a closed macro-cell with w points per edge
+// (storage.cu); shared by the device tables and their host check.
+void splitTables(int64_t w, int col, std::vector<dev::SplitRow>& rows, std::vector<unsigned>& points);
+
 struct Error : std::runtime_error {
   int code;
   Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}

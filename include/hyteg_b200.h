@@ -161,6 +161,11 @@ int hg_mesh_halo_table(const hg_mesh* m, int level, int group, int64_t* dst, int
  * the order C E W N S NW SE TC TW TS TSE BC BE BN BNW. Faces: entries (layer, dx, dy, weight),
  * layer 0 = face, 1 + n = ghost layer of neighbour cell n. Edges / vertices: entries
  * (relative slot, weight). Entry 0 is the diagonal. cap = capacity of the output arrays. */
+/* Verification of the colour-split SOR tables (schedule 3) on the host for level `level`: every
+ * interior point of every colour is listed once, in order, and each of its 15 slots is the split
+ * position of the right neighbour, recomputed from the neighbour's coordinates. points = interior
+ * points checked; mismatches = points whose entry is wrong or missing, plus surplus entries. */
+int hg_split_tables_check(int level, int64_t* points, int64_t* mismatches);
 /* Verification of the device re-assembly's term lists (hg_operator_reassemble) on the host:
  * every stencil entry of (level, form) summed from its terms in order, compared bit for bit with
  * the assembled tables. targets / terms: sizes of the lists; mismatches: entries that differ. */

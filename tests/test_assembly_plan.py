@@ -24,3 +24,14 @@ def test_terms_reproduce_the_tables(mesh, form):
         assert targets >= 16 * nc
         if lev >= 2:
             assert terms > targets // 2
+
+
+def test_colour_split_tables():
+    """The per-colour point and row tables of the colour-split SOR (schedule 3): every interior
+    point once, in order, with its 15 slots equal to the split positions of its neighbours
+    recomputed from their coordinates (levels 2-6)."""
+    for level in range(2, 7):
+        n = 2 ** level
+        points, bad = hg.split_tables_check(level)
+        assert bad == 0, level
+        assert points == (n - 3) * (n - 2) * (n - 1) // 6  # interior points of a macro-cell
