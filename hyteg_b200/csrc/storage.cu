@@ -1585,10 +1585,8 @@ void Storage::reassembleOperator(int id, bool onDevice) {
   if (o.plans.empty()) {
     for (int L = o.minL; L <= o.maxL; ++L) {
       const AssemblyPlan p = buildAssemblyPlan(disc, L, (FormKind)o.form);
-      const dev::StencilDev<double>& sd = o.d[L - o.minL];
       argCheck(p.nCell == (int64_t)topo.cells.size() * 16 && p.nFace == (int64_t)topo.faces.size() * 16,
                "re-assembly: target layout");
-      (void)sd;
       Operator::DevPlan dp;
       dp.first = (const int64_t*)upload(o.keep, p.first, stream);
       dp.terms = (const dev::PlanTermDev*)upload(o.keep, p.terms, stream);
