@@ -47,6 +47,9 @@ def parse():
                    help="also append the run's figures as one row to this SQLite file (FixedSizeSQLDB rows)")
     p.add_argument("--sor-schedule", type=int, default=None, choices=[0, 1, 2, 3],
                    help="force one SOR cell-phase schedule on every level instead of autotuning (profiling runs)")
+    p.add_argument("--sor-schedules", default=None,
+                   help="FP64 schedule per level instead of autotuning, e.g. 2=3,3=1,8=0 (profiling runs, whose "
+                        "serialised launches would mislead the autotuner)")
     p.add_argument("--cycle-only", action="store_true",
                    help="only the kernels, autotuner and timed cycles (profiling runs); implies no serving")
     p.add_argument("--stokes-level", type=int, default=6,
@@ -471,7 +474,9 @@ def fp32_kernels(hg, st, A, x, b, L, Inner, N_in, Nc, timed):
     g = hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 50, 1e-16),
                                     hg.P1toP1LinearRestriction(), hg.P1toP1LinearProlongation(), 0, L, 3, 3,
                                     dtype=np.float32)
-    t_cycle = timed(lambda: g.solve(A, xf, bf, L), 3)
+    # a new solver's first cycles run eagerly (they allocate its buffers) and the next one is
+    # captured into a graph: warm up past the capture so that only replays are timed
+    t_cycle = timed(lambda: g.solve(A, xf, bf, L), 3, warm=4)
     out = {k: {"ms": v * 1e3, "GBs_algorithmic": BYTES[k] / 2 * N_in / v / 1e9} for k, v in t.items()}
     out["cell_sor_single_pass"] = {"ms": t_cells * 1e3, "GBs_algorithmic": BYTES["sor_sweep"] / 2 * Nc / t_cells / 1e9}
     out["vcycle"] = {"ms": t_cycle * 1e3}
@@ -578,8 +583,8 @@ def run_ours(args):
     def ev():
         return torch.cuda.Event(enable_timing=True)
 
-    def timed(fn, reps):
-        for _ in range(2):
+    def timed(fn, reps, warm=2):
+        for _ in range(warm):
             fn()
         torch.cuda.synchronize()
         e0, e1 = ev(), ev()
@@ -629,8 +634,13 @@ def run_ours(args):
     if args.sor_schedule is not None:
         st.set_sor_schedule(args.sor_schedule)
         autotune = {"forced_schedule": args.sor_schedule}
+    if args.sor_schedules:
+        picks = {int(a): int(b) for a, b in (kv.split("=") for kv in args.sor_schedules.split(","))}
+        for lv, sch in picks.items():
+            st.set_sor_schedule_level(lv, sch, np.float64)
+        autotune = {"forced_schedules_fp64": {str(k): v for k, v in picks.items()}}
     for name, dt in (("fp64", np.float64), ("fp32", np.float32)):
-        if args.sor_schedule is not None:
+        if args.sor_schedule is not None or args.sor_schedules:
             break
         picks = st.autotune_sor(2, L, dtype=dt, reps=3)
         autotune[name] = {str(lv): {"schedule": c, "ms_single_pass": t0, "ms_colour_passes": t1,

@@ -269,6 +269,11 @@ class PrimitiveStorage:
         arrays (converted once per group of sweeps)."""
         call("hg_storage_set_sor_schedule", self._h, int(schedule))
 
+    def set_sor_schedule_level(self, level, schedule, dtype=np.float64):
+        """One level's SOR schedule for one precision (-1: the storage-wide schedule)."""
+        prec = {np.dtype(np.float64): 8, np.dtype(np.float32): 4}[np.dtype(dtype)]
+        call("hg_storage_set_sor_schedule_level", self._h, int(level), prec, int(schedule))
+
     def autotune_sor(self, minLevel, maxLevel, dtype=np.float64, reps=3):
         """Times the four SOR schedules per level (groups of three sweeps) and keeps the fastest;
         returns {level: (chosen schedule, ms per sweep of schedules 0, 1, 2, 3)}."""

@@ -213,6 +213,18 @@ int hg_storage_set_sor_schedule(hg_storage* h, int schedule) {
   HG_CATCH
 }
 
+int hg_storage_set_sor_schedule_level(hg_storage* h, int level, int precision, int schedule) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  hg::argCheck(level >= 0 && level <= s.maxLevel(), "level out of range");
+  hg::argCheck(precision == 8 || precision == 4, "precision must be 8 or 4");
+  hg::argCheck(schedule >= -1 && schedule <= 3, "SOR schedule must be -1 (storage default) or 0..3");
+  if ((int)s.sorScheduleLevel.size() < 2 * (s.maxLevel() + 1)) s.sorScheduleLevel.assign(2 * (s.maxLevel() + 1), -1);
+  s.sorScheduleLevel[2 * level + (precision == 4 ? 1 : 0)] = schedule;
+  ++s.generation;
+  HG_CATCH
+}
+
 int hg_storage_autotune_sor(hg_storage* h, int min_level, int max_level, int precision, int reps, double* ms,
                             int* chosen) {
   HG_TRY

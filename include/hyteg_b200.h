@@ -128,6 +128,9 @@ int hg_storage_set_sor_schedule(hg_storage* s, int schedule);
  * 0, 1, 2, 3 per level; chosen (nullable): the schedule kept per level. */
 int hg_storage_autotune_sor(hg_storage* s, int min_level, int max_level, int precision, int reps, double* ms,
                             int* chosen);
+/* The SOR schedule of one level and precision (8 or 4), as the autotuner sets it (-1: back to the
+ * storage-wide hg_storage_set_sor_schedule). */
+int hg_storage_set_sor_schedule_level(hg_storage* s, int level, int precision, int schedule);
 /* Topology export: for kind HG_VERTEX ids[0..2]=unused, coords[3]; HG_EDGE ids[2]; HG_FACE ids[3];
  * HG_CELL ids[4]; flag = mesh boundary flag. */
 int hg_primitive_vertices(const hg_storage* s, int kind, int prim, int ids[4], double coords[3], int* flag);
