@@ -1899,11 +1899,25 @@ static __global__ void __launch_bounds__(kBlock)
 // ---------------------------------------------------------------------------------------
 // Halo refresh: copy slots <- owner slots (one gather; every source is an owned slot).
 // ---------------------------------------------------------------------------------------
+// Four entries per thread and round, table reads first, so that four independent gathers are in
+// flight; every source is an owned slot and every destination a copy slot, so the order of the
+// copies does not matter.
+constexpr int kCommUnroll = 4;
 template <class T>
 __global__ void commGatherKernel(T* buf, const uint2* __restrict__ table, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const uint2 t = table[i];
-    buf[t.x] = buf[t.y];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < n; i0 += kCommUnroll * stride) {
+    uint2 t[kCommUnroll];
+    T v[kCommUnroll];
+#pragma unroll
+    for (int k = 0; k < kCommUnroll; ++k)
+      if (i0 + k * stride < n) t[k] = table[i0 + k * stride];
+#pragma unroll
+    for (int k = 0; k < kCommUnroll; ++k)
+      if (i0 + k * stride < n) v[k] = buf[t[k].y];
+#pragma unroll
+    for (int k = 0; k < kCommUnroll; ++k)
+      if (i0 + k * stride < n) buf[t[k].x] = v[k];
   }
 }
 
