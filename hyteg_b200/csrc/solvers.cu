@@ -137,8 +137,10 @@ void TimingTree::start(cudaStream_t st, const std::string& name) {
 void TimingTree::stop(cudaStream_t st, const std::string& name, int applications) {
   argCheck(stack.size() > 1, "timing tree: stop without start");
   Node& n = *stack.back();
-  argCheck(stack[stack.size() - 2]->child(name).open == n.open && n.open != nullptr,
-           "timing tree: \"" + name + "\" is not the innermost open timer");
+  const Node* named = nullptr;  // look the name up without inserting (an insertion could move n)
+  for (auto& c : stack[stack.size() - 2]->children)
+    if (c.first == name) named = &c.second;
+  argCheck(named == &n && n.open != nullptr, "timing tree: \"" + name + "\" is not the innermost open timer");
   cudaEvent_t e;
   if (!pool.empty()) {
     e = pool.back();
