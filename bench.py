@@ -47,6 +47,8 @@ def parse():
                    help="also append the run's figures as one row to this SQLite file (FixedSizeSQLDB rows)")
     p.add_argument("--sor-schedule", type=int, default=None, choices=[0, 1, 2, 3],
                    help="force one SOR cell-phase schedule on every level instead of autotuning (profiling runs)")
+    p.add_argument("--p2-only", action="store_true",
+                   help="only the P2 kernels (apply, SOR sweep, V-cycle) on P2 level LEVEL-2, one JSON line")
     p.add_argument("--sor-schedules", default=None,
                    help="FP64 schedule per level instead of autotuning, e.g. 2=3,3=1,8=0 (profiling runs, whose "
                         "serialised launches would mislead the autotuner)")
@@ -402,6 +404,13 @@ def p2_kernels(hg, st, L2, timed):
     t_sor = timed(lambda: A.smooth_sor(x, b, 1.0, L2, Inner), 3)
     g = hg.P2GeometricMultigridSolver(st, A, 0, L2, 3, 3, 1.0)
     t_cycle = timed(lambda: g.solve(x, b, L2), 2, warm=4)  # past the solver's graph capture
+    import torch
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("p2_ops")  # one sweep and one apply, for a launch list
+    A.smooth_sor(x, b, 1.0, L2, Inner)
+    A.apply(x, y, L2, hg.Inner)
+    st.synchronize()
+    torch.cuda.nvtx.range_pop()
     return {"p2_level": L2, "inner_dofs": n_in,
             "apply": {"ms": t_apply * 1e3, "gdofs": n_in / t_apply / 1e9, "GBs_algorithmic": 16 * n_in / t_apply / 1e9},
             "sor_sweep": {"ms": t_sor * 1e3, "gdofs": n_in / t_sor / 1e9},
@@ -594,6 +603,11 @@ def run_ours(args):
         e1.record(stream)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps * 1e-3
+
+    if args.p2_only:  # profiling runs of the P2 path alone
+        if rank == 0:
+            print(json.dumps({"p2": p2_kernels(hg, st, L - 2, timed)}), flush=True)
+        return
 
     # --- standalone kernels on the seeded source vector ----------------------------------
     x.from_numpy(L, host_b.numpy())
