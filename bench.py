@@ -213,9 +213,13 @@ def dist_setup(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        backend = os.environ.get("HG_BENCH_BACKEND", "nccl")  # gloo: the rank plumbing on CPU (tests)
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
 
@@ -224,7 +228,7 @@ def max_over_ranks(v, pg):
     if pg is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device="cuda" if pg.get_backend() == "nccl" else "cpu")
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
