@@ -127,65 +127,26 @@ class Clocks:
 # reference CPU kernels (oracle/_ref, compiled from the reference's own generated kernels)
 # ----------------------------------------------------------------------------------------
 def reference_cpu_pass(L, steps, warmup, threads):
-    """Finest-level cell-interior work of one V(3,3) cycle on the 48 macro-cells of the cube
-    with the reference's generated kernels (sor_3D_macrocell_P1 x 6, apply (residual),
-    restrict_3D_macrocell_P1_pull_additive, prolongate_3D_macrocell_P1_push_additive),
-    parallel over macro-cells on `threads` host threads. Returns seconds per pass."""
+    """Whole V(3,3) cycles of the reference's P1 multigrid on the 48-tet cube, in the reference's
+    own per-primitive layout and through its generated kernels (oracle/_ref: cell and face SOR,
+    face and cell apply, assign, restriction, prolongation, face <-> cell halo copies), levels L
+    .. 1, on `threads` host threads. Mesh, stencils and neighbour counts come from the oracle only
+    (the product library is not loaded). Returns (seconds per cycle list, inner DoFs the cycle
+    updates on level L, threads used), or None without oracle/_ref."""
     from oracle import oracle
-    import hyteg_b200 as hg
-    ref = oracle.ref_lib()
-    if ref is None:
+    if oracle.ref_lib() is None:
         return None
-    mesh = hg.HostMesh.cuboid((0, 0, 0), (1, 1, 1), 2, 2, 2, L)
-    nv, ne, nf, nc = mesh.counts()
-    w = 2 ** L + 1
-    wc = 2 ** (L - 1) + 1
-    size = w * (w + 1) * (w + 2) // 6
-    csize = wc * (wc + 1) * (wc + 2) // 6
-    rng = np.random.default_rng(1)
-    cells = []
-    for c in range(nc):
-        st = np.ascontiguousarray(mesh.cell_stencil(L, 0, c))
-        verts = mesh.primitive(hg.CELL, c)[0]
-        ncount = lambda kind, prim: float(len(mesh.neighbours(kind, prim, hg.CELL)))  # noqa: E731
-        # neighbour counts of the cell's edges, faces and vertices (P1toP1LinearRestriction.cpp:186-233)
-        edges = [mesh.neighbours(hg.VERTEX, verts[a], hg.EDGE) for a in range(4)]
-        epairs = [(0, 1), (0, 2), (1, 2), (0, 3), (1, 3), (2, 3)]
-        eid = []
-        for a, b in epairs:
-            common = set(edges[a]) & set(edges[b])
-            eid.append(common.pop())
-        fverts = [(0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3)]
-        fid = []
-        for t in fverts:
-            s = set(mesh.neighbours(hg.VERTEX, verts[t[0]], hg.FACE))
-            for k in t[1:]:
-                s &= set(mesh.neighbours(hg.VERTEX, verts[k], hg.FACE))
-            fid.append(s.pop())
-        nE = np.array([ncount(hg.EDGE, e) for e in eid])
-        nF = np.array([ncount(hg.FACE, f) for f in fid])
-        nV = np.array([ncount(hg.VERTEX, v) for v in verts])
-        cells.append(dict(u=rng.uniform(-1, 1, size), f=rng.uniform(-1, 1, size), r=np.zeros(size),
-                          c=np.zeros(csize), w=st, nE=nE, nF=nF, nV=nV))
-    dp = oracle.dp
-
-    def work(cd):
-        for _ in range(3):
-            ref.ref_sor_cell(dp(cd["u"]), dp(cd["f"]), L, dp(cd["w"]), 1.0)
-        ref.ref_apply_cell(dp(cd["r"]), dp(cd["u"]), L, dp(cd["w"]), 0)
-        ref.ref_restrict_cell(dp(cd["c"]), dp(cd["r"]), L - 1, dp(cd["nE"]), dp(cd["nF"]), dp(cd["nV"]))
-        ref.ref_prolongate_cell(dp(cd["c"]), dp(cd["u"]), L - 1, dp(cd["nE"]), dp(cd["nF"]), dp(cd["nV"]))
-        for _ in range(3):
-            ref.ref_sor_cell(dp(cd["u"]), dp(cd["f"]), L, dp(cd["w"]), 1.0)
-
-    times = []
-    with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as ex:
-        for i in range(warmup + steps):
-            t0 = time.perf_counter()
-            list(ex.map(work, cells))
-            if i >= warmup:
-                times.append(time.perf_counter() - t0)
-    return times
+    coords, tets = oracle.cuboid_mesh((0, 0, 0), (1, 1, 1), 2, 2, 2)
+    rc = oracle.RefCycle(coords, tets, L, 3, 3, seed=1)
+    times, used = [], threads
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        used = rc.run(threads)
+        if i >= warmup:
+            times.append(time.perf_counter() - t0)
+    dofs = rc.timed_dofs()
+    del rc
+    return times, dofs, used
 
 
 def host_threads():
@@ -196,10 +157,11 @@ def host_threads():
 
 
 def reference_sample_text(L):
-    return ("finest-level cell-interior work of one V(3,3) cycle (6 lexicographic SOR sweeps, residual, restriction, "
-            "prolongation) on the 48 macro-cells of the level-%d cube with the reference's generated kernels "
-            "(oracle/_ref), threads over macro-cells; faces/edges/vertices and coarser levels not included "
-            "(<3%% and ~1/7 of the work)" % L)
+    return ("one whole V(3,3) cycle per step on levels %d..1 of the 48-tet cube in the reference's own layout, through "
+            "its generated kernels compiled from its sources (oracle/_ref): face and cell SOR, face and cell apply, "
+            "r = b - Ax, restriction, prolongation, face<->cell halo copies; macro-primitives over host threads; "
+            "value = cell- and face-interior DoFs of level %d (the vertex/edge phases, 0.005%% of the inner DoFs, "
+            "and the level-0 CG are not run)" % (L, L))
 
 
 # ----------------------------------------------------------------------------------------
@@ -248,9 +210,9 @@ def run_reference(args):
             out = {"impl": "reference", "unavailable": "oracle/_ref (reference kernels) was not built"}
         else:
             thr = host_threads()
-            times = reference_cpu_pass(L, args.steps, args.warmup, thr)
+            times, dofs, thr = reference_cpu_pass(L, args.steps, args.warmup, thr)
             t = float(np.mean(times))
-            v = inner_dofs(L) / t / 1e9
+            v = dofs / t / 1e9
             out = {"impl": "reference", "metric": "GDoF/s", "value": v, "unit": "GDoF/s", "n_gpus": args.gpus,
                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
                    "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -565,6 +527,40 @@ def time_to_solution(hg, st, A, L, N_in, Inner):
     return out
 
 
+def convergence_by_level(hg, st, L, cycles=20):
+    """Per-level V(3,3) convergence on the manufactured problem (b = M I(3 pi^2 u), x0 = 0, CG on
+    level 0): the residual factor of each of `cycles` cycles on levels 3 .. L, the mean of the
+    first ten and the asymptotic factor (geometric mean of cycles 15-20, or of the last six above
+    the rounding floor of the residual)."""
+    inn = hg.Inner | hg.NeumannBoundary
+    out = {}
+    for lv in range(3, L + 1):
+        A = hg.P1ConstantLaplaceOperator(st, 0, lv)
+        M = hg.P1ConstantMassOperator(st, lv, lv)
+        x, b, r, f = (hg.P1Function(n, st, 0, lv) for n in ("cx", "cb", "cr", "cf"))
+        f.interpolate_sines(3 * np.pi ** 2, 1.0, lv)
+        M.apply(f, b, lv, hg.Inner)
+        g = hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 50, 1e-16),
+                                        hg.P1toP1LinearRestriction(), hg.P1toP1LinearProlongation(), 0, lv, 3, 3)
+
+        def res():
+            A.residual(x, b, r, lv, inn)
+            return float(np.sqrt(r.dotGlobal(r, lv, inn)))
+
+        h = [res()]
+        for _ in range(cycles):
+            g.solve(A, x, b, lv)
+            h.append(res())
+        fac = [h[i + 1] / h[i] for i in range(cycles)]
+        above = [i for i in range(cycles) if h[i + 1] / h[0] > 1e-12]
+        tail = above[-6:] if len(above) >= 6 else list(range(cycles - 6, cycles))
+        out[str(lv)] = {"factors": fac, "mean_first_10": float(np.exp(np.mean(np.log(fac[:10])))),
+                        "asymptotic": float(np.exp(np.mean(np.log([fac[i] for i in tail])))),
+                        "asymptotic_cycles": [tail[0] + 1, tail[-1] + 1]}
+        del g, A, M, x, b, r, f
+    return out
+
+
 def run_ours(args):
     import torch
     import hyteg_b200 as hg
@@ -667,6 +663,8 @@ def run_ours(args):
 
     # --- time to solution: FP64 GMG vs mixed precision (FP32 cycles inside FP64 defect correction)
     solve = None if args.cycle_only else time_to_solution(hg, st, A, L, N_in, Inner)
+    if solve is not None:
+        solve["convergence_by_level"] = convergence_by_level(hg, st, L)
     x.from_numpy(L, host_b.numpy())
 
     # --- the timed region: K V(3,3) cycles --------------------------------------------------
@@ -692,40 +690,51 @@ def run_ours(args):
     value = world * N_in * args.steps / t_max / 1e9
 
     # --- end to end through the public API with host buffers --------------------------------
-    # Every step uploads its right-hand side from pinned host memory and reads its residual norm
-    # back. The upload of step k + 1 runs on a copy stream into the second of two right-hand-side
-    # hierarchies while step k solves (double buffering); the first upload is not overlapped.
+    # Every step uploads its right-hand side from pinned host memory, runs one V(3,3) cycle, and
+    # downloads the step's result -- the whole level buffer of the solution x -- into pinned host
+    # memory. Two (x, b) pairs alternate: the upload of step k + 1 (one copy stream) and the
+    # download of step k's solution (a second copy stream) overlap the cycle of step k + 1 on the
+    # other pair; events order each buffer's copies against the cycles that use it. The first
+    # upload and the last download are not overlapped.
+    x2 = hg.P1Function("x2", st, 0, L)
     b2 = hg.P1Function("b2", st, 0, L)
-    bufs = (b, b2)
-    copy_stream = torch.cuda.Stream()
+    xs2, bs2 = (x, x2), (b, b2)
     host_np = host_b.numpy()
+    host_x = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    x2.from_numpy(L, host_np)
     b2.from_numpy(L, host_np)
-    for _ in range(3):  # the cycles on the second buffer run eagerly, then from their own graph
-        gmg.solve(A, x, b2, L)
+    for _ in range(3):  # the cycles on the second pair run eagerly, then from their own graph
+        gmg.solve(A, x2, b2, L)
     torch.cuda.synchronize()
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
     barrier(pg)
-    copied = [ev(), ev()]
-    released = [ev(), ev()]
+    uploaded, solved, downloaded = [ev(), ev()], [ev(), ev()], [ev(), ev()]
     e0, e1 = ev(), ev()
     e0.record(stream)
-    copy_stream.wait_stream(stream)
-    bufs[0].upload_async(L, host_np, copy_stream.cuda_stream)
-    copied[0].record(copy_stream)
+    up.wait_stream(stream)
+    bs2[0].upload_async(L, host_np, up.cuda_stream)
+    uploaded[0].record(up)
     for k in range(args.steps):
         cur = k % 2
-        if k + 1 < args.steps:  # the next step's input, behind the step that last used its buffer
+        if k + 1 < args.steps:  # the next step's input, behind the cycle that last read its buffer
             if k >= 1:
-                copy_stream.wait_event(released[1 - cur])
-            bufs[1 - cur].upload_async(L, host_np, copy_stream.cuda_stream)
-            copied[1 - cur].record(copy_stream)
-        stream.wait_event(copied[cur])
-        gmg.solve(A, x, bufs[cur], L)
-        A.residual(x, bufs[cur], r, L, Inner)
-        _ = r.dotGlobal(r, L, Inner)           # D2H of the step's result (residual norm)
-        released[cur].record(stream)
+                up.wait_event(solved[1 - cur])
+            bs2[1 - cur].upload_async(L, host_np, up.cuda_stream)
+            uploaded[1 - cur].record(up)
+        stream.wait_event(uploaded[cur])
+        if k >= 2:
+            stream.wait_event(downloaded[cur])  # the pair's previous solution has left the device
+        gmg.solve(A, xs2[cur], bs2[cur], L)
+        solved[cur].record(stream)
+        down.wait_event(solved[cur])
+        xs2[cur].download_async(L, host_x[cur].numpy(), down.cuda_stream)
+        downloaded[cur].record(down)
+    stream.wait_stream(down)
     e1.record(stream)
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) * 1e-3, pg)
+    e2e_finite = bool(np.isfinite(host_x[(args.steps - 1) % 2].numpy()[:1000]).all())
+    del x2, b2
 
     # --- where one cycle's time goes: the solver's timing tree (device events, eager cycle) ----
     gmg.set_timing(A, True)
@@ -753,9 +762,12 @@ def run_ours(args):
                      "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": BYTES["sor_sweep"] * Nc},
         "e2e": {"value": world * N_in * args.steps / t_e2e / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": n * 8,
-                "d2h_bytes_per_step": 8,
-                "pipelining": "two right-hand-side buffers: the pinned-host upload of step k+1 (copy stream) "
-                              "overlaps the cycle of step k; the first upload is not overlapped"},
+                "d2h_bytes_per_step": n * 8, "ms_per_step": t_e2e / args.steps * 1e3,
+                "result_downloaded": "the whole level-%d buffer of the solution x every step (finite: %s)"
+                                     % (L, e2e_finite),
+                "pipelining": "two (x, b) pairs alternate: the pinned-host upload of step k+1 and the download of "
+                              "step k's solution (two copy streams) overlap the cycle of step k+1; the first "
+                              "upload and the last download are not overlapped"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "kernels": kernels,
@@ -767,14 +779,15 @@ def run_ours(args):
         out["serving"] = serving_bench(hg, args.serving_requests)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         thr = host_threads()
-        times = reference_cpu_pass(L, 5, 1, thr)  # median of five passes on all host threads
-        if times:
-            out["cpu_baseline"] = {"value": inner_dofs(L) / statistics.median(times) / 1e9, "unit": "GDoF/s",
+        ref = reference_cpu_pass(L, 5, 1, thr)  # median of five cycles on all host threads
+        if ref:
+            times, dofs, thr = ref
+            out["cpu_baseline"] = {"value": dofs / statistics.median(times) / 1e9, "unit": "GDoF/s",
                                    "cores": thr, "kind": "reference", "repeats": len(times),
                                    "sample": reference_sample_text(L)}
-            one = reference_cpu_pass(L, 1, 0, 1)  # and one pass on a single core
+            one = reference_cpu_pass(L, 1, 0, 1)  # and one cycle on a single core
             if one:
-                out["cpu_baseline"]["single_core_value"] = inner_dofs(L) / one[0] / 1e9
+                out["cpu_baseline"]["single_core_value"] = one[1] / one[0][0] / 1e9
     if rank == 0:
         print(json.dumps(out), flush=True)
         if args.sqlite:

@@ -355,6 +355,15 @@ class P1Function:
         call("hg_function_upload_async", self.storage.handle, self.id, level, a.ctypes.data_as(ctypes.c_void_p), a.size,
              ctypes.c_void_p(stream))
 
+    def download_async(self, level, a, stream):
+        """Enqueue the download of the level buffer into the contiguous host array `a` (pinned
+        memory for an asynchronous copy) on the CUDA stream handle `stream`, without waiting; `a`
+        holds the values once the stream has passed the copy."""
+        if a.dtype != self.dtype or not a.flags["C_CONTIGUOUS"] or not a.flags["WRITEABLE"]:
+            raise ValueError("download_async: a writeable contiguous array of the function's precision is required")
+        call("hg_function_download_async", self.storage.handle, self.id, level, a.ctypes.data_as(ctypes.c_void_p),
+             a.size, ctypes.c_void_p(stream))
+
     def communicate(self, level):
         call("hg_communicate", self.storage.handle, self.id, level)
 

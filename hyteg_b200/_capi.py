@@ -78,6 +78,7 @@ _SIGS = {
     "hg_function_device_ptr": (c_int, [c_void_p, c_int, c_int, P(c_void_p)]),
     "hg_function_upload": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64]),
     "hg_function_upload_async": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p]),
+    "hg_function_download_async": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p]),
     "hg_function_download": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64]),
     "hg_communicate": (c_int, [c_void_p, c_int, c_int]),
     "hg_interpolate_const": (c_int, [c_void_p, c_int, c_double, c_int, c_uint]),

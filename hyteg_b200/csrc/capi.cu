@@ -359,6 +359,17 @@ int hg_function_download(hg_storage* h, int fn, int level, void* host, int64_t n
   HG_CATCH
 }
 
+int hg_function_download_async(hg_storage* h, int fn, int level, void* host, int64_t n, void* stream) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  hg::Function& f = s.fn(fn);
+  hg::argCheck(host != nullptr, "null host buffer");
+  hg::argCheck(n == s.disc.level(level).total, "download size must equal the level buffer size");
+  hg::cudaCheck(cudaMemcpyAsync(host, s.data(fn, level), (size_t)n * f.prec, cudaMemcpyDeviceToHost, (cudaStream_t)stream),
+                "download");
+  HG_CATCH
+}
+
 int hg_communicate(hg_storage* h, int fn, int level) {
   HG_TRY
   S(h).communicate(fn, level, (1 << hg::G_COUNT) - 1);

@@ -8,7 +8,6 @@
 // below, which every GPU that loads the library holds until the process exits.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/hyteg_b200.h"
@@ -23,34 +22,36 @@ namespace {
 constexpr int kMaxPartials = 65536;
 static __device__ __align__(256) double g_dotScratch[kMaxPartials];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-double* g_scratch[kMaxDevices] = {};
+// Makes the storage's device current for the lifetime of the guard (its stream and buffers
+// belong to that device) and restores the caller's device afterwards.
+struct DeviceGuard {
+  int prev = -1;
+  cudaError_t err = cudaSuccess;
+  explicit DeviceGuard(int dev) {
+    err = cudaGetDevice(&prev);
+    if (err == cudaSuccess && prev != dev) err = cudaSetDevice(dev);
+    else if (err == cudaSuccess) prev = -1;  // already current: nothing to restore
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
-// Device address of g_dotScratch on the current device, looked up on the first call per device.
-// (In host code the symbol g_dotScratch is a host-side stand-in, not a device address.)
-int scratchForCurrentDevice(double** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) {
-    hg::g_lastError = std::string("cudaGetDevice: ") + cudaGetErrorString(e);
-    return HG_ERR_CUDA;
-  }
-  if (dev < 0 || dev >= kMaxDevices) {
-    hg::g_lastError = "device ordinal beyond the supported range";
-    return HG_ERR_CUDA;
-  }
-  std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_scratch[dev]) {
+// Device address of g_dotScratch on the storage's device (current when called), looked up on
+// the storage's first call and kept in the storage. In host code the symbol g_dotScratch is a
+// host-side stand-in, not a device address. A storage never outlives a cudaDeviceReset of its
+// device (its buffers would be gone too), so a kept address is never stale.
+int scratchFor(hg::Storage& s, double** out) {
+  if (!s.noallocScratch) {
     void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_dotScratch);
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_dotScratch);
     if (e != cudaSuccess) {
       hg::g_lastError = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
       return HG_ERR_CUDA;
     }
-    g_scratch[dev] = static_cast<double*>(p);
+    s.noallocScratch = static_cast<double*>(p);
   }
-  *out = g_scratch[dev];
+  *out = s.noallocScratch;
   return HG_OK;
 }
 
@@ -70,8 +71,13 @@ extern "C" int hg_dot_noalloc(hg_storage* h, const void* a, const void* b, int p
       throw hg::Error(HG_ERR_ARG, "hg_dot_noalloc: level " + std::to_string(level) + " needs " + std::to_string(nb) +
                                       " partial sums, more than the " + std::to_string(kMaxPartials) +
                                       " of its static scratch; use hg_dot");
+    DeviceGuard guard(s.device);
+    if (guard.err != cudaSuccess) {
+      hg::g_lastError = std::string("hg_dot_noalloc: selecting the storage's device: ") + cudaGetErrorString(guard.err);
+      return HG_ERR_CUDA;
+    }
     double* scratch = nullptr;
-    const int rc = scratchForCurrentDevice(&scratch);
+    const int rc = scratchFor(s, &scratch);
     if (rc != HG_OK) return rc;
     // Every slot the reduction reads is written first by this call's own partial-sum kernel,
     // so nothing of the previous call's contents needs clearing.

@@ -66,6 +66,7 @@ static unsigned char dofType(int meshFlag) {
 }
 
 Storage::Storage(const Topology& topo, int maxLevel) : disc(topo, maxLevel) {
+  cudaCheck(cudaGetDevice(&device), "cudaGetDevice");
   cudaCheck(cudaStreamCreateWithFlags(&ownStream, cudaStreamNonBlocking), "cudaStreamCreate");
   cudaCheck(cudaFuncSetAttribute(dev::cellSorWaveKernel<double, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)dev::waveSmemBytes<double, 0>(dev::kWaveMaxN)),

@@ -129,6 +129,8 @@ struct Storage {
   int maxLevel() const { return disc.maxLevel(); }
 
   Discretization disc;
+  int device = 0;                       // CUDA device current at creation; owns stream and buffers
+  double* noallocScratch = nullptr;     // device address of hg_dot_noalloc's static scratch on `device`
   cudaStream_t ownStream = nullptr;
   cudaStream_t stream = nullptr;
   std::deque<LevelData> levels;

@@ -196,6 +196,12 @@ int hg_function_download(hg_storage* s, int fn, int level, void* host, int64_t n
  * asynchronous copy) alive until it completes. For pipelining the next input's copy with the
  * current solve. */
 int hg_function_upload_async(hg_storage* s, int fn, int level, const void* host, int64_t n, void* stream);
+/* The download enqueued on the caller's CUDA stream, without waiting (the counterpart of
+ * hg_function_upload_async): the caller orders it after the work that produced the values (an
+ * event recorded on the storage's stream) and before the next work that changes them, and reads
+ * the host buffer only after the copy completed. For pipelining a result's copy with the next
+ * solve. */
+int hg_function_download_async(hg_storage* s, int fn, int level, void* host, int64_t n, void* stream);
 int hg_communicate(hg_storage* s, int fn, int level);
 int hg_interpolate_const(hg_storage* s, int fn, double value, int level, unsigned flag);
 /* Built-in expressions at the flagged DoFs (then the halo is refreshed): expr 0 =
@@ -213,9 +219,11 @@ int hg_dot(hg_storage* s, int a, int b, int level, unsigned flag, double* out);
  * the reference. a, b: device pointers to one level buffer each (hg_function_device_ptr) of the
  * given precision (8 or 4); result: device pointer to one double, written on the storage's
  * stream (no synchronisation, no host copy). The scratch is a static device array of 65,536
- * partial sums: levels that need more blocks are rejected with HG_ERR_ARG. The first call on a
- * device looks up the array's device address, so make it before any stream capture. Every call
- * shares the one array: calls that overlap on the GPU (other streams, other threads) race. */
+ * partial sums: levels that need more blocks are rejected with HG_ERR_ARG. The call runs with the
+ * storage's device current (the device that was current when the storage was created) and then
+ * restores the caller's device. The first call on a storage looks up the array's device address
+ * on that device, so make it before any stream capture. Every call shares the one array: calls
+ * that overlap on the GPU (other streams, other threads) race. */
 int hg_dot_noalloc(hg_storage* s, const void* a, const void* b, int precision, int level, unsigned flag,
                    double* result);
 
@@ -388,10 +396,6 @@ int hg_gmg_create(hg_storage* s, int op, int min_level, int max_level, int pre_s
 int hg_gmg_destroy(hg_storage* s, int gmg);
 /* One cycle: x <- MG(x, b) on max_level (x, b of the solver's precision). */
 int hg_gmg_solve(hg_storage* s, int gmg, int x, int b, int level);
-/* Iterate to ||b - A x|| <= tol ||b - A x0|| (at most max_iter iterations); x, b are FP64. An FP64
- * solver repeats its cycle; an FP32 solver (precision 4) runs FP64 defect correction: r = b - A x
- * in FP64, one FP32 cycle on A e = r from e = 0 (its coarse CG in FP64), x += e in FP64.
- * history (nullable) receives the relative residual after each iteration. */
 /* Device-timed phases of the multigrid (walberla::WcTimingTree around GeometricMultigridSolver,
  * GeometricMultigridSolver.hpp:127-234, and CGSolver): on = 1 starts an empty tree (cycles then run
  * eagerly, not from graphs), 0 drops it. Nodes as in the reference: "Geometric Multigrid Solver" >
@@ -407,6 +411,10 @@ int hg_gmg_timing_json(hg_storage* s, int gmg, char* buf, int64_t cap, int64_t* 
  * captured; any change of a buffer address (for example an odd number of SOR sweeps on one of
  * the functions elsewhere) selects or captures another graph. Results are identical either way. */
 int hg_gmg_set_graphs(hg_storage* s, int gmg, int enable);
+/* Iterate to ||b - A x|| <= tol ||b - A x0|| (at most max_iter iterations); x, b are FP64. An FP64
+ * solver repeats its cycle; an FP32 solver (precision 4) runs FP64 defect correction: r = b - A x
+ * in FP64, one FP32 cycle on A e = r from e = 0 (its coarse CG in FP64), x += e in FP64.
+ * history (nullable) receives the relative residual after each iteration. */
 int hg_gmg_solve_to(hg_storage* s, int gmg, int x, int b, int level, double tol, int max_iter, int* iterations,
                     double* rel_residual, double* history, int history_cap);
 

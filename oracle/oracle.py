@@ -399,3 +399,102 @@ def cuboid_mesh(lo, hi, nx, ny, nz):
                 for t in range(6):
                     tets.append([vid(ix + off[m][0], iy + off[m][1], iz + off[m][2]) for m in tnode[t]])
     return np.array(coords), np.array(tets, dtype=np.int32)
+
+
+class RefCycle:
+    """One V(pre, post) cycle of the reference's P1 multigrid in the reference's own layout,
+    through the reference's generated kernels (oracle/ref_cycle.cpp in oracle/_ref): the timed
+    CPU baseline. Everything it needs comes from the oracle: the macro-mesh (`coords`, `tets`,
+    e.g. `cuboid_mesh`), each cell's 15-point stencil and its one-sided face stencil on level 2
+    (`Oracle.cell_local_stencil`; level l uses them scaled by 2^(2 - l)), each face's neighbour
+    cells with their cell-local vertex IDs, and the neighbour-cell counts of every cell's edges,
+    faces and vertices (the scaling of the transfer kernels, P1toP1LinearRestriction.cpp:186-233).
+    The right-hand side and initial guess are seeded values in [-1, 1)."""
+
+    EDGES = [(0, 1), (0, 2), (1, 2), (0, 3), (1, 3), (2, 3)]
+    FACES = [(0, 1, 2), (0, 1, 3), (0, 2, 3), (1, 2, 3)]
+
+    def __init__(self, coords, tets, L, pre=3, post=3, seed=1):
+        r = ref_lib()
+        if r is None:
+            raise RuntimeError("oracle/_ref (the reference's kernels) was not built")
+        self._r = r
+        r.ref_cycle_create.restype = c_void_p
+        r.ref_cycle_create.argtypes = [c_int, c_int, c_int, P(c_double), P(c_double), P(c_int), P(c_int), P(c_int),
+                                       P(c_double), c_int, c_int, ctypes.c_uint]
+        r.ref_cycle_destroy.argtypes = [c_void_p]
+        r.ref_cycle_destroy.restype = None
+        r.ref_cycle_run.argtypes = [c_void_p, c_int, c_double]
+        r.ref_cycle_run.restype = c_int
+        r.ref_cycle_checksum.argtypes = [c_void_p]
+        r.ref_cycle_checksum.restype = c_double
+        tets = [list(map(int, t)) for t in tets]
+        nc = len(tets)
+        orc = Oracle(coords, np.array(tets, dtype=np.int32), 2)
+        cellW = np.array([orc.cell_local_stencil(2, c, 1, 1, 1) for c in range(nc)])
+        del orc
+        faces = {}
+        for c, t in enumerate(tets):
+            for fl in self.FACES:
+                key = tuple(sorted(t[i] for i in fl))
+                faces.setdefault(key, []).append(c)
+        keys = sorted(faces)
+        nf = len(keys)
+        faceNc = np.zeros(nf, dtype=np.int32)
+        faceCell = np.zeros((nf, 2), dtype=np.int32)
+        faceLid = np.zeros((nf, 2, 3), dtype=np.int32)
+        faceW = np.zeros((nf, 2, 15))
+        # one-sided face stencil of each (face, neighbour cell) in the face-local frame (x along
+        # the face's vertices 0 -> 1, y along 0 -> 2, z into the cell): the stencil at a face point
+        # of the cell re-ordered as (face vertices, opposite vertex)
+        sides = []
+        for f, key in enumerate(keys):
+            cells = sorted(faces[key])
+            faceNc[f] = len(cells)
+            for k, c in enumerate(cells):
+                faceCell[f, k] = c
+                faceLid[f, k] = [tets[c].index(v) for v in key]
+                sides.append(list(key) + [v for v in tets[c] if v not in key])
+        so = Oracle(coords, np.array(sides, dtype=np.int32), 2)
+        i = 0
+        for f in range(nf):
+            for k in range(faceNc[f]):
+                faceW[f, k] = so.cell_local_stencil(2, i, 1, 1, 0)
+                i += 1
+        del so
+        vcount, ecount = {}, {}
+        for t in tets:
+            for v in t:
+                vcount[v] = vcount.get(v, 0) + 1
+            for a, b in self.EDGES:
+                e = tuple(sorted((t[a], t[b])))
+                ecount[e] = ecount.get(e, 0) + 1
+        counts = np.zeros((nc, 14))
+        for c, t in enumerate(tets):
+            counts[c, :6] = [ecount[tuple(sorted((t[a], t[b])))] for a, b in self.EDGES]
+            counts[c, 6:10] = [len(faces[tuple(sorted(t[i] for i in fl))]) for fl in self.FACES]
+            counts[c, 10:] = [vcount[v] for v in t]
+        self.L, self.nc, self.nf = L, nc, nf
+        self.interior_faces = int((faceNc == 2).sum())
+        self._keep = [np.ascontiguousarray(a) for a in (cellW, counts, faceNc, faceCell, faceLid, faceW)]
+        cw, cn, fn, fc, fl, fw = self._keep
+        self.h = r.ref_cycle_create(L, nc, nf, dp(cw), dp(cn), fn.ctypes.data_as(P(c_int)), fc.ctypes.data_as(P(c_int)),
+                                    fl.ctypes.data_as(P(c_int)), dp(fw), pre, post, seed)
+
+    def timed_dofs(self):
+        """Inner DoFs whose work one cycle runs on the finest level: the cell interiors and the
+        interiors of faces shared by two cells (edges and vertices are not run)."""
+        N = 2 ** self.L
+        return self.nc * (N - 1) * (N - 2) * (N - 3) // 6 + self.interior_faces * (N - 1) * (N - 2) // 2
+
+    def run(self, threads, relax=1.0):
+        """One cycle on `threads` host threads; returns the threads used."""
+        return self._r.ref_cycle_run(self.h, threads, relax)
+
+    def checksum(self):
+        return self._r.ref_cycle_checksum(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self._r.ref_cycle_destroy(self.h)
+            self.h = None

@@ -39,7 +39,9 @@ def read_msh(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HYTEG_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_mesh_fixtures.py <reference root>  (or set HYTEG_REFERENCE)")
     out = {}
     for name in NAMES:
         p = os.path.join(ref, "data", "meshes", "3D", name + ".msh")

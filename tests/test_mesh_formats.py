@@ -18,7 +18,8 @@ import pytest
 
 import hyteg_b200 as hg
 
-REF_MESHES = "/root/reference/data/meshes/3D"
+REF_MESHES = os.path.join(os.environ.get("HYTEG_REFERENCE", ""), "data", "meshes", "3D") \
+    if os.environ.get("HYTEG_REFERENCE") else ""
 
 
 def describe(m, L):
@@ -146,7 +147,7 @@ def test_gmsh_errors(tmp_path, case):
         hg.HostMesh.from_gmsh(tmp_path / "missing.msh", 1)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_MESHES), reason="reference tree not present")
+@pytest.mark.skipif(not os.path.isdir(REF_MESHES), reason="reference tree not given (HYTEG_REFERENCE)")
 def test_reference_mesh_files_parse():
     expect = {"tet_1el.msh": (4, 6, 4, 1), "cube_6el.msh": (8, 19, 18, 6), "cube_48el.msh": (27, 98, 120, 48)}
     for name in sorted(os.listdir(REF_MESHES)):
