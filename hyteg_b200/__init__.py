@@ -817,7 +817,8 @@ class _StokesUzawaGmg:
 class StokesGeometricMultigridSolver:
     """GeometricMultigridSolver for P2P1TaylorHoodStokesOperator with an UzawaSmoother and the
     P2P1StokesToP2P1Stokes restriction / prolongation (quadratic velocity, linear pressure); the
-    coarsest level is solved by the pseudo-inverse of the operator on its unknowns."""
+    coarsest level is solved by the pseudo-inverse of the operator on its unknowns (up to 1024 of
+    them), a larger one by preconditioned MINRES to a relative residual of 1e-11."""
 
     def __init__(self, storage, S, smoother, minLevel, maxLevel, preSmoothSteps=2, postSmoothSteps=2):
         self.storage = storage

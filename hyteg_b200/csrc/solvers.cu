@@ -783,7 +783,11 @@ void StokesGmg::buildCoarse() {
   const int Lv = minL + 1, Lp = minL;
   P2Additive& av = s.p2Additive(Lv);
   P2Additive& ap = s.p2Additive(Lp);
-  argCheck(!av.hostOwner.empty() && !ap.hostOwner.empty(), "Stokes multigrid: coarse level too large");
+  if (av.hostOwner.empty() || ap.hostOwner.empty()) {  // too large for host-side owner lists
+    coarseIterative = true;
+    coarseN = 0;
+    return;
+  }
   std::vector<int64_t> idx;
   std::vector<unsigned char> comp;
   for (int k = 0; k < 3; ++k)
@@ -797,7 +801,11 @@ void StokesGmg::buildCoarse() {
     comp.push_back(3);
   }
   const int n = (int)idx.size();
-  argCheck(n <= kCoarseMax, "Stokes multigrid: more than 1024 coarse unknowns");
+  if (n > kCoarseMax) {
+    coarseIterative = true;
+    coarseN = 0;
+    return;
+  }
   const int64_t nv = s.disc.level(Lv).total, np = s.disc.level(Lp).total;
   int e[4], y[4];
   for (int k = 0; k < 4; ++k) {
@@ -854,6 +862,10 @@ void StokesGmg::buildCoarse() {
 // x += K^+ (b - K x) on the coarse unknowns
 void StokesGmg::coarseSolve(const int u[3], int p, const int f[3], int g) {
   buildCoarse();
+  if (coarseIterative) {
+    coarseIterations = stokesMinres(s, op, u, p, f, g, minL, 2, kCoarseMaxIter, kCoarseTol, nullptr, nullptr, 0);
+    return;
+  }
   if (coarseN == 0) return;
   stokesResidual(s, op, u, p, f, g, tu, tp, minL);
   dev::BlockPtrs bp;

@@ -143,9 +143,14 @@ struct P2Gmg {
 // velocity, linear on the pressure). Velocity DoFs flagged Inner | Neumann are unknowns; the
 // pressure is all-inner (every DoF an unknown, P2P1TaylorHoodFunction.hpp:61). The coarsest level
 // is solved by the pseudo-inverse of the operator on its unknowns (the constant pressure and the
-// pressure DoFs coupled to no free velocity DoF span its null space), built once. FP64.
+// pressure DoFs coupled to no free velocity DoF span its null space), built once, when it has at
+// most kCoarseMax unknowns; a larger coarsest level (the reference solves it by LU) is solved by
+// preconditioned MINRES to a relative residual of kCoarseTol (zero-mean pressure, as the
+// pseudo-inverse gives). FP64.
 struct StokesGmg {
   static constexpr int kCoarseMax = 1024;
+  static constexpr double kCoarseTol = 1e-11;
+  static constexpr int kCoarseMaxIter = 1000;
   StokesGmg(Storage& s, int op, int minL, int maxL, int pre, int post, double omega, int velocitySweeps);
   ~StokesGmg();
   void smooth(const int u[3], int p, const int f[3], int g, int L);
@@ -169,7 +174,9 @@ struct StokesGmg {
   int ru[3], rp;               // Uzawa residuals
   int tu[3], tp;               // Stokes residual / restricted right-hand sides
   std::vector<int> invDiag;    // per pressure level minL..maxL: 1 / diag(PSPG)
-  int coarseN = -1;
+  int coarseN = -1;            // coarse unknowns of the dense pseudo-inverse; 0: none
+  bool coarseIterative = false;  // the coarsest level is solved by MINRES instead
+  int coarseIterations = 0;      // MINRES iterations of the last coarse solve
   std::unique_ptr<DevBuf> coarseIdx, coarseComp, coarseInv;
 };
 

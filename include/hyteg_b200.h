@@ -285,7 +285,9 @@ int hg_p2p1_stokes_minres_mixed(hg_storage* s, int op, const int u[3], int p, co
  * composite transfers (P2P1StokesToP2P1StokesRestriction / Prolongation.hpp: quadratic on the
  * velocity, linear on the pressure). Velocity DoFs flagged Inner | Neumann are unknowns, every
  * pressure DoF is one (all-inner, P2P1TaylorHoodFunction.hpp:61). The coarsest level is solved by
- * the pseudo-inverse of the operator on its unknowns (at most 1024). u, f: velocity P2 functions,
+ * the pseudo-inverse of the operator on its unknowns when it has at most 1024 of them, else by
+ * hg_p2p1_stokes_minres (nu = 2) to a relative residual of 1e-11, where the reference uses an LU
+ * solver; the operator must then cover level 0. u, f: velocity P2 functions,
  * p, g: pressure P1 functions, covering [min_level, max_level].
  *   smooth:   one UzawaSmoother::solve step on level
  *   solve:    one V(pre, post) cycle
