@@ -56,8 +56,10 @@ def parse():
                    help="only the kernels, autotuner and timed cycles (profiling runs); implies no serving")
     p.add_argument("--stokes-level", type=int, default=6,
                    help="P2 level of the Taylor-Hood measurements (capped at level - 2)")
-    p.add_argument("--serving-requests", type=int, default=200,
+    p.add_argument("--serving-requests", type=int, default=2000,
                    help="requests of the batched-serving measurement (0 skips it)")
+    p.add_argument("--serving-sequential", type=int, default=400,
+                   help="requests of the stream solved one at a time in FP64 (the sequential service rate)")
     return p.parse_args()
 
 
@@ -298,15 +300,17 @@ def reassembly_bench(hg, k=4, L=6, reps=5):
     return res
 
 
-def serving_bench(hg, n_requests, seed=2024):
-    """Batched serving on a seeded request stream (config 5, bounded sample): k in U{1..4}
-    sub-cubes per direction (6..384 tets), level in U{3..6}, coefficient log-uniform in
-    [0.1, 10], right-hand side uniform[-1,1] from the request's seed, tolerance 1e-8, mixed
-    precision, Poisson arrivals. The same requests are first solved one after another with plain
-    FP64 cycles (one worker); one mixed-precision server (8 workers, two resident hierarchies per
-    shape built ahead) then runs them at arrival rates of 2x, 4x and 8x that sequential service
-    rate (the last saturates it: its throughput is the server's capacity).
-    Latency = completion - arrival (server clock)."""
+def serving_bench(hg, n_requests, n_sequential, seed=2024):
+    """Batched serving on a seeded request stream (config 5): k in U{1..4} sub-cubes per direction
+    (6..384 tets), level in U{3..6}, coefficient log-uniform in [0.1, 10], right-hand side
+    uniform[-1,1] from the request's seed, tolerance 1e-8, mixed precision, Poisson arrivals. The
+    first n_sequential requests are solved one after another with plain FP64 cycles (one worker):
+    their service rate sets the arrival rates. One mixed-precision server (8 workers, two
+    resident hierarchies per shape built ahead) then runs the whole stream at arrival rates of 2x,
+    4x and 8x that sequential service rate (the last saturates it: its throughput is the server's
+    capacity). Latency = completion - arrival (server clock). Setup = admission to the start of
+    the solve: the stencil re-assembly for the request's coefficient on a resident hierarchy, or
+    building a hierarchy when none of the request's shape is free."""
     rng = np.random.default_rng(seed)
     reqs = [(int(rng.integers(1, 5)), int(rng.integers(3, 7)), float(np.exp(rng.uniform(np.log(0.1), np.log(10.0)))),
              int(rng.integers(1, 2 ** 62))) for _ in range(n_requests)]
@@ -319,11 +323,11 @@ def serving_bench(hg, n_requests, seed=2024):
                 srv.prewarm(k, L)
         return srv
 
-    def run(srv, rate):
-        arr = np.cumsum(rng.exponential(1.0 / rate, len(reqs))) if rate else np.zeros(len(reqs))
+    def run(srv, rate, stream):
+        arr = np.cumsum(rng.exponential(1.0 / rate, len(stream))) if rate else np.zeros(len(stream))
         t0 = time.perf_counter()
         ids = []
-        for (k, L, c, sd), ta in zip(reqs, arr):
+        for (k, L, c, sd), ta in zip(stream, arr):
             d = ta - (time.perf_counter() - t0)
             if d > 0:
                 time.sleep(d)
@@ -335,24 +339,31 @@ def serving_bench(hg, n_requests, seed=2024):
         lat = np.array([r["t_end"] - r["t_submit"] for r in res])
         span = max(r["t_end"] for r in res) - min(r["t_submit"] for r in res)
         dofs = sum(r["inner_dofs"] for r in res)
+        setup = np.array([r["t_solve"] - r["t_start"] for r in res])
+        built = np.array([r["built_hierarchy"] for r in res])
         return {"requests": len(res), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "seconds": span, "gdofs": dofs / span / 1e9,
                 "max_rel_residual": max(r["rel_residual"] for r in res),
                 "mean_iterations": float(np.mean([r["iterations"] for r in res])), "peak_bytes": st["peak_bytes"],
-                "mean_setup_ms": float(np.mean([r["t_solve"] - r["t_start"] for r in res]) * 1e3),
+                "mean_setup_ms": float(setup.mean() * 1e3),
+                "hierarchies_built_on_admission": int(built.sum()),
+                "mean_setup_ms_resident": float(setup[~built].mean() * 1e3) if (~built).any() else None,
+                "mean_setup_ms_built": float(setup[built].mean() * 1e3) if built.any() else None,
                 "mean_solve_ms": float(np.mean([r["t_end"] - r["t_solve"] for r in res]) * 1e3)}
 
     srv = make(1, 8, 1)
-    seq = run(srv, 0)  # all submitted at once, one worker: sequential FP64 solves
+    seq = run(srv, 0, reqs[:n_sequential])  # all submitted at once, one worker: sequential FP64 solves
     srv.close()
     mu = seq["requests"] / seq["seconds"]
     out = {"workload": "%d seeded requests: k in U{1..4}, level in U{3..6}, coefficient log-U[0.1,10], "
-                       "tol 1e-8, Poisson arrivals" % n_requests,
+                       "tol 1e-8, Poisson arrivals; the sequential FP64 rate from its first %d"
+                       % (n_requests, n_sequential),
            "sequential_fp64": seq}
     srv = make(8, 4, 2)  # resident hierarchies: two per shape, kept across the three runs
     for mult in (2.0, 4.0, 8.0):
-        out["mixed_rate_%gx" % mult] = dict(run(srv, mult * mu), arrival_rate_per_s=mult * mu)
+        out["mixed_rate_%gx" % mult] = dict(run(srv, mult * mu, reqs), arrival_rate_per_s=mult * mu)
     srv.close()
+    out["capacity_vs_sequential"] = out["mixed_rate_8x"]["gdofs"] / seq["gdofs"]
     return out
 
 
@@ -516,11 +527,20 @@ def time_to_solution(hg, st, A, L, N_in, Inner):
                      for c in range(nc)])
     st.set_cell_coefficients(1.0 + 0.5 * np.sin(2 * np.pi * cent[:, 0]) * np.cos(2 * np.pi * cent[:, 1]) * cent[:, 2])
     Ak = hg.P1ConstantLaplaceOperator(st, 0, L)
+    # With k piecewise constant, the smooth u above does not satisfy the flux conditions across
+    # the macro-cell interfaces, so it is no solution of -div(k grad u) = f. The manufactured
+    # solution is therefore discrete: b = A_k I(u), whose exact discrete solution is I(u).
+    bm.interpolate(0.0, L, hg.All)
+    Ak.apply(u, bm, L, Inner)
     v64 = run(Ak, bm, np.float64, 1e-10)
+    v64["err_vs_manufactured"] = rms(xs, u) / rms(u)
     x64.assign([1.0], [xs], L, hg.All)
     v32 = run(Ak, bm, np.float32, 1e-10)
+    v32["err_vs_manufactured"] = rms(xs, u) / rms(u)
     v32["err_vs_fp64_solve"] = rms(xs, x64) / rms(x64)
     out["variable_k"] = {"k": "1 + 0.5 sin(2 pi x) cos(2 pi y) z at macro-cell centroids", "target_rel_residual": 1e-10,
+                         "problem": "b = A_k I(u), u = sin(pi x) sin(pi y) sin(pi z): the manufactured discrete solution "
+                                    "is I(u); errors are relative discrete L2 (RMS over inner DoFs)",
                          "fp64": v64, "mixed": v32, "speedup_mixed_vs_fp64": v64["seconds"] / v32["seconds"]}
     del Ak
     st.set_cell_coefficients(np.ones(nc))
@@ -776,7 +796,7 @@ def run_ours(args):
         "timing_tree_one_cycle_ms": cycle_tree,
     }
     if world == 1 and args.serving_requests > 0 and not args.cycle_only:
-        out["serving"] = serving_bench(hg, args.serving_requests)
+        out["serving"] = serving_bench(hg, args.serving_requests, min(args.serving_sequential, args.serving_requests))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         thr = host_threads()
         ref = reference_cpu_pass(L, 5, 1, thr)  # median of five cycles on all host threads

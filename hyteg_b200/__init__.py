@@ -867,16 +867,21 @@ class SolveServer:
         return bool(d.value)
 
     def result(self, rid):
-        """dict(status, iterations, rel_residual, t_submit, t_start, t_solve, t_end, inner_dofs);
-        raises for a failed request."""
+        """dict(status, iterations, rel_residual, t_submit, t_start, t_solve, t_end, inner_dofs,
+        built_hierarchy); raises for a failed request. built_hierarchy: no resident hierarchy of the
+        request's shape was free when it was admitted, so one was built for it (its setup time,
+        t_solve - t_start, includes that)."""
         st, it = ctypes.c_int(), ctypes.c_int()
         rel = ctypes.c_double()
         t = np.zeros(4)
         n = ctypes.c_int64()
+        built = ctypes.c_int()
         call("hg_server_result", self._h, int(rid), ctypes.byref(st), ctypes.byref(it), ctypes.byref(rel), dptr(t),
              ctypes.byref(n))
+        call("hg_server_request_setup", self._h, int(rid), ctypes.byref(built))
         return {"status": st.value, "iterations": it.value, "rel_residual": rel.value, "t_submit": t[0],
-                "t_start": t[1], "t_solve": t[2], "t_end": t[3], "inner_dofs": n.value}
+                "t_start": t[1], "t_solve": t[2], "t_end": t[3], "inner_dofs": n.value,
+                "built_hierarchy": bool(built.value)}
 
     def solution(self, rid):
         n = ctypes.c_int64()

@@ -135,6 +135,7 @@ _SIGS = {
     "hg_server_submit": (c_int, [c_void_p, c_int, c_int, c_double, ctypes.c_uint64, c_double, c_int, c_int, P(c_int64)]),
     "hg_server_wait": (c_int, [c_void_p, c_int64, c_double, P(c_int)]),
     "hg_server_result": (c_int, [c_void_p, c_int64, P(c_int), P(c_int), P(c_double), P(c_double), P(c_int64)]),
+    "hg_server_request_setup": (c_int, [c_void_p, c_int64, P(c_int)]),
     "hg_server_solution": (c_int, [c_void_p, c_int64, P(c_double), c_int64, P(c_int64)]),
     "hg_server_stats": (c_int, [c_void_p, P(c_int64)]),
     "hg_function_fill_random": (c_int, [c_void_p, c_int, c_int, c_uint, ctypes.c_uint64, c_double, c_double]),

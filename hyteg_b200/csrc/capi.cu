@@ -1135,6 +1135,14 @@ int hg_server_result(hg_server* srv, int64_t id, int* status, int* iterations, d
   HG_CATCH
 }
 
+int hg_server_request_setup(hg_server* srv, int64_t id, int* built_hierarchy) {
+  HG_TRY
+  hg::argCheck(built_hierarchy != nullptr, "null output pointer");
+  auto r = SV(srv).request(id);
+  *built_hierarchy = r->builtHierarchy ? 1 : 0;
+  HG_CATCH
+}
+
 int hg_server_solution(hg_server* srv, int64_t id, double* host, int64_t n, int64_t* size) {
   HG_TRY
   auto r = SV(srv).request(id);

@@ -1408,39 +1408,26 @@ __global__ void __launch_bounds__(kBlock) p2ProlongKernel(LevelDev lvc, LevelDev
     }
 }
 
-// coarse += P^T (fine / multiplicity) over every node of the closed macro-cells: each cell adds
-// its share (a DoF on a face, edge or vertex is split evenly among its cells) into its own
-// coarse closure slots; the owners are summed afterwards. coarse must be zero on entry.
+// coarse = P^T (fine / multiplicity) on the closed macro-cells, as a gather: each cell writes its
+// share (a DoF on a face, edge or vertex is split evenly among its cells) into its own coarse
+// closure slots; the owners are summed afterwards. One thread per coarse node of a cell sums its
+// contributions in the fixed order of the gather lists (compressed rows, the same for every
+// cell), so the result does not depend on scheduling.
 template <class T>
-__global__ void __launch_bounds__(kBlock) p2RestrictKernel(LevelDev lvc, LevelDev lvf, P2Tables tb, P2TransferDev tr,
-                                                           const T* __restrict__ wts, const T* __restrict__ fine,
-                                                           const unsigned char* __restrict__ mult, T* coarse) {
-  const int Mf = lvf.N, Mc = lvc.N, N = Mc / 2, nPl = Mf + 1, wf = lvf.w, wc = lvc.w;
-  const int c = blockIdx.x / nPl, Z = blockIdx.x % nPl;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  T* cc = coarse + lvc.cellOff[c];
+__global__ void __launch_bounds__(kBlock) p2RestrictGatherKernel(LevelDev lvc, LevelDev lvf, const int* __restrict__ ptr,
+                                                                 const int* __restrict__ idx, const T* __restrict__ w,
+                                                                 int nCoarse, int blocksPerCell, const T* __restrict__ fine,
+                                                                 const unsigned char* __restrict__ mult, T* coarse) {
+  const int c = blockIdx.x / blocksPerCell;
+  const int node = (blockIdx.x - c * blocksPerCell) * kBlock + threadIdx.x;
+  if (node >= nCoarse) return;
   const int64_t fb = lvf.cellOff[c];
-  auto cidx = [wc](int x, int y, int z) { return int(tetSize(wc) - tetSize(wc - z)) + rowStart(wc - z, y) + x; };
-  const int pb = int(tetSize(wf) - tetSize(wf - Z));
-  for (int Y = warp; Y <= Mf - Z; Y += kBlock / 32)
-    for (int X = lane; X <= Mf - Z - Y; X += 32) {
-      const int64_t i = fb + pb + rowStart(wf - Z, Y) + X;
-      const T v = fine[i] / T(mult[i]);
-      if (((X | Y | Z) & 1) == 0) {
-        atomicAdd(cc + cidx(X >> 1, Y >> 1, Z >> 1), v);
-      } else {
-        const int r = (X & 3) | ((Y & 3) << 2) | ((Z & 3) << 4);
-        int ax, ay, az;
-        const int k = p2PickCandidate<T>(tr, tb, r, X >> 2, Y >> 2, Z >> 2, N, ax, ay, az);
-        if (k < 0) continue;
-        const int t = tr.cand[r * kP2TrCand + k] & 7;
-        const T* w = wts + (r * kP2TrCand + k) * 10;
-#pragma unroll
-        for (int m = 0; m < 10; ++m)
-          if (w[m] != T(0))
-            atomicAdd(cc + cidx(2 * ax + tb.off[t][m][0], 2 * ay + tb.off[t][m][1], 2 * az + tb.off[t][m][2]), w[m] * v);
-      }
-    }
+  T acc = T(0);
+  for (int j = ptr[node], e = ptr[node + 1]; j < e; ++j) {
+    const int64_t i = fb + idx[j];
+    acc += w[j] * (fine[i] / T(mult[i]));
+  }
+  coarse[lvc.cellOff[c] + node] = acc;
 }
 
 // owner <- its first cell-closure copy (values that every cell computes alike)

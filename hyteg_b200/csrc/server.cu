@@ -205,6 +205,7 @@ void Server::worker() {
       if (r) {
         r->status = 1;
         r->tStart = now();
+        r->builtHierarchy = !slot;
         ++admitted_;
         peak_ = std::max(peak_, active_ + resident_);
       }

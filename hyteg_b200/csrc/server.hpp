@@ -40,6 +40,7 @@ struct ServerRequest {
   int iterations = 0;
   double relResidual = 0.0;
   double tSubmit = 0.0, tStart = 0.0, tSolve = 0.0, tEnd = 0.0;  // seconds since the server started
+  bool builtHierarchy = false;  // no resident hierarchy of its shape was free: one was built for it
   int64_t innerDofs = 0;
   std::vector<double> solution;  // level buffer of x at the request's level (keepSolution)
 };

@@ -1205,6 +1205,9 @@ static void buildP2Transfer(P2Transfer& tr, cudaStream_t stream) {
       }
   }
   std::vector<float> wfl(w.begin(), w.end());
+  tr.hNCand = nc;
+  tr.hCand = cand;
+  tr.hW = w;
   tr.nCand.alloc(nc.size());
   tr.cand.alloc(cand.size());
   tr.wd.alloc(w.size() * sizeof(double));
@@ -1215,6 +1218,67 @@ static void buildP2Transfer(P2Transfer& tr, cudaStream_t stream) {
   cudaCheck(cudaMemcpyAsync(tr.wf.p, wfl.data(), wfl.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "p2 transfer");
   cudaCheck(cudaStreamSynchronize(stream), "p2 transfer");
   tr.built = true;
+}
+
+// The restriction's gather lists for fine lattice level Lff: every fine node Q of the closed
+// reference cell contributes to the coarse nodes its prolongation reads (the same candidate
+// micro-cell as p2PickCandidate picks, nonzero basis values only; even nodes are injected), and
+// each coarse node lists its contributions in the order of Q (z, y, x), then of the basis node.
+const P2Gather& Storage::p2Gather(int Lff) {
+  P2Gather& g = p2gather[Lff];
+  if (g.built) return g;
+  if (!p2tr.built) buildP2Transfer(p2tr, stream);
+  const dev::P2Tables& tb = p2TablesOnce();
+  const int Mf = disc.level(Lff).N, Mc = Mf / 2, N = Mc / 2, wf = Mf + 1, wc = Mc + 1;
+  auto tet = [](int64_t w) { return w * (w + 1) * (w + 2) / 6; };
+  auto row = [](int64_t W, int64_t y) { return y * (W + 1) - y * (y + 1) / 2; };
+  auto cidx = [&](int x, int y, int z) { return int(tet(wc) - tet(wc - z) + row(wc - z, y) + x); };
+  auto fidx = [&](int x, int y, int z) { return int(tet(wf) - tet(wf - z) + row(wf - z, y) + x); };
+  const int nC = (int)tet(wc);
+  std::vector<std::vector<std::pair<int, double>>> lists((size_t)nC);
+  for (int Z = 0; Z <= Mf; ++Z)
+    for (int Y = 0; Y <= Mf - Z; ++Y)
+      for (int X = 0; X <= Mf - Z - Y; ++X) {
+        const int q = fidx(X, Y, Z);
+        if (((X | Y | Z) & 1) == 0) {
+          lists[(size_t)cidx(X >> 1, Y >> 1, Z >> 1)].push_back({q, 1.0});
+          continue;
+        }
+        const int r = (X & 3) | ((Y & 3) << 2) | ((Z & 3) << 4);
+        for (int k = 0; k < p2tr.hNCand[r]; ++k) {  // the first candidate inside the cell
+          const int c = p2tr.hCand[(size_t)r * dev::kP2TrCand + k], t = c & 7, d = c >> 3;
+          const int ax = (X >> 2) - (d & 1), ay = (Y >> 2) - ((d >> 1) & 1), az = (Z >> 2) - ((d >> 2) & 1);
+          if (!(ax >= 0 && ay >= 0 && az >= 0 && ax + ay + az < N - tb.widthRed[t])) continue;
+          const double* w = &p2tr.hW[(size_t)(r * dev::kP2TrCand + k) * 10];
+          for (int m = 0; m < 10; ++m)
+            if (w[m] != 0.0)
+              lists[(size_t)cidx(2 * ax + tb.off[t][m][0], 2 * ay + tb.off[t][m][1], 2 * az + tb.off[t][m][2])]
+                  .push_back({q, w[m]});
+          break;
+        }
+      }
+  std::vector<int> ptr((size_t)nC + 1, 0), idx;
+  std::vector<double> wd;
+  for (int c = 0; c < nC; ++c) {
+    for (const auto& e : lists[(size_t)c]) {
+      idx.push_back(e.first);
+      wd.push_back(e.second);
+    }
+    ptr[(size_t)c + 1] = (int)idx.size();
+  }
+  std::vector<float> wfl(wd.begin(), wd.end());
+  g.nCoarse = nC;
+  g.ptr.alloc(ptr.size() * sizeof(int));
+  cudaCheck(cudaMemcpyAsync(g.ptr.p, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice, stream), "p2 gather");
+  g.idx.alloc(idx.size() * sizeof(int));
+  g.wd.alloc(wd.size() * sizeof(double));
+  g.wf.alloc(wfl.size() * sizeof(float));
+  cudaCheck(cudaMemcpyAsync(g.idx.p, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, stream), "p2 gather");
+  cudaCheck(cudaMemcpyAsync(g.wd.p, wd.data(), wd.size() * sizeof(double), cudaMemcpyHostToDevice, stream), "p2 gather");
+  cudaCheck(cudaMemcpyAsync(g.wf.p, wfl.data(), wfl.size() * sizeof(float), cudaMemcpyHostToDevice, stream), "p2 gather");
+  cudaCheck(cudaStreamSynchronize(stream), "p2 gather");
+  g.built = true;
+  return g;
 }
 
 int Storage::p2Scratch(int Lf, int prec) {
@@ -1268,22 +1332,25 @@ void Storage::p2Restrict(int id, int Lf, unsigned mask) {
   const LevelData& lf = levels[Lff];
   P2Additive& adf = p2Additive(Lff);
   P2Additive& adc = p2Additive(Lcf);
+  const P2Gather& gt = p2Gather(Lff);
   communicate(id, Lff, 1 << G_CELL);
   cudaCheck(cudaMemsetAsync(data(id, Lcf), 0, (size_t)lc.lay->total * f.prec, stream), "P2 restriction");
-  const dev::P2TransferDev tr{(const unsigned char*)p2tr.nCand.p, (const unsigned char*)p2tr.cand.p};
-  const int nb = lf.lv.nCells * (lf.lv.N + 1), na = (adc.n + dev::kBlock - 1) / dev::kBlock;
+  const int bpc = (gt.nCoarse + dev::kBlock - 1) / dev::kBlock;
+  const int nb = lf.lv.nCells * bpc, na = (adc.n + dev::kBlock - 1) / dev::kBlock;
   if (f.prec == 8) {
-    dev::p2RestrictKernel<double><<<nb, dev::kBlock, 0, stream>>>(lc.lv, lf.lv, p2TablesOnce(), tr,
-                                                                (const double*)p2tr.wd.p, (const double*)data(id, Lff),
-                                                                (const unsigned char*)adf.mult.p, (double*)data(id, Lcf));
+    dev::p2RestrictGatherKernel<double><<<nb, dev::kBlock, 0, stream>>>(
+        lc.lv, lf.lv, (const int*)gt.ptr.p, (const int*)gt.idx.p, (const double*)gt.wd.p, gt.nCoarse, bpc,
+        (const double*)data(id, Lff),
+        (const unsigned char*)adf.mult.p, (double*)data(id, Lcf));
     if (adc.n)
       dev::p2AddKernel<double, dev::MODE_REPLACE><<<na, dev::kBlock, 0, stream>>>(
           (const int64_t*)adc.owner.p, (const int*)adc.ptr.p, (const int64_t*)adc.copies.p,
           (const unsigned char*)adc.type.p, adc.n, (double*)data(id, Lcf), nullptr, mask, nullptr, -1);
   } else {
-    dev::p2RestrictKernel<float><<<nb, dev::kBlock, 0, stream>>>(lc.lv, lf.lv, p2TablesOnce(), tr,
-                                                               (const float*)p2tr.wf.p, (const float*)data(id, Lff),
-                                                               (const unsigned char*)adf.mult.p, (float*)data(id, Lcf));
+    dev::p2RestrictGatherKernel<float><<<nb, dev::kBlock, 0, stream>>>(
+        lc.lv, lf.lv, (const int*)gt.ptr.p, (const int*)gt.idx.p, (const float*)gt.wf.p, gt.nCoarse, bpc,
+        (const float*)data(id, Lff),
+        (const unsigned char*)adf.mult.p, (float*)data(id, Lcf));
     if (adc.n)
       dev::p2AddKernel<float, dev::MODE_REPLACE><<<na, dev::kBlock, 0, stream>>>(
           (const int64_t*)adc.owner.p, (const int*)adc.ptr.p, (const int64_t*)adc.copies.p,

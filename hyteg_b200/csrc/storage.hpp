@@ -113,10 +113,22 @@ struct P2Additive {
   std::vector<unsigned char> hostOwnerType;  // and its DoF type
 };
 
-// Candidate micro-cells and coarse P2 basis values for the fine nodes of the 64 residue classes.
+// Candidate micro-cells and coarse P2 basis values for the fine nodes of the 64 residue classes
+// (device tables, and their host copies for building the restriction's gather lists).
 struct P2Transfer {
   bool built = false;
   DevBuf nCand, cand, wd, wf;
+  std::vector<unsigned char> hNCand, hCand;
+  std::vector<double> hW;
+};
+
+// The P2 restriction as a gather (the transpose of the quadratic prolongation of one macro-cell,
+// the same for every cell): for each coarse node of the closed reference cell, its contributing
+// fine nodes and weights in a fixed order (compressed rows: ptr[nCoarse + 1], then the entries).
+struct P2Gather {
+  bool built = false;
+  int nCoarse = 0;
+  DevBuf ptr, idx, wd, wf;  // row starts; int32 fine local index; FP64 / FP32 weight
 };
 
 struct Gmg;
@@ -195,6 +207,8 @@ struct Storage {
   int p2Diagonal(int op, int L, int prec);
   std::map<std::pair<int, int>, int> p2scratch;  // (lattice level, precision) -> scratch function
   P2Transfer p2tr;
+  std::map<int, P2Gather> p2gather;  // by fine lattice level
+  const P2Gather& p2Gather(int Lff);
   // Quadratic prolongation from P2 level Lc to Lc + 1 of function id (fine = P coarse, or += with
   // add) and its transpose, the restriction from P2 level Lf to Lf - 1.
   void p2Prolongate(int id, int Lc, unsigned mask, bool add);

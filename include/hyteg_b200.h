@@ -347,6 +347,11 @@ int hg_server_wait(hg_server* srv, int64_t id, double timeout_seconds, int* done
 int hg_server_result(hg_server* srv, int64_t id, int* status, int* iterations, double* rel_residual, double times[4],
                      int64_t* inner_dofs);
 /* Level buffer of the solution (requests submitted with keep_solution); *size = elements. */
+/* Whether request id's hierarchy was built when it was admitted (1: no resident hierarchy of its
+ * shape was free, so its setup time includes building one: storage, tables, stencils and a first
+ * cycle) or was a resident one (0: its setup is the re-assembly of the stencils for its
+ * coefficient). */
+int hg_server_request_setup(hg_server* srv, int64_t id, int* built_hierarchy);
 int hg_server_solution(hg_server* srv, int64_t id, double* host, int64_t n, int64_t* size);
 /* admitted, completed, failed, resident idle hierarchies, their bytes, peak bytes in use. */
 int hg_server_stats(hg_server* srv, int64_t stats[6]);

@@ -223,8 +223,8 @@ def test_p2_multicolour_sor_level4(cube2l4, backwards):
 
 
 def test_p2_graph_cycles_match_eager_cycles(cube2):
-    # replayed CUDA graphs launch the same kernels; the restriction's atomic sums make the
-    # agreement one of rounding, not of bits
+    # replayed CUDA graphs launch the same kernels, and every kernel of the cycle sums in a fixed
+    # order (the restriction is a gather), so the two agree bit for bit
     st, orc, maps = cube2
     L = 3
     node, owned = maps[L]
@@ -245,7 +245,36 @@ def test_p2_graph_cycles_match_eager_cycles(cube2):
         out.append((x.to_numpy(L), launches))
     (xe, le), (xg, lg) = out
     assert le == lg
-    assert np.abs(xe - xg).max() / np.abs(xe).max() < 1e-13
+    assert np.array_equal(xe, xg)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_p2_restriction_and_cycles_are_bit_reproducible(cube2, dtype):
+    """The P2 restriction gathers each coarse value from its fine contributions in a fixed order,
+    so repeated restrictions and repeated multigrid solves give identical bits."""
+    st, orc, maps = cube2
+    L = 3
+    f = hg.P2Function("rf", st, 0, L, dtype=dtype)
+    outs = []
+    for _ in range(2):
+        f.fill_random(17, L, hg.Inner)
+        hg.P2toP2QuadraticRestriction().restrict(f, L, hg.Inner)
+        outs.append(f.to_numpy(L - 1))
+    assert np.array_equal(outs[0], outs[1])
+    if dtype == np.float32:
+        return
+    res = []
+    for _ in range(2):
+        A = hg.P2ConstantLaplaceOperator(st, 0, L)
+        x, b = hg.P2Function("x", st, 0, L), hg.P2Function("b", st, 0, L)
+        b.fill_random(19, L, hg.Inner)
+        gmg = hg.P2GeometricMultigridSolver(st, A, 0, L, 3, 3, 1.0)
+        gmg.set_graphs(False)
+        for _ in range(3):
+            gmg.solve(x, b, L)
+        res.append(x.to_numpy(L))
+        del gmg, A
+    assert np.array_equal(res[0], res[1])
 
 
 def test_p2_multigrid_exact_coarse_solve_on_3x3x3_cube(cube3):

@@ -3,7 +3,7 @@ oracle's restatement (oracle.Oracle.uzawa_smooth / stokes_uzawa_cycle: assembled
 multicolour P2 SOR, the composite transfers and a numpy pseudo-inverse on the coarsest level).
 
 Tolerances: one smoothing step and the pressure transfers 1e-13 relative; two V-cycles 1e-11
-relative (the P2 restriction sums with atomics, so the agreement is one of rounding); the
+relative (the oracle sums in another order, so the agreement is one of rounding); the
 relaxation estimate (15 power iterations from the same seeded start) 1e-11 relative; V(3,3)
 cycles with the estimated relaxation reduce the residual monotonically."""
 import numpy as np
