@@ -269,6 +269,11 @@ class PrimitiveStorage:
         arrays (converted once per group of sweeps)."""
         call("hg_storage_set_sor_schedule", self._h, int(schedule))
 
+    def set_sor_fused_phases(self, on):
+        """Face, edge and vertex phases of the SOR as one launch per phase (True, default) or one
+        launch per colour and halo refresh (False); the sweep is the same bit for bit."""
+        call("hg_storage_set_sor_fused_phases", self.handle, 1 if on else 0)
+
     def set_sor_schedule_level(self, level, schedule, dtype=np.float64):
         """One level's SOR schedule for one precision (-1: the storage-wide schedule)."""
         prec = {np.dtype(np.float64): 8, np.dtype(np.float32): 4}[np.dtype(dtype)]

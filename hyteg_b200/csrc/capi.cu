@@ -203,6 +203,14 @@ int hg_storage_set_cell_coefficients(hg_storage* h, const double* k, int ncells)
   HG_CATCH
 }
 
+int hg_storage_set_sor_fused_phases(hg_storage* h, int on) {
+  HG_TRY
+  hg::argCheck(on == 0 || on == 1, "fused SOR phases: on must be 0 or 1");
+  S(h).fusedSorPhases = on;
+  ++S(h).generation;
+  HG_CATCH
+}
+
 int hg_storage_set_sor_schedule(hg_storage* h, int schedule) {
   HG_TRY
   hg::argCheck(schedule >= 0 && schedule <= 3,

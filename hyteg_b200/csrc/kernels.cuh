@@ -807,6 +807,103 @@ __global__ void __launch_bounds__(kBlock) faceSorKernel(LevelDev lv, StencilDev<
   }
 }
 
+// ---------------------------------------------------------------------------------------
+// SOR phases in one launch each: a block per primitive refreshes the copies of its own array
+// that the reference refreshes before the phase (its entries range[p] = [begin, end) of the halo
+// table; their owners are not changed by the phase, so no block reads what another writes), then
+// runs every colour of the phase with a block barrier between colours. Primitives of one kind
+// are independent within their phase (each reads only its own array), so this equals one launch
+// per colour over all primitives.
+// ---------------------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ void gatherRange(T* buf, T* cells, const uint2* __restrict__ table, int begin, int end,
+                                            int64_t cellEnd) {
+  for (int i = begin + (int)threadIdx.x; i < end; i += (int)blockDim.x) {
+    const uint2 t = table[i];
+    if (cells) {  // cell arrays in their colour-split copy: slots below cellEnd live there
+      const T v = t.y < cellEnd ? cells[t.y] : buf[t.y];
+      if (t.x < cellEnd) cells[t.x] = v;
+      else buf[t.x] = v;
+    } else {
+      buf[t.x] = buf[t.y];
+    }
+  }
+}
+
+// Edges (both colours x mod 2) or vertices: block b is primitive firstPrim + b.
+template <class T>
+__global__ void __launch_bounds__(kBlock) lowSorPhaseKernel(LevelDev lv, StencilDev<T> st, T* u, const T* __restrict__ rhs,
+                                                            unsigned mask, T omega, int firstPrim, int backwards,
+                                                            const uint2* __restrict__ table, const int2* __restrict__ range,
+                                                            T* cells, int64_t cellEnd) {
+  const int p = firstPrim + blockIdx.x;
+  if (range) {
+    gatherRange(u, cells, table, range[p].x, range[p].y, cellEnd);
+    __syncthreads();
+  }
+  if (!(lv.lowType[p] & mask)) return;
+  const int first = lv.lowFirst[p], count = lv.lowCount[p];
+  const int64_t o = lv.lowOff[p];
+  const int e0 = st.lowEntOff[p], e1 = st.lowEntOff[p + 1];
+  const int passes = p < lv.nEdges ? 2 : 1;
+  const T om1 = T(1) - omega;
+  for (int pass = 0; pass < passes; ++pass) {
+    const int colour = passes == 2 ? (backwards ? 1 - pass : pass) : -1;
+    for (int x = first + threadIdx.x; x < first + count; x += kBlock) {
+      if (colour >= 0 && (x & 1) != colour) continue;
+      const int64_t c = o + x;
+      T s = rhs[c];
+      for (int k = e0 + 1; k < e1; ++k) s -= st.lowEntW[k] * u[c + st.lowEntRel[k]];
+      u[c] = om1 * u[c] + (s * omega) / st.lowEntW[e0];
+    }
+    __syncthreads();
+  }
+}
+
+// Faces, the three colours (x + 2y) mod 3; block b is face b, kFacePhaseThreads threads (the
+// warps take the rows).
+constexpr int kFacePhaseThreads = 1024;
+template <class T>
+__global__ void __launch_bounds__(kFacePhaseThreads) faceSorPhaseKernel(LevelDev lv, StencilDev<T> st, T* u,
+                                                                        const T* __restrict__ rhs, unsigned mask, T omega,
+                                                                        int backwards, const uint2* __restrict__ table,
+                                                                        const int2* __restrict__ range, T* cells,
+                                                                        int64_t cellEnd) {
+  constexpr int kWarps = kFacePhaseThreads / 32;
+  const int face = blockIdx.x;
+  if (range) {
+    gatherRange(u, cells, table, range[face].x, range[face].y, cellEnd);
+    __syncthreads();
+  }
+  if (!(lv.faceType[face] & mask)) return;
+  __shared__ FaceEnt<T> ent[16];
+  __shared__ int off[kWarps][16];
+  const int ne = st.faceEntCount[face];
+  if (threadIdx.x < ne) ent[threadIdx.x] = st.faceEnt[16 * face + threadIdx.x];
+  __syncthreads();
+  const int w = lv.w, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t base = lv.faceOff[face];
+  T* uf = u + base;
+  const T* __restrict__ f = rhs + base;
+  const T om = omega, om1 = T(1) - omega;
+  for (int pass = 0; pass < 3; ++pass) {
+    const int colour = backwards ? 2 - pass : pass;
+    for (int y = 1 + warp; y < w - 2; y += kWarps) {
+      if (lane < ne) off[warp][lane] = faceSlot(w, ent[lane].layer, ent[lane].dx, y + ent[lane].dy);
+      __syncwarp();
+      const int len = w - 2 - y, r0 = rowStart(w, y);
+      const int x0 = 1 + (((colour - 2 * y - 1) % 3) + 3) % 3;
+      for (int x = x0 + 3 * lane; x <= len; x += 96) {
+        T s = f[r0 + x];
+        for (int k = 1; k < ne; ++k) s -= ent[k].w * uf[off[warp][k] + x];
+        uf[r0 + x] = om1 * uf[r0 + x] + (s * om) / ent[0].w;
+      }
+      __syncwarp();
+    }
+    __syncthreads();
+  }
+}
+
 // Restriction at coarse face-interior points from the fine face and its ghost layers: the fine
 // stencil structure of the face with weight 1 at the centre and 1/2 at every neighbour.
 template <class T>

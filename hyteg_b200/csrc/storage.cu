@@ -181,11 +181,41 @@ void Storage::buildLevel(int L) {
 
   // halo table in the five destination groups
   std::vector<uint2> comm;
-  for (int k = 0; k < G_COUNT; ++k) {
-    ld.commBegin[k] = (int64_t)comm.size();
-    for (size_t i = 0; i < lay.commDst[k].size(); ++i)
-      comm.push_back(make_uint2((unsigned)lay.commDst[k][i], (unsigned)lay.commSrc[k][i]));
-    ld.commCount[k] = (int64_t)comm.size() - ld.commBegin[k];
+  for (int g : kCommOrder) {
+    ld.commBegin[g] = (int64_t)comm.size();
+    for (size_t i = 0; i < lay.commDst[g].size(); ++i)
+      comm.push_back(make_uint2((unsigned)lay.commDst[g][i], (unsigned)lay.commSrc[g][i]));
+    ld.commCount[g] = (int64_t)comm.size() - ld.commBegin[g];
+  }
+  argCheck(comm.size() < (size_t(1) << 31), "halo table exceeds 32-bit ranges");
+  // Each primitive's entries of a group are contiguous (the tables are generated primitive by
+  // primitive): the range of every primitive's destination array, found from its offsets.
+  auto ranges = [&](int g, int kind, int nPrim) {
+    std::vector<int2> r((size_t)nPrim, make_int2(0, 0));
+    std::vector<char> seen((size_t)nPrim, 0);
+    int last = -1;
+    for (int64_t i = ld.commBegin[g]; i < ld.commBegin[g] + ld.commCount[g]; ++i) {
+      const int64_t d = comm[(size_t)i].x;
+      const auto& offs = lay.off[kind];
+      const int p = int(std::upper_bound(offs.begin(), offs.end(), d) - offs.begin()) - 1;
+      argCheck(p >= 0 && p < nPrim && d < offs[(size_t)p] + lay.size[kind][(size_t)p], "halo entry outside its group's kind");
+      if (p != last) {
+        argCheck(!seen[(size_t)p], "halo entries of a primitive are not contiguous");
+        seen[(size_t)p] = 1;
+        r[(size_t)p].x = (int)i;
+        last = p;
+      }
+      r[(size_t)p].y = (int)i + 1;
+    }
+    return r;
+  };
+  {
+    std::vector<int2> low = ranges(G_EDGE, KE, lv.nEdges);
+    std::vector<int2> vr = ranges(G_VERT, KV, (int)topo.verts.size());
+    low.insert(low.end(), vr.begin(), vr.end());
+    std::vector<int2> fr = ranges(G_FACE_BOUNDARY, KF, lv.nFaces);
+    if (!low.empty()) ld.lowRange = (const int2*)upload(ld.keep, low, stream);
+    if (!fr.empty()) ld.faceRange = (const int2*)upload(ld.keep, fr, stream);
   }
 
   auto& keep = ld.keep;
@@ -314,16 +344,16 @@ void Storage::communicate(int id, int L, int groupMask) {
   Function& f = fn(id);
   void* d = data(id, L);
   const LevelData& ld = levels[L];
-  // one gather per contiguous run of selected groups
-  int k = 0;
+  // one gather per contiguous run of selected groups in the table
+  int k = 0;  // position in the table order
   while (k < G_COUNT) {
-    if (!(groupMask & (1 << k))) {
+    if (!(groupMask & (1 << kCommOrder[k]))) {
       ++k;
       continue;
     }
-    const int64_t begin = ld.commBegin[k];
+    const int64_t begin = ld.commBegin[kCommOrder[k]];
     int64_t n = 0;
-    while (k < G_COUNT && (groupMask & (1 << k))) n += ld.commCount[k++];
+    while (k < G_COUNT && (groupMask & (1 << kCommOrder[k]))) n += ld.commCount[kCommOrder[k++]];
     if (n == 0) continue;
     if (f.prec == 8)
       dev::commGatherKernel<double><<<grid1d(n), 256, 0, stream>>>((double*)d, ld.comm + begin, n);
@@ -339,15 +369,15 @@ void Storage::communicateSplit(T* buf, T* cells, int L, int groupMask) {
   buildSplit(L);
   const LevelData& ld = levels[L];
   const uint2* table = ld.commSplit;
-  int k = 0;
+  int k = 0;  // position in the table order
   while (k < G_COUNT) {
-    if (!(groupMask & (1 << k))) {
+    if (!(groupMask & (1 << kCommOrder[k]))) {
       ++k;
       continue;
     }
-    const int64_t begin = ld.commBegin[k];
+    const int64_t begin = ld.commBegin[kCommOrder[k]];
     int64_t n = 0;
-    while (k < G_COUNT && (groupMask & (1 << k))) n += ld.commCount[k++];
+    while (k < G_COUNT && (groupMask & (1 << kCommOrder[k]))) n += ld.commCount[kCommOrder[k++]];
     if (n == 0) continue;
     dev::commGatherSplitKernel<T><<<grid1d(n), 256, 0, stream>>>(buf, cells, table + begin, n, ld.nonCellBegin);
     ++launches;
@@ -432,10 +462,10 @@ void Storage::buildSplit(int L) {
     }
     return (unsigned)slot;
   };
-  std::vector<uint2> comm;
-  for (int k = 0; k < G_COUNT; ++k)
-    for (size_t i = 0; i < lay.commDst[k].size(); ++i)
-      comm.push_back(make_uint2(map(lay.commDst[k][i]), map(lay.commSrc[k][i])));
+  std::vector<uint2> comm;  // the same entries in the same order as the level's table
+  for (int g : kCommOrder)
+    for (size_t i = 0; i < lay.commDst[g].size(); ++i)
+      comm.push_back(make_uint2(map(lay.commDst[g][i]), map(lay.commSrc[g][i])));
   const uint2* commSplit = comm.empty() ? ld.comm : (const uint2*)upload(ld.keep, comm, stream);
   // rows and points per colour
   for (int col = 0; col < 4; ++col) {
@@ -1866,6 +1896,48 @@ void Storage::sorT(Operator& o, int dstId, int L, T* u, const T* rhs, unsigned m
       }
     }
   };
+  // Fused phases: one launch per face, edge and vertex phase. The refresh of a group is folded
+  // into the phase when no owner of its copies belongs to a primitive of the phase: face boundary
+  // rows (owned by edges and vertices) before the faces, vertex ghosts (owned by edges, faces and
+  // cells) before the vertices of a backward sweep. Edge ghost layers end on the neighbouring
+  // edges and face ghost layers on other faces, so those refreshes stay launches of their own.
+  if (fusedSorPhases) {
+    const uint2* table = cellU ? ld.commSplit : ld.comm;
+    const int64_t cellEnd = ld.nonCellBegin;
+    T* cellsBuf = cellU;
+    auto lowPhase = [&](bool edgesNotVerts, bool gather, bool rev) {
+      const int first = edgesNotVerts ? 0 : lv.nEdges, n = edgesNotVerts ? lv.nEdges : lv.nLow - lv.nEdges;
+      if (n == 0 || !(kinds & (1 << (edgesNotVerts ? KE : KV)))) return;
+      dev::lowSorPhaseKernel<T><<<n, dev::kBlock, 0, stream>>>(lv, st, u, rhs, mask, omega, first, rev ? 1 : 0, table,
+                                                             gather && refresh ? ld.lowRange : nullptr, cellsBuf, cellEnd);
+      ++launches;
+    };
+    auto facePhase = [&](bool gather, bool rev) {
+      if (lv.nFaceBlocks == 0 || !(kinds & (1 << KF))) return;
+      dev::faceSorPhaseKernel<T><<<lv.nFaces, dev::kFacePhaseThreads, 0, stream>>>(
+          lv, st, u, rhs, mask, omega, rev ? 1 : 0, table, gather && refresh ? ld.faceRange : nullptr, cellsBuf, cellEnd);
+      ++launches;
+    };
+    if (!backwards) {
+      comm((1 << G_VERT) | (1 << G_FACE_GHOST));
+      lowPhase(false, false, false);  // vertices
+      comm(1 << G_EDGE);              // Vertex -> Edge
+      lowPhase(true, false, false);   // edges
+      facePhase(true, false);         // Edge -> Face, faces
+      comm(1 << G_CELL);              // Face -> Cell
+      cellPhase(false);
+    } else {
+      comm((1 << G_CELL) | (1 << G_FACE_BOUNDARY));
+      cellPhase(true);
+      comm(1 << G_FACE_GHOST);        // Cell -> Face
+      facePhase(false, true);
+      comm(1 << G_EDGE);              // Face -> Edge
+      lowPhase(true, false, true);    // edges
+      lowPhase(false, true, true);    // Edge -> Vertex, vertices
+    }
+    cudaCheck(cudaGetLastError(), "sor");
+    return;
+  }
   // Only the copies the reference refreshes between phases are refreshed here, so ghost
   // values that reach a primitive from outside its closure keep their start-of-sweep value.
   // At the start only the groups read before their own refresh in this sweep are brought up to

@@ -25,6 +25,11 @@ struct DevBuf {
   void* alloc(size_t n);
 };
 
+// Order of the halo groups in a level's table: every group set one SOR phase refreshes at once
+// (vertex ghosts with face ghost layers, cell closures with face boundary rows, all five) is one
+// contiguous run, so a refresh is one launch.
+constexpr int kCommOrder[G_COUNT] = {G_EDGE, G_VERT, G_FACE_GHOST, G_CELL, G_FACE_BOUNDARY};
+
 struct LevelData {
   const LevelLayout* lay = nullptr;
   dev::LevelDev lv{};
@@ -45,6 +50,10 @@ struct LevelData {
   dev::WaveTile* waveTiles[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   int nWaveTiles[2][2] = {{0, 0}, {0, 0}};
   int64_t nonCellBegin = 0;  // first slot after the cell arrays (faces, edges, vertices follow)
+  // per primitive, its entries (begin, end) in comm of the group the SOR refreshes before its
+  // phase: low primitives (edges: G_EDGE, vertices: G_VERT), faces (G_FACE_BOUNDARY)
+  const int2* lowRange = nullptr;
+  const int2* faceRange = nullptr;
   // SOR schedule 3 (built on first use): the halo table with every cell slot at its colour-split
   // position (same groups as comm), and per colour the rows and points of the cell interiors
   const uint2* commSplit = nullptr;
@@ -163,6 +172,9 @@ struct Storage {
   // wavefront pass with the shorter tile geometry, 3 = four colour passes on a copy of the
   // cell arrays in the colour-split order (converted once per group of sweeps).
   int sorSchedule = 0;
+  // Face, edge and vertex phases of the SOR: one launch per phase with the refresh of each
+  // primitive's copies folded in (1, default), or one launch per colour and per refresh (0).
+  int fusedSorPhases = 1;
   std::vector<int> sorScheduleLevel;  // [2 L + (FP32 ? 1 : 0)]: schedule chosen by autotuneSor (-1: sorSchedule)
   int sorScheduleFor(int L, int prec) const;
   // Times the four schedules of the SOR on levels [minL, maxL] in the given precision, in groups

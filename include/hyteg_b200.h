@@ -120,6 +120,12 @@ int hg_storage_set_cell_coefficients(hg_storage* s, const double* k, int ncells)
  * of a multigrid smoothing step and the result is copied back). All give the same multicolour
  * sweep. */
 int hg_storage_set_sor_schedule(hg_storage* s, int schedule);
+/* Launch structure of the face, edge and vertex phases of the multicolour SOR (no counterpart in
+ * the reference; the same sweep either way, bit for bit): on = 1 (default) runs each phase as one
+ * launch, a block per primitive doing the phase's colours in turn, with the refresh of the face
+ * boundary rows (before the faces) and of the vertex ghosts (before the vertices of a backward
+ * sweep) folded in; on = 0 runs one launch per colour and per refresh. */
+int hg_storage_set_sor_fused_phases(hg_storage* s, int on);
 /* Autotuner (no counterpart in the reference): times the multicolour SOR under the four
  * schedules on every level in [min_level, max_level] (precision 8 or 4; `reps` timed groups of
  * three sweeps, the smoothing step of a V(3,3) cycle, after one warm-up group; CUDA events on the

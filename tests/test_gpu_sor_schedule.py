@@ -168,3 +168,26 @@ def test_colour_split_cycles_equal_colour_pass_cycles(cube6, dtype, tol, graphs)
                 st.set_sor_schedule(0)
         m = owned == 1
         assert np.abs(res[0][m] - res[1][m]).max() / np.abs(res[0][m]).max() < tol
+
+
+@pytest.mark.parametrize("L", [3, 6])
+@pytest.mark.parametrize("backwards", [False, True])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("schedule", [0, 1, 3])
+def test_fused_phases_equal_per_colour_launches(cube6, L, backwards, dtype, schedule):
+    """The face, edge and vertex phases as one launch each (halo refreshes folded in where no
+    owner changes) against one launch per colour and per refresh: the whole level buffer, copies
+    included, must agree bit for bit after two sweeps."""
+    st, mesh = cube6
+    n = st.level_size(L)
+    rng = np.random.default_rng(40 + L + 3 * backwards)
+    x0 = rng.uniform(-1, 1, n).astype(dtype)
+    b0 = rng.uniform(-1, 1, n).astype(dtype)
+    out = []
+    try:
+        for fused in (True, False):
+            st.set_sor_fused_phases(fused)
+            out.append(run_sor(st, L, x0, b0, dtype, schedule, 2, backwards))
+    finally:
+        st.set_sor_fused_phases(True)
+    assert np.array_equal(out[0], out[1])
