@@ -310,7 +310,10 @@ def serving_bench(hg, n_requests, n_sequential, seed=2024):
     4x and 8x that sequential service rate (the last saturates it: its throughput is the server's
     capacity). Latency = completion - arrival (server clock). Setup = admission to the start of
     the solve: the stencil re-assembly for the request's coefficient on a resident hierarchy, or
-    building a hierarchy when none of the request's shape is free."""
+    building a hierarchy when none of the request's shape is free. A second server adds batched
+    solves: every shape of levels 3-5 also gets a union hierarchy of 8 disjoint copies, in which up
+    to 8 queued requests of that shape are solved together (one launch per kernel for all of
+    them); it runs the stream at 2x and 8x."""
     rng = np.random.default_rng(seed)
     reqs = [(int(rng.integers(1, 5)), int(rng.integers(3, 7)), float(np.exp(rng.uniform(np.log(0.1), np.log(10.0)))),
              int(rng.integers(1, 2 ** 62))) for _ in range(n_requests)]
@@ -341,6 +344,7 @@ def serving_bench(hg, n_requests, n_sequential, seed=2024):
         dofs = sum(r["inner_dofs"] for r in res)
         setup = np.array([r["t_solve"] - r["t_start"] for r in res])
         built = np.array([r["built_hierarchy"] for r in res])
+        bsz = np.array([r["batch_size"] for r in res])
         return {"requests": len(res), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "seconds": span, "gdofs": dofs / span / 1e9,
                 "max_rel_residual": max(r["rel_residual"] for r in res),
@@ -349,7 +353,8 @@ def serving_bench(hg, n_requests, n_sequential, seed=2024):
                 "hierarchies_built_on_admission": int(built.sum()),
                 "mean_setup_ms_resident": float(setup[~built].mean() * 1e3) if (~built).any() else None,
                 "mean_setup_ms_built": float(setup[built].mean() * 1e3) if built.any() else None,
-                "mean_solve_ms": float(np.mean([r["t_end"] - r["t_solve"] for r in res]) * 1e3)}
+                "mean_solve_ms": float(np.mean([r["t_end"] - r["t_solve"] for r in res]) * 1e3),
+                "requests_batched": int((bsz > 1).sum()), "mean_batch_size": float(bsz.mean())}
 
     srv = make(1, 8, 1)
     seq = run(srv, 0, reqs[:n_sequential])  # all submitted at once, one worker: sequential FP64 solves
@@ -364,6 +369,19 @@ def serving_bench(hg, n_requests, n_sequential, seed=2024):
         out["mixed_rate_%gx" % mult] = dict(run(srv, mult * mu, reqs), arrival_rate_per_s=mult * mu)
     srv.close()
     out["capacity_vs_sequential"] = out["mixed_rate_8x"]["gdofs"] / seq["gdofs"]
+    # batched solves: the shapes of levels 3-5 also get one union hierarchy of 8 copies each; two
+    # or more queued requests of such a shape are solved together in it
+    t0 = time.perf_counter()
+    srv = make(8, 4, 2)
+    for k, L in shapes:
+        if L <= 5:
+            srv.prewarm_batch(k, L, 8)
+    srv.set_batching(5)
+    out["batched_prewarm_seconds"] = time.perf_counter() - t0
+    for mult in (2.0, 8.0):
+        out["batched_rate_%gx" % mult] = dict(run(srv, mult * mu, reqs), arrival_rate_per_s=mult * mu)
+    srv.close()
+    out["batched_capacity_vs_sequential"] = out["batched_rate_8x"]["gdofs"] / seq["gdofs"]
     return out
 
 

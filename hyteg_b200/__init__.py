@@ -72,6 +72,13 @@ class HostMesh:
         return cls(h, max_level)
 
     @classmethod
+    def cuboid_copies(cls, k, copies, max_level):
+        """The solve server's union macro-mesh: `copies` disjoint copies of the k^3 cube."""
+        h = ctypes.c_void_p()
+        call("hg_mesh_create_cuboid_copies", int(k), int(copies), max_level, ctypes.byref(h))
+        return cls(h, max_level)
+
+    @classmethod
     def cubed_domain(cls, cubes, cube_type, max_level):
         """MeshInfo::meshCubedDomain(cubeCoordinates, cubeType) (MeshGenCubedDomain.cpp:115-383)."""
         h = ctypes.c_void_p()
@@ -860,6 +867,16 @@ class SolveServer:
     def prewarm(self, k, level):
         call("hg_server_prewarm", self._h, int(k), int(level))
 
+    def set_batching(self, max_level):
+        """Solve queued requests of levels up to max_level (-1: none) together, several in one
+        union hierarchy of their shape (see prewarm_batch), when at least two of a shape wait."""
+        call("hg_server_set_batching", self._h, int(max_level))
+
+    def prewarm_batch(self, k, level, copies):
+        """Build one resident union hierarchy: `copies` disjoint copies of shape (k, level) in one
+        storage, which solves up to `copies` requests of that shape at once."""
+        call("hg_server_prewarm_batch", self._h, int(k), int(level), int(copies))
+
     def submit(self, k, level, coefficient=1.0, seed=0, tol=1e-8, max_iter=100, keep_solution=False):
         i = ctypes.c_int64()
         call("hg_server_submit", self._h, int(k), int(level), float(coefficient), ctypes.c_uint64(seed), float(tol),
@@ -873,7 +890,8 @@ class SolveServer:
 
     def result(self, rid):
         """dict(status, iterations, rel_residual, t_submit, t_start, t_solve, t_end, inner_dofs,
-        built_hierarchy); raises for a failed request. built_hierarchy: no resident hierarchy of the
+        built_hierarchy, batch_size); raises for a failed request. batch_size: the requests solved
+        together with it in one union hierarchy (1: solved alone). built_hierarchy: no resident hierarchy of the
         request's shape was free when it was admitted, so one was built for it (its setup time,
         t_solve - t_start, includes that)."""
         st, it = ctypes.c_int(), ctypes.c_int()
@@ -884,9 +902,11 @@ class SolveServer:
         call("hg_server_result", self._h, int(rid), ctypes.byref(st), ctypes.byref(it), ctypes.byref(rel), dptr(t),
              ctypes.byref(n))
         call("hg_server_request_setup", self._h, int(rid), ctypes.byref(built))
+        batch = ctypes.c_int()
+        call("hg_server_request_batch", self._h, int(rid), ctypes.byref(batch))
         return {"status": st.value, "iterations": it.value, "rel_residual": rel.value, "t_submit": t[0],
                 "t_start": t[1], "t_solve": t[2], "t_end": t[3], "inner_dofs": n.value,
-                "built_hierarchy": bool(built.value)}
+                "built_hierarchy": bool(built.value), "batch_size": batch.value}
 
     def solution(self, rid):
         n = ctypes.c_int64()

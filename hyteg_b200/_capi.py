@@ -53,6 +53,7 @@ _SIGS = {
     "hg_level_size": (c_int, [c_void_p, c_int, P(c_int64)]),
     "hg_mesh_create_cuboid": (c_int, [P(c_double), P(c_double), c_int, c_int, c_int, c_int, P(c_void_p)]),
     "hg_mesh_create_tets": (c_int, [c_int, P(c_double), c_int, P(c_int), c_int, P(c_void_p)]),
+    "hg_mesh_create_cuboid_copies": (c_int, [c_int, c_int, c_int, P(c_void_p)]),
     "hg_mesh_create_cubed_domain": (c_int, [c_int, P(c_int), c_int, c_int, P(c_void_p)]),
     "hg_mesh_create_gmsh": (c_int, [c_char_p, c_int, c_int, P(c_void_p)]),
     "hg_mesh_write_gmsh": (c_int, [c_void_p, c_char_p]),
@@ -137,6 +138,9 @@ _SIGS = {
     "hg_server_wait": (c_int, [c_void_p, c_int64, c_double, P(c_int)]),
     "hg_server_result": (c_int, [c_void_p, c_int64, P(c_int), P(c_int), P(c_double), P(c_double), P(c_int64)]),
     "hg_server_request_setup": (c_int, [c_void_p, c_int64, P(c_int)]),
+    "hg_server_set_batching": (c_int, [c_void_p, c_int]),
+    "hg_server_prewarm_batch": (c_int, [c_void_p, c_int, c_int, c_int]),
+    "hg_server_request_batch": (c_int, [c_void_p, c_int64, P(c_int)]),
     "hg_server_solution": (c_int, [c_void_p, c_int64, P(c_double), c_int64, P(c_int64)]),
     "hg_server_stats": (c_int, [c_void_p, P(c_int64)]),
     "hg_function_fill_random": (c_int, [c_void_p, c_int, c_int, c_uint, ctypes.c_uint64, c_double, c_double]),

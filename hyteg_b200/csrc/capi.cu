@@ -592,6 +592,14 @@ int hg_mesh_create_cuboid(const double lo[3], const double hi[3], int nx, int ny
   HG_CATCH
 }
 
+int hg_mesh_create_cuboid_copies(int k, int copies, int max_level, hg_mesh** out) {
+  HG_TRY
+  hg::argCheck(k >= 1 && k <= 16 && copies >= 1 && copies <= 64, "copies of a cube: k in [1, 16], copies in [1, 64]");
+  hg::argCheck(max_level >= 0 && max_level <= 10, "max_level out of range [0,10]");
+  return meshFrom(hg::meshCuboidCopies(k, copies), max_level, out);
+  HG_CATCH
+}
+
 int hg_mesh_create_tets(int nverts, const double* coords, int ncells, const int* tets, int max_level, hg_mesh** out) {
   HG_TRY
   hg::argCheck(nverts > 0 && ncells > 0 && coords && tets, "empty mesh");
@@ -1140,6 +1148,27 @@ int hg_server_result(hg_server* srv, int64_t id, int* status, int* iterations, d
   }
   if (inner_dofs) *inner_dofs = r->innerDofs;
   if (r->status < 0) throw hg::Error(HG_ERR_STATE, "request failed: " + r->error);
+  HG_CATCH
+}
+
+int hg_server_set_batching(hg_server* srv, int max_level) {
+  HG_TRY
+  hg::argCheck(max_level >= -1 && max_level <= 8, "batching: max_level must be in [-1, 8]");
+  SV(srv).setBatching(max_level);
+  HG_CATCH
+}
+
+int hg_server_prewarm_batch(hg_server* srv, int k, int level, int copies) {
+  HG_TRY
+  hg::argCheck(k >= 1 && k <= 16 && level >= 2 && level <= 8, "shape out of range");
+  SV(srv).prewarmBatch(k, level, copies);
+  HG_CATCH
+}
+
+int hg_server_request_batch(hg_server* srv, int64_t id, int* batch_size) {
+  HG_TRY
+  hg::argCheck(batch_size != nullptr, "null output pointer");
+  *batch_size = SV(srv).request(id)->batchSize;
   HG_CATCH
 }
 

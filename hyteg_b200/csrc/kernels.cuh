@@ -985,12 +985,15 @@ __global__ void __launch_bounds__(kBlock) lowStencilKernel(LevelDev lv, StencilD
 }
 
 // ---------------------------------------------------------------------------------------
-// Coarse-grid CG in one block (CGSolver.hpp:69-150 with the identity preconditioner) for a
-// level whose DoFs all sit on vertices and edges (levels 0 and 1). The halo refresh, stencil,
-// dot products and updates of every iteration run on the device, so a multigrid cycle needs no
-// host synchronisation. Vector updates touch the owned DoFs; the copies of the source of every
-// apply, and of x at the end, are refreshed from their owners. r, p and ap are workspace level
-// buffers; info[0] = iterations, info[1] = final residual norm.
+// Coarse-grid CG (CGSolver.hpp:69-150 with the identity preconditioner) for a level whose DoFs
+// all sit on vertices and edges (levels 0 and 1), one block per group of unknowns: the whole
+// mesh, or one copy of a storage of disjoint copies (the copies' systems are not coupled, so
+// each copy iterates and stops on its own, exactly as a single mesh of it does). The halo
+// refresh, stencil, dot products and updates of every iteration run on the device, so a
+// multigrid cycle needs no host synchronisation. Vector updates touch the group's owned DoFs
+// (a flat list, thread t takes every blockDim-th); the copies of the source of every apply, and
+// of x at the end, are refreshed from their owners. r, p and ap are workspace level buffers;
+// info (optional): per group [iterations, final residual norm].
 // ---------------------------------------------------------------------------------------
 __device__ __forceinline__ double blockSum(double v, double* red) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -1007,49 +1010,50 @@ __device__ __forceinline__ double blockSum(double v, double* red) {
   return red[32];
 }
 
-static __global__ void __launch_bounds__(kBlock) coarseCgKernel(LevelDev lv, StencilDev<double> st, const uint2* __restrict__ comm,
-                                                        int64_t nComm, double* x, const double* __restrict__ b,
-                                                        double* r, double* p, double* ap, unsigned mask, int maxIter,
-                                                        double tol, double* info) {
+// One owned DoF of the coarse CG: its slot and the stencil entries [e0, e1) of its primitive.
+struct CoarseDof {
+  int64_t slot;
+  int e0, e1;
+};
+
+static __global__ void __launch_bounds__(kBlock) coarseCgKernel(StencilDev<double> st, const CoarseDof* __restrict__ dofs,
+                                                        const int* __restrict__ dofOff, const uint2* __restrict__ comm,
+                                                        const int* __restrict__ commOff, double* x,
+                                                        const double* __restrict__ b, double* r, double* p, double* ap,
+                                                        int maxIter, double tol, double* info) {
   __shared__ double red[33];
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, g = blockIdx.x;
+  const int d0 = dofOff[g], d1 = dofOff[g + 1], c0 = commOff[g], c1 = commOff[g + 1];
   auto refresh = [&](double* v) {
     __syncthreads();
-    for (int64_t i = tid; i < nComm; i += blockDim.x) {
+    for (int i = c0 + tid; i < c1; i += blockDim.x) {
       const uint2 t = comm[i];
       v[t.x] = v[t.y];
     }
     __syncthreads();
   };
-  // visit every owned DoF of the flagged vertices and edges: f(slot)
   auto forOwned = [&](auto f) {
-    for (int blk = 0; blk < lv.nLowBlocks; ++blk) {
-      const LowBlock lb = lv.lowBlocks[blk];
-      if (!(lv.lowType[lb.prim] & mask)) continue;
-      for (int xx = lb.start + tid; xx < lb.start + (int)blockDim.x && xx < lv.lowFirst[lb.prim] + lv.lowCount[lb.prim];
-           xx += blockDim.x)
-        f(lb.prim, lv.lowOff[lb.prim] + xx);
-    }
+    for (int i = d0 + tid; i < d1; i += blockDim.x) f(dofs[i]);
   };
-  auto apply = [&](double* dst, double* src) {  // dst = A src on the flagged DoFs
+  auto apply = [&](double* dst, double* src) {  // dst = A src on the group's DoFs
     refresh(src);
-    forOwned([&](int prim, int64_t c) {
+    forOwned([&](const CoarseDof& d) {
       double s = 0;
-      for (int k = st.lowEntOff[prim]; k < st.lowEntOff[prim + 1]; ++k) s += st.lowEntW[k] * src[c + st.lowEntRel[k]];
-      dst[c] = s;
+      for (int k = d.e0; k < d.e1; ++k) s += st.lowEntW[k] * src[d.slot + st.lowEntRel[k]];
+      dst[d.slot] = s;
     });
     __syncthreads();
   };
   auto dot = [&](const double* u, const double* v) {
     double s = 0;
-    forOwned([&](int, int64_t c) { s += u[c] * v[c]; });
+    forOwned([&](const CoarseDof& d) { s += u[d.slot] * v[d.slot]; });
     return blockSum(s, red);
   };
   // r = b - A x; p = z = r (identity preconditioner)
   apply(p, x);
-  forOwned([&](int, int64_t c) {
-    r[c] = b[c] - p[c];
-    p[c] = r[c];
+  forOwned([&](const CoarseDof& d) {
+    r[d.slot] = b[d.slot] - p[d.slot];
+    p[d.slot] = r[d.slot];
   });
   __syncthreads();
   double prsold = dot(r, r);
@@ -1060,24 +1064,24 @@ static __global__ void __launch_bounds__(kBlock) coarseCgKernel(LevelDev lv, Ste
       it = i + 1;
       apply(ap, p);
       const double alpha = prsold / dot(p, ap);
-      forOwned([&](int, int64_t c) {
-        x[c] += alpha * p[c];
-        r[c] -= alpha * ap[c];
+      forOwned([&](const CoarseDof& d) {
+        x[d.slot] += alpha * p[d.slot];
+        r[d.slot] -= alpha * ap[d.slot];
       });
       __syncthreads();
       const double rsnew = dot(r, r);
       res = sqrt(rsnew);
       if (res < tol) break;
       const double beta = rsnew / prsold;
-      forOwned([&](int, int64_t c) { p[c] = r[c] + beta * p[c]; });
+      forOwned([&](const CoarseDof& d) { p[d.slot] = r[d.slot] + beta * p[d.slot]; });
       __syncthreads();
       prsold = rsnew;
     }
   }
   refresh(x);
   if (tid == 0 && info) {
-    info[0] = it;
-    info[1] = res;
+    info[2 * g] = it;
+    info[2 * g + 1] = res;
   }
 }
 
@@ -2231,6 +2235,62 @@ static __global__ void __launch_bounds__(kBlock) reduceKernel(const double* __re
   for (int i = threadIdx.x; i < n; i += blockDim.x) v += partial[i];
   const double r = blockReduce<double>(v);
   if (threadIdx.x == 0) *out = r;
+}
+
+// ---------------------------------------------------------------------------------------
+// Batched solves: a union storage holds `copies` disjoint copies of one macro-mesh, each kind of
+// primitive (cells, faces, edges, vertices, the level buffer's order) copy after copy, each copy
+// in a single mesh's order. Per kind: the first slot of the union, the slots of one copy, and the
+// first slot of the kind in one copy's own layout. Per segment of the dot product's partial sums
+// (cell, face, edge and vertex blocks): the first block of the union and the blocks of one copy.
+// ---------------------------------------------------------------------------------------
+struct BatchMap {
+  int copies;
+  int64_t uBase[4], size[4], aBase[4];
+  int bBase[4], bCount[4];
+};
+
+// Right-hand sides of the copies: copy i < active gets at every slot of its flagged primitives
+// the value a storage of the single mesh gets from seeds[i] at the same slot of its own layout
+// (randomFillKernel); the copies from `active` on get 0. A chunk lies in one primitive array.
+template <class T>
+__global__ void __launch_bounds__(kBlock) randomFillBatchKernel(const Chunk* __restrict__ chunks, unsigned mask, T* dst,
+                                                                BatchMap bm, const uint64_t* __restrict__ seeds,
+                                                                int active, double lo, double hi) {
+  const Chunk ch = chunks[blockIdx.x];
+  if (!(ch.type & mask)) return;
+  int k = 3;
+  while (k > 0 && ch.start < bm.uBase[k]) --k;
+  const int64_t rel = ch.start - bm.uBase[k];
+  const int copy = int(rel / bm.size[k]);
+  if (copy >= active) {
+    for (int i = threadIdx.x; i < ch.len; i += blockDim.x) dst[ch.start + i] = T(0);
+    return;
+  }
+  const int64_t local0 = bm.aBase[k] + (rel - int64_t(copy) * bm.size[k]);
+  const uint64_t s = splitmix64(seeds[copy]);
+  for (int i = threadIdx.x; i < ch.len; i += blockDim.x) {
+    const double u = double(splitmix64(s ^ uint64_t(local0 + i)) >> 11) * (1.0 / 9007199254740992.0);
+    dst[ch.start + i] = T(lo + (hi - lo) * u);
+  }
+}
+
+// Per-copy dot products from dotKernel's per-block partial sums of the union: block i sums copy
+// i's partials in the order reduceKernel sums those of a single mesh (cell, face, edge, vertex
+// blocks; thread t takes every blockDim-th), so each copy's value equals its single-mesh dot
+// product bit for bit.
+static __global__ void __launch_bounds__(kBlock) batchReduceKernel(const double* __restrict__ partial, BatchMap bm,
+                                                                   double* out) {
+  const int copy = blockIdx.x;
+  const int n = bm.bCount[0] + bm.bCount[1] + bm.bCount[2] + bm.bCount[3];
+  double v = 0.0;
+  for (int a = threadIdx.x; a < n; a += blockDim.x) {
+    int k = 0, r = a;
+    while (r >= bm.bCount[k]) r -= bm.bCount[k++];
+    v += partial[bm.bBase[k] + copy * bm.bCount[k] + r];
+  }
+  const double r = blockReduce<double>(v);
+  if (threadIdx.x == 0) out[copy] = r;
 }
 
 }  // namespace dev

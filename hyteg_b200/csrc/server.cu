@@ -7,6 +7,7 @@
 #include <cmath>
 
 #include "../../include/hyteg_b200.h"
+#include "kernels.cuh"
 #include "solvers.hpp"
 #include "storage.hpp"
 #include "topology.hpp"
@@ -14,6 +15,7 @@
 namespace hg {
 
 ServerSlot::~ServerSlot() = default;
+BatchSlot::~BatchSlot() = default;
 
 Server::Server(int workers, int64_t budgetBytes, int precision)
     : precision_(precision), budget_(budgetBytes), t0_(std::chrono::steady_clock::now()) {
@@ -43,6 +45,7 @@ Server::~Server() {
   doneCv_.notify_all();
   for (auto& t : threads_) t.join();
   idle_.clear();
+  idleBatch_.clear();
 }
 
 double Server::now() const {
@@ -112,6 +115,108 @@ std::unique_ptr<ServerSlot> Server::buildSlot(int k, int level) {
   return s;
 }
 
+std::unique_ptr<BatchSlot> Server::buildBatchSlot(int k, int level, int copies) {
+  std::unique_ptr<BatchSlot> s(new BatchSlot());
+  s->k = k;
+  s->level = level;
+  s->copies = copies;
+  Topology t = meshCuboidCopies(k, copies);
+  t.setBoundaryFlags(1, 0);
+  s->st.reset(new Storage(t, level));
+  Storage& st = *s->st;
+  s->x = st.createFunction(0, level, 8);
+  s->b = st.createFunction(0, level, 8);
+  s->xOut = st.createFunction(level, level, 8);
+  s->op = st.createOperator(0, 0, level);
+  st.reassembleOperator(s->op, true);  // the term lists, so that batches only run the kernels
+  s->gmg = st.nextId++;
+  st.gmgs[s->gmg].reset(new Gmg(st, s->op, 0, level, 3, 3, 1.0, 0, 200, 1e-16, precision_));
+  if (st.gmgs[s->gmg]->deviceCoarse()) st.gmgs[s->gmg]->setCoarseGroups(copies);  // copies stop on their own
+  s->seeds.reset(new DevBuf());
+  s->seeds->alloc((size_t)copies * sizeof(uint64_t));
+  s->norms.reset(new DevBuf());
+  s->norms->alloc((size_t)copies * sizeof(double));
+  // one iteration over all copies, so that every buffer and graph exists before the footprint
+  const dev::BatchMap bm = st.batchMap(level, copies);
+  std::vector<uint64_t> seeds((size_t)copies, 1);
+  cudaCheck(cudaMemcpyAsync(s->seeds->p, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, st.stream), "seeds");
+  st.fillRandomBatch(s->b, level, HG_INNER, bm, (const uint64_t*)s->seeds->p, copies, -1.0, 1.0);
+  std::vector<double> tol((size_t)copies, 1e-30), rel((size_t)copies);
+  std::vector<int> maxIt((size_t)copies, 1), its((size_t)copies);
+  st.gmgs[s->gmg]->solveToBatch(s->x, s->b, s->xOut, level, tol.data(), maxIt.data(), bm, copies,
+                                (double*)s->norms->p, its.data(), rel.data());
+  cudaCheck(cudaStreamSynchronize(st.stream), "batch slot build");
+  s->bytes = st.deviceBytes();
+  return s;
+}
+
+void Server::setBatching(int maxLevel) {
+  std::lock_guard<std::mutex> lk(mu_);
+  batchMaxLevel_ = maxLevel;
+}
+
+void Server::prewarmBatch(int k, int level, int copies) {
+  argCheck(copies >= 2 && copies <= 64, "batch copies must be in [2, 64]");
+  std::unique_ptr<BatchSlot> s = buildBatchSlot(k, level, copies);
+  std::lock_guard<std::mutex> lk(mu_);
+  if (active_ + resident_ + s->bytes > budget_) throw Error(HG_ERR_OOM, "batch prewarm exceeds the HBM budget");
+  resident_ += s->bytes;
+  peak_ = std::max(peak_, active_ + resident_);
+  s->lastUse = ++useClock_;
+  idleBatch_.push_back(std::move(s));
+}
+
+// A batch: one solve of up to s.copies requests of one shape in the union hierarchy. The cells of
+// copy i take request i's coefficient (device re-assembly), copy i's right-hand side is the one
+// its seed gives a single cube, the other copies get 0.
+void Server::runBatch(std::vector<std::shared_ptr<ServerRequest>>& rs, BatchSlot& s) {
+  Storage& st = *s.st;
+  const int L = s.level, active = (int)rs.size();
+  const dev::BatchMap bm = st.batchMap(L, s.copies);
+  auto& cells = const_cast<Topology&>(st.disc.topo()).cells;
+  const size_t per = cells.size() / (size_t)s.copies;
+  bool changed = false;
+  for (int i = 0; i < active; ++i)
+    for (size_t c = (size_t)i * per; c < (size_t)(i + 1) * per; ++c)
+      if (cells[c].k != rs[(size_t)i]->coefficient) {
+        cells[c].k = rs[(size_t)i]->coefficient;
+        changed = true;
+      }
+  if (changed) st.reassembleOperator(s.op, true);
+  std::vector<uint64_t> seeds((size_t)s.copies, 0);
+  std::vector<double> tol((size_t)active), rel((size_t)active);
+  std::vector<int> maxIt((size_t)active), its((size_t)active);
+  for (int i = 0; i < active; ++i) {
+    seeds[(size_t)i] = rs[(size_t)i]->seed;
+    tol[(size_t)i] = rs[(size_t)i]->tol;
+    maxIt[(size_t)i] = rs[(size_t)i]->maxIter;
+  }
+  {
+    const double t = now();
+    std::lock_guard<std::mutex> lk(mu_);
+    for (auto& r : rs) r->tSolve = t;
+  }
+  cudaCheck(cudaMemcpyAsync(s.seeds->p, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, st.stream), "seeds");
+  st.fillRandomBatch(s.b, L, HG_INNER, bm, (const uint64_t*)s.seeds->p, active, -1.0, 1.0);
+  st.lincomb(s.x, L, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+  st.gmgs[s.gmg]->solveToBatch(s.x, s.b, s.xOut, L, tol.data(), maxIt.data(), bm, active, (double*)s.norms->p,
+                               its.data(), rel.data());
+  for (int i = 0; i < active; ++i) {
+    ServerRequest& r = *rs[(size_t)i];
+    r.iterations = its[(size_t)i];
+    r.relResidual = rel[(size_t)i];
+    if (r.keepSolution) {  // the copy's slots, at their places in a single cube's level buffer
+      r.solution.assign((size_t)(bm.aBase[3] + bm.size[3]), 0.0);
+      for (int q = 0; q < 4; ++q)
+        if (bm.size[q] > 0)
+          cudaCheck(cudaMemcpyAsync(r.solution.data() + bm.aBase[q], (const double*)st.data(s.xOut, L) + bm.uBase[q] + i * bm.size[q],
+                                    (size_t)bm.size[q] * sizeof(double), cudaMemcpyDeviceToHost, st.stream),
+                    "solution download");
+    }
+  }
+  cudaCheck(cudaStreamSynchronize(st.stream), "batch sync");
+}
+
 void Server::prewarm(int k, int level) {
   std::unique_ptr<ServerSlot> s = buildSlot(k, level);
   std::lock_guard<std::mutex> lk(mu_);
@@ -153,6 +258,8 @@ void Server::worker() {
   for (;;) {
     std::shared_ptr<ServerRequest> r;
     std::unique_ptr<ServerSlot> slot;
+    std::unique_ptr<BatchSlot> bslot;
+    std::vector<std::shared_ptr<ServerRequest>> batch;
     std::vector<std::unique_ptr<ServerSlot>> evict;
     int64_t est = 0;
     {
@@ -161,6 +268,41 @@ void Server::worker() {
         if (stopping_) return;
         if (!queue_.empty()) {
           std::shared_ptr<ServerRequest> h = queue_.front();
+          if (h->level <= batchMaxLevel_ && !idleBatch_.empty()) {
+            // requests of the head's shape waiting, in arrival order: with two or more, the smallest
+            // idle union hierarchy of the shape that takes them all (else the largest) takes the
+            // first of them
+            int nSame = 0;
+            for (auto& q : queue_)
+              if (q->k == h->k && q->level == h->level) ++nSame;
+            int best = -1;
+            for (int i = 0; i < (int)idleBatch_.size() && nSame >= 2; ++i) {
+              const BatchSlot& b = *idleBatch_[(size_t)i];
+              if (b.k != h->k || b.level != h->level) continue;
+              if (best < 0) {
+                best = i;
+                continue;
+              }
+              const int cb = idleBatch_[(size_t)best]->copies;
+              const bool fitsB = b.copies >= nSame, fitsBest = cb >= nSame;
+              if ((fitsB && (!fitsBest || b.copies < cb)) || (!fitsB && !fitsBest && b.copies > cb)) best = i;
+            }
+            if (best >= 0) {
+              bslot = std::move(idleBatch_[(size_t)best]);
+              idleBatch_.erase(idleBatch_.begin() + best);
+              resident_ -= bslot->bytes;
+              active_ += bslot->bytes;
+              std::deque<std::shared_ptr<ServerRequest>> rest;
+              for (auto& q : queue_) {
+                if ((int)batch.size() < bslot->copies && q->k == h->k && q->level == h->level)
+                  batch.push_back(q);
+                else
+                  rest.push_back(q);
+              }
+              queue_.swap(rest);
+              break;
+            }
+          }
           auto same = std::find_if(idle_.begin(), idle_.end(), [&](const std::unique_ptr<ServerSlot>& s) {
             return s->k == h->k && s->level == h->level;
           });
@@ -209,8 +351,51 @@ void Server::worker() {
         ++admitted_;
         peak_ = std::max(peak_, active_ + resident_);
       }
+      if (bslot) {
+        const double t = now();
+        for (auto& q : batch) {
+          q->status = 1;
+          q->tStart = t;
+          q->batchSize = (int)batch.size();
+          ++admitted_;
+        }
+        peak_ = std::max(peak_, active_ + resident_);
+      }
     }
     evict.clear();
+    if (bslot) {
+      std::string err;
+      try {
+        runBatch(batch, *bslot);
+      } catch (const std::exception& e) {
+        err = e.what();
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        const double t = now();
+        for (auto& q : batch) {
+          q->tEnd = t;
+          if (err.empty()) {
+            q->status = 2;
+            ++completed_;
+          } else {
+            q->status = -1;
+            q->error = err;
+            ++failed_;
+          }
+        }
+        active_ -= bslot->bytes;
+        if (err.empty()) {
+          bslot->lastUse = ++useClock_;
+          resident_ += bslot->bytes;
+          idleBatch_.push_back(std::move(bslot));
+        }
+      }
+      bslot.reset();  // a failed union hierarchy is released
+      cv_.notify_all();
+      doneCv_.notify_all();
+      continue;
+    }
     if (!r) continue;
     std::string err;
     if (!slot) {
@@ -286,7 +471,7 @@ void Server::stats(int64_t out[6]) {
   out[0] = admitted_;
   out[1] = completed_;
   out[2] = failed_;
-  out[3] = (int64_t)idle_.size();
+  out[3] = (int64_t)(idle_.size() + idleBatch_.size());
   out[4] = resident_;
   out[5] = peak_;
 }

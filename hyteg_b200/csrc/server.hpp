@@ -26,6 +26,7 @@ namespace hg {
 
 struct Storage;
 struct Gmg;
+struct DevBuf;
 
 struct ServerRequest {
   int64_t id = 0;
@@ -41,6 +42,7 @@ struct ServerRequest {
   double relResidual = 0.0;
   double tSubmit = 0.0, tStart = 0.0, tSolve = 0.0, tEnd = 0.0;  // seconds since the server started
   bool builtHierarchy = false;  // no resident hierarchy of its shape was free: one was built for it
+  int batchSize = 1;            // requests solved together with it in one union hierarchy (itself included)
   int64_t innerDofs = 0;
   std::vector<double> solution;  // level buffer of x at the request's level (keepSolution)
 };
@@ -55,12 +57,30 @@ struct ServerSlot {
   ~ServerSlot();
 };
 
+// A resident union hierarchy: `copies` disjoint copies of one shape in one storage
+// (meshCuboidCopies). Up to `copies` queued requests of that shape are solved in it together:
+// every kernel launch of the solve covers all of them (Gmg::solveToBatch).
+struct BatchSlot {
+  int k = 0, level = 0, copies = 0;
+  std::unique_ptr<Storage> st;
+  int op = -1, x = -1, b = -1, xOut = -1, gmg = -1;
+  std::unique_ptr<DevBuf> seeds, norms;  // per copy: seeds of the right-hand sides, residual norms
+  int64_t bytes = 0;
+  uint64_t lastUse = 0;
+  ~BatchSlot();
+};
+
 class Server {
  public:
   Server(int workers, int64_t budgetBytes, int precision);
   ~Server();
   int64_t submit(int k, int level, double coefficient, uint64_t seed, double tol, int maxIter, bool keepSolution);
   void prewarm(int k, int level);
+  // Batching: requests of levels up to maxLevel (-1: none) that find an idle union hierarchy of
+  // their shape, with at least one more request of that shape queued behind them, are solved
+  // together in it; prewarmBatch builds one union hierarchy of `copies` copies of a shape.
+  void setBatching(int maxLevel);
+  void prewarmBatch(int k, int level, int copies);
   bool wait(int64_t id, double timeoutSeconds);
   std::shared_ptr<ServerRequest> request(int64_t id);
   void stats(int64_t out[6]);  // admitted, completed, failed, resident slots, resident bytes, peak bytes
@@ -70,6 +90,8 @@ class Server {
   bool admissible();                                      // under mu
   std::unique_ptr<ServerSlot> buildSlot(int k, int level);  // outside mu
   void run(ServerRequest& r, ServerSlot& s);
+  std::unique_ptr<BatchSlot> buildBatchSlot(int k, int level, int copies);  // outside mu
+  void runBatch(std::vector<std::shared_ptr<ServerRequest>>& rs, BatchSlot& s);
   int64_t estimate(int k, int level) const;                // under mu
   double now() const;
 
@@ -82,6 +104,8 @@ class Server {
   std::deque<std::shared_ptr<ServerRequest>> queue_;
   std::map<int64_t, std::shared_ptr<ServerRequest>> all_;
   std::vector<std::unique_ptr<ServerSlot>> idle_;
+  std::vector<std::unique_ptr<BatchSlot>> idleBatch_;
+  int batchMaxLevel_ = -1;
   std::map<std::pair<int, int>, int64_t> measured_;  // footprint of a built slot per shape
   int64_t active_ = 0, resident_ = 0, peak_ = 0;      // bytes: admitted requests, idle slots
   int64_t nextId_ = 1, admitted_ = 0, completed_ = 0, failed_ = 0;

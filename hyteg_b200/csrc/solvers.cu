@@ -71,6 +71,72 @@ Gmg::Gmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int post_, double
     b32 = s.createFunction(minL, maxL, 4);
     r64 = s.createFunction(maxL, maxL, 8);
   }
+  if (deviceCoarse()) setCoarseGroups(1);
+}
+
+// Work lists of the device coarse CG. Group of a slot: the copy it belongs to when the storage
+// holds `groups` disjoint copies (each kind of primitive copy after copy, Storage::batchMap),
+// else 0. Per group its owned DoFs (low primitives in order, points in order) and its halo
+// entries (in the level table's order); a copy's lists are the single mesh's, shifted.
+void Gmg::setCoarseGroups(int groups) {
+  argCheck(groups >= 1, "coarse CG: at least one group");
+  argCheck(deviceCoarse(), "coarse CG groups need a coarse level with vertex and edge DoFs only");
+  const LevelData& ld = s.levels[minL];
+  const LevelLayout& lay = *ld.lay;
+  const dev::LevelDev& lv = ld.lv;
+  const LevelStencils& hs = s.op(op).host[minL - s.op(op).minL];
+  dev::BatchMap bm{};
+  if (groups > 1) bm = s.batchMap(minL, groups);
+  auto groupOf = [&](int64_t slot) {
+    if (groups == 1) return 0;
+    int q = 3;
+    while (q > 0 && slot < bm.uBase[q]) --q;
+    argCheck(bm.size[q] > 0, "coarse CG: slot outside the copies");
+    return int((slot - bm.uBase[q]) / bm.size[q]);
+  };
+  const unsigned mask = HG_INNER | HG_NEUMANN | HG_FREESLIP;
+  std::vector<std::vector<dev::CoarseDof>> dofs((size_t)groups);
+  int e = 0;
+  for (int q = 0; q < lv.nLow; ++q) {
+    const bool isEdge = q < lv.nEdges;
+    const int n = (int)(isEdge ? hs.edge[(size_t)q].size() : hs.vert[(size_t)(q - lv.nEdges)].size());
+    if (ld.hostLowType[(size_t)q] & mask) {
+      const int64_t off = isEdge ? lay.off[KE][(size_t)q] : lay.off[KV][(size_t)(q - lv.nEdges)];
+      const int first = isEdge ? 1 : 0;
+      const int count = isEdge ? (int)std::max<int64_t>(lay.N - 1, 0) : 1;
+      for (int xx = first; xx < first + count; ++xx)
+        dofs[(size_t)groupOf(off + xx)].push_back({off + xx, e, e + n});
+    }
+    e += n;
+  }
+  std::vector<std::vector<uint2>> comm((size_t)groups);
+  for (int g : kCommOrder)
+    for (size_t i = 0; i < lay.commDst[g].size(); ++i) {
+      const int gd = groupOf(lay.commDst[g][i]);
+      argCheck(gd == groupOf(lay.commSrc[g][i]), "coarse CG: a halo entry crosses copies");
+      comm[(size_t)gd].push_back(make_uint2((unsigned)lay.commDst[g][i], (unsigned)lay.commSrc[g][i]));
+    }
+  std::vector<dev::CoarseDof> flatDofs;
+  std::vector<uint2> flatComm;
+  std::vector<int> dofOff{0}, commOff{0};
+  for (int g = 0; g < groups; ++g) {
+    flatDofs.insert(flatDofs.end(), dofs[(size_t)g].begin(), dofs[(size_t)g].end());
+    flatComm.insert(flatComm.end(), comm[(size_t)g].begin(), comm[(size_t)g].end());
+    dofOff.push_back((int)flatDofs.size());
+    commOff.push_back((int)flatComm.size());
+  }
+  auto put = [&](std::unique_ptr<DevBuf>& buf, const void* h, size_t bytes) {
+    buf.reset(new DevBuf());
+    buf->alloc(std::max<size_t>(bytes, 16));
+    if (bytes) cudaCheck(cudaMemcpyAsync(buf->p, h, bytes, cudaMemcpyHostToDevice, s.stream), "coarse lists");
+  };
+  put(cgDofs, flatDofs.data(), flatDofs.size() * sizeof(dev::CoarseDof));
+  put(cgComm, flatComm.data(), flatComm.size() * sizeof(uint2));
+  put(cgDofOff, dofOff.data(), dofOff.size() * sizeof(int));
+  put(cgCommOff, commOff.data(), commOff.size() * sizeof(int));
+  cudaCheck(cudaStreamSynchronize(s.stream), "coarse lists");
+  coarseGroups = groups;
+  cache.clear();
 }
 
 Gmg::~Gmg() {
@@ -284,8 +350,8 @@ void GraphCache::run(Storage& s, const std::function<std::vector<uintptr_t>()>& 
   }
 }
 
-// The coarse CG: on the device in one block when the coarse level has only vertex and edge DoFs
-// (no host synchronisation), else the host-driven cgSolve. Same iteration either way.
+// The coarse CG: on the device, one block per group, when the coarse level has only vertex and
+// edge DoFs (no host synchronisation), else the host-driven cgSolve. Same iteration either way.
 void Gmg::coarseSolve(int x, int b, int L) {
   int xs = x, bs = b;
   if (prec == 4) {  // FP32 hierarchy: the coarse problem is solved in FP64 and rounded back
@@ -296,14 +362,11 @@ void Gmg::coarseSolve(int x, int b, int L) {
   }
   if (timing) timing->start(s.stream, "CG Solver");
   if (deviceCoarse()) {
-    const LevelData& ld = s.levels[L];
     Operator& o = s.op(op);
-    int64_t nComm = 0;
-    for (int g = 0; g < G_COUNT; ++g) nComm += ld.commCount[g];
-    dev::coarseCgKernel<<<1, dev::kBlock, 0, s.stream>>>(
-        ld.lv, o.d[L - o.minL], ld.comm, nComm, (double*)s.data(xs, L), (const double*)s.data(bs, L),
-        (double*)s.data(cr, L), (double*)s.data(cp, L), (double*)s.data(cap, L), HG_INNER | HG_NEUMANN | HG_FREESLIP,
-        coarseMaxIter, coarseTol, nullptr);
+    dev::coarseCgKernel<<<coarseGroups, dev::kBlock, 0, s.stream>>>(
+        o.d[L - o.minL], (const dev::CoarseDof*)cgDofs->p, (const int*)cgDofOff->p, (const uint2*)cgComm->p,
+        (const int*)cgCommOff->p, (double*)s.data(xs, L), (const double*)s.data(bs, L), (double*)s.data(cr, L),
+        (double*)s.data(cp, L), (double*)s.data(cap, L), coarseMaxIter, coarseTol, nullptr);
     ++s.launches;
     cudaCheck(cudaGetLastError(), "coarse CG");
   } else {
@@ -332,6 +395,8 @@ std::vector<uintptr_t> Gmg::signature(int x, int b, int L) {
   }
   for (int id : {cp, cz, cap, cr, cx64, cb64})
     if (id >= 0) sig.push_back((uintptr_t)s.data(id, minL));
+  sig.push_back(cgDofs ? (uintptr_t)cgDofs->p : 0);
+  sig.push_back((uintptr_t)coarseGroups);
   return sig;
 }
 
@@ -424,6 +489,62 @@ int Gmg::solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, d
   }
   if (relRes) *relRes = r0 > 0.0 ? rel : 0.0;
   return it;
+}
+
+void Gmg::solveToBatch(int x, int b, int xOut, int L, const double* tol, const int* maxIter, const dev::BatchMap& bm,
+                       int active, double* dNorms, int* iterations, double* relRes) {
+  const unsigned flag = HG_INNER | HG_NEUMANN;
+  argCheck(L >= minL && L <= maxL, "gmg: level outside the solver's range");
+  argCheck(active >= 0 && active <= bm.copies, "batch: active copies out of range");
+  argCheck(s.fn(x).prec == 8 && s.fn(b).prec == 8 && s.fn(xOut).prec == 8, "solveToBatch: FP64 functions required");
+  const int r = prec == 8 ? tmp : r64;
+  std::vector<double> h((size_t)bm.copies);
+  auto norms = [&]() {
+    s.dotBatchAsync(r, r, L, flag, bm, dNorms);
+    cudaCheck(cudaMemcpyAsync(h.data(), dNorms, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s.stream), "batch norms");
+    cudaCheck(cudaStreamSynchronize(s.stream), "batch norms");
+  };
+  s.residual(op, x, b, r, L, flag);
+  norms();
+  std::vector<double> r0((size_t)active);
+  std::vector<char> done((size_t)active, 0);
+  int left = 0;
+  for (int i = 0; i < active; ++i) {
+    r0[(size_t)i] = std::sqrt(h[(size_t)i]);
+    iterations[i] = 0;
+    if (!(maxIter[i] > 0 && 1.0 > tol[i] && r0[(size_t)i] > 0.0)) {  // solveTo takes no iteration
+      relRes[i] = r0[(size_t)i] > 0.0 ? 1.0 : 0.0;
+      s.copyBatchSlots(x, xOut, L, bm, i);
+      done[(size_t)i] = 1;
+    } else {
+      ++left;
+    }
+  }
+  int it = 0;
+  while (left > 0) {
+    if (prec == 8) {
+      runCycle(x, b, L);
+    } else {  // defect correction: FP32 cycle on A e = r (zero start), x += e in FP64
+      s.copyCast(b32, r, L, HG_ALL, false);
+      for (int l = minL; l <= L; ++l) s.lincomb(x32, l, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+      runCycle(x32, b32, L);
+      s.copyCast(x, x32, L, flag, true);
+    }
+    ++it;
+    s.residual(op, x, b, r, L, flag);
+    norms();
+    for (int i = 0; i < active; ++i) {
+      if (done[(size_t)i]) continue;
+      const double rel = std::sqrt(h[(size_t)i]) / r0[(size_t)i];
+      if (!(it < maxIter[i] && rel > tol[i])) {
+        iterations[i] = it;
+        relRes[i] = rel;
+        s.copyBatchSlots(x, xOut, L, bm, i);
+        done[(size_t)i] = 1;
+        --left;
+      }
+    }
+  }
 }
 
 void Gmg::solve(int x, int b, int L) {

@@ -12,6 +12,10 @@
 
 namespace hg {
 
+namespace dev {
+struct BatchMap;
+}
+
 struct Storage;
 struct DevBuf;
 
@@ -77,6 +81,15 @@ struct Gmg {
   // Cycles (prec 8) or FP64 defect-correction steps around one FP32 cycle (prec 4; x, b FP64)
   // until ||b - A x|| <= tol * ||b - A x0|| or maxIter; returns the iterations taken.
   int solveTo(int x, int b, int L, double tol, int maxIter, double* relRes, double* history, int historyCap);
+  // solveTo for the first `active` copies of a storage of disjoint copies (dev::BatchMap) at once:
+  // one cycle (or defect-correction step) of the whole storage per iteration, then every copy's
+  // residual norm (dNorms: device scratch of bm.copies doubles). Copy i stops at the first
+  // iteration its own relative residual reaches tol[i] (or at maxIter[i]): its x of that iteration is
+  // copied to xOut, and iterations[i], relRes[i] are its own. The copies are not coupled and the
+  // per-copy norms equal their single-mesh norms bit for bit; with one coarse-CG group per copy
+  // (setCoarseGroups) every copy's iterates are its single-mesh iterates bit for bit.
+  void solveToBatch(int x, int b, int xOut, int L, const double* tol, const int* maxIter, const dev::BatchMap& bm,
+                    int active, double* dNorms, int* iterations, double* relRes);
   void coarseSolve(int x, int b, int L);
   // One cycle x <- MG(x, b) on level L: replayed from a captured CUDA graph when the coarse solve
   // runs on the device and pre + post is even (every smoothed buffer returns to its address).
@@ -100,6 +113,12 @@ struct Gmg {
   int tmp, cp, cz, cap, cr;
   // FP32 solvers: FP64 coarse-grid workspace and the FP32 correction / defect hierarchy
   int cx64 = -1, cb64 = -1, x32 = -1, b32 = -1, r64 = -1;
+  // Device coarse CG: one block per group of unknowns, the whole mesh (1) or each copy of a
+  // storage of `groups` disjoint copies, so copies iterate and stop independently. The work
+  // lists (per group its owned DoFs and halo entries) are built here, on the host.
+  void setCoarseGroups(int groups);
+  int coarseGroups = 1;
+  std::unique_ptr<DevBuf> cgDofs, cgDofOff, cgComm, cgCommOff;
 };
 
 // P2 geometric multigrid on P2 levels [minL, maxL] (the P2 DoFs of level L are the vertex DoFs

@@ -568,6 +568,97 @@ void Storage::dotAsync(int a, int b, int L, unsigned mask, double* dOut) {
   cudaCheck(cudaGetLastError(), "dot");
 }
 
+dev::BatchMap Storage::batchMap(int L, int copies) const {
+  argCheck(copies >= 1, "batch: at least one copy");
+  const LevelData& ld = levels[L];
+  const LevelLayout& lay = *ld.lay;
+  const dev::LevelDev& lv = ld.lv;
+  dev::BatchMap bm{};
+  bm.copies = copies;
+  const int kinds[4] = {KC, KF, KE, KV};
+  int64_t a = 0;
+  for (int q = 0; q < 4; ++q) {
+    const auto& off = lay.off[kinds[q]];
+    const auto& sz = lay.size[kinds[q]];
+    const int n = (int)off.size();
+    argCheck(n % copies == 0, "batch: primitives are not a multiple of the copies");
+    const int per = n / copies;
+    int64_t end = lay.total;  // the kind's block ends where the next non-empty kind begins
+    for (int r = q + 1; r < 4; ++r)
+      if (!lay.off[kinds[r]].empty()) {
+        end = lay.off[kinds[r]][0];
+        break;
+      }
+    bm.uBase[q] = n ? off[0] : end;
+    bm.size[q] = n ? (end - off[0]) / copies : 0;
+    argCheck(!n || bm.size[q] * copies == end - off[0], "batch: kind block is not a multiple of the copies");
+    for (int i = 0; i < copies && n; ++i)
+      for (int p = 0; p < per; ++p) {
+        const size_t u = (size_t)i * per + p;
+        argCheck(off[u] - (bm.uBase[q] + i * bm.size[q]) == off[(size_t)p] - bm.uBase[q] && sz[u] == sz[(size_t)p],
+                 "batch: the copies' layouts differ");
+      }
+    bm.aBase[q] = a;
+    a += bm.size[q];
+  }
+  const int nCellGrid = lv.N >= 4 ? lv.nCells * (lv.N - 3) : 0;
+  const int counts[4] = {nCellGrid, lv.nFaceBlocks, lv.nLowEdgeBlocks, lv.nLowBlocks - lv.nLowEdgeBlocks};
+  int base = 0;
+  for (int q = 0; q < 4; ++q) {
+    argCheck(counts[q] % copies == 0, "batch: work blocks are not a multiple of the copies");
+    bm.bBase[q] = base;
+    bm.bCount[q] = counts[q] / copies;
+    base += counts[q];
+  }
+  return bm;
+}
+
+void Storage::fillRandomBatch(int id, int L, unsigned mask, const dev::BatchMap& bm, const uint64_t* dSeeds, int active,
+                              double lo, double hi) {
+  Function& f = fn(id);
+  const LevelData& ld = levels[L];
+  if (ld.nChunks) {
+    if (f.prec == 8)
+      dev::randomFillBatchKernel<double><<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (double*)data(id, L), bm,
+                                                                               dSeeds, active, lo, hi);
+    else
+      dev::randomFillBatchKernel<float><<<ld.nChunks, dev::kBlock, 0, stream>>>(ld.chunks, mask, (float*)data(id, L), bm,
+                                                                              dSeeds, active, lo, hi);
+    ++launches;
+    cudaCheck(cudaGetLastError(), "batch random fill");
+  }
+  communicate(id, L, kAllGroups);
+}
+
+void Storage::dotBatchAsync(int a, int b, int L, unsigned mask, const dev::BatchMap& bm, double* dOut) {
+  Function& fa = fn(a);
+  argCheck(fa.prec == fn(b).prec, "dot requires functions of equal precision");
+  const LevelData& ld = levels[L];
+  const int nb = ld.lv.nCellBlocks + ld.lv.nFaceBlocks + ld.lv.nLowBlocks;
+  if (fa.prec == 8)
+    dev::dotKernel<double><<<nb, dev::kBlock, 0, stream>>>(ld.lv, (const double*)data(a, L), (const double*)data(b, L), mask,
+                                                           (double*)ld.partial.p);
+  else
+    dev::dotKernel<float><<<nb, dev::kBlock, 0, stream>>>(ld.lv, (const float*)data(a, L), (const float*)data(b, L), mask,
+                                                          (double*)ld.partial.p);
+  dev::batchReduceKernel<<<bm.copies, dev::kBlock, 0, stream>>>((const double*)ld.partial.p, bm, dOut);
+  launches += 2;
+  cudaCheck(cudaGetLastError(), "batch dot");
+}
+
+void Storage::copyBatchSlots(int src, int dst, int L, const dev::BatchMap& bm, int copy) {
+  Function& fs = fn(src);
+  argCheck(fs.prec == fn(dst).prec, "batch copy: precision mismatch");
+  char* d = (char*)data(dst, L);
+  const char* sp = (const char*)data(src, L);
+  for (int q = 0; q < 4; ++q)
+    if (bm.size[q] > 0) {
+      const size_t o = (size_t)(bm.uBase[q] + copy * bm.size[q]) * fs.prec;
+      cudaCheck(cudaMemcpyAsync(d + o, sp + o, (size_t)bm.size[q] * fs.prec, cudaMemcpyDeviceToDevice, stream),
+                "batch copy");
+    }
+}
+
 void Storage::interpolateExpr(int id, int L, unsigned mask, int expr, const double* p) {
   argCheck(expr == 0 || expr == 1, "unknown expression");
   Function& f = fn(id);

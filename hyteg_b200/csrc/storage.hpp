@@ -199,6 +199,15 @@ struct Storage {
   // dst = a / b elementwise on the flagged primitives' slots (FP64)
   void divideBy(int dst, int a, int b, int L, unsigned mask);
   void dotAsync(int a, int b, int L, unsigned mask, double* dOut);
+  // Batched solves on a storage of `copies` disjoint copies of one macro-mesh (meshCuboidCopies):
+  // the map of level L (checked against the layout), the right-hand sides of the first `active`
+  // copies from their seeds (device array; the others 0), the dot product of every copy
+  // (dOut[copies], device), and the copy of one copy's slots of level L from src to dst.
+  dev::BatchMap batchMap(int L, int copies) const;
+  void fillRandomBatch(int id, int L, unsigned mask, const dev::BatchMap& bm, const uint64_t* dSeeds, int active,
+                       double lo, double hi);
+  void dotBatchAsync(int a, int b, int L, unsigned mask, const dev::BatchMap& bm, double* dOut);
+  void copyBatchSlots(int src, int dst, int L, const dev::BatchMap& bm, int copy);
   void interpolateExpr(int id, int L, unsigned mask, int expr, const double* params);
   // Seeded uniform [lo, hi) values at the flagged primitives' DoFs, then a full halo refresh.
   void fillRandom(int id, int L, unsigned mask, uint64_t seed, double lo, double hi);

@@ -131,10 +131,44 @@ void Topology::setBoundaryFlags(int onBoundary, int inner) {
   for (auto& c : cells) c.flag = inner;
 }
 
+static void cuboidTets(const double p0[3], const double p1[3], int nx, int ny, int nz,
+                       std::vector<std::array<double, 3>>& coords, std::vector<std::array<int, 4>>& tets);
+
 Topology meshCuboid(const double p0[3], const double p1[3], int nx, int ny, int nz) {
+  std::vector<std::array<double, 3>> coords;
+  std::vector<std::array<int, 4>> tets;
+  cuboidTets(p0, p1, nx, ny, nz, coords, tets);
+  return Topology::fromTets(coords, tets);
+}
+
+// `copies` disjoint copies of the unit cube split into k^3 sub-cubes (meshCuboid), copy i
+// translated by 2i along x and its vertex IDs offset by i times the vertices of one copy. As
+// fromTets orders cells, edges and faces by their vertex IDs, every kind of primitive of the
+// union is the copies' own primitives, copy after copy, each in the order of a single cube.
+Topology meshCuboidCopies(int k, int copies) {
+  if (k <= 0 || copies <= 0) throw std::runtime_error("meshCuboidCopies: non-positive size or copies");
+  const double lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+  std::vector<std::array<double, 3>> c1, coords;
+  std::vector<std::array<int, 4>> t1, tets;
+  cuboidTets(lo, hi, k, k, k, c1, t1);
+  const int nv = (int)c1.size();
+  for (int i = 0; i < copies; ++i) {
+    for (auto p : c1) {
+      p[0] += 2.0 * i;
+      coords.push_back(p);
+    }
+    for (auto t : t1) {
+      for (int& v : t) v += i * nv;
+      tets.push_back(t);
+    }
+  }
+  return Topology::fromTets(coords, tets);
+}
+
+static void cuboidTets(const double p0[3], const double p1[3], int nx, int ny, int nz,
+                       std::vector<std::array<double, 3>>& coords, std::vector<std::array<int, 4>>& tets) {
   if (nx <= 0 || ny <= 0 || nz <= 0) throw std::runtime_error("meshCuboid: non-positive subdivision");
   // MeshGenCuboid.cpp:58-80: vertices in (z, y, x) loop order
-  std::vector<std::array<double, 3>> coords;
   const double hx = (p1[0] - p0[0]) / nx, hy = (p1[1] - p0[1]) / ny, hz = (p1[2] - p0[2]) / nz;
   for (int iz = 0; iz <= nz; ++iz)
     for (int iy = 0; iy <= ny; ++iy)
@@ -146,7 +180,6 @@ Topology meshCuboid(const double p0[3], const double p1[3], int nx, int ny, int 
   static const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
                                 {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
   auto vid = [&](int i, int j, int k) { return k * (nx + 1) * (ny + 1) + j * (nx + 1) + i; };
-  std::vector<std::array<int, 4>> tets;
   for (int iz = 0; iz < nz; ++iz)
     for (int iy = 0; iy < ny; ++iy)
       for (int ix = 0; ix < nx; ++ix)
@@ -158,7 +191,6 @@ Topology meshCuboid(const double p0[3], const double p1[3], int nx, int ny, int 
           }
           tets.push_back(c);
         }
-  return Topology::fromTets(coords, tets);
 }
 
 }  // namespace hg

@@ -65,6 +65,9 @@ struct Topology {
 
 // MeshInfo::meshCuboid(p0, p1, nx, ny, nz) followed by SetupPrimitiveStorage.
 Topology meshCuboid(const double p0[3], const double p1[3], int nx, int ny, int nz);
+// `copies` disjoint translated copies of meshCuboid((0,0,0), (1,1,1), k, k, k) in one macro-mesh;
+// each kind of primitive holds the copies' primitives copy after copy, in a single cube's order.
+Topology meshCuboidCopies(int k, int copies);
 
 // MeshInfo::meshCubedDomain(cubeCoordinates, cubeType) followed by SetupPrimitiveStorage
 // (src/hyteg/mesh/MeshGenCubedDomain.cpp:115-383): unit cubes at the given integer positions,

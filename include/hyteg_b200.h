@@ -150,6 +150,10 @@ int hg_level_size(const hg_storage* s, int level, int64_t* n);
  * layout, halo tables and stencil tables, for inspection and CPU-side verification. ---- */
 int hg_mesh_create_cuboid(const double lo[3], const double hi[3], int nx, int ny, int nz, int max_level, hg_mesh** out);
 int hg_mesh_create_tets(int nverts, const double* coords, int ncells, const int* tets, int max_level, hg_mesh** out);
+/* The macro-mesh of the solve server's union hierarchies: `copies` disjoint copies of the unit
+ * cube split into k^3 sub-cubes (meshCuboid), copy i translated by 2i along x; every kind of
+ * primitive holds the copies' primitives copy after copy, each in a single cube's order. */
+int hg_mesh_create_cuboid_copies(int k, int copies, int max_level, hg_mesh** out);
 int hg_mesh_create_cubed_domain(int ncubes, const int* cubes, int cube_type, int max_level, hg_mesh** out);
 int hg_mesh_create_gmsh(const char* path, int max_level, int flags_from_file, hg_mesh** out);
 int hg_mesh_write_gmsh(const hg_mesh* m, const char* path);
@@ -353,6 +357,19 @@ int hg_server_wait(hg_server* srv, int64_t id, double timeout_seconds, int* done
 int hg_server_result(hg_server* srv, int64_t id, int* status, int* iterations, double* rel_residual, double times[4],
                      int64_t* inner_dofs);
 /* Level buffer of the solution (requests submitted with keep_solution); *size = elements. */
+/* Batched solves (no counterpart in the reference): requests of levels up to max_level (-1, the
+ * default: none) are solved together when a resident union hierarchy of their shape is idle and
+ * at least two requests of that shape are queued. A union hierarchy (hg_server_prewarm_batch) is
+ * one storage holding `copies` disjoint copies of the shape's macro-mesh: up to `copies` queued
+ * requests of the shape share one solve, every kernel launch of which covers all of them. Copy i
+ * takes request i's coefficient and right-hand side; each request stops counting iterations at
+ * its own tolerance (its solution is taken at that iteration), so it gets the iterations and,
+ * to rounding (the coarse-grid CG runs once over all copies), the solution it gets alone.
+ * hg_server_request_batch: the number of requests solved together with request id (itself
+ * included; 1 when it was solved alone). */
+int hg_server_set_batching(hg_server* srv, int max_level);
+int hg_server_prewarm_batch(hg_server* srv, int k, int level, int copies);
+int hg_server_request_batch(hg_server* srv, int64_t id, int* batch_size);
 /* Whether request id's hierarchy was built when it was admitted (1: no resident hierarchy of its
  * shape was free, so its setup time includes building one: storage, tables, stencils and a first
  * cycle) or was a resident one (0: its setup is the re-assembly of the stencils for its

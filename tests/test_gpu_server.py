@@ -7,7 +7,11 @@
   the results are in fact identical).
 - Every request of a mix reaches its tolerance; the admission respects the HBM budget (a small
   budget serialises the requests and evicts idle hierarchies; a request larger than the budget
-  fails with an error instead of running)."""
+  fails with an error instead of running).
+- Batched solves: requests queued behind a busy worker are solved together in one union
+  hierarchy (disjoint copies of their shape in one storage, one launch per kernel for all of
+  them, the coarse-grid CG one block per copy); each gets the iterations, residual and solution
+  of its direct solve bit for bit."""
 import numpy as np
 import pytest
 
@@ -98,4 +102,28 @@ def test_budget_admission(gpu):
     assert srv.wait(big, 60.0)
     with pytest.raises(hg.HygError):
         srv.result(big)
+    srv.close()
+
+
+@pytest.mark.parametrize("precision,dtype", [(4, np.float32), (8, np.float64)])
+def test_batched_requests_equal_direct_solves(gpu, precision, dtype):
+    k, L = 2, 4
+    reqs = [(0.3, 5), (2.5, 7), (1.0, 9), (7.0, 11), (0.12, 13)]
+    srv = hg.SolveServer(workers=1, precision=precision)
+    srv.prewarm_batch(k, L, 4)
+    srv.set_batching(L)
+    busy = srv.submit(3, 5, 1.0, 1, TOL)  # the single worker builds and solves this one meanwhile
+    ids = [srv.submit(k, L, c, sd, TOL, keep_solution=True) for c, sd in reqs]
+    for i in [busy] + ids:
+        assert srv.wait(i, 300.0)
+    sizes = []
+    for (c, sd), rid in zip(reqs, ids):
+        res = srv.result(rid)
+        ref, it_ref, rel_ref, owned = direct_solve(k, L, c, sd, dtype)
+        assert res["status"] == 2 and res["rel_residual"] <= TOL
+        assert res["iterations"] == it_ref
+        assert res["rel_residual"] == rel_ref
+        assert rel_diff(srv.solution(rid), ref, owned) == 0.0
+        sizes.append(res["batch_size"])
+    assert sizes[:4] == [4, 4, 4, 4] and sizes[4] == 1, sizes
     srv.close()
