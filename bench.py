@@ -310,10 +310,11 @@ def serving_bench(hg, n_requests, n_sequential, seed=2024):
     4x and 8x that sequential service rate (the last saturates it: its throughput is the server's
     capacity). Latency = completion - arrival (server clock). Setup = admission to the start of
     the solve: the stencil re-assembly for the request's coefficient on a resident hierarchy, or
-    building a hierarchy when none of the request's shape is free. A second server adds batched
-    solves: every shape of levels 3-5 also gets a union hierarchy of 8 disjoint copies, in which up
-    to 8 queued requests of that shape are solved together (one launch per kernel for all of
-    them); it runs the stream at 2x and 8x."""
+    building a hierarchy when its shape has none (a request whose shape's hierarchies are all busy
+    waits for one). A second server adds batched solves: every shape of levels 3-5 also gets union
+    hierarchies of 2, 4 and 8 disjoint copies, in which queued requests of that shape that find no
+    single hierarchy free are solved together (one launch per kernel for all of them); it runs the
+    stream at 2x and 8x."""
     rng = np.random.default_rng(seed)
     reqs = [(int(rng.integers(1, 5)), int(rng.integers(3, 7)), float(np.exp(rng.uniform(np.log(0.1), np.log(10.0)))),
              int(rng.integers(1, 2 ** 62))) for _ in range(n_requests)]
@@ -369,13 +370,15 @@ def serving_bench(hg, n_requests, n_sequential, seed=2024):
         out["mixed_rate_%gx" % mult] = dict(run(srv, mult * mu, reqs), arrival_rate_per_s=mult * mu)
     srv.close()
     out["capacity_vs_sequential"] = out["mixed_rate_8x"]["gdofs"] / seq["gdofs"]
-    # batched solves: the shapes of levels 3-5 also get one union hierarchy of 8 copies each; two
-    # or more queued requests of such a shape are solved together in it
+    # batched solves: the shapes of levels 3-5 also get union hierarchies of 2, 4 and 8 copies;
+    # two or more queued requests of such a shape that find no single hierarchy free are solved
+    # together in the smallest idle union that takes them all
     t0 = time.perf_counter()
     srv = make(8, 4, 2)
     for k, L in shapes:
         if L <= 5:
-            srv.prewarm_batch(k, L, 8)
+            for copies in (2, 4, 8):
+                srv.prewarm_batch(k, L, copies)
     srv.set_batching(5)
     out["batched_prewarm_seconds"] = time.perf_counter() - t0
     for mult in (2.0, 8.0):

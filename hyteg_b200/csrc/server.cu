@@ -4,6 +4,7 @@
 #include "server.hpp"
 
 #include <algorithm>
+#include <set>
 #include <cmath>
 
 #include "../../include/hyteg_b200.h"
@@ -106,10 +107,12 @@ std::unique_ptr<ServerSlot> Server::buildSlot(int k, int level) {
   st.reassembleOperator(s->op, true);  // builds the term lists now, so requests only run the kernels
   s->gmg = st.nextId++;
   st.gmgs[s->gmg].reset(new Gmg(st, s->op, 0, level, 3, 3, 1.0, 0, 200, 1e-16, precision_));
-  // one iteration so that the smoother's spare buffers exist before the footprint is taken
+  // three iterations before the footprint is taken: eager ones, which create the smoother's spare
+  // buffers, until the buffer state settles, then the capture of the cycle's CUDA graph, so that
+  // requests only replay it (no capture or instantiation while other requests run)
   st.fillRandom(s->b, level, HG_INNER, 0, -1.0, 1.0);
   double rel = 0;
-  st.gmgs[s->gmg]->solveTo(s->x, s->b, level, 1e-30, 1, &rel, nullptr, 0);
+  st.gmgs[s->gmg]->solveTo(s->x, s->b, level, 1e-30, 3, &rel, nullptr, 0);
   cudaCheck(cudaStreamSynchronize(st.stream), "slot build");
   s->bytes = st.deviceBytes();
   return s;
@@ -136,13 +139,14 @@ std::unique_ptr<BatchSlot> Server::buildBatchSlot(int k, int level, int copies) 
   s->seeds->alloc((size_t)copies * sizeof(uint64_t));
   s->norms.reset(new DevBuf());
   s->norms->alloc((size_t)copies * sizeof(double));
-  // one iteration over all copies, so that every buffer and graph exists before the footprint
+  // three iterations over all copies (eager ones, then the capture), so that every buffer and
+  // graph exists before the footprint
   const dev::BatchMap bm = st.batchMap(level, copies);
   std::vector<uint64_t> seeds((size_t)copies, 1);
   cudaCheck(cudaMemcpyAsync(s->seeds->p, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, st.stream), "seeds");
   st.fillRandomBatch(s->b, level, HG_INNER, bm, (const uint64_t*)s->seeds->p, copies, -1.0, 1.0);
   std::vector<double> tol((size_t)copies, 1e-30), rel((size_t)copies);
-  std::vector<int> maxIt((size_t)copies, 1), its((size_t)copies);
+  std::vector<int> maxIt((size_t)copies, 3), its((size_t)copies);
   st.gmgs[s->gmg]->solveToBatch(s->x, s->b, s->xOut, level, tol.data(), maxIt.data(), bm, copies,
                                 (double*)s->norms->p, its.data(), rel.data());
   cudaCheck(cudaStreamSynchronize(st.stream), "batch slot build");
@@ -225,6 +229,7 @@ void Server::prewarm(int k, int level) {
   resident_ += s->bytes;
   peak_ = std::max(peak_, active_ + resident_);
   s->lastUse = ++useClock_;
+  ++shapeSlots_[{k, level}];
   idle_.push_back(std::move(s));
 }
 
@@ -266,15 +271,29 @@ void Server::worker() {
       std::unique_lock<std::mutex> lk(mu_);
       for (;;) {
         if (stopping_) return;
-        if (!queue_.empty()) {
-          std::shared_ptr<ServerRequest> h = queue_.front();
-          if (h->level <= batchMaxLevel_ && !idleBatch_.empty()) {
-            // requests of the head's shape waiting, in arrival order: with two or more, the smallest
-            // idle union hierarchy of the shape that takes them all (else the largest) takes the
-            // first of them
-            int nSame = 0;
-            for (auto& q : queue_)
-              if (q->k == h->k && q->level == h->level) ++nSame;
+        // Scan the queue in arrival order; the first request that can start now starts. A request
+        // whose shape has hierarchies that are all busy waits for one of them (building another
+        // takes seconds, a solve milliseconds) and the requests behind it may pass it; a request
+        // that waits for HBM is passed by none.
+        // One pass over the queue: the requests of every shape (for batching) and the shapes found
+        // to wait, whose later requests are skipped at once (a scan is linear in the queue).
+        bool evicted = false;
+        std::map<std::pair<int, int>, int> queued;
+        std::set<std::pair<int, int>> waiting;
+        if (batchMaxLevel_ >= 0 && !idleBatch_.empty())
+          for (auto& q : queue_) ++queued[{q->k, q->level}];
+        for (size_t qi = 0; qi < queue_.size() && !r && !bslot && !evicted; ++qi) {
+          std::shared_ptr<ServerRequest> h = queue_[qi];
+          const std::pair<int, int> shape{h->k, h->level};
+          if (waiting.count(shape)) continue;
+          auto same = std::find_if(idle_.begin(), idle_.end(), [&](const std::unique_ptr<ServerSlot>& s) {
+            return s->k == h->k && s->level == h->level;
+          });
+          if (same == idle_.end() && h->level <= batchMaxLevel_ && !idleBatch_.empty()) {
+            // no single hierarchy of this shape is free and requests of the shape wait, in arrival
+            // order: with two or more, the smallest idle union hierarchy of the shape that takes
+            // them all (else the largest) takes the first of them
+            const int nSame = queued[shape];
             int best = -1;
             for (int i = 0; i < (int)idleBatch_.size() && nSame >= 2; ++i) {
               const BatchSlot& b = *idleBatch_[(size_t)i];
@@ -303,17 +322,18 @@ void Server::worker() {
               break;
             }
           }
-          auto same = std::find_if(idle_.begin(), idle_.end(), [&](const std::unique_ptr<ServerSlot>& s) {
-            return s->k == h->k && s->level == h->level;
-          });
           if (same != idle_.end()) {  // a resident hierarchy of this shape is free
             slot = std::move(*same);
             idle_.erase(same);
             resident_ -= slot->bytes;
             active_ += slot->bytes;
             r = h;
-            queue_.pop_front();
+            queue_.erase(queue_.begin() + (std::ptrdiff_t)qi);
             break;
+          }
+          if (shapeSlots_[shape] > 0) {  // its shape's hierarchies are busy: wait for one
+            waiting.insert(shape);
+            continue;
           }
           est = estimate(h->k, h->level);
           while (active_ + resident_ + est > budget_ && !idle_.empty()) {  // release LRU idle hierarchies
@@ -322,13 +342,15 @@ void Server::worker() {
                                           return a->lastUse < b->lastUse;
                                         });
             resident_ -= (*lru)->bytes;
+            --shapeSlots_[{(*lru)->k, (*lru)->level}];
             evict.push_back(std::move(*lru));
             idle_.erase(lru);
           }
-          if (active_ + resident_ + est <= budget_) {
+          if (active_ + resident_ + est <= budget_) {  // build a hierarchy for it
             active_ += est;
+            ++shapeSlots_[{h->k, h->level}];
             r = h;
-            queue_.pop_front();
+            queue_.erase(queue_.begin() + (std::ptrdiff_t)qi);
             break;
           }
           if (active_ == 0 && idle_.empty()) {  // cannot fit even on an empty device budget
@@ -336,12 +358,16 @@ void Server::worker() {
             h->error = "request exceeds the HBM budget";
             h->tEnd = now();
             ++failed_;
-            queue_.pop_front();
+            queue_.erase(queue_.begin() + (std::ptrdiff_t)qi);
+            --queued[shape];
+            --qi;
             doneCv_.notify_all();
             continue;
           }
-          if (!evict.empty()) break;  // free the evicted memory, then look again
+          evicted = !evict.empty();  // free the evicted memory, then look again
+          break;                     // else it waits for HBM, and so do the requests behind it
         }
+        if (r || bslot || evicted) break;
         cv_.wait(lk);
       }
       if (r) {
@@ -411,6 +437,7 @@ void Server::worker() {
         peak_ = std::max(peak_, active_ + resident_);
       } else {
         active_ -= est;
+        --shapeSlots_[{r->k, r->level}];
       }
     }
     if (slot && err.empty()) {
@@ -437,6 +464,8 @@ void Server::worker() {
           slot->lastUse = ++useClock_;
           resident_ += slot->bytes;
           idle_.push_back(std::move(slot));
+        } else {
+          --shapeSlots_[{r->k, r->level}];
         }
       }
     }

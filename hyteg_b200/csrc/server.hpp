@@ -8,7 +8,9 @@
 // shape (k, L) with its own CUDA stream, so the sweeps of concurrent requests overlap on the
 // device and requests that arrive while others run join as soon as a slot frees up. Idle
 // hierarchies stay resident for the next request of their shape and are released, least
-// recently used first, only when a new shape needs the memory.
+// recently used first, only when a new shape needs the memory. A hierarchy is built only for a
+// shape that has none: a request whose shape's hierarchies are all busy waits for one (a build
+// takes seconds, a solve milliseconds), and requests of other shapes behind it may pass it.
 #pragma once
 
 #include <chrono>
@@ -76,9 +78,11 @@ class Server {
   ~Server();
   int64_t submit(int k, int level, double coefficient, uint64_t seed, double tol, int maxIter, bool keepSolution);
   void prewarm(int k, int level);
-  // Batching: requests of levels up to maxLevel (-1: none) that find an idle union hierarchy of
-  // their shape, with at least one more request of that shape queued behind them, are solved
-  // together in it; prewarmBatch builds one union hierarchy of `copies` copies of a shape.
+  // Batching: requests of levels up to maxLevel (-1: none) that find no single hierarchy of their
+  // shape free but an idle union hierarchy of it, with at least one more request of that shape
+  // queued, are solved together in it (under light load requests keep the latency of a single
+  // solve; under a backlog they share launches); prewarmBatch builds one union hierarchy of
+  // `copies` copies of a shape.
   void setBatching(int maxLevel);
   void prewarmBatch(int k, int level, int copies);
   bool wait(int64_t id, double timeoutSeconds);
@@ -107,6 +111,7 @@ class Server {
   std::vector<std::unique_ptr<BatchSlot>> idleBatch_;
   int batchMaxLevel_ = -1;
   std::map<std::pair<int, int>, int64_t> measured_;  // footprint of a built slot per shape
+  std::map<std::pair<int, int>, int> shapeSlots_;    // hierarchies per shape: idle, running or being built
   int64_t active_ = 0, resident_ = 0, peak_ = 0;      // bytes: admitted requests, idle slots
   int64_t nextId_ = 1, admitted_ = 0, completed_ = 0, failed_ = 0;
   uint64_t useClock_ = 0;
