@@ -775,6 +775,24 @@ def run_ours(args):
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) * 1e-3, pg)
     e2e_finite = bool(np.isfinite(host_x[(args.steps - 1) % 2].numpy()[:1000]).all())
+    # the host link alone, outside the timed region: one step's upload and download issued
+    # together on the two copy streams (the pipelined loop overlaps exactly these with a cycle)
+    def copies():
+        bs2[1].upload_async(L, host_np, up.cuda_stream)
+        xs2[0].download_async(L, host_x[0].numpy(), down.cuda_stream)
+    copies()
+    torch.cuda.synchronize()
+    c0, c1 = ev(), ev()
+    c0.record(stream)
+    for _ in range(3):
+        up.wait_stream(stream)
+        down.wait_stream(stream)
+        copies()
+        stream.wait_stream(up)
+        stream.wait_stream(down)
+    c1.record(stream)
+    torch.cuda.synchronize()
+    t_link = c0.elapsed_time(c1) * 1e-3 / 3
     del x2, b2
 
     # --- where one cycle's time goes: the solver's timing tree (device events, eager cycle) ----
@@ -808,7 +826,14 @@ def run_ours(args):
                                      % (L, e2e_finite),
                 "pipelining": "two (x, b) pairs alternate: the pinned-host upload of step k+1 and the download of "
                               "step k's solution (two copy streams) overlap the cycle of step k+1; the first "
-                              "upload and the last download are not overlapped"},
+                              "upload and the last download are not overlapped",
+                "host_link_ms_per_step": t_link * 1e3,
+                "host_link_GBs_per_direction": n * 8 / t_link / 1e9,
+                "bound_ms_per_step": (max(t_link, t_max / args.steps) * (args.steps - 1) + 2 * t_link
+                                      + t_max / args.steps) / args.steps * 1e3,
+                "bound_note": "one step's upload and download together (host_link_ms_per_step) against the "
+                              "device cycle: steps - 1 pipelined periods of the slower of the two, plus the "
+                              "unoverlapped first upload, last cycle and last download, per step"},
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "kernels": kernels,

@@ -338,14 +338,18 @@ int hg_p2_gmg_set_graphs(hg_storage* s, int gmg, int enable);
  * refined to `level`, Dirichlet 0 on the boundary, constant coefficient, right-hand side
  * uniform[-1,1] at the inner DoFs from `seed` (hg_function_fill_random), x0 = 0, solved to the
  * relative residual `tol` with V(3,3) cycles (precision 8) or FP64 defect correction around
- * FP32 V(3,3) cycles (precision 4). `workers` threads admit queued requests in arrival order
- * while the request's device footprint fits `hbm_budget_bytes`; each admitted request runs on
- * a resident hierarchy of its shape with its own CUDA stream, concurrently with the others.
+ * FP32 V(3,3) cycles (precision 4). `workers` threads scan the queue in arrival order and start
+ * the first request that can start: on an idle resident hierarchy of its shape, or on a new one
+ * built for it when its shape has none and its device footprint fits `hbm_budget_bytes`. A
+ * request whose shape's hierarchies are all busy waits for one while the requests behind it may
+ * pass it; a request waiting for memory is passed by none. Each running request has its own CUDA
+ * stream, concurrent with the others.
  * --------------------------------------------------------------------------------------- */
 typedef struct hg_server hg_server;
 int hg_server_create(int workers, int64_t hbm_budget_bytes, int precision, hg_server** out);
 int hg_server_destroy(hg_server* srv);
-/* Build one resident hierarchy of shape (k, level) ahead of the first request. */
+/* Build one resident hierarchy of shape (k, level) ahead of the first request (its cycle's CUDA
+ * graph is captured here, so that requests only replay it). */
 int hg_server_prewarm(hg_server* srv, int k, int level);
 int hg_server_submit(hg_server* srv, int k, int level, double coefficient, uint64_t seed, double tol, int max_iter,
                      int keep_solution, int64_t* id);
@@ -356,25 +360,27 @@ int hg_server_wait(hg_server* srv, int64_t id, double timeout_seconds, int* done
  * and the right-hand side are set up), end, in seconds since hg_server_create. */
 int hg_server_result(hg_server* srv, int64_t id, int* status, int* iterations, double* rel_residual, double times[4],
                      int64_t* inner_dofs);
-/* Level buffer of the solution (requests submitted with keep_solution); *size = elements. */
 /* Batched solves (no counterpart in the reference): requests of levels up to max_level (-1, the
- * default: none) are solved together when a resident union hierarchy of their shape is idle and
- * at least two requests of that shape are queued. A union hierarchy (hg_server_prewarm_batch) is
- * one storage holding `copies` disjoint copies of the shape's macro-mesh: up to `copies` queued
- * requests of the shape share one solve, every kernel launch of which covers all of them. Copy i
- * takes request i's coefficient and right-hand side; each request stops counting iterations at
- * its own tolerance (its solution is taken at that iteration), so it gets the iterations and,
- * to rounding (the coarse-grid CG runs once over all copies), the solution it gets alone.
+ * default: none) that find no single hierarchy of their shape idle are solved together when a
+ * union hierarchy of their shape is idle and at least two requests of that shape are queued; the
+ * smallest idle union that takes them all is used, else the largest. A union hierarchy
+ * (hg_server_prewarm_batch) is one storage holding `copies` disjoint copies of the shape's
+ * macro-mesh: up to `copies` queued requests of the shape share one solve, every kernel launch of
+ * which covers all of them. Copy i takes request i's coefficient and right-hand side, its
+ * residual norms are its own, and the coarse-grid CG runs one block per copy; each request stops
+ * at its own tolerance (its solution is taken at that iteration), so it gets the iterations,
+ * residual and solution it gets alone, bit for bit.
  * hg_server_request_batch: the number of requests solved together with request id (itself
  * included; 1 when it was solved alone). */
 int hg_server_set_batching(hg_server* srv, int max_level);
 int hg_server_prewarm_batch(hg_server* srv, int k, int level, int copies);
 int hg_server_request_batch(hg_server* srv, int64_t id, int* batch_size);
-/* Whether request id's hierarchy was built when it was admitted (1: no resident hierarchy of its
- * shape was free, so its setup time includes building one: storage, tables, stencils and a first
- * cycle) or was a resident one (0: its setup is the re-assembly of the stencils for its
+/* Whether request id's hierarchy was built when it was admitted (1: its shape had no resident
+ * hierarchy, so its setup time includes building one: storage, tables, stencils and the first
+ * cycles) or was a resident one (0: its setup is the re-assembly of the stencils for its
  * coefficient). */
 int hg_server_request_setup(hg_server* srv, int64_t id, int* built_hierarchy);
+/* Level buffer of the solution (requests submitted with keep_solution); *size = elements. */
 int hg_server_solution(hg_server* srv, int64_t id, double* host, int64_t n, int64_t* size);
 /* admitted, completed, failed, resident idle hierarchies, their bytes, peak bytes in use. */
 int hg_server_stats(hg_server* srv, int64_t stats[6]);
