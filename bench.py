@@ -732,54 +732,53 @@ def run_ours(args):
 
     # --- end to end through the public API with host buffers --------------------------------
     # Every step uploads its right-hand side from pinned host memory, runs one V(3,3) cycle, and
-    # downloads the step's result -- the whole level buffer of the solution x -- into pinned host
-    # memory. Two (x, b) pairs alternate: the upload of step k + 1 (one copy stream) and the
-    # download of step k's solution (a second copy stream) overlap the cycle of step k + 1 on the
-    # other pair; events order each buffer's copies against the cycles that use it. The first
-    # upload and the last download are not overlapped.
+    # downloads the step's result -- the solution x -- into pinned host memory, both as the packed
+    # owned DoFs of the level (every DoF once; hg_function_*_owned_async). Two (x, b) pairs
+    # alternate. Per step, in this order: the cycle on its pair; the download of its solution
+    # (packed on the storage's stream behind the cycle, copied on one copy stream); the upload of
+    # the next step's right-hand side into the other pair (copied on a second copy stream while the
+    # cycle runs, unpacked behind it). The library orders each staging buffer's uses by events.
+    # The first upload and the last download are not overlapped.
     x2 = hg.P1Function("x2", st, 0, L)
     b2 = hg.P1Function("b2", st, 0, L)
     xs2, bs2 = (x, x2), (b, b2)
-    host_np = host_b.numpy()
-    host_x = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(2)]
-    x2.from_numpy(L, host_np)
-    b2.from_numpy(L, host_np)
-    for _ in range(3):  # the cycles on the second pair run eagerly, then from their own graph
-        gmg.solve(A, x2, b2, L)
-    torch.cuda.synchronize()
+    slots = st.host().owned_slots(L)
+    n_own = len(slots)
+    assert st.owned_count(L) == n_own
+    host_bo = torch.empty(n_own, dtype=torch.float64, pin_memory=True)
+    host_bo.numpy()[:] = host_b.numpy()[slots]
+    host_x = [torch.empty(n_own, dtype=torch.float64, pin_memory=True) for _ in range(2)]
     up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    for bb in (b, b2):  # both right-hand sides set, then the second pair's cycles run eagerly and get a graph
+        bb.upload_owned_async(L, host_bo.numpy(), up.cuda_stream)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        gmg.solve(A, x2, b2, L)
+        xs2[1].download_owned_async(L, host_x[1].numpy(), down.cuda_stream)
+    torch.cuda.synchronize()
     barrier(pg)
-    uploaded, solved, downloaded = [ev(), ev()], [ev(), ev()], [ev(), ev()]
     e0, e1 = ev(), ev()
     e0.record(stream)
     up.wait_stream(stream)
-    bs2[0].upload_async(L, host_np, up.cuda_stream)
-    uploaded[0].record(up)
+    down.wait_stream(stream)
+    bs2[0].upload_owned_async(L, host_bo.numpy(), up.cuda_stream)
     for k in range(args.steps):
         cur = k % 2
-        if k + 1 < args.steps:  # the next step's input, behind the cycle that last read its buffer
-            if k >= 1:
-                up.wait_event(solved[1 - cur])
-            bs2[1 - cur].upload_async(L, host_np, up.cuda_stream)
-            uploaded[1 - cur].record(up)
-        stream.wait_event(uploaded[cur])
-        if k >= 2:
-            stream.wait_event(downloaded[cur])  # the pair's previous solution has left the device
         gmg.solve(A, xs2[cur], bs2[cur], L)
-        solved[cur].record(stream)
-        down.wait_event(solved[cur])
-        xs2[cur].download_async(L, host_x[cur].numpy(), down.cuda_stream)
-        downloaded[cur].record(down)
+        xs2[cur].download_owned_async(L, host_x[cur].numpy(), down.cuda_stream)
+        if k + 1 < args.steps:
+            bs2[1 - cur].upload_owned_async(L, host_bo.numpy(), up.cuda_stream)
     stream.wait_stream(down)
     e1.record(stream)
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(e0.elapsed_time(e1) * 1e-3, pg)
     e2e_finite = bool(np.isfinite(host_x[(args.steps - 1) % 2].numpy()[:1000]).all())
-    # the host link alone, outside the timed region: one step's upload and download issued
-    # together on the two copy streams (the pipelined loop overlaps exactly these with a cycle)
+    # the host link alone, outside the timed region: one step's download and upload issued
+    # together on the two copy streams, in the loop's order (the pipelined loop overlaps exactly
+    # these with a cycle)
     def copies():
-        bs2[1].upload_async(L, host_np, up.cuda_stream)
-        xs2[0].download_async(L, host_x[0].numpy(), down.cuda_stream)
+        xs2[0].download_owned_async(L, host_x[0].numpy(), down.cuda_stream)
+        bs2[1].upload_owned_async(L, host_bo.numpy(), up.cuda_stream)
     copies()
     torch.cuda.synchronize()
     c0, c1 = ev(), ev()
@@ -820,15 +819,16 @@ def run_ours(args):
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": BYTES["sor_sweep"] * Nc},
-        "e2e": {"value": world * N_in * args.steps / t_e2e / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": n * 8,
-                "d2h_bytes_per_step": n * 8, "ms_per_step": t_e2e / args.steps * 1e3,
-                "result_downloaded": "the whole level-%d buffer of the solution x every step (finite: %s)"
-                                     % (L, e2e_finite),
-                "pipelining": "two (x, b) pairs alternate: the pinned-host upload of step k+1 and the download of "
-                              "step k's solution (two copy streams) overlap the cycle of step k+1; the first "
+        "e2e": {"value": world * N_in * args.steps / t_e2e / 1e9, "unit": "GDoF/s", "h2d_bytes_per_step": n_own * 8,
+                "d2h_bytes_per_step": n_own * 8, "ms_per_step": t_e2e / args.steps * 1e3,
+                "result_downloaded": "the solution x every step: all %d DoFs of level %d, packed (finite: %s)"
+                                     % (n_own, L, e2e_finite),
+                "pipelining": "two (x, b) pairs alternate: per step the cycle, the download of its solution "
+                              "(packed behind the cycle, one copy stream) and the upload of the next right-hand "
+                              "side (second copy stream, overlapping the cycle; unpacked behind it); the first "
                               "upload and the last download are not overlapped",
                 "host_link_ms_per_step": t_link * 1e3,
-                "host_link_GBs_per_direction": n * 8 / t_link / 1e9,
+                "host_link_GBs_per_direction": n_own * 8 / t_link / 1e9,
                 "bound_ms_per_step": (max(t_link, t_max / args.steps) * (args.steps - 1) + 2 * t_link
                                       + t_max / args.steps) / args.steps * 1e3,
                 "bound_note": "one step's upload and download together (host_link_ms_per_step) against the "

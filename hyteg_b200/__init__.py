@@ -144,6 +144,15 @@ class HostMesh:
         call("hg_mesh_slot_info", self._h, level, dptr(xyz), owned.ctypes.data_as(ctypes.POINTER(ctypes.c_byte)), n)
         return xyz, owned
 
+    def owned_slots(self, level):
+        """The level-buffer slot of each entry of the packed owned-DoF order (every DoF of the
+        level once, in level-buffer order), as used by P1Function.upload_owned_async."""
+        n = ctypes.c_int64()
+        call("hg_mesh_owned_slots", self._h, level, None, ctypes.byref(n))
+        slots = np.zeros(n.value, dtype=np.int64)
+        call("hg_mesh_owned_slots", self._h, level, slots.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.byref(n))
+        return slots
+
     def halo_table(self, level, group):
         n = ctypes.c_int64()
         call("hg_mesh_halo_table", self._h, level, group, None, None, ctypes.byref(n))
@@ -299,6 +308,12 @@ class PrimitiveStorage:
     def set_stream(self, stream_ptr):
         call("hg_storage_set_stream", self._h, ctypes.c_void_p(stream_ptr))
 
+    def owned_count(self, level):
+        """Number of DoFs of a level (each once): the size of the packed owned-DoF transfers."""
+        n = ctypes.c_int64()
+        call("hg_owned_count", self._h, level, ctypes.byref(n))
+        return n.value
+
     def synchronize(self):
         call("hg_storage_synchronize", self._h)
 
@@ -375,6 +390,25 @@ class P1Function:
             raise ValueError("download_async: a writeable contiguous array of the function's precision is required")
         call("hg_function_download_async", self.storage.handle, self.id, level, a.ctypes.data_as(ctypes.c_void_p),
              a.size, ctypes.c_void_p(stream))
+
+    def upload_owned_async(self, level, a, stream):
+        """Enqueue the upload of the owned DoFs (packed, level-buffer order, PrimitiveStorage.
+        owned_count elements) from the contiguous host array `a` on the CUDA stream handle
+        `stream`; the scatter into the level buffer and the halo refresh follow on the storage's
+        stream. `a` (pinned for an asynchronous copy) must stay alive until the copy is done."""
+        if a.dtype != self.dtype or not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("upload_owned_async: a contiguous array of the function's precision is required")
+        call("hg_function_upload_owned_async", self.storage.handle, self.id, level,
+             a.ctypes.data_as(ctypes.c_void_p), a.size, ctypes.c_void_p(stream))
+
+    def download_owned_async(self, level, a, stream):
+        """Enqueue the download of the owned DoFs (packed, level-buffer order) into the contiguous
+        host array `a`: packed on the storage's stream, copied on the CUDA stream handle `stream`;
+        `a` holds the values once `stream` has passed the copy."""
+        if a.dtype != self.dtype or not a.flags["C_CONTIGUOUS"] or not a.flags["WRITEABLE"]:
+            raise ValueError("download_owned_async: a writeable contiguous array of the function's precision is required")
+        call("hg_function_download_owned_async", self.storage.handle, self.id, level,
+             a.ctypes.data_as(ctypes.c_void_p), a.size, ctypes.c_void_p(stream))
 
     def communicate(self, level):
         call("hg_communicate", self.storage.handle, self.id, level)

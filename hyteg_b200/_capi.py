@@ -65,6 +65,7 @@ _SIGS = {
     "hg_mesh_primitive_layout": (c_int, [c_void_p, c_int, c_int, c_int, P(c_int64), P(c_int64)]),
     "hg_mesh_level_size": (c_int, [c_void_p, c_int, P(c_int64)]),
     "hg_mesh_slot_info": (c_int, [c_void_p, c_int, P(c_double), P(ctypes.c_byte), c_int64]),
+    "hg_mesh_owned_slots": (c_int, [c_void_p, c_int, P(c_int64), P(c_int64)]),
     "hg_mesh_halo_table": (c_int, [c_void_p, c_int, c_int, P(c_int64), P(c_int64), P(c_int64)]),
     "hg_split_tables_check": (c_int, [c_int, P(c_int64), P(c_int64)]),
     "hg_mesh_assembly_plan_check": (c_int, [c_void_p, c_int, c_int, P(c_int64), P(c_int64), P(c_int64)]),
@@ -81,6 +82,9 @@ _SIGS = {
     "hg_function_upload": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64]),
     "hg_function_upload_async": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p]),
     "hg_function_download_async": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p]),
+    "hg_owned_count": (c_int, [c_void_p, c_int, P(c_int64)]),
+    "hg_function_upload_owned_async": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p]),
+    "hg_function_download_owned_async": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64, c_void_p]),
     "hg_function_download": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int64]),
     "hg_communicate": (c_int, [c_void_p, c_int, c_int]),
     "hg_interpolate_const": (c_int, [c_void_p, c_int, c_double, c_int, c_uint]),

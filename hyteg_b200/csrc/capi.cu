@@ -378,6 +378,25 @@ int hg_function_download_async(hg_storage* h, int fn, int level, void* host, int
   HG_CATCH
 }
 
+int hg_owned_count(hg_storage* h, int level, int64_t* n) {
+  HG_TRY
+  hg::argCheck(n != nullptr, "null output");
+  *n = S(h).ownedPack(level).count;
+  HG_CATCH
+}
+
+int hg_function_upload_owned_async(hg_storage* h, int fn, int level, const void* host, int64_t n, void* stream) {
+  HG_TRY
+  S(h).uploadOwned(fn, level, host, n, (cudaStream_t)stream);
+  HG_CATCH
+}
+
+int hg_function_download_owned_async(hg_storage* h, int fn, int level, void* host, int64_t n, void* stream) {
+  HG_TRY
+  S(h).downloadOwned(fn, level, host, n, (cudaStream_t)stream);
+  HG_CATCH
+}
+
 int hg_communicate(hg_storage* h, int fn, int level) {
   HG_TRY
   S(h).communicate(fn, level, (1 << hg::G_COUNT) - 1);
@@ -767,6 +786,24 @@ int hg_mesh_slot_info(const hg_mesh* m, int level, double* xyz, signed char* own
         const hg::Slot o = d.owner(level, b);
         owned[g] = (o.kind == kind && o.prim == (int)p && o.local == s) ? 1 : 0;
       }
+  HG_CATCH
+}
+
+int hg_mesh_owned_slots(const hg_mesh* m, int level, int64_t* slots, int64_t* n) {
+  HG_TRY
+  const hg::Discretization& d = *M(m)->d;
+  hg::argCheck(level >= 0 && level <= d.maxLevel(), "level out of range");
+  hg::argCheck(n != nullptr, "null output");
+  const std::vector<hg::SlotRun> runs = hg::ownedRuns(d, level);
+  int64_t count = 0;
+  for (const auto& r : runs) count += r.len;
+  if (slots) {
+    hg::argCheck(*n == count, "slots must hold the owned count");
+    int64_t k = 0;
+    for (const auto& r : runs)
+      for (int64_t i = 0; i < r.len; ++i) slots[k++] = r.slot + i;
+  }
+  *n = count;
   HG_CATCH
 }
 

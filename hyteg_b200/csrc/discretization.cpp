@@ -74,6 +74,22 @@ int64_t Discretization::ownedCount(int L, int kind) const {
   }
 }
 
+std::vector<SlotRun> ownedRuns(const Discretization& d, int L) {
+  const LevelLayout& lay = d.level(L);
+  const int64_t N = lay.N, w = lay.w;
+  std::vector<SlotRun> runs;
+  for (int64_t off : lay.off[KC])
+    for (int64_t z = 1; z <= N - 3; ++z)
+      for (int64_t y = 1; y <= N - 2 - z; ++y) runs.push_back({off + cellIdx(w, 1, y, z), N - 1 - y - z});
+  for (int64_t off : lay.off[KF])
+    for (int64_t y = 1; y <= N - 2; ++y) runs.push_back({off + faceIdx(w, 1, y), N - 1 - y});
+  for (int64_t off : lay.off[KE])
+    if (N >= 2) runs.push_back({off + 1, N - 1});
+  for (int64_t off : lay.off[KV]) runs.push_back({off, 1});
+  std::sort(runs.begin(), runs.end(), [](const SlotRun& a, const SlotRun& b) { return a.slot < b.slot; });
+  return runs;
+}
+
 static int cellOppositeVertex(const MacroCell& c, const MacroFace& f) {
   for (int i = 0; i < 4; ++i)
     if (c.v[i] != f.v[0] && c.v[i] != f.v[1] && c.v[i] != f.v[2]) return c.v[i];

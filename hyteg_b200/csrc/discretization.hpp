@@ -92,6 +92,15 @@ class Discretization {
   std::map<std::array<int, 4>, int> cellByVerts_;
 };
 
+// The owned DoFs of level L (every DoF exactly once) in level-buffer order, as runs of
+// consecutive slots of their owning primitives: per cell its interior rows (x, y, z >= 1,
+// x + y + z <= N - 1), per face the interior rows of its own triangle, per edge its interior
+// points, per vertex its own slot.
+struct SlotRun {
+  int64_t slot, len;
+};
+std::vector<SlotRun> ownedRuns(const Discretization& d, int L);
+
 // ---------------------------------------------------------------------------------------
 // Constant stencils. The element matrix of every micro-tetrahedron is accumulated into the
 // rows of the owned DoFs (P1Elements.hpp:430-496, P1ConstantOperator.cpp:543-595); entries

@@ -2293,5 +2293,29 @@ static __global__ void __launch_bounds__(kBlock) batchReduceKernel(const double*
   if (threadIdx.x == 0) out[copy] = r;
 }
 
+// ---------------------------------------------------------------------------------------
+// Owned DoFs packed in level-buffer order (the host transfers of hg_function_*_owned_async):
+// run r copies slots [slot, slot + len) of the level buffer to [packed, packed + len) of the
+// packed vector (PACK) or back. One warp per run, lanes over consecutive slots.
+// ---------------------------------------------------------------------------------------
+struct OwnedRun {
+  int64_t slot, packed;
+  int len, pad;
+};
+
+template <class T, bool PACK>
+__global__ void __launch_bounds__(kBlock) ownedPackKernel(const OwnedRun* __restrict__ runs, int64_t nRuns, T* buf,
+                                                          T* packed) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nWarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < nRuns; r += nWarps) {
+    const OwnedRun run = runs[r];
+    for (int i = lane; i < run.len; i += 32) {
+      if (PACK) packed[run.packed + i] = buf[run.slot + i];
+      else buf[run.slot + i] = packed[run.packed + i];
+    }
+  }
+}
+
 }  // namespace dev
 }  // namespace hg

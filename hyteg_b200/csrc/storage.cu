@@ -568,6 +568,99 @@ void Storage::dotAsync(int a, int b, int L, unsigned mask, double* dOut) {
   cudaCheck(cudaGetLastError(), "dot");
 }
 
+PackStage::~PackStage() {
+  if (copied) cudaEventDestroy(copied);
+  if (used) cudaEventDestroy(used);
+}
+
+const OwnedPack& Storage::ownedPack(int L) {
+  argCheck(L >= 0 && L <= maxLevel(), "level out of range");
+  std::unique_ptr<OwnedPack>& op = ownedPacks[L];
+  if (!op) {
+    const std::vector<SlotRun> runs = ownedRuns(disc, L);
+    std::vector<dev::OwnedRun> dr;
+    dr.reserve(runs.size());
+    int64_t packed = 0;
+    for (const SlotRun& r : runs) {
+      argCheck(r.len > 0 && r.len < (int64_t(1) << 31), "owned run length");
+      dr.push_back({r.slot, packed, (int)r.len, 0});
+      packed += r.len;
+    }
+    std::unique_ptr<OwnedPack> p(new OwnedPack());
+    p->nRuns = (int64_t)dr.size();
+    p->count = packed;
+    p->runs.alloc(std::max<size_t>(dr.size(), 1) * sizeof(dev::OwnedRun));
+    if (!dr.empty())
+      cudaCheck(cudaMemcpyAsync(p->runs.p, dr.data(), dr.size() * sizeof(dev::OwnedRun), cudaMemcpyHostToDevice, stream),
+                "owned runs");
+    cudaCheck(cudaStreamSynchronize(stream), "owned runs");
+    op = std::move(p);
+  }
+  return *op;
+}
+
+static PackStage& packStage(Function& f, int L, int64_t count) {
+  std::unique_ptr<PackStage>& ps = f.stage[L];
+  if (!ps) {
+    ps.reset(new PackStage());
+    ps->buf.alloc(std::max<size_t>((size_t)count * f.prec, 16));
+    cudaCheck(cudaEventCreateWithFlags(&ps->copied, cudaEventDisableTiming), "event");
+    cudaCheck(cudaEventCreateWithFlags(&ps->used, cudaEventDisableTiming), "event");
+  }
+  return *ps;
+}
+
+static unsigned packGrid(int64_t nRuns) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((nRuns + 7) / 8, 148 * 16)); }
+
+void Storage::uploadOwned(int id, int L, const void* host, int64_t n, cudaStream_t copyStream) {
+  Function& f = fn(id);
+  argCheck(L >= f.minL && L <= f.maxL, "level outside the function's range");
+  argCheck(host != nullptr, "null host buffer");
+  const OwnedPack& op = ownedPack(L);
+  argCheck(n == op.count, "upload size must equal the number of owned DoFs of the level");
+  PackStage& ps = packStage(f, L, op.count);
+  cudaCheck(cudaStreamWaitEvent(copyStream, ps.used, 0), "wait");  // the previous unpack has read the buffer
+  cudaCheck(cudaMemcpyAsync(ps.buf.p, host, (size_t)n * f.prec, cudaMemcpyHostToDevice, copyStream), "owned upload");
+  cudaCheck(cudaEventRecord(ps.copied, copyStream), "event");
+  cudaCheck(cudaStreamWaitEvent(stream, ps.copied, 0), "wait");
+  if (op.nRuns) {
+    if (f.prec == 8)
+      dev::ownedPackKernel<double, false><<<packGrid(op.nRuns), dev::kBlock, 0, stream>>>(
+          (const dev::OwnedRun*)op.runs.p, op.nRuns, (double*)data(id, L), (double*)ps.buf.p);
+    else
+      dev::ownedPackKernel<float, false><<<packGrid(op.nRuns), dev::kBlock, 0, stream>>>(
+          (const dev::OwnedRun*)op.runs.p, op.nRuns, (float*)data(id, L), (float*)ps.buf.p);
+    ++launches;
+    cudaCheck(cudaGetLastError(), "owned unpack");
+  }
+  cudaCheck(cudaEventRecord(ps.used, stream), "event");
+  communicate(id, L, kAllGroups);
+}
+
+void Storage::downloadOwned(int id, int L, void* host, int64_t n, cudaStream_t copyStream) {
+  Function& f = fn(id);
+  argCheck(L >= f.minL && L <= f.maxL, "level outside the function's range");
+  argCheck(host != nullptr, "null host buffer");
+  const OwnedPack& op = ownedPack(L);
+  argCheck(n == op.count, "download size must equal the number of owned DoFs of the level");
+  PackStage& ps = packStage(f, L, op.count);
+  cudaCheck(cudaStreamWaitEvent(stream, ps.copied, 0), "wait");  // the previous download has left the buffer
+  if (op.nRuns) {
+    if (f.prec == 8)
+      dev::ownedPackKernel<double, true><<<packGrid(op.nRuns), dev::kBlock, 0, stream>>>(
+          (const dev::OwnedRun*)op.runs.p, op.nRuns, (double*)data(id, L), (double*)ps.buf.p);
+    else
+      dev::ownedPackKernel<float, true><<<packGrid(op.nRuns), dev::kBlock, 0, stream>>>(
+          (const dev::OwnedRun*)op.runs.p, op.nRuns, (float*)data(id, L), (float*)ps.buf.p);
+    ++launches;
+    cudaCheck(cudaGetLastError(), "owned pack");
+  }
+  cudaCheck(cudaEventRecord(ps.used, stream), "event");
+  cudaCheck(cudaStreamWaitEvent(copyStream, ps.used, 0), "wait");
+  cudaCheck(cudaMemcpyAsync(host, ps.buf.p, (size_t)n * f.prec, cudaMemcpyDeviceToHost, copyStream), "owned download");
+  cudaCheck(cudaEventRecord(ps.copied, copyStream), "event");
+}
+
 dev::BatchMap Storage::batchMap(int L, int copies) const {
   argCheck(copies >= 1, "batch: at least one copy");
   const LevelData& ld = levels[L];

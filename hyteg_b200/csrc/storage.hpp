@@ -64,9 +64,28 @@ struct LevelData {
   std::vector<std::unique_ptr<DevBuf>> keep;
 };
 
+// Staging of a function's owned DoFs on one level for the packed host transfers. copied is
+// recorded on the copy stream after each host copy, used on the storage's stream after each pack
+// or unpack: every use of the buffer waits for the previous one on the other stream.
+struct PackStage {
+  DevBuf buf;
+  cudaEvent_t copied = nullptr, used = nullptr;
+  PackStage() = default;
+  PackStage(const PackStage&) = delete;
+  PackStage& operator=(const PackStage&) = delete;
+  ~PackStage();
+};
+
 struct Function {
   int minL = 0, maxL = 0, prec = 8;
   std::vector<std::unique_ptr<DevBuf>> levels;
+  std::map<int, std::unique_ptr<PackStage>> stage;  // level -> staging of the packed transfers
+};
+
+// The owned-DoF runs of one level on the device (dev::OwnedRun), built on first use.
+struct OwnedPack {
+  DevBuf runs;
+  int64_t nRuns = 0, count = 0;
 };
 
 struct Operator {
@@ -183,6 +202,13 @@ struct Storage {
   void autotuneSor(int minL, int maxL, int prec, int reps, double* ms);
   unsigned long long generation = 0;  // bumped when level tables or schedules change (captured graphs)
   std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> spare;  // (level, precision) -> buffer
+  std::map<int, std::unique_ptr<OwnedPack>> ownedPacks;           // level -> owned-DoF runs
+  const OwnedPack& ownedPack(int L);
+  // Packed host transfers of a function's owned DoFs (level-buffer order, ownedRuns): the host
+  // copy runs on copyStream, the pack / unpack on the storage's stream, ordered by events; an
+  // upload ends with a full halo refresh.
+  void uploadOwned(int id, int L, const void* host, int64_t n, cudaStream_t copyStream);
+  void downloadOwned(int id, int L, void* host, int64_t n, cudaStream_t copyStream);
   std::map<std::pair<int, int>, std::unique_ptr<DevBuf>> splitRhs;  // (level, precision) -> split rhs copy
   DevBuf& spareBuf(std::map<std::pair<int, int>, std::unique_ptr<DevBuf>>& pool, int L, int prec);
   void buildSplit(int L);  // the schedule-3 tables of level L (no-op once built)

@@ -167,6 +167,9 @@ int hg_mesh_level_size(const hg_mesh* m, int level, int64_t* n);
 /* Coordinates (3 per slot) of the micro-vertex each slot of a level buffer holds, and per slot
  * 1 = owned DoF, 0 = copy of a DoF owned elsewhere, -1 = alignment padding. */
 int hg_mesh_slot_info(const hg_mesh* m, int level, double* xyz, signed char* owned, int64_t n);
+/* The level-buffer slot of each entry of the packed owned-DoF order (hg_function_*_owned_async):
+ * slots == null returns the count in *n; else *n must equal it. */
+int hg_mesh_owned_slots(const hg_mesh* m, int level, int64_t* slots, int64_t* n);
 /* Halo table of one group (0 vertex ghosts, 1 edge copies, 2 face boundary rows, 3 face ghost
  * layers, 4 cell closures): pass dst = src = NULL to query *n. */
 int hg_mesh_halo_table(const hg_mesh* m, int level, int group, int64_t* dst, int64_t* src, int64_t* n);
@@ -212,6 +215,21 @@ int hg_function_upload_async(hg_storage* s, int fn, int level, const void* host,
  * the host buffer only after the copy completed. For pipelining a result's copy with the next
  * solve. */
 int hg_function_download_async(hg_storage* s, int fn, int level, void* host, int64_t n, void* stream);
+/* Packed transfers of the owned DoFs only (no counterpart in the reference, whose functions live
+ * in host memory): every DoF of the level once, in level-buffer order (hg_mesh_owned_slots gives
+ * the slot of each entry), n = hg_owned_count elements of the function's precision; about 9 %
+ * fewer bytes than the level buffer on the 48-tet cube. The host copy runs on the caller's
+ * stream, the packing on the storage's stream; a per-function staging buffer on the device
+ * (allocated by the first call for a function and level) sits in between, and events order each
+ * use of it after the previous one, so successive calls need no ordering by the caller beyond
+ * that of the function itself. upload: the values are scattered into the owners' slots and every
+ * copy slot is refreshed from its owner (the level buffer is then consistent), in order on the
+ * storage's stream; the host buffer must stay alive (and pinned, for an asynchronous copy) until
+ * the copy stream has passed the copy. download: the owners' values as of the storage's stream
+ * at the call, in the host buffer once the caller's stream has passed the copy. */
+int hg_owned_count(hg_storage* s, int level, int64_t* n);
+int hg_function_upload_owned_async(hg_storage* s, int fn, int level, const void* host, int64_t n, void* stream);
+int hg_function_download_owned_async(hg_storage* s, int fn, int level, void* host, int64_t n, void* stream);
 int hg_communicate(hg_storage* s, int fn, int level);
 int hg_interpolate_const(hg_storage* s, int fn, double value, int level, unsigned flag);
 /* Built-in expressions at the flagged DoFs (then the halo is refreshed): expr 0 =

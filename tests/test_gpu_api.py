@@ -1,6 +1,9 @@
 """Host-facing entry points: the asynchronous upload on a caller's stream gives the same level
 buffer as the synchronous one, and a double-buffered pipeline (upload of the next right-hand
-side overlapping the current cycle) gives the same iterates as the plain loop."""
+side overlapping the current cycle) gives the same iterates as the plain loop. The packed
+owned-DoF transfers: a download gives the owned slots of the level buffer; an upload of them
+gives back the whole level buffer (every copy slot refreshed from its owner), bit for bit, in
+FP64 and FP32, twice in a row through the same staging buffer."""
 import numpy as np
 import pytest
 
@@ -80,3 +83,29 @@ def test_double_buffered_pipeline_gives_the_same_iterates(env):
         released[cur].record(stream)
     torch.cuda.synchronize()
     assert np.array_equal(plain, y.to_numpy(L))
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_owned_transfers_round_trip(env, dtype):
+    import torch
+    st, L, stream = env
+    slots = st.host().owned_slots(L)
+    assert st.owned_count(L) == len(slots)
+    _, owned = st.host().slot_info(L)
+    dof = owned >= 0  # owned DoFs and their copies (not the alignment padding)
+    src, dst = hg.P1Function("src", st, L, L, dtype=dtype), hg.P1Function("dst", st, L, L, dtype=dtype)
+    cs = torch.cuda.Stream()
+    tdt = torch.float64 if dtype == np.float64 else torch.float32
+    packed = torch.empty(len(slots), dtype=tdt, pin_memory=True)
+    for seed in (3, 4):  # twice: the staging buffer is reused
+        src.fill_random(seed, L, hg.All)
+        full = src.to_numpy(L)
+        src.download_owned_async(L, packed.numpy(), cs.cuda_stream)
+        cs.synchronize()
+        assert np.array_equal(packed.numpy(), full[slots])
+        dst.interpolate(0.0, L)
+        dst.upload_owned_async(L, packed.numpy(), cs.cuda_stream)
+        st.synchronize()
+        assert np.array_equal(dst.to_numpy(L)[dof], full[dof])
+    with pytest.raises(hg.HygError):
+        dst.upload_owned_async(L, packed.numpy()[:-1], cs.cuda_stream)
