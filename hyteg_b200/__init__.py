@@ -925,9 +925,9 @@ class SolveServer:
     def result(self, rid):
         """dict(status, iterations, rel_residual, t_submit, t_start, t_solve, t_end, inner_dofs,
         built_hierarchy, batch_size); raises for a failed request. batch_size: the requests solved
-        together with it in one union hierarchy (1: solved alone). built_hierarchy: no resident hierarchy of the
-        request's shape was free when it was admitted, so one was built for it (its setup time,
-        t_solve - t_start, includes that)."""
+        together with it in one union hierarchy (1: solved alone). built_hierarchy: the request's
+        shape had no resident hierarchy when it was admitted, so one was built for it (its setup
+        time, t_solve - t_start, includes that)."""
         st, it = ctypes.c_int(), ctypes.c_int()
         rel = ctypes.c_double()
         t = np.zeros(4)

@@ -517,7 +517,7 @@ __global__ void __launch_bounds__(kBlock) cellSorSplitKernel(LevelDev lv, const 
 // ---------------------------------------------------------------------------------------
 // Register-blocked 2.5-D cell sweep (the kernel behind apply and residual on cell interiors).
 // A warp owns a strip of 30 x-columns (lanes 1..30; lanes 0 and 31 only carry the x-halo) by
-// kStripR rows and marches up z through a range of planes. Each lane keeps the rows
+// R rows (StripCfg) and marches up z through a range of planes. Each lane keeps the rows
 // y0-1 .. y0+R of the planes z-1, z, z+1 of its own column in registers and has plane z+2
 // (and the second vector's rows of plane z+1) in flight while plane z is computed;
 // x-neighbours come from the adjacent lanes through warp shuffles. Addresses advance
@@ -525,12 +525,25 @@ __global__ void __launch_bounds__(kBlock) cellSorSplitKernel(LevelDev lv, const 
 // Every value is loaded (R+2)/R times per sweep (the extra rows are the neighbouring strips'
 // rows, L1 hits). No shared memory, no block synchronisation.
 // ---------------------------------------------------------------------------------------
-constexpr int kStripR = 4;                          // rows per strip
-constexpr int kStripH = kStripR + 2;                // rows held per plane (with y-halo)
 constexpr int kStripX = 30;                         // computed columns per warp
-constexpr int kStripWarps = kBlock / 32;            // strips per block (stacked in y)
 constexpr int kStripZ = 32;                         // planes per work item
-constexpr int kStripRows = kStripR * kStripWarps;   // rows per block
+constexpr int kStripRows = 32;                      // rows per block (strips stacked in y)
+// Rows per strip and blocks per SM by precision. An FP32 lane holds twice the rows in the same
+// registers, so an FP32 warp has twice the loads in flight and re-reads fewer halo rows.
+template <class T>
+struct StripCfg;
+template <>
+struct StripCfg<double> {
+  static constexpr int R = 4, MIN_BLOCKS = 2;
+};
+template <>
+struct StripCfg<float> {
+  static constexpr int R = 8, MIN_BLOCKS = 4;
+};
+template <class T>
+constexpr int stripThreads() {
+  return 32 * (kStripRows / StripCfg<T>::R);
+}
 
 struct StripItem {
   int cell, x0, y0, z0, z1, pad0, pad1, pad2;  // columns [x0, x0+30), rows [y0, y0+32), planes [z0, z1)
@@ -548,10 +561,11 @@ __device__ __forceinline__ T shDown(T v) {  // value of lane + 1 (x + 1)
 }
 
 template <class T, int OP>
-__global__ void __launch_bounds__(kBlock, 2) cellStripKernel(LevelDev lv, const StripItem* __restrict__ items,
-                                                             const T* __restrict__ cellW, T* __restrict__ dst,
-                                                             const T* __restrict__ src, const T* __restrict__ rhs,
-                                                             unsigned mask) {
+__global__ void __launch_bounds__(stripThreads<T>(), StripCfg<T>::MIN_BLOCKS)
+    cellStripKernel(LevelDev lv, const StripItem* __restrict__ items, const T* __restrict__ cellW, T* __restrict__ dst,
+                    const T* __restrict__ src, const T* __restrict__ rhs, unsigned mask) {
+  constexpr int kStripR = StripCfg<T>::R;       // rows per strip
+  constexpr int kStripH = kStripR + 2;          // rows held per plane (with y-halo)
   const StripItem it = items[blockIdx.x];
   if (!(lv.cellType[it.cell] & mask)) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

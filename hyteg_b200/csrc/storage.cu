@@ -1943,7 +1943,8 @@ void Storage::stencilOp(Operator& o, int L, T* dst, const T* src, const T* rhs, 
   if (ld.nTiles && (kinds & (1 << KC))) {
     constexpr int op =
         MODE == dev::MODE_REPLACE ? dev::STRIP_REPLACE : MODE == dev::MODE_ADD ? dev::STRIP_ADD : dev::STRIP_RESIDUAL;
-    dev::cellStripKernel<T, op><<<ld.nTiles, dev::kBlock, 0, stream>>>(ld.lv, ld.tiles, st.cellW, dst, src, rhs, mask);
+    dev::cellStripKernel<T, op><<<ld.nTiles, dev::stripThreads<T>(), 0, stream>>>(ld.lv, ld.tiles, st.cellW, dst, src,
+                                                                                  rhs, mask);
     ++launches;
   }
   if (ld.lv.nFaceBlocks && (kinds & (1 << KF))) {

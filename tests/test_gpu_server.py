@@ -8,6 +8,8 @@
 - Every request of a mix reaches its tolerance; the admission respects the HBM budget (a small
   budget serialises the requests and evicts idle hierarchies; a request larger than the budget
   fails with an error instead of running).
+- Admission: requests of a shape whose resident hierarchy is busy wait for it instead of
+  building another, and a request of another shape behind them starts first.
 - Batched solves: requests queued behind a busy worker are solved together in one union
   hierarchy (disjoint copies of their shape in one storage, one launch per kernel for all of
   them, the coarse-grid CG one block per copy); each gets the iterations, residual and solution
@@ -126,4 +128,25 @@ def test_batched_requests_equal_direct_solves(gpu, precision, dtype):
         assert rel_diff(srv.solution(rid), ref, owned) == 0.0
         sizes.append(res["batch_size"])
     assert sizes[:4] == [4, 4, 4, 4] and sizes[4] == 1, sizes
+    srv.close()
+
+
+def test_busy_shape_waits_and_other_shapes_pass(gpu):
+    srv = hg.SolveServer(workers=2, precision=4)
+    srv.prewarm(2, 6)
+    srv.prewarm(1, 3)
+    first = srv.submit(2, 6, 1.0, 1, TOL)            # takes the one (2, 6) hierarchy
+    waiting = [srv.submit(2, 6, 1.0 + i, 2 + i, TOL) for i in range(3)]
+    other = srv.submit(1, 3, 1.0, 9, TOL)            # behind them in the queue, another shape
+    for rid in [first] + waiting + [other]:
+        assert srv.wait(rid, 300.0)
+    res = {rid: srv.result(rid) for rid in [first] + waiting + [other]}
+    assert not any(r["built_hierarchy"] for r in res.values())  # nothing was built on admission
+    # the (2, 6) requests ran one after another on their hierarchy ...
+    runs = sorted((res[r]["t_start"], res[r]["t_end"]) for r in [first] + waiting)
+    assert all(a[1] <= b[0] for a, b in zip(runs, runs[1:]))
+    # ... and the later request of another shape did not wait for them
+    assert res[other]["t_start"] < max(res[r]["t_start"] for r in waiting)
+    st = srv.stats()
+    assert st["completed"] == 5 and st["failed"] == 0
     srv.close()
