@@ -681,6 +681,8 @@ def run_ours(args):
     if L >= 3 and not args.cycle_only:
         kernels["p2"] = p2_kernels(hg, st, L - 2, timed)
         kernels["stokes"] = stokes_bench(hg, st, min(L - 2, args.stokes_level))
+        if min(L - 2, args.stokes_level) > 5:  # the smaller Stokes case (P2 level 5) beside it
+            kernels["stokes_p2_level_5"] = stokes_bench(hg, st, 5)
     if not args.cycle_only:
         kernels["reassembly"] = reassembly_bench(hg)
 

@@ -109,3 +109,49 @@ def test_owned_transfers_round_trip(env, dtype):
         assert np.array_equal(dst.to_numpy(L)[dof], full[dof])
     with pytest.raises(hg.HygError):
         dst.upload_owned_async(L, packed.numpy()[:-1], cs.cuda_stream)
+
+
+def test_packed_pipeline_gives_the_same_iterates(env):
+    """The bench's end-to-end loop: per step a cycle, the packed download of its solution and the
+    packed upload of the next right-hand side, on two copy streams, two (x, b) pairs. Every
+    downloaded solution equals the plain loop's iterate at that step."""
+    import torch
+    st, L, stream = env
+    slots = st.host().owned_slots(L)
+    A = hg.P1ConstantLaplaceOperator(st, 0, L)
+    rhs = []
+    for k in range(5):
+        h = torch.empty(len(slots), dtype=torch.float64, pin_memory=True)
+        h.numpy()[:] = np.random.default_rng(20 + k).uniform(-1, 1, len(slots))
+        rhs.append(h)
+
+    def solver():
+        return hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 50, 1e-16),
+                                           hg.P1toP1LinearRestriction(), hg.P1toP1LinearProlongation(), 0, L, 3, 3)
+
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    # plain loop, one pair: x is carried from step to step on each pair below, so the plain loop
+    # keeps one x per pair as well
+    xs = (hg.P1Function("px0", st, 0, L), hg.P1Function("px1", st, 0, L))
+    b = hg.P1Function("pb", st, 0, L)
+    g = solver()
+    expect = []
+    for k, h in enumerate(rhs):
+        b.upload_owned_async(L, h.numpy(), up.cuda_stream)
+        g.solve(A, xs[k % 2], b, L)
+        expect.append(xs[k % 2].to_numpy(L)[slots])
+    # pipelined loop
+    xp = (hg.P1Function("qx0", st, 0, L), hg.P1Function("qx1", st, 0, L))
+    bp = (hg.P1Function("qb0", st, 0, L), hg.P1Function("qb1", st, 0, L))
+    out = [torch.empty(len(slots), dtype=torch.float64, pin_memory=True) for _ in rhs]
+    g2 = solver()
+    bp[0].upload_owned_async(L, rhs[0].numpy(), up.cuda_stream)
+    for k in range(len(rhs)):
+        cur = k % 2
+        g2.solve(A, xp[cur], bp[cur], L)
+        xp[cur].download_owned_async(L, out[k].numpy(), down.cuda_stream)
+        if k + 1 < len(rhs):
+            bp[1 - cur].upload_owned_async(L, rhs[k + 1].numpy(), up.cuda_stream)
+    torch.cuda.synchronize()
+    for k in range(len(rhs)):
+        assert np.array_equal(out[k].numpy(), expect[k]), k
