@@ -158,6 +158,20 @@ class P1Function {
   void upload(uint_t level, const std::vector<real_t>& v) const {
     check(hg_function_upload(h(), id_, (int)level, v.data(), (int64_t)v.size()));
   }
+  // Every DoF of the level once, packed in level-buffer order (no counterpart in the reference):
+  // asynchronous copies on the caller's CUDA stream (a cudaStream_t); the host buffer, pinned for
+  // an asynchronous copy, must stay alive until the stream has passed the copy.
+  int64_t ownedCount(uint_t level) const {
+    int64_t n = 0;
+    check(hg_owned_count(h(), (int)level, &n));
+    return n;
+  }
+  void uploadOwnedAsync(uint_t level, const real_t* host, int64_t n, void* stream) const {
+    check(hg_function_upload_owned_async(h(), id_, (int)level, host, n, stream));
+  }
+  void downloadOwnedAsync(uint_t level, real_t* host, int64_t n, void* stream) const {
+    check(hg_function_download_owned_async(h(), id_, (int)level, host, n, stream));
+  }
 
  private:
   hg_storage* h() const { return storage_->handle(); }
