@@ -1,0 +1,105 @@
+"""Two of the reference's own known-answer tests, run through the GPU path on its 3-D mesh
+fixtures (tests/golden/meshes.json, the reference's .msh files):
+
+- VertexDoFLinearProlongation3DTest (tests/hyteg/vertexdofspace/VertexDoFLinearProlongation3DTest.cpp):
+  linear prolongation reproduces constants and linear functions, err.err < 1e-15 over
+  Inner | NeumannBoundary (lower levels 0, 1 and 3); prolongateAndAdd equals prolongate followed
+  by add, err.err < 1e-15 (lower levels 0, 1 and 3).
+- P1GSConvergenceTest (tests/hyteg/convergence/P1GSConvergenceTest.cpp): level 4, Dirichlet data
+  sin(x) sinh(y), random inner start, zero right-hand side; every one of 20 forward (and,
+  separately, backward) SOR sweeps with omega = 1 reduces the residual norm over the inner DoFs.
+  The smoother here is the GPU's multicolour SOR, not the reference's lexicographic one."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import hyteg_b200 as hg
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+with open(os.path.join(HERE, "golden", "meshes.json")) as _f:
+    MESHES = json.load(_f)
+MESHES_3D = ["tet_1el", "pyramid_2el", "pyramid_4el", "pyramid_tilted_4el", "regular_octahedron_8el"]
+FREE = hg.Inner | hg.NeumannBoundary
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    if hg.device_count() == 0:
+        pytest.skip("no CUDA device")
+
+
+def storage(name, max_level):
+    m = MESHES[name]
+    return hg.PrimitiveStorage.from_tets(np.array(m["coords"], dtype=np.float64), np.array(m["tets"], dtype=np.int32),
+                                         max_level)
+
+
+@pytest.mark.parametrize("name", MESHES_3D)
+@pytest.mark.parametrize("lower", [0, 1, 3])
+def test_linear_prolongation_is_exact(gpu, name, lower):
+    st = storage(name, lower + 1)
+    u, exact, err = (hg.P1Function(n, st, lower, lower + 1) for n in ("u", "exact", "err"))
+    P = hg.P1toP1LinearProlongation()
+    # 0, 1, 42, 42 x, 42 x + y as a + b x + c y + d z
+    for coef in ((0, 0, 0, 0), (1, 0, 0, 0), (42, 0, 0, 0), (0, 42, 0, 0), (0, 42, 1, 0)):
+        u.interpolate_linear(*coef, lower, hg.All)
+        exact.interpolate_linear(*coef, lower + 1, FREE)
+        P.prolongate(u, lower, FREE)
+        err.assign([1.0, -1.0], [u, exact], lower + 1, FREE)
+        assert err.dotGlobal(err, lower + 1, FREE) < 1e-15, (name, lower, coef)
+
+
+@pytest.mark.parametrize("name", MESHES_3D)
+@pytest.mark.parametrize("lower", [0, 1, 3])
+def test_prolongate_and_add(gpu, name, lower):
+    st = storage(name, lower + 1)
+    up, ua, upa, err = (hg.P1Function(n, st, lower, lower + 1) for n in ("up", "ua", "upa", "err"))
+
+    def term_prolongate(x, y, z):
+        return np.sin(x) + np.sinh(y) + z * z
+
+    def term_add(x, y, z):
+        return np.cos(x) + np.cosh(y) + z * z * z
+
+    up.interpolate(term_prolongate, lower, hg.All)
+    up.interpolate(term_add, lower + 1, hg.All)
+    ua.interpolate(term_add, lower + 1, hg.All)
+    upa.interpolate(term_prolongate, lower, hg.All)
+    upa.interpolate(term_add, lower + 1, hg.All)
+    P = hg.P1toP1LinearProlongation()
+    P.prolongate(up, lower, FREE)
+    P.prolongateAndAdd(upa, lower, FREE)
+    up.add([1.0], [ua], lower + 1, FREE)
+    err.assign([1.0, -1.0], [up, upa], lower + 1, FREE)
+    assert err.dotGlobal(err, lower + 1, FREE) < 1e-15, (name, lower)
+
+
+@pytest.mark.parametrize("name", ["tet_1el", "regular_octahedron_8el"])
+@pytest.mark.parametrize("backwards", [False, True])
+def test_gauss_seidel_reduces_the_residual_every_sweep(gpu, name, backwards):
+    L = 4
+    st = storage(name, L)
+    A = hg.P1ConstantLaplaceOperator(st, L, L)
+    x, rhs, Lu, res = (hg.P1Function(n, st, L, L) for n in ("x", "rhs", "Lu", "res"))
+    x.interpolate(lambda px, py, pz: np.sin(px) * np.sinh(py), L, hg.DirichletBoundary)
+    x.fill_random(0, L, hg.Inner, 0.0, 1.0)
+    rhs.interpolate(0.0, L)
+
+    def norm():
+        A.apply(x, Lu, L, hg.Inner)
+        res.assign([1.0, -1.0], [rhs, Lu], L, hg.Inner)
+        return np.sqrt(res.dotGlobal(res, L, hg.Inner))
+
+    old = norm()
+    assert old > 0
+    for i in range(20):
+        if backwards:
+            A.smooth_sor_backwards(x, rhs, 1.0, L, hg.Inner)
+        else:
+            A.smooth_sor(x, rhs, 1.0, L, hg.Inner)
+        new = norm()
+        assert new < old, (name, backwards, i, new, old)
+        old = new
