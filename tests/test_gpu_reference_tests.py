@@ -1,10 +1,13 @@
-"""Two of the reference's own known-answer tests, run through the GPU path on its 3-D mesh
+"""Three of the reference's own known-answer tests, run through the GPU path on its 3-D mesh
 fixtures (tests/golden/meshes.json, the reference's .msh files):
 
 - VertexDoFLinearProlongation3DTest (tests/hyteg/vertexdofspace/VertexDoFLinearProlongation3DTest.cpp):
   linear prolongation reproduces constants and linear functions, err.err < 1e-15 over
   Inner | NeumannBoundary (lower levels 0, 1 and 3); prolongateAndAdd equals prolongate followed
   by add, err.err < 1e-15 (lower levels 0, 1 and 3).
+- P1LaplaceOperator3DTest (tests/hyteg/P1/P1LaplaceOperator3DTest.cpp): A u = 0 at the inner
+  DoFs for u = 0, 1, 42 x and 42 x + y + 1337 z, discrete L2 error sqrt(e.e / #inner) < 2.8e-13,
+  on its seven (mesh, level) cases.
 - P1GSConvergenceTest (tests/hyteg/convergence/P1GSConvergenceTest.cpp): level 4, Dirichlet data
   sin(x) sinh(y), random inner start, zero right-hand side; every one of 20 forward (and,
   separately, backward) SOR sweeps with omega = 1 reduces the residual norm over the inner DoFs.
@@ -103,3 +106,20 @@ def test_gauss_seidel_reduces_the_residual_every_sweep(gpu, name, backwards):
         new = norm()
         assert new < old, (name, backwards, i, new, old)
         old = new
+
+
+@pytest.mark.parametrize("name,L", [("tet_1el", 2), ("tet_1el", 3), ("pyramid_2el", 2), ("pyramid_2el", 3),
+                                    ("pyramid_4el", 3), ("pyramid_tilted_4el", 3), ("regular_octahedron_8el", 3)])
+def test_laplace_annihilates_constants_and_linears(gpu, name, L):
+    st = storage(name, L)
+    A = hg.P1ConstantLaplaceOperator(st, L, L)
+    u, result, err, one = (hg.P1Function(n, st, L, L) for n in ("u", "result", "err", "one"))
+    one.interpolate(1.0, L, hg.All)
+    n_points = one.dotGlobal(one, L, hg.Inner)
+    for coef in ((0, 0, 0, 0), (1, 0, 0, 0), (0, 42, 0, 0), (0, 42, 1, 1337)):
+        u.interpolate_linear(*coef, L, hg.All)
+        result.interpolate(0.0, L, hg.DirichletBoundary)
+        A.apply(u, result, L, hg.Inner)
+        err.assign([1.0], [result], L, hg.All)  # the exact result is 0 everywhere
+        l2 = np.sqrt(err.dotGlobal(err, L, hg.Inner) / n_points)
+        assert l2 < 2.8e-13, (name, L, coef, l2)
