@@ -1,4 +1,4 @@
-"""Three of the reference's own known-answer tests, run through the GPU path on its 3-D mesh
+"""The reference's own known-answer tests for this path, run through the GPU path on its 3-D mesh
 fixtures (tests/golden/meshes.json, the reference's .msh files):
 
 - VertexDoFLinearProlongation3DTest (tests/hyteg/vertexdofspace/VertexDoFLinearProlongation3DTest.cpp):
@@ -11,7 +11,16 @@ fixtures (tests/golden/meshes.json, the reference's .msh files):
 - P1GSConvergenceTest (tests/hyteg/convergence/P1GSConvergenceTest.cpp): level 4, Dirichlet data
   sin(x) sinh(y), random inner start, zero right-hand side; every one of 20 forward (and,
   separately, backward) SOR sweeps with omega = 1 reduces the residual norm over the inner DoFs.
-  The smoother here is the GPU's multicolour SOR, not the reference's lexicographic one."""
+  The smoother here is the GPU's multicolour SOR, not the reference's lexicographic one.
+- P2QuadraticProlongation3DTest (tests/hyteg/P2/P2QuadraticProlongation3DTest.cpp): quadratic
+  prolongation reproduces constants, linears and 2x^2 + 3x + 13 + 4y + 5y^2 + z^2 + 6, err.err <
+  1e-15 over Inner | NeumannBoundary (lower levels 0, 1 and 3); prolongateAndAdd equals
+  prolongate followed by add.
+- P2GMG3DConvergenceTest (tests/hyteg/convergence/P2GMG3DConvergenceTest.cpp): the octahedron,
+  P2 levels 0-3, random inner start, Dirichlet data sin(x) sinh(y) z, f = 0, ten V(2,2) cycles;
+  every cycle reduces the discrete squared residual (r.r / #inner) by a factor below 3e-2. The
+  smoother is the GPU's multicolour P2 SOR (the reference's Gauss-Seidel smoother is
+  lexicographic) and the coarsest level is solved exactly (the reference runs CG to 1e-16)."""
 import json
 import os
 
@@ -123,3 +132,73 @@ def test_laplace_annihilates_constants_and_linears(gpu, name, L):
         err.assign([1.0], [result], L, hg.All)  # the exact result is 0 everywhere
         l2 = np.sqrt(err.dotGlobal(err, L, hg.Inner) / n_points)
         assert l2 < 2.8e-13, (name, L, coef, l2)
+
+
+QUADRATICS = [lambda x, y, z: 0.0 * x, lambda x, y, z: 1.0 + 0.0 * x, lambda x, y, z: 42.0 + 0.0 * x,
+              lambda x, y, z: 42.0 * x, lambda x, y, z: 42.0 * x + y + 1337.0 * z,
+              lambda x, y, z: 2.0 * x * x + 3.0 * x + 13.0 + 4.0 * y + 5.0 * y * y + z * z + 6.0]
+
+
+@pytest.mark.parametrize("name", MESHES_3D)
+@pytest.mark.parametrize("lower", [0, 1, 3])
+def test_quadratic_prolongation_is_exact(gpu, name, lower):
+    st = storage(name, lower + 2)  # P2 level lower + 1 lives on the vertex lattice lower + 2
+    u, exact, err = (hg.P2Function(n, st, lower, lower + 1) for n in ("u", "exact", "err"))
+    P = hg.P2toP2QuadraticProlongation()
+    for i, fn in enumerate(QUADRATICS):
+        u.interpolate(fn, lower, hg.All)
+        exact.interpolate(fn, lower + 1, FREE)
+        P.prolongate(u, lower, FREE)
+        err.assign([1.0, -1.0], [u, exact], lower + 1, FREE)
+        assert err.dotGlobal(err, lower + 1, FREE) < 1e-15, (name, lower, i)
+
+
+@pytest.mark.parametrize("name", MESHES_3D)
+@pytest.mark.parametrize("lower", [0, 1, 3])
+def test_p2_prolongate_and_add(gpu, name, lower):
+    st = storage(name, lower + 2)
+    up, ua, upa, err = (hg.P2Function(n, st, lower, lower + 1) for n in ("up", "ua", "upa", "err"))
+
+    def term_prolongate(x, y, z):
+        return np.sin(x) + np.sinh(y) + z * z
+
+    def term_add(x, y, z):
+        return np.cos(x) + np.cosh(y) + z * z * z
+
+    up.interpolate(term_prolongate, lower, hg.All)
+    up.interpolate(term_add, lower + 1, hg.All)
+    ua.interpolate(term_add, lower + 1, hg.All)
+    upa.interpolate(term_prolongate, lower, hg.All)
+    upa.interpolate(term_add, lower + 1, hg.All)
+    P = hg.P2toP2QuadraticProlongation()
+    P.prolongate(up, lower, FREE)
+    P.prolongateAndAdd(upa, lower, FREE)
+    up.assign([1.0, 1.0], [up, ua], lower + 1, FREE)
+    err.assign([1.0, -1.0], [up, upa], lower + 1, FREE)
+    assert err.dotGlobal(err, lower + 1, FREE) < 1e-15, (name, lower)
+
+
+def test_p2_multigrid_reference_convergence_bound(gpu):
+    minL, maxL = 0, 3
+    st = storage("regular_octahedron_8el", maxL + 1)
+    A = hg.P2ConstantLaplaceOperator(st, minL, maxL)
+    u, f, res, one = (hg.P2Function(n, st, minL, maxL) for n in ("u", "f", "res", "one"))
+    u.fill_random(0, maxL, hg.Inner, 0.0, 1.0)
+    u.interpolate(lambda x, y, z: np.sin(x) * np.sinh(y) * z, maxL, hg.DirichletBoundary)
+    f.interpolate(0.0, maxL, hg.All)
+    one.interpolate(1.0, maxL, hg.All)
+    n_points = one.dotGlobal(one, maxL, hg.Inner)
+    gmg = hg.P2GeometricMultigridSolver(st, A, minL, maxL, 2, 2)
+
+    def sq_res():
+        A.apply(u, res, maxL, hg.Inner)
+        return res.dotGlobal(res, maxL, hg.Inner) / n_points
+
+    last = sq_res()
+    rates = []
+    for _ in range(10):
+        gmg.solve(u, f, maxL)
+        cur = sq_res()
+        rates.append(cur / last)
+        last = cur
+    assert max(rates) < 3.0e-2, rates
