@@ -8,7 +8,7 @@ import json
 import os
 import sys
 
-NAMES = ["tet_1el", "pyramid_2el", "pyramid_4el", "pyramid_tilted_4el", "regular_octahedron_8el", "cube_6el",
+NAMES = ["tet_1el", "tet_tilted_1el", "pyramid_2el", "pyramid_4el", "pyramid_tilted_4el", "regular_octahedron_8el", "cube_6el",
          "cube_24el"]
 
 
