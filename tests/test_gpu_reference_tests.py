@@ -23,7 +23,14 @@ fixtures (tests/golden/meshes.json, the reference's .msh files):
   P2 levels 0-3, random inner start, Dirichlet data sin(x) sinh(y) z, f = 0, ten V(2,2) cycles;
   every cycle reduces the discrete squared residual (r.r / #inner) by a factor below 3e-2. The
   smoother is the GPU's multicolour P2 SOR (the reference's Gauss-Seidel smoother is
-  lexicographic) and the coarsest level is solved exactly (the reference runs CG to 1e-16)."""
+  lexicographic) and the coarsest level is solved exactly (the reference runs CG to 1e-16).
+- P2P1Stokes3DMinResConvergenceTest (tests/hyteg/convergence/P2P1Stokes3DMinResConvergenceTest.cpp):
+  cube_24el, P2 level 2, colliding-flow Dirichlet data, zero right-hand sides, 20 MINRES
+  iterations at tolerance 1e-13; the sum of the velocity components' discrete L2 errors < 0.6417,
+  the pressure's < 4.003 (both pressures with zero mean) and the residual's < 0.01934, each
+  sqrt(e.e / #DoFs of the Taylor-Hood function). The reference preconditions the pressure block
+  only; this solver adds P2 V(2,2) cycles on the velocity, which can only lower the errors after
+  20 iterations."""
 import json
 import os
 
@@ -225,3 +232,29 @@ def test_p2_laplace_annihilates_constants_and_linears(gpu, name, L):
         err.assign([1.0], [result], L, hg.All)  # the exact result is 0 everywhere
         l2 = np.sqrt(err.dotGlobal(err, L, hg.Inner) / n_points) if n_points > 0 else 0.0
         assert l2 < 4.0e-12, (name, L, i, l2)
+
+
+def test_stokes_minres_reference_bounds(gpu):
+    L = 2
+    st = storage("cube_24el", L + 1)
+    S = hg.P2P1TaylorHoodStokesOperator(st, 0, L)
+    u = [hg.P2Function("u%d" % k, st, 0, L) for k in range(3)]
+    f = [hg.P2Function("f%d" % k, st, 0, L) for k in range(3)]
+    r = [hg.P2Function("r%d" % k, st, 0, L) for k in range(3)]
+    p, g, q = (hg.P1Function(n, st, 0, L) for n in ("p", "g", "q"))
+    exact_u = [lambda x, y, z: 20.0 * x * y ** 3, lambda x, y, z: 5.0 * x ** 4 - 5.0 * y ** 4,
+               lambda x, y, z: 0.0 * x]
+    u[0].interpolate(exact_u[0], L, hg.DirichletBoundary)
+    u[1].interpolate(exact_u[1], L, hg.DirichletBoundary)
+    S.minres(u, p, f, g, L, nu=2, max_iter=20, tol=1e-13)
+    host = st.host()
+    sv, sp = host.owned_slots(L + 1), host.owned_slots(L)  # every velocity / pressure DoF once
+    xv, xp = host.slot_info(L + 1)[0][sv], host.slot_info(L)[0][sp]
+    n_dofs = 3 * len(sv) + len(sp)
+    err_u = sum(np.sqrt(np.sum((u[k].to_numpy(L)[sv] - exact_u[k](*xv.T)) ** 2) / n_dofs) for k in range(3))
+    pn = p.to_numpy(L)[sp]
+    pe = 60.0 * xp[:, 0] ** 2 * xp[:, 1] - 20.0 * xp[:, 1] ** 3
+    err_p = np.sqrt(np.sum(((pn - pn.mean()) - (pe - pe.mean())) ** 2) / n_dofs)
+    S.apply(u, p, r, q, L, hg.Inner | hg.NeumannBoundary, hg.All)
+    res = np.sqrt((sum(r[k].dotGlobal(r[k], L) for k in range(3)) + q.dotGlobal(q, L)) / n_dofs)
+    assert err_u < 0.6417 and err_p < 4.003 and res < 0.01934, (err_u, err_p, res)
