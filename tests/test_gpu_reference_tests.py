@@ -12,6 +12,10 @@ fixtures (tests/golden/meshes.json, the reference's .msh files):
   sin(x) sinh(y), random inner start, zero right-hand side; every one of 20 forward (and,
   separately, backward) SOR sweeps with omega = 1 reduces the residual norm over the inner DoFs.
   The smoother here is the GPU's multicolour SOR, not the reference's lexicographic one.
+- P1CG3DConvergenceTest (tests/hyteg/convergence/P1CG3DConvergenceTest.cpp): CG (tolerance
+  1e-16, no iteration limit) on the octahedron at levels 3 and 4 from a random inner start with
+  Dirichlet data sin(x) sinh(y) z and f = 0: residual sqrt(r.r / #inner) < 6.9e-17 and < 3.88e-17,
+  error against the interpolated solution < 4.4e-4 and < 1e-4.
 - P2QuadraticProlongation3DTest (tests/hyteg/P2/P2QuadraticProlongation3DTest.cpp): quadratic
   prolongation reproduces constants, linears and 2x^2 + 3x + 13 + 4y + 5y^2 + z^2 + 6, err.err <
   1e-15 over Inner | NeumannBoundary (lower levels 0, 1 and 3); prolongateAndAdd equals
@@ -258,3 +262,28 @@ def test_stokes_minres_reference_bounds(gpu):
     S.apply(u, p, r, q, L, hg.Inner | hg.NeumannBoundary, hg.All)
     res = np.sqrt((sum(r[k].dotGlobal(r[k], L) for k in range(3)) + q.dotGlobal(q, L)) / n_dofs)
     assert err_u < 0.6417 and err_p < 4.003 and res < 0.01934, (err_u, err_p, res)
+
+
+def test_cg_reference_convergence_bounds(gpu):
+    lower, higher = 3, 4
+    st = storage("regular_octahedron_8el", higher)
+    A = hg.P1ConstantLaplaceOperator(st, lower, higher)
+    u, f, res, exact, err, one = (hg.P1Function(n, st, lower, higher) for n in ("u", "f", "res", "exact", "err", "one"))
+
+    def solution(x, y, z):
+        return np.sin(x) * np.sinh(y) * z
+
+    cg = hg.CGSolver(st, lower, higher, 2 ** 31 - 1, 1e-16)
+    for L, res_bound, err_bound in ((lower, 6.9e-17, 4.4e-4), (higher, 3.88e-17, 1.0e-4)):
+        u.fill_random(7 + L, L, hg.Inner, 0.0, 1.0)
+        u.interpolate(solution, L, hg.DirichletBoundary)
+        f.interpolate(0.0, L, hg.All)
+        exact.interpolate(solution, L, hg.All)
+        one.interpolate(1.0, L, hg.All)
+        n_points = one.dotGlobal(one, L, hg.Inner)
+        cg.solve(A, u, f, L)
+        err.assign([1.0, -1.0], [u, exact], L, hg.All)
+        A.apply(u, res, L, hg.Inner)
+        l2_err = np.sqrt(err.dotGlobal(err, L, hg.Inner) / n_points)
+        l2_res = np.sqrt(res.dotGlobal(res, L, hg.Inner) / n_points)
+        assert l2_res < res_bound and l2_err < err_bound, (L, l2_res, l2_err)
