@@ -16,6 +16,9 @@ fixtures (tests/golden/meshes.json, the reference's .msh files):
   1e-16, no iteration limit) on the octahedron at levels 3 and 4 from a random inner start with
   Dirichlet data sin(x) sinh(y) z and f = 0: residual sqrt(r.r / #inner) < 6.9e-17 and < 3.88e-17,
   error against the interpolated solution < 4.4e-4 and < 1e-4.
+- P2GSConvergenceTest (tests/hyteg/convergence/P2GSConvergenceTest.cpp): the same for P2 at
+  level 4 on tet_1el and the octahedron, 20 forward (and, separately, backward) sweeps of the
+  GPU's multicolour P2 SOR.
 - P2QuadraticProlongation3DTest (tests/hyteg/P2/P2QuadraticProlongation3DTest.cpp): quadratic
   prolongation reproduces constants, linears and 2x^2 + 3x + 13 + 4y + 5y^2 + z^2 + 6, err.err <
   1e-15 over Inner | NeumannBoundary (lower levels 0, 1 and 3); prolongateAndAdd equals
@@ -287,3 +290,31 @@ def test_cg_reference_convergence_bounds(gpu):
         l2_err = np.sqrt(err.dotGlobal(err, L, hg.Inner) / n_points)
         l2_res = np.sqrt(res.dotGlobal(res, L, hg.Inner) / n_points)
         assert l2_res < res_bound and l2_err < err_bound, (L, l2_res, l2_err)
+
+
+@pytest.mark.parametrize("name", ["tet_1el", "regular_octahedron_8el"])
+@pytest.mark.parametrize("backwards", [False, True])
+def test_p2_gauss_seidel_reduces_the_residual_every_sweep(gpu, name, backwards):
+    L = 4
+    st = storage(name, L + 1)
+    A = hg.P2ConstantLaplaceOperator(st, L, L)
+    x, rhs, Lu, res = (hg.P2Function(n, st, L, L) for n in ("x", "rhs", "Lu", "res"))
+    x.interpolate(lambda px, py, pz: np.sin(px) * np.sinh(py), L, hg.DirichletBoundary)
+    x.fill_random(0, L, hg.Inner, 0.0, 1.0)
+    rhs.interpolate(0.0, L)
+
+    def norm():
+        A.apply(x, Lu, L, hg.Inner)
+        res.assign([1.0, -1.0], [rhs, Lu], L, hg.Inner)
+        return np.sqrt(res.dotGlobal(res, L, hg.Inner))
+
+    old = norm()
+    assert old > 0
+    for i in range(20):
+        if backwards:
+            A.smooth_sor_backwards(x, rhs, 1.0, L, hg.Inner)
+        else:
+            A.smooth_sor(x, rhs, 1.0, L, hg.Inner)
+        new = norm()
+        assert new < old, (name, backwards, i, new, old)
+        old = new
