@@ -220,7 +220,8 @@ int hg_function_download_async(hg_storage* s, int fn, int level, void* host, int
  * the slot of each entry), n = hg_owned_count elements of the function's precision; about 9 %
  * fewer bytes than the level buffer on the 48-tet cube. The host copy runs on the caller's
  * stream, the packing on the storage's stream; a per-function staging buffer on the device
- * (allocated by the first call for a function and level) sits in between, and events order each
+ * (allocated by the first call for a function and level; the level's table of owned runs by the
+ * first hg_owned_count or transfer on that level) sits in between, and events order each
  * use of it after the previous one, so successive calls need no ordering by the caller beyond
  * that of the function itself. upload: the values are scattered into the owners' slots and every
  * copy slot is refreshed from its owner (the level buffer is then consistent), in order on the
