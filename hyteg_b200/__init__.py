@@ -285,6 +285,11 @@ class PrimitiveStorage:
         arrays (converted once per group of sweeps)."""
         call("hg_storage_set_sor_schedule", self._h, int(schedule))
 
+    def set_concurrent_components(self, on):
+        """Stokes MINRES: the three velocity V-cycles of a preconditioner application on three
+        CUDA streams at once (True, default) or one after another (False); same iterates."""
+        call("hg_storage_set_concurrent_components", self.handle, 1 if on else 0)
+
     def set_sor_fused_phases(self, on):
         """Face, edge and vertex phases of the SOR as one launch per phase (True, default) or one
         launch per colour and halo refresh (False); the sweep is the same bit for bit."""

@@ -76,6 +76,7 @@ _SIGS = {
     "hg_function_destroy": (c_int, [c_void_p, c_int]),
     "hg_storage_set_sor_schedule": (c_int, [c_void_p, c_int]),
     "hg_storage_set_sor_fused_phases": (c_int, [c_void_p, c_int]),
+    "hg_storage_set_concurrent_components": (c_int, [c_void_p, c_int]),
     "hg_storage_set_sor_schedule_level": (c_int, [c_void_p, c_int, c_int, c_int]),
     "hg_storage_autotune_sor": (c_int, [c_void_p, c_int, c_int, c_int, c_int, P(c_double), P(c_int)]),
     "hg_function_device_ptr": (c_int, [c_void_p, c_int, c_int, P(c_void_p)]),

@@ -203,6 +203,13 @@ int hg_storage_set_cell_coefficients(hg_storage* h, const double* k, int ncells)
   HG_CATCH
 }
 
+int hg_storage_set_concurrent_components(hg_storage* h, int on) {
+  HG_TRY
+  hg::argCheck(on == 0 || on == 1, "concurrent components: on must be 0 or 1");
+  S(h).concurrentComponents = on == 1;
+  HG_CATCH
+}
+
 int hg_storage_set_sor_fused_phases(hg_storage* h, int on) {
   HG_TRY
   hg::argCheck(on == 0 || on == 1, "fused SOR phases: on must be 0 or 1");

@@ -671,7 +671,7 @@ std::vector<uintptr_t> P2Gmg::signature(int x, int b, int L) {
   P2Operator& o = s.p2op(op);
   for (int l = minL; l <= L; ++l) {
     for (int id : {x, b, tmp}) sig.push_back((uintptr_t)s.data(id, l + 1));
-    auto sc = s.p2scratch.find({l + 1, prec});
+    auto sc = s.p2scratch.find(s.p2ScratchKey(l + 1, prec));
     sig.push_back(sc != s.p2scratch.end() ? (uintptr_t)s.data(sc->second, l + 1) : 0);
     auto dg = o.diag.find({l, prec});
     sig.push_back(dg != o.diag.end() ? (uintptr_t)s.data(dg->second, l + 1) : 0);
@@ -683,6 +683,12 @@ std::vector<uintptr_t> P2Gmg::signature(int x, int b, int L) {
 }
 
 void P2Gmg::runCycle(int x, int b, int L) {
+  struct LaneGuard {  // the cycle's scratch lane, restored on every exit
+    Storage& s;
+    int old;
+    ~LaneGuard() { s.p2Lane = old; }
+  } guard{s, s.p2Lane};
+  s.p2Lane = lane;
   if (!graphs || !buildCoarseDirect()) {
     solveRecursively(x, b, L);
     return;
@@ -1095,20 +1101,65 @@ int stokesMinres(Storage& s, int op, const int u[3], int p, const int f[3], int 
   s.apply(mass, ones, lumped, Lp, fp, 0);
   const double nP = s.dot(ones, ones, Lp, fp);
   argCheck(precondPrec == 8 || precondPrec == 4, "preconditioner precision must be 8 or 4");
-  P2Gmg mg(s, op, 0, L, nu, nu, 1.0, 1000, 1e-14, precondPrec);
-  mg.symmetric = true;
-  // the V-cycle's own x and b (FP32 for a mixed-precision preconditioner; cast at level L)
-  const int px = s.createFunction(1, Lv, precondPrec), pb = s.createFunction(1, Lv, precondPrec);
-  made.push_back(px);
-  made.push_back(pb);
+  // One V-cycle solver per velocity component, each with its own x and b (FP32 for a
+  // mixed-precision preconditioner; cast at level L) and its own P2 scratch lane. The three cycles
+  // of an application are independent. After the first application, which runs them in order and
+  // builds every table, scratch function and graph they use, they run concurrently on three
+  // streams, when the coarse level is solved directly on the device: a CG coarse solve takes dot
+  // products, whose partial sums share one buffer per level.
+  std::unique_ptr<P2Gmg> mg[3];
+  int px[3], pb[3];
+  for (int k = 0; k < 3; ++k) {
+    mg[k].reset(new P2Gmg(s, op, 0, L, nu, nu, 1.0, 1000, 1e-14, precondPrec));
+    mg[k]->symmetric = true;
+    mg[k]->lane = k;
+    px[k] = s.createFunction(1, Lv, precondPrec);
+    pb[k] = s.createFunction(1, Lv, precondPrec);
+    made.push_back(px[k]);
+    made.push_back(pb[k]);
+  }
+  struct Lanes {  // the two extra streams and the fork / join events, released on every exit
+    cudaStream_t aux[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+    ~Lanes() {
+      for (cudaStream_t st : aux)
+        if (st) cudaStreamDestroy(st);
+      for (cudaEvent_t e : {fork, join[0], join[1]})
+        if (e) cudaEventDestroy(e);
+    }
+  } lanes;
+  const bool lanesOk = s.concurrentComponents && mg[0]->buildCoarseDirect();
+  if (lanesOk) {
+    for (int k = 0; k < 2; ++k) {
+      cudaCheck(cudaStreamCreateWithFlags(&lanes.aux[k], cudaStreamNonBlocking), "stream");
+      cudaCheck(cudaEventCreateWithFlags(&lanes.join[k], cudaEventDisableTiming), "event");
+    }
+    cudaCheck(cudaEventCreateWithFlags(&lanes.fork, cudaEventDisableTiming), "event");
+  }
+  bool concurrent = false;
   auto precond = [&](const Blk& src, const Blk& dst) {
     const double one = 1.0;
-    for (int k = 0; k < 3; ++k) {
-      s.copyCast(pb, src.u[k], Lv, fv, false);
-      for (int l = 1; l <= Lv; ++l) s.lincomb(px, l, HG_ALL, 0, nullptr, nullptr, false, 0.0);
-      mg.runCycle(px, pb, L);
-      s.copyCast(dst.u[k], px, Lv, fv, false);
+    struct StreamGuard {  // the storage's stream, restored on every exit
+      Storage& s;
+      cudaStream_t home;
+      ~StreamGuard() { s.stream = home; }
+    } guard{s, s.stream};
+    if (concurrent) {
+      cudaCheck(cudaEventRecord(lanes.fork, guard.home), "event");
+      for (int k = 0; k < 2; ++k) cudaCheck(cudaStreamWaitEvent(lanes.aux[k], lanes.fork, 0), "wait");
     }
+    for (int k = 0; k < 3; ++k) {
+      s.stream = concurrent && k > 0 ? lanes.aux[k - 1] : guard.home;
+      s.copyCast(pb[k], src.u[k], Lv, fv, false);
+      for (int l = 1; l <= Lv; ++l) s.lincomb(px[k], l, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+      mg[k]->runCycle(px[k], pb[k], L);
+      s.copyCast(dst.u[k], px[k], Lv, fv, false);
+      if (concurrent && k > 0) cudaCheck(cudaEventRecord(lanes.join[k - 1], s.stream), "event");
+    }
+    s.stream = guard.home;
+    if (concurrent)
+      for (int k = 0; k < 2; ++k) cudaCheck(cudaStreamWaitEvent(guard.home, lanes.join[k], 0), "wait");
+    concurrent = lanesOk;
     s.divideBy(dst.p, src.p, lumped, Lp, fp);
     const double mean = s.dot(dst.p, ones, Lp, fp) / nP;
     s.lincomb(dst.p, Lp, fp, 1, &one, &dst.p, false, -mean);

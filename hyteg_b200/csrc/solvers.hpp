@@ -151,6 +151,7 @@ struct P2Gmg {
   int prec = 8;                      // precision of the cycle (4: FP32 hierarchy, coarse CG in FP64)
   int cx64 = -1, cb64 = -1;          // FP64 coarse-level copies for an FP32 cycle
   bool symmetric = false;  // post-smoothing with backward sweeps (a symmetric cycle)
+  int lane = 0;            // the storage's P2 scratch lane its cycles use (Storage::p2Lane)
 };
 
 // Geometric multigrid on the whole P2-P1 Taylor-Hood system (GeometricMultigridSolver with

@@ -1294,7 +1294,7 @@ void Storage::p2SorT(P2Operator& o, int opId, int x, int b, int L, unsigned mask
   const int Lf = L + 1;
   const int prec = (int)sizeof(T);
   const int dg = p2Diagonal(opId, L, prec);
-  auto key = std::make_pair(Lf, prec);
+  const auto key = p2ScratchKey(Lf, prec);
   if (!p2scratch.count(key)) p2scratch[key] = createFunction(Lf, Lf, prec);
   const int ax = p2scratch[key];
   const LevelData& ld = levels[Lf];
@@ -1496,7 +1496,7 @@ const P2Gather& Storage::p2Gather(int Lff) {
 }
 
 int Storage::p2Scratch(int Lf, int prec) {
-  auto key = std::make_pair(Lf, prec);
+  const auto key = p2ScratchKey(Lf, prec);
   if (!p2scratch.count(key)) p2scratch[key] = createFunction(Lf, Lf, prec);
   return p2scratch[key];
 }

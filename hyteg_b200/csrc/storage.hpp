@@ -252,7 +252,14 @@ struct Storage {
   P2Operator& p2op(int id);
   P2Additive& p2Additive(int Lf);
   int p2Diagonal(int op, int L, int prec);
-  std::map<std::pair<int, int>, int> p2scratch;  // (lattice level, precision) -> scratch function
+  std::map<std::pair<int, int>, int> p2scratch;  // (lattice level, precision key) -> scratch function
+  // Lane of the P2 work being issued: P2 cycles that run concurrently on different streams use
+  // different lanes, and every lane has its own P2 scratch functions.
+  int p2Lane = 0;
+  std::pair<int, int> p2ScratchKey(int Lf, int prec) const { return {Lf, prec + 64 * p2Lane}; }
+  // Whether the Stokes MINRES preconditioner runs its three velocity V-cycles concurrently, one
+  // stream each (default on; the iterates are the same either way).
+  bool concurrentComponents = true;
   P2Transfer p2tr;
   std::map<int, P2Gather> p2gather;  // by fine lattice level
   const P2Gather& p2Gather(int Lff);

@@ -197,3 +197,28 @@ def test_stokes_apply_level3_interior_stencils(env3):
         assert rel(got, vr[k], inner) < 1e-13
     gq = H.gather_owned(q.to_numpy(L), maps[L][0], maps[L][1], np_)
     assert rel(gq, qr, np.ones(np_, dtype=bool)) < 1e-13
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_minres_concurrent_components_match_in_order(env, dtype):
+    """The three velocity V-cycles of each preconditioner application on three streams give the
+    iterates of the same cycles one after another, bit for bit (FP64 and FP32 cycles)."""
+    st, orc, maps = env
+    L = LMAX
+    S = hg.P2P1TaylorHoodStokesOperator(st, 0, LMAX)
+    xyz = maps[L + 1][2]
+    lid = np.where(np.abs(xyz[:, 2] - 1.0) < 1e-12, 1.0, 0.0)
+    out = []
+    for concurrent in (False, True, True):
+        st.set_concurrent_components(concurrent)
+        u, p = funcs(st)
+        f, g = funcs(st)
+        u[0].from_numpy(L, lid)
+        it, relres, hist = S.minres(u, p, f, g, L, nu=2, max_iter=40, tol=1e-10, precondition_dtype=dtype)
+        out.append((it, relres, hist, [uk.to_numpy(L) for uk in u], p.to_numpy(L)))
+    st.set_concurrent_components(True)
+    for o in out[1:]:
+        assert o[0] == out[0][0] and o[1] == out[0][1] and np.array_equal(o[2], out[0][2])
+        for k in range(3):
+            assert np.array_equal(o[3][k], out[0][3][k])
+        assert np.array_equal(o[4], out[0][4])
