@@ -812,9 +812,20 @@ StokesGmg::StokesGmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int p
   tp = s.createFunction(minL, maxL, 8);
   pspg = s.createOperator(FORM_PSPG, minL, maxL);
   for (int L = minL; L <= maxL; ++L) invDiag.push_back(s.p1Diagonal(pspg, L));
+  smoothedInOrder.assign((size_t)(maxL - minL + 1), 0);
+  for (int k = 0; k < 2; ++k) {
+    cudaCheck(cudaStreamCreateWithFlags(&laneStream[k], cudaStreamNonBlocking), "stream");
+    cudaCheck(cudaEventCreateWithFlags(&joinEvent[k], cudaEventDisableTiming), "event");
+  }
+  cudaCheck(cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming), "event");
 }
 
 StokesGmg::~StokesGmg() {
+  for (int k = 0; k < 2; ++k) {
+    if (laneStream[k]) cudaStreamDestroy(laneStream[k]);
+    if (joinEvent[k]) cudaEventDestroy(joinEvent[k]);
+  }
+  if (forkEvent) cudaEventDestroy(forkEvent);
   for (int k = 0; k < 3; ++k) {
     s.fns.erase(ru[k]);
     s.fns.erase(tu[k]);
@@ -836,8 +847,35 @@ void StokesGmg::smooth(const int u[3], int p, const int f[3], int g, int L) {
     const int src[2] = {f[k], ru[k]};
     s.lincomb(ru[k], Lv, fv, 2, a, src, false, 0.0);
   }
-  for (int i = 0; i < velocitySweeps; ++i)
-    for (int k = 0; k < 3; ++k) s.p2Sor(op, u[k], ru[k], 1.0, L, fv, false);
+  // the velocity sweeps, component by component: on three streams (one P2 scratch lane each) once
+  // this level has been smoothed in order
+  char& warmed = smoothedInOrder[(size_t)(L - minL)];
+  const bool concurrent = warmed && s.concurrentComponents;
+  {
+    struct Restore {  // the storage's stream and lane, restored on every exit
+      Storage& s;
+      cudaStream_t home;
+      int lane;
+      ~Restore() {
+        s.stream = home;
+        s.p2Lane = lane;
+      }
+    } restore{s, s.stream, s.p2Lane};
+    if (concurrent) {
+      cudaCheck(cudaEventRecord(forkEvent, restore.home), "event");
+      for (int k = 0; k < 2; ++k) cudaCheck(cudaStreamWaitEvent(laneStream[k], forkEvent, 0), "wait");
+    }
+    for (int k = 0; k < 3; ++k) {
+      s.stream = concurrent && k > 0 ? laneStream[k - 1] : restore.home;
+      s.p2Lane = k;
+      for (int i = 0; i < velocitySweeps; ++i) s.p2Sor(op, u[k], ru[k], 1.0, L, fv, false);
+      if (concurrent && k > 0) cudaCheck(cudaEventRecord(joinEvent[k - 1], s.stream), "event");
+    }
+    s.stream = restore.home;
+    if (concurrent)
+      for (int k = 0; k < 2; ++k) cudaCheck(cudaStreamWaitEvent(restore.home, joinEvent[k], 0), "wait");
+  }
+  warmed = 1;
   s.stokesDiv(op, u, rp, L, fp);
   const int src[2] = {g, rp};
   s.lincomb(rp, L, fp, 2, a, src, false, 0.0);

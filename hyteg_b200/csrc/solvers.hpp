@@ -198,6 +198,12 @@ struct StokesGmg {
   bool coarseIterative = false;  // the coarsest level is solved by MINRES instead
   int coarseIterations = 0;      // MINRES iterations of the last coarse solve
   std::unique_ptr<DevBuf> coarseIdx, coarseComp, coarseInv;
+  // The velocity sweeps of a smoothing step run one stream per component (each with its own P2
+  // scratch lane) once the level has been smoothed in order (which builds every table they use)
+  // and the storage allows it (concurrentComponents).
+  cudaStream_t laneStream[2] = {nullptr, nullptr};
+  cudaEvent_t forkEvent = nullptr, joinEvent[2] = {nullptr, nullptr};
+  std::vector<char> smoothedInOrder;  // per level minL..maxL
 };
 
 // MinResSolver (solvers/MinresSolver.hpp:63-125) for the P2-P1 Taylor-Hood Stokes system on

@@ -127,10 +127,12 @@ int hg_storage_set_sor_schedule(hg_storage* s, int schedule);
  * sweep) folded in; on = 0 runs one launch per colour and per refresh. */
 int hg_storage_set_sor_fused_phases(hg_storage* s, int on);
 /* Whether hg_p2p1_stokes_minres[_mixed] runs the three velocity V-cycles of each preconditioner
- * application concurrently, one CUDA stream each, with one multigrid workspace per component (no
+ * application concurrently, one CUDA stream each, with one multigrid workspace per component, and
+ * the Uzawa smoother (hg_p2p1_stokes_uzawa_*) its three components' velocity sweeps (no
  * counterpart in the reference, which applies them one after another; the iterates are the same
- * bit for bit): on = 1 (default) from the second application on, when the coarse level is solved
- * directly on the device; on = 0 one after another on the storage's stream. */
+ * bit for bit): on = 1 (default) once the first application (or smoothing of a level) has run in
+ * order, and for MINRES when the coarse level is solved directly on the device; on = 0 one after
+ * another on the storage's stream. */
 int hg_storage_set_concurrent_components(hg_storage* s, int on);
 /* Autotuner (no counterpart in the reference): times the multicolour SOR under the four
  * schedules on every level in [min_level, max_level] (precision 8 or 4; `reps` timed groups of

@@ -221,3 +221,28 @@ def test_reference_uzawa_convergence_test_on_cube_24el():
     assert sum(err_u) < 3e-3, err_u
     assert err_p < 0.8, err_p
     assert residual < 5e-5, residual
+
+
+def test_uzawa_concurrent_components_match_in_order(env):
+    """The velocity sweeps of each Uzawa smoothing step on three streams (one per component) give
+    the cycles of the same sweeps one after another, bit for bit."""
+    st, orc, maps = env
+    L = 2
+    S = hg.P2P1TaylorHoodStokesOperator(st, 0, LMAX)
+    uu, pp, ff, gg = random_state(orc, L, 91)
+    out = []
+    for concurrent in (False, True):
+        st.set_concurrent_components(concurrent)
+        sm = hg.UzawaSmoother(st, S, 0, LMAX, 0.3, 3)
+        mg = hg.StokesGeometricMultigridSolver(st, S, sm, 0, LMAX, 2, 2)
+        u, p = funcs(st, "c%d" % concurrent)
+        f, g = funcs(st, "d%d" % concurrent)
+        put(maps, L, u, p, uu, pp)
+        put(maps, L, f, g, ff, gg)
+        for _ in range(3):  # the first smoothing of every level runs in order, the later ones not
+            mg.solve(u, p, f, g, L)
+        out.append(([x.to_numpy(L) for x in u], p.to_numpy(L)))
+    st.set_concurrent_components(True)
+    for k in range(3):
+        assert np.array_equal(out[0][0][k], out[1][0][k])
+    assert np.array_equal(out[0][1], out[1][1])
