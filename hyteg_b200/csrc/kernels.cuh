@@ -2152,7 +2152,11 @@ __global__ void __launch_bounds__(kBlock) p2SorOwnersKernel(const int64_t* __res
     T s = T(0);
     for (int k = ptr[j]; k < ptr[j + 1]; ++k) s += ax[copies[k]];
     const int64_t o = owner[j];
-    x[o] += omega * (b[o] - s) / diag[o];
+    const T v = x[o] + omega * (b[o] - s) / diag[o];
+    x[o] = v;
+    // the owner's copies in the cell closures of x take the new value at once (the refresh of this
+    // colour's copies before the next colour pass)
+    for (int k = ptr[j]; k < ptr[j + 1]; ++k) x[copies[k]] = v;
   } else if (t < nAdd + nInner) {
     const int q = t - nAdd;
     if (!(innerType[q] & mask)) return;

@@ -1119,23 +1119,6 @@ P2Additive& Storage::p2Additive(int Lf) {
       cudaCheck(cudaMemcpyAsync(ad.updInnerType.p, innerTyFlat.data(), innerTyFlat.size(), cudaMemcpyHostToDevice, stream),
                 "p2 update lists");
     }
-    // the cell-closure halo entries by the colour of their owner: after a colour pass only the
-    // copies of that colour's owners change
-    {
-      std::vector<std::vector<uint2>> byCol(11);
-      for (size_t i = 0; i < cd.size(); ++i)
-        byCol[col[(size_t)cs[i]] & 0x7f].push_back(make_uint2((unsigned)cd[i], (unsigned)cs[i]));
-      std::vector<uint2> flat;
-      for (int k = 0; k < 11; ++k) {
-        ad.cellCommBegin[k] = (int)flat.size();
-        flat.insert(flat.end(), byCol[k].begin(), byCol[k].end());
-      }
-      ad.cellCommBegin[11] = (int)flat.size();
-      ad.cellComm.alloc(std::max<size_t>(1, flat.size()) * sizeof(uint2));
-      if (!flat.empty())
-        cudaCheck(cudaMemcpyAsync(ad.cellComm.p, flat.data(), flat.size() * sizeof(uint2), cudaMemcpyHostToDevice, stream),
-                  "p2 cell comm");
-    }
     ad.closureList.alloc(std::max<size_t>(1, list.size()) * sizeof(dev::P2ClosureNode));
     if (!list.empty())
       cudaCheck(cudaMemcpyAsync(ad.closureList.p, list.data(), list.size() * sizeof(dev::P2ClosureNode),
@@ -1305,17 +1288,9 @@ void Storage::p2SorT(P2Operator& o, int opId, int x, int b, int L, unsigned mask
   const unsigned char* col = (const unsigned char*)ad.colour.p;
   for (int k = 0; k < 11; ++k) {
     const int c = backwards ? 10 - k : k;
-    if (k == 0) {
-      communicate(x, Lf, 1 << G_CELL);
-    } else {  // only the copies of the previous colour's owners changed
-      const int cp = backwards ? c + 1 : c - 1;
-      const int n = ad.cellCommBegin[cp + 1] - ad.cellCommBegin[cp];
-      if (n > 0) {
-        dev::commGatherKernel<T><<<grid1d(n), 256, 0, stream>>>((T*)data(x, Lf), (const uint2*)ad.cellComm.p +
-                                                                                      ad.cellCommBegin[cp], n);
-        ++launches;
-      }
-    }
+    // the cell-closure copies: all at the first colour; after that the owners kernel of each colour
+    // writes its owners' new values into their copies
+    if (k == 0) communicate(x, Lf, 1 << G_CELL);
     T* xd = (T*)data(x, Lf);
     const T* bd = (const T*)data(b, Lf);
     T* axd = (T*)data(ax, Lf);

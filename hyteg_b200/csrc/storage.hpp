@@ -129,8 +129,6 @@ struct P2Additive {
   DevBuf colour;  // per slot: SOR colour of the DoF (0..10), bit 7 on its owner slot
   DevBuf mult;    // per slot: number of macro-cells holding the DoF (1 for cell-owned)
   DevBuf classOfColour;  // per cell: [0..10] parity class of colour k's interior nodes (or -1), [11] vertex colour step
-  DevBuf cellComm;                          // the cell-closure halo entries (dst, src) sorted by the owner's colour
-  int cellCommBegin[12] = {0};
   DevBuf updAdd;                            // owner-table indices of the face/edge/vertex DoFs by colour
   int updAddBegin[12] = {0};
   DevBuf updInner, updInnerType;            // interior vertex slots (and their cell's type) by colour
