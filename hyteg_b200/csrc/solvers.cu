@@ -441,10 +441,10 @@ void Gmg::solveRecursively(int x, int b, int L) {
   }
   s.residual(op, x, b, tmp, L, flag);
   start("Restriction");
-  s.restrictFn(tmp, L, flag);
+  // straight into the coarse right-hand side: the restriction writes the flagged coarse DoFs,
+  // the only ones of b that the coarser level reads
+  s.restrictFn(tmp, L, flag, b);
   stop("Restriction");
-  const double one = 1.0;
-  s.lincomb(b, L - 1, flag, 1, &one, &tmp, false, 0.0);
   s.lincomb(x, L - 1, HG_ALL, 0, nullptr, nullptr, false, 0.0);
   stop(lvl);
   solveRecursively(x, b, L - 1);

@@ -2192,11 +2192,11 @@ const Operator& Storage::structure() {
 }
 
 template <class T>
-void Storage::restrictT(int id, int Lf, unsigned mask) {
+void Storage::restrictT(int id, int Lf, unsigned mask, int coarseDst) {
   const int Lc = Lf - 1;
   const LevelData& lc = levels[Lc];
   const LevelData& lf = levels[Lf];
-  T* coarse = (T*)data(id, Lc);
+  T* coarse = (T*)data(coarseDst >= 0 ? coarseDst : id, Lc);
   const T* fine = (const T*)data(id, Lf);
   Operator& so = const_cast<Operator&>(structure());
   const dev::StencilDev<T>& stf = stencilOf<T>(so, Lf);
@@ -2216,11 +2216,15 @@ void Storage::restrictT(int id, int Lf, unsigned mask) {
   cudaCheck(cudaGetLastError(), "restrict");
 }
 
-void Storage::restrictFn(int id, int Lf, unsigned mask) {
+void Storage::restrictFn(int id, int Lf, unsigned mask, int coarseDst) {
   Function& f = fn(id);
   argCheck(Lf - 1 >= f.minL && Lf <= f.maxL, "restrict: levels outside the function's range");
-  if (f.prec == 8) restrictT<double>(id, Lf, mask);
-  else restrictT<float>(id, Lf, mask);
+  if (coarseDst >= 0) {
+    const Function& d = fn(coarseDst);
+    argCheck(d.prec == f.prec && Lf - 1 >= d.minL && Lf - 1 <= d.maxL, "restrict: coarse function mismatch");
+  }
+  if (f.prec == 8) restrictT<double>(id, Lf, mask, coarseDst);
+  else restrictT<float>(id, Lf, mask, coarseDst);
 }
 
 template <class T>

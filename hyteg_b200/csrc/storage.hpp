@@ -296,7 +296,8 @@ struct Storage {
   // converted into the colour-split order once, and dst is converted back after the last sweep.
   void smoothSorSweeps(int op, int dst, int rhs, double omega, int L, unsigned mask, int sweeps, bool backwards,
                        bool rhsReady);
-  void restrictFn(int id, int Lf, unsigned mask);
+  // Restriction of id's level Lf to level Lf - 1 of id, or of coarseDst (>= 0) when given.
+  void restrictFn(int id, int Lf, unsigned mask, int coarseDst = -1);
   void prolongate(int id, int Lc, unsigned mask, bool add);
   const Operator& structure();
 
@@ -309,7 +310,7 @@ struct Storage {
   template <class T>
   void communicateSplit(T* buf, T* cells, int L, int groupMask);
   template <class T>
-  void restrictT(int id, int Lf, unsigned mask);
+  void restrictT(int id, int Lf, unsigned mask, int coarseDst);
   template <class T>
   void prolongT(int id, int Lc, unsigned mask, bool add);
 
