@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--sor-schedules", default=None,
                    help="FP64 schedule per level instead of autotuning, e.g. 2=3,3=1,8=0 (profiling runs, whose "
                         "serialised launches would mislead the autotuner)")
+    p.add_argument("--compact", default=None,
+                   help="MAX_DOFS,BLOCKS of the timed cycle's compact coarse cycle (default: the solver's own)")
     p.add_argument("--cycle-only", action="store_true",
                    help="only the kernels, autotuner and timed cycles (profiling runs); implies no serving")
     p.add_argument("--stokes-level", type=int, default=6,
@@ -628,6 +630,8 @@ def run_ours(args):
     b.communicate(L)
     gmg = hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 50, 1e-16),
                                       hg.P1toP1LinearRestriction(), hg.P1toP1LinearProlongation(), 0, L, 3, 3)
+    if args.compact:
+        gmg.set_compact(A, *(int(v) for v in args.compact.split(",")))
     Inner = hg.Inner | hg.NeumannBoundary
 
     def ev():
@@ -841,6 +845,9 @@ def run_ours(args):
         "kernels": kernels,
         "solve": solve,
         "autotune_sor": autotune,
+        # levels 0 .. compact_top of every timed cycle run as one launch (the compact coarse
+        # cycle); the timing tree below times the level-by-level cycle
+        "compact_top": gmg.compact_top(A),
         "timing_tree_one_cycle_ms": cycle_tree,
     }
     if world == 1 and args.serving_requests > 0 and not args.cycle_only:

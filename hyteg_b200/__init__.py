@@ -625,6 +625,17 @@ class GeometricMultigridSolver:
         """Replay cycles from captured CUDA graphs (default on; identical results)."""
         call("hg_gmg_set_graphs", self.storage.handle, self._handle(A), 1 if enable else 0)
 
+    def set_compact(self, A, max_dofs, cluster_blocks=1):
+        """Run the coarse levels with at most max_dofs unknowns per group as one launch per cycle
+        (0: off; default 6000 unknowns, one block per group)."""
+        call("hg_gmg_set_compact", self.storage.handle, self._handle(A), int(max_dofs), int(cluster_blocks))
+
+    def compact_top(self, A):
+        """Highest level of the compact coarse cycle (-1: none)."""
+        t = ctypes.c_int()
+        call("hg_gmg_compact_top", self.storage.handle, self._handle(A), ctypes.byref(t))
+        return t.value
+
     def set_timing(self, A, enable):
         """Device-timed phases in a timing tree (the reference's WcTimingTree nodes); cycles run
         eagerly while on."""

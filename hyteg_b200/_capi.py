@@ -152,6 +152,8 @@ _SIGS = {
     "hg_gmg_set_timing": (c_int, [c_void_p, c_int, c_int]),
     "hg_gmg_timing_json": (c_int, [c_void_p, c_int, c_char_p, c_int64, P(c_int64)]),
     "hg_gmg_set_graphs": (c_int, [c_void_p, c_int, c_int]),
+    "hg_gmg_set_compact": (c_int, [c_void_p, c_int, c_int, c_int]),
+    "hg_gmg_compact_top": (c_int, [c_void_p, c_int, P(c_int)]),
     "hg_gmg_solve_to": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_double, c_int, P(c_int), P(c_double), P(c_double),
                                 c_int]),
 }

@@ -15,7 +15,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libhyteg_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-SOURCES = ["topology.cpp", "discretization.cpp", "storage.cu", "solvers.cu", "capi.cu", "noalloc.cu", "server.cu"]
+SOURCES = ["topology.cpp", "discretization.cpp", "storage.cu", "solvers.cu", "compact.cu", "capi.cu", "noalloc.cu", "server.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
 

@@ -1268,6 +1268,25 @@ int hg_gmg_set_graphs(hg_storage* h, int gmg, int enable) {
   HG_CATCH
 }
 
+int hg_gmg_set_compact(hg_storage* h, int gmg, int max_dofs, int cluster_blocks) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  auto it = s.gmgs.find(gmg);
+  hg::argCheck(it != s.gmgs.end(), "unknown multigrid handle");
+  it->second->setCompact(max_dofs, cluster_blocks);
+  HG_CATCH
+}
+
+int hg_gmg_compact_top(hg_storage* h, int gmg, int* top) {
+  HG_TRY
+  hg::Storage& s = S(h);
+  auto it = s.gmgs.find(gmg);
+  hg::argCheck(it != s.gmgs.end(), "unknown multigrid handle");
+  hg::argCheck(top != nullptr, "hg_gmg_compact_top: null output");
+  *top = it->second->compactTop;
+  HG_CATCH
+}
+
 int hg_gmg_set_timing(hg_storage* h, int gmg, int enable) {
   HG_TRY
   hg::Storage& s = S(h);

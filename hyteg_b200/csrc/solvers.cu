@@ -5,6 +5,7 @@
 #include <cstdio>
 
 #include "../../include/hyteg_b200.h"
+#include "compact.hpp"
 #include "solvers.hpp"
 #include "storage.hpp"
 
@@ -71,7 +72,10 @@ Gmg::Gmg(Storage& st, int op_, int minL_, int maxL_, int pre_, int post_, double
     b32 = s.createFunction(minL, maxL, 4);
     r64 = s.createFunction(maxL, maxL, 8);
   }
-  if (deviceCoarse()) setCoarseGroups(1);
+  if (deviceCoarse())
+    setCoarseGroups(1);
+  else
+    buildCompact();
 }
 
 // Work lists of the device coarse CG. Group of a slot: the copy it belongs to when the storage
@@ -137,6 +141,37 @@ void Gmg::setCoarseGroups(int groups) {
   cudaCheck(cudaStreamSynchronize(s.stream), "coarse lists");
   coarseGroups = groups;
   cache.clear();
+  buildCompact();
+}
+
+void Gmg::setCompact(int maxDofs, int cluster) {
+  argCheck(cluster == 1 || cluster == 2 || cluster == 4 || cluster == 8, "compact cycle: 1, 2, 4 or 8 blocks per group");
+  compactMaxDofs = maxDofs;
+  compactCluster = cluster;
+  buildCompact(true);
+}
+
+// The highest level within reach (at most compactMaxDofs unknowns per group, at most
+// kCompactMaxLevels levels) tops the compact cycle. By default a mesh outside its structural
+// assumptions (argument errors of the builder) keeps the level-by-level cycle; an explicit
+// request (strict) reports them.
+void Gmg::buildCompact(bool strict) {
+  cache.clear();
+  compact.reset();
+  compactTop = -1;
+  if (cycle != 0 || compactMaxDofs <= 0) return;
+  int top = -1;
+  for (int l = minL + 1; l <= std::min(maxL, minL + dev::kCompactMaxLevels - 1); ++l)
+    if (compactGroupDofs(s, l, coarseGroups) <= compactMaxDofs) top = l;
+  if (top < 0) return;
+  try {
+    compact = buildCompactCycle(s, op, minL, top, coarseGroups, compactCluster, prec, HG_INNER | HG_NEUMANN,
+                                HG_INNER | HG_NEUMANN | HG_FREESLIP);
+    compactTop = top;
+  } catch (const Error& e) {
+    if (strict || e.code != HG_ERR_ARG) throw;
+    compact.reset();
+  }
 }
 
 Gmg::~Gmg() {
@@ -397,6 +432,8 @@ std::vector<uintptr_t> Gmg::signature(int x, int b, int L) {
     if (id >= 0) sig.push_back((uintptr_t)s.data(id, minL));
   sig.push_back(cgDofs ? (uintptr_t)cgDofs->p : 0);
   sig.push_back((uintptr_t)coarseGroups);
+  sig.push_back(compact ? (uintptr_t)compact->scratch.p : 0);
+  sig.push_back((uintptr_t)(intptr_t)compactTop);
   return sig;
 }
 
@@ -407,7 +444,7 @@ void Gmg::runCycle(int x, int b, int L) {
     timing->stop(s.stream, "Geometric Multigrid Solver");
     return;
   }
-  if (!graphs || (pre + post) % 2 != 0 || !deviceCoarse()) {
+  if (!graphs || (pre + post) % 2 != 0 || !(deviceCoarse() || (compact && L >= compactTop))) {
     solveRecursively(x, b, L);
     return;
   }
@@ -433,6 +470,10 @@ void Gmg::solveRecursively(int x, int b, int L) {
     stop(lvl);
     return;
   }
+  if (compact && !tt && L == compactTop) {
+    runCompactCycle(*compact, s, s.data(x, L), s.data(b, L), false, pre, post, omega, coarseMaxIter, coarseTol);
+    return;
+  }
   start(lvl);
   if (pre > 0) {
     start("Smoother");
@@ -445,10 +486,17 @@ void Gmg::solveRecursively(int x, int b, int L) {
   // the only ones of b that the coarser level reads
   s.restrictFn(tmp, L, flag, b);
   stop("Restriction");
-  s.lincomb(x, L - 1, HG_ALL, 0, nullptr, nullptr, false, 0.0);
+  // the compact cycle starts the coarser level from zero itself
+  const bool compactBelow = compact && !tt && L - 1 == compactTop;
+  if (!compactBelow) s.lincomb(x, L - 1, HG_ALL, 0, nullptr, nullptr, false, 0.0);
   stop(lvl);
-  solveRecursively(x, b, L - 1);
-  if (cycle == 1) solveRecursively(x, b, L - 1);
+  if (compactBelow) {
+    runCompactCycle(*compact, s, s.data(x, L - 1), s.data(b, L - 1), true, pre, post, omega, coarseMaxIter,
+                    coarseTol);
+  } else {
+    solveRecursively(x, b, L - 1);
+    if (cycle == 1) solveRecursively(x, b, L - 1);
+  }
   start(lvl);
   start("Prolongation");
   s.prolongate(x, L - 1, flag, true);

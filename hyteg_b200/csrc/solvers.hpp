@@ -18,6 +18,7 @@ struct BatchMap;
 
 struct Storage;
 struct DevBuf;
+struct CompactCycle;
 
 // Hierarchical timers of a solver's phases measured on the device (the reference's
 // walberla::WcTimingTree around GeometricMultigridSolver / CGSolver). start/stop record CUDA
@@ -119,6 +120,14 @@ struct Gmg {
   void setCoarseGroups(int groups);
   int coarseGroups = 1;
   std::unique_ptr<DevBuf> cgDofs, cgDofOff, cgComm, cgCommOff;
+  // Compact coarse cycle (compact.hpp): levels minL .. compactTop of a V-cycle as one launch, one
+  // block (or cluster of compactCluster blocks) per group. compactTop is the highest level whose
+  // unknowns per group are at most compactMaxDofs (-1: none, or a W-cycle). Off while the timing
+  // tree is on, which times the cycle level by level.
+  int compactMaxDofs = 6000, compactCluster = 1, compactTop = -1;
+  std::unique_ptr<CompactCycle> compact;
+  void setCompact(int maxDofs, int cluster);
+  void buildCompact(bool strict = false);
 };
 
 // P2 geometric multigrid on P2 levels [minL, maxL] (the P2 DoFs of level L are the vertex DoFs

@@ -474,6 +474,19 @@ int hg_gmg_timing_json(hg_storage* s, int gmg, char* buf, int64_t cap, int64_t* 
  * captured; any change of a buffer address (for example an odd number of SOR sweeps on one of
  * the functions elsewhere) selects or captures another graph. Results are identical either way. */
 int hg_gmg_set_graphs(hg_storage* s, int gmg, int enable);
+/* Compact coarse cycle of a V-cycle solver: the levels from the coarsest up to the highest one
+ * with at most max_dofs unknowns per group (the whole mesh, or each copy of a storage of
+ * disjoint copies after hg_gmg_set_coarse_groups) run as ONE launch per cycle: smoothing,
+ * residuals, transfers and the coarse CG of those levels on owner-indexed vectors in device
+ * scratch, one block (cluster_blocks 1) or one thread-block cluster of 2, 4 or 8 blocks per
+ * group. Same multicolour order and coarse CG as the level-by-level cycle, so the iterates agree
+ * up to rounding (the sums run in another order). max_dofs 0 turns it off; the default is 6000
+ * unknowns and one block. Not used while the timing tree is on, nor for W-cycles.
+ * Replaces the levels' share of GeometricMultigridSolver::solveRecursively
+ * (src/hyteg/solvers/GeometricMultigridSolver.hpp:136-235) in one launch. */
+int hg_gmg_set_compact(hg_storage* s, int gmg, int max_dofs, int cluster_blocks);
+/* The highest level the compact coarse cycle covers, -1 when none. */
+int hg_gmg_compact_top(hg_storage* s, int gmg, int* top);
 /* Iterate to ||b - A x|| <= tol ||b - A x0|| (at most max_iter iterations); x, b are FP64. An FP64
  * solver repeats its cycle; an FP32 solver (precision 4) runs FP64 defect correction: r = b - A x
  * in FP64, one FP32 cycle on A e = r from e = 0 (its coarse CG in FP64), x += e in FP64.
