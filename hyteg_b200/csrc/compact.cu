@@ -115,9 +115,9 @@ __global__ void __launch_bounds__(kCompactThreads, 1) compactCycleKernel(const _
     const T s = compactRowSum<T, true, true>(b[row.idx], w, stride, L.cols, row.e0, row.e1, x, snap);
     x[row.idx] = om1 * x[row.idx] + (s * omega) / w[0];
   };
-  // Sweeps: the vertex rows update while the edge and face values are saved (vertex rows read
-  // no saved value, edge and face rows no vertex value through a halo copy), then one barrier
-  // per colour group.
+  // Sweeps. The vertex rows update while the edge and face values are saved: they write only
+  // vertex values, and they read edge and face values from x, which this sweep has not changed
+  // yet; only edge and face rows read the saved values. Then one barrier per colour group.
   auto sweeps = [&](const CompactLevel<T>& L, int count) {
     T* x = sc + L.x;
     const T* b = sc + L.b;

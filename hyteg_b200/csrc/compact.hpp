@@ -5,7 +5,8 @@
 // dense owner-indexed vector in device scratch, so no halo slot is ever refreshed: every
 // stencil entry is resolved on the host to the index of the DoF's owner. On the coarse levels
 // of the multi-launch cycle the time goes to launch latency (about ten launches per sweep of a
-// level with a few thousand DoFs); here a sweep is a few block- or cluster-wide barriers.
+// level with a few thousand DoFs); here a sweep is one block- or cluster-wide barrier per colour
+// group, ten at most.
 //
 // Order of the SOR: the same multicolour order as the multi-launch smoother (vertices; edges by
 // x mod 2; faces by (x + 2y) mod 3; cells by (x + 2y + 3z) mod 4, each in the frame of the
