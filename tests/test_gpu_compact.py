@@ -144,3 +144,30 @@ def test_timing_tree_keeps_the_level_by_level_cycle(env):
     for _ in range(2):
         gmg.solve(A, x, b, L)
     assert relerr(down(x, L, maps, orc.n(L)), got, ~orc.dirichlet(L)) < 1e-12
+
+
+@pytest.mark.parametrize("minL", [1, 2])
+def test_compact_cycle_above_level_zero(env, minL):
+    """Coarsest level 1 or 2: the coarse CG then has edge, face and cell unknowns (on level 2)
+    and runs inside the compact cycle on the device."""
+    st, orc, maps = env
+    L = 4
+    n = orc.n(L)
+    bg = np.random.default_rng(13).uniform(-1, 1, n)
+    A = hg.P1ConstantLaplaceOperator(st, 0, LMAX)
+    out = {}
+    for compact in (True, False):
+        x, b = hg.P1Function("x", st, 0, LMAX), hg.P1Function("b", st, 0, LMAX)
+        up(b, L, bg, maps)
+        gmg = hg.GeometricMultigridSolver(st, hg.SORSmoother(1.0), hg.CGSolver(st, 0, 0, 2000, 1e-16),
+                                          hg.P1toP1LinearRestriction(), hg.P1toP1LinearProlongation(), minL, LMAX,
+                                          3, 3)
+        gmg.set_compact(A, 6000 if compact else 0, 1)
+        assert gmg.compact_top(A) == (3 if compact else -1)
+        for _ in range(3):
+            gmg.solve(A, x, b, L)
+        out[compact] = down(x, L, maps, n)
+    inner = ~orc.dirichlet(L)
+    oref, _ = orc.gmg(L, minL, np.zeros(n), bg, 3, 3, 3, 1.0, multicolour=True, cg_iter=2000, cg_tol=1e-16)
+    assert relerr(out[True], oref, inner) < 1e-12
+    assert relerr(out[False], oref, inner) < 1e-12
