@@ -468,9 +468,9 @@ int hg_gmg_set_timing(hg_storage* s, int gmg, int on);
 /* The tree as JSON (waLBerla TimingTree layout with "Remainder" nodes, seconds): waits for the
  * recorded events; *len = the full length; buf (nullable) receives up to cap-1 bytes and a 0. */
 int hg_gmg_timing_json(hg_storage* s, int gmg, char* buf, int64_t cap, int64_t* len);
-/* Cycles are captured as CUDA graphs and replayed (default on) when the coarse level has only
- * vertex and edge DoFs (its CG then runs on the device in one block) and pre + post smoothing
- * steps are even. The first cycle with a given set of buffers runs eagerly, the second is
+/* Cycles are captured as CUDA graphs and replayed (default on) when the coarse solve runs on the
+ * device (a coarse level with only vertex and edge DoFs, whose CG runs in one block, or a
+ * compact coarse cycle that covers it) and pre + post smoothing steps are even. The first cycle with a given set of buffers runs eagerly, the second is
  * captured; any change of a buffer address (for example an odd number of SOR sweeps on one of
  * the functions elsewhere) selects or captures another graph. Results are identical either way. */
 int hg_gmg_set_graphs(hg_storage* s, int gmg, int enable);
